@@ -1,0 +1,239 @@
+"""ctypes binding of oracle/fmm3d_oracle.c (test infrastructure only).
+
+The C file restates FMMLIB3D's Laplace particle FMM (lfmm3dparttarg and its
+tree, lists, expansion orders and operators) and the O(N^2) direct sum
+l3dpartdirect.  See the header of fmm3d_oracle.c for the parity status.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle_fmm3d.so")
+_lib = None
+
+c_int = ctypes.c_int
+c_dbl = ctypes.c_double
+P = ctypes.c_void_p
+
+
+def build():
+    """Compile the oracle with the committed Makefile (gcc, OpenMP)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        _lib = ctypes.CDLL(_LIB)
+        _lib.oracle_hkrand.restype = c_dbl
+        _lib.oracle_hkrand.argtypes = [c_int]
+        _lib.oracle_l3dterms.restype = c_int
+        _lib.oracle_l3dterms.argtypes = [c_dbl]
+        _lib.oracle_lap_eps.restype = c_dbl
+        _lib.oracle_lap_eps.argtypes = [c_int]
+        _lib.oracle_lap_nbox.restype = c_int
+        _lib.oracle_lap_nbox.argtypes = [c_int, c_int, c_int]
+        _lib.oracle_tree_build.restype = P
+        _lib.oracle_tree_build.argtypes = [c_int, P, c_int, P, c_int]
+        for f in ("oracle_tree_nboxes", "oracle_tree_nlev"):
+            getattr(_lib, f).restype = c_int
+            getattr(_lib, f).argtypes = [P]
+        _lib.oracle_tree_list_len.restype = c_int
+        _lib.oracle_tree_list_len.argtypes = [P, c_int]
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(P)
+
+
+def _c128(a, n):
+    if a is None:
+        return np.zeros(max(n, 1), np.complex128)
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _f64(a, shape):
+    if a is None:
+        return np.zeros(shape, np.float64)
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def hkrand_stream(count, reset=True):
+    """`count` successive values of the examples/hkrand.f generator."""
+    L = lib()
+    if reset:
+        L.oracle_hkrand_reset()
+    return np.array([L.oracle_hkrand(0) for _ in range(count)])
+
+
+def l3dterms(eps):
+    return lib().oracle_l3dterms(eps)
+
+
+def l3dterms_list2(eps):
+    t = np.zeros(343, np.int32)
+    lib().oracle_l3dterms_list2(c_dbl(eps), _p(t))
+    return t.reshape(7, 7, 7)
+
+
+def lap_eps(iprec):
+    return lib().oracle_lap_eps(iprec)
+
+
+def lap_nbox(iprec, ns, nt):
+    return lib().oracle_lap_nbox(iprec, ns, nt)
+
+
+def l3dpartdirect(source, charge=None, dipstr=None, dipvec=None, target=None,
+                  ifpot=1, iffld=1, ifpottarg=1, iffldtarg=1):
+    """Full O(N^2) direct sum.  Arrays are (N,3) / (N,) numpy arrays."""
+    src = _f64(source, (0, 3))
+    n = src.shape[0]
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _c128(charge, n)
+    ds = _c128(dipstr, n)
+    dv = _f64(dipvec, (max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    lib().oracle_l3dpartdirect(
+        c_int(n), _p(src), c_int(int(charge is not None)), _p(q), c_int(int(dipstr is not None)),
+        _p(ds), _p(dv), c_int(ifpot), _p(pot), c_int(iffld), _p(fld), c_int(m), _p(trg),
+        c_int(ifpottarg if m else 0), _p(pt), c_int(iffldtarg if m else 0), _p(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def direct_at(source, pts, skip=None, charge=None, dipstr=None, dipvec=None):
+    """Direct pot/fld at arbitrary points; skip[k] = source index excluded."""
+    src = _f64(source, (0, 3))
+    n = src.shape[0]
+    pts = _f64(pts, (0, 3))
+    k = pts.shape[0]
+    q = _c128(charge, n)
+    ds = _c128(dipstr, n)
+    dv = _f64(dipvec, (max(n, 1), 3))
+    sk = None if skip is None else np.ascontiguousarray(skip, dtype=np.int64)
+    pot = np.zeros(max(k, 1), np.complex128)
+    fld = np.zeros((max(k, 1), 3), np.complex128)
+    lib().oracle_l3ddirect_points(
+        c_int(n), _p(src), c_int(int(charge is not None)), _p(q), c_int(int(dipstr is not None)),
+        _p(ds), _p(dv), c_int(k), _p(pts), _p(sk), _p(pot), _p(fld))
+    return pot[:k], fld[:k]
+
+
+def lfmm3dparttarg(iprec, source, charge=None, dipstr=None, dipvec=None, target=None,
+                   ifpot=1, iffld=1, ifpottarg=1, iffldtarg=1, timing=False):
+    src = _f64(source, (0, 3))
+    n = src.shape[0]
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _c128(charge, n)
+    ds = _c128(dipstr, n)
+    dv = _f64(dipvec, (max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = c_int(0)
+    tinfo = np.zeros(8)
+    lib().oracle_lfmm3dparttarg(
+        ctypes.byref(ier), c_int(iprec), c_int(n), _p(src), c_int(int(charge is not None)), _p(q),
+        c_int(int(dipstr is not None)), _p(ds), _p(dv), c_int(ifpot), _p(pot), c_int(iffld), _p(fld),
+        c_int(m), _p(trg if m else np.zeros((1, 3))), c_int(ifpottarg if m else 0), _p(pt),
+        c_int(iffldtarg if m else 0), _p(ft), _p(tinfo))
+    out = (ier.value, pot[:n], fld[:n], pt[:m], ft[:m])
+    return out + (tinfo,) if timing else out
+
+
+class Tree:
+    """The oracle's octree (d3tstrcr semantics) exported as numpy arrays."""
+
+    def __init__(self, source, target, nbox):
+        L = lib()
+        src = _f64(source, (0, 3))
+        trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+        n, m = src.shape[0], trg.shape[0]
+        h = L.oracle_tree_build(c_int(n), _p(src), c_int(m), _p(trg if m else np.zeros((1, 3))), c_int(nbox))
+        try:
+            nb = L.oracle_tree_nboxes(h)
+            self.nboxes = nb
+            self.nlev = L.oracle_tree_nlev(h)
+            g = np.zeros(4)
+            L.oracle_tree_geometry(P(h), _p(g))
+            self.center0, self.size = g[:3].copy(), g[3]
+            self.box = np.zeros((nb, 20), np.int32)
+            self.centers = np.zeros((nb, 3))
+            self.iz = np.zeros(max(n, 1), np.int32)
+            self.iztarg = np.zeros(max(m, 1), np.int32)
+            L.oracle_tree_boxes(P(h), _p(self.box), _p(self.centers), _p(self.iz), _p(self.iztarg),
+                                c_int(n), c_int(m))
+            self.iz = self.iz[:n]
+            self.iztarg = self.iztarg[:m]
+            self.lists = {}
+            for ty in range(1, 6):
+                ln = L.oracle_tree_list_len(P(h), c_int(ty))
+                st = np.zeros(nb + 1, np.int32)
+                ix = np.zeros(max(ln, 1), np.int32)
+                L.oracle_tree_list(P(h), c_int(ty), _p(st), _p(ix))
+                self.lists[ty] = (st, ix[:ln])
+        finally:
+            L.oracle_tree_free(P(h))
+
+    def list_of(self, ty, b):
+        st, ix = self.lists[ty]
+        return ix[st[b]:st[b + 1]]
+
+
+def _cdouble_arr(n):
+    return np.zeros(n, np.complex128)
+
+
+def formmp(src, c, p, charge=None, dipstr=None, dipvec=None):
+    src = _f64(src, (0, 3)); n = src.shape[0]
+    mp = _cdouble_arr((p + 1) ** 2)
+    lib().oracle_formmp(c_int(n), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                        c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))),
+                        _p(_f64(c, (3,))), c_int(p), _p(mp))
+    return mp
+
+
+def formta(src, c, p, charge=None, dipstr=None, dipvec=None):
+    src = _f64(src, (0, 3)); n = src.shape[0]
+    lo = _cdouble_arr((p + 1) ** 2)
+    lib().oracle_formta(c_int(n), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                        c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))),
+                        _p(_f64(c, (3,))), c_int(p), _p(lo))
+    return lo
+
+
+def mpeval(c, mp, p, pts):
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128)
+    lib().oracle_mpeval(_p(_f64(c, (3,))), _p(np.ascontiguousarray(mp, np.complex128)), c_int(p), c_int(k),
+                        _p(pts), _p(pot), _p(fld))
+    return pot, fld
+
+
+def taeval(c, lo, p, pts):
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128)
+    lib().oracle_taeval(_p(_f64(c, (3,))), _p(np.ascontiguousarray(lo, np.complex128)), c_int(p), c_int(k),
+                        _p(pts), _p(pot), _p(fld))
+    return pot, fld
+
+
+def translate(kind, c_from, c_to, coef, p, nt=None):
+    """kind 0 = M2M, 1 = M2L (truncated to nt), 2 = L2L; returns the new expansion."""
+    out = _cdouble_arr((p + 1) ** 2)
+    lib().oracle_translate(c_int(kind), _p(_f64(c_from, (3,))), _p(_f64(c_to, (3,))),
+                           _p(np.ascontiguousarray(coef, np.complex128)), c_int(p),
+                           c_int(p if nt is None else nt), _p(out))
+    return out
