@@ -1,0 +1,172 @@
+"""fmmlib3d_b200 -- FMMLIB3D's particle FMM on one NVIDIA B200 (sm_100a).
+
+Python mirror of the reference calling sequences (the ``cf2py`` interfaces of
+src/lfmm3dpart.f:217-236): ``lfmm3dpartself``, ``lfmm3dparttarg``,
+``lfmm3dpart`` and ``l3dpartdirect`` return ``ier`` and the requested
+outputs.  Every call goes through the C ABI of ``libfmm3d_b200.so``
+(include/fmm3d_b200.h); there is no CPU path.  Importing this package on a
+machine without the built library raises immediately.
+
+Array conventions follow the Fortran layouts: ``source`` is (N, 3) C-order
+(= ``source(3, N)`` in Fortran), complex strengths are complex128, ``fld`` is
+(N, 3) complex128.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libfmm3d_b200.so")
+
+if not os.path.exists(LIBPATH):
+    raise ImportError(
+        "fmmlib3d_b200: %s is missing; build it with `python -m fmmlib3d_b200.build`" % LIBPATH)
+
+_lib = ctypes.CDLL(LIBPATH)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_IP = ctypes.POINTER(ctypes.c_int)
+
+for _name in ("lfmm3dpart_", "lfmm3dpartself_"):
+    getattr(_lib, _name).restype = None
+_lib.lfmm3dparttarg_.restype = None
+_lib.l3dpartdirect_.restype = None
+_lib.fmm3d_lfmm3dparttarg_device.restype = _I
+_lib.fmm3d_lfmm3dparttarg_device.argtypes = [_I, _I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
+                                             _I, _P, _P]
+_lib.fmm3d_l3dpartdirect_device.restype = _I
+_lib.fmm3d_l3dpartdirect_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
+_lib.fmm3d_set_timing.argtypes = [_I]
+_lib.fmm3d_last_timing.argtypes = [_P, _I]
+_lib.fmm3d_last_timing.restype = _I
+_lib.fmm3d_last_stats.argtypes = [_P, _I]
+_lib.fmm3d_last_stats.restype = _I
+_lib.fmm3d_last_error.restype = ctypes.c_char_p
+
+PASSES = ["tree", "sort", "p2m", "m2m", "p2l", "m2l", "l2l", "eval", "p2p", "scatter", "total"]
+
+
+def lib():
+    return _lib
+
+
+def _iref(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+def _pts(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim == 2 and a.shape[0] == 3 and a.shape[1] != 3:
+        a = np.ascontiguousarray(a.T)
+    return a.reshape(-1, 3) if a.size else np.zeros((0, 3))
+
+
+def _cplx(a, n):
+    if a is None:
+        return np.zeros(max(n, 1), np.complex128)
+    return np.ascontiguousarray(a, dtype=np.complex128).reshape(-1)
+
+
+def lfmm3dparttarg(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld,
+                   target=None, ifpottarg=0, iffldtarg=0):
+    """Laplace FMM over sources and targets; returns (ier, pot, fld, pottarg, fldtarg).
+
+    Same arguments and outputs as lfmm3dparttarg (src/lfmm3dpart.f:138-522);
+    unrequested outputs are returned as zero arrays.
+    """
+    src = _pts(source)
+    n = src.shape[0]
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _cplx(charge, n)
+    ds = _cplx(dipstr, n)
+    dv = _pts(dipvec) if (ifdipole == 1 and dipvec is not None) else np.zeros((max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = ctypes.c_int(0)
+    _lib.lfmm3dparttarg_(ctypes.byref(ier), _iref(iprec), _iref(n), _ptr(src), _iref(ifcharge), _ptr(q),
+                         _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld),
+                         _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg),
+                         _ptr(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dpartself(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld):
+    """Laplace FMM among sources; returns (ier, pot, fld) as lfmm3dpartself."""
+    ier, pot, fld, _, _ = lfmm3dparttarg(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec,
+                                         ifpot, iffld)
+    return ier, pot, fld
+
+
+lfmm3dpart = lfmm3dpartself
+
+
+def l3dpartdirect(source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld,
+                  target=None, ifpottarg=0, iffldtarg=0):
+    """O(N^2) Laplace sum on the GPU; returns (pot, fld, pottarg, fldtarg) as l3dpartdirect."""
+    src = _pts(source)
+    n = src.shape[0]
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _cplx(charge, n)
+    ds = _cplx(dipstr, n)
+    dv = _pts(dipvec) if (ifdipole == 1 and dipvec is not None) else np.zeros((max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    _lib.l3dpartdirect_(_iref(n), _ptr(src), _iref(ifcharge), _ptr(q), _iref(ifdipole), _ptr(ds), _ptr(dv),
+                        _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld), _iref(m), _ptr(trg if m else src),
+                        _iref(ifpottarg), _ptr(pt), _iref(iffldtarg), _ptr(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dparttarg_device(iprec, source, charge, dipstr, dipvec, pot, fld, target=None, pottarg=None,
+                          fldtarg=None, stream=0):
+    """FMM on device-resident torch tensors (float64 views of the Fortran layouts).
+
+    ``source``/``target``/``dipvec``: (N,3) float64 CUDA tensors; ``charge``/
+    ``dipstr``: (N,2) float64 (re, im); outputs ``pot`` (N,2) and ``fld``
+    (N,6) float64, or None when not requested.  Returns ier.
+    """
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = source.shape[0]
+    m = 0 if target is None else target.shape[0]
+    return _lib.fmm3d_lfmm3dparttarg_device(
+        iprec, n, ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
+        ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m, ptr(target),
+        int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
+
+
+def set_timing(on=True):
+    _lib.fmm3d_set_timing(1 if on else 0)
+
+
+def last_timing():
+    """Per-pass device milliseconds of the last call on this thread."""
+    out = np.zeros(len(PASSES))
+    k = _lib.fmm3d_last_timing(_ptr(out), len(PASSES))
+    return dict(zip(PASSES[:k], out[:k]))
+
+
+def last_stats():
+    out = np.zeros(9 + 128, np.int64)
+    k = _lib.fmm3d_last_stats(_ptr(out), out.size)
+    if k == 0:
+        return {}
+    names = ["nboxes", "nlev", "nleaves", "nterms", "_l1", "_l3", "_l4", "p2p_pairs", "m2l_pairs"]
+    d = {nm: int(out[i]) for i, nm in enumerate(names) if not nm.startswith("_")}
+    d["m2l_pt_hist"] = {i: int(out[9 + i]) for i in range(128) if out[9 + i]}
+    return d
+
+
+def last_error():
+    return _lib.fmm3d_last_error().decode()

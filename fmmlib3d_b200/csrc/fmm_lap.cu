@@ -1,0 +1,694 @@
+// Laplace particle FMM driver and the C ABI (include/fmm3d_b200.h).
+//
+// Host orchestration of lfmm3dparttarg (src/lfmm3dpart.f:138-522) and
+// lfmm3dparttargmain (:528-1169) on one B200: the iprec tables, the octree,
+// the expansion order, the eight passes and the unsort run as CUDA kernels on
+// one stream; the host only sizes buffers and enqueues launches.
+#include <math.h>
+#include <string.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <algorithm>
+#include <vector>
+
+#include "../../include/fmm3d_b200.h"
+#include "lap_kernels.cuh"
+#include "tree.cuh"
+
+namespace fmm {
+
+// ---------------------------------------------------------------- iprec tables
+// src/lfmm3dpart.f:277-300
+static bool lap_iprec(int iprec, int ns, int nt, double &eps, int &nbox)
+{
+    static const double e[] = {.5e0, .5e-1, .5e-2, .5e-3, .5e-6, .5e-9, .5e-12, .5e-15, 0.0};
+    static const int nb[] = {40, 50, 80, 160, 400, 800, 1200, 1400};
+    if (iprec < -2 || iprec > 6) return false;
+    eps = e[iprec + 2];
+    nbox = iprec == 6 ? ns + nt : nb[iprec + 2];
+    return true;
+}
+
+// l3dterms, src/l3dterms.f:34-77
+static int l3dterms(double eps)
+{
+    double z1 = 1.5, z2 = sqrt(3.0) / 2.0, jfun = z2, hfun = 1.0 / (z1 * z1);
+    for (int j = 2; j <= 1000; j++) {
+        hfun = hfun / z1;
+        jfun = jfun * z2;
+        if (jfun * hfun < eps) return j;
+    }
+    return 1;
+}
+
+// l3dterms_list2, src/l3dterms.f:136-248; itab[(i+3)*49+(j+3)*7+(k+3)]
+static void l3dterms_list2(double eps, int *itab)
+{
+    int tab[2][4][4];
+    for (int ii = 2; ii <= 3; ii++)
+        for (int jj = 0; jj <= 3; jj++)
+            for (int kk = 0; kk <= 3; kk++) {
+                double dx = ii, dy = jj, dz = kk;
+                if (dx > 0) dx -= .5;
+                if (dy > 0) dy -= .5;
+                if (dz > 0) dz -= .5;
+                double rr = sqrt(dx * dx + dy * dy + dz * dz);
+                double z2 = sqrt(3.0) / 2.0, jfun = z2, hfun = 1.0 / (rr * rr);
+                int nt = 1;
+                for (int j = 2; j <= 1000; j++) {
+                    hfun = hfun / rr;
+                    jfun = jfun * z2;
+                    if (jfun * hfun < eps) { nt = j; break; }
+                }
+                tab[ii - 2][jj][kk] = nt;
+            }
+    for (int i = -3; i <= 3; i++)
+        for (int j = -3; j <= 3; j++)
+            for (int k = -3; k <= 3; k++) {
+                int v = 0, ai = abs(i), aj = abs(j), ak = abs(k);
+                if (ai > 1) v = tab[ai - 2][aj][ak];
+                else if (aj > 1) v = tab[aj - 2][ai][ak];
+                if (ai <= 1 && aj <= 1 && ak > 1) v = ai >= aj ? tab[ak - 2][ai][aj] : tab[ak - 2][aj][ai];
+                itab[(i + 3) * 49 + (j + 3) * 7 + (k + 3)] = v;
+            }
+}
+
+// ---------------------------------------------------------------- per-thread state
+struct ThreadInfo {
+    bool timing = false;
+    std::vector<double> ms;
+    std::vector<long long> stats;
+    std::string err;
+    int launches = 0;
+};
+static thread_local ThreadInfo g_ti;
+
+static cudaStream_t thread_stream()
+{
+    static thread_local cudaStream_t s = nullptr;
+    static thread_local int sdev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!s || sdev != dev) {
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        sdev = dev;
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- operator plan (per device, p, eps)
+// Rotation matrices for every direction class, the slot tables of the three
+// translation kinds and the sqrt-binomial table.  Built once on the device
+// and kept for the life of the process.
+struct LapPlan {
+    int p = 0;
+    int ncls = 0;
+    int lddc = 0;
+    DBuf<double> rot, dc;
+    DBuf<Slot> slots;        // [0, 1512): M2L 8 octants x 189; [1512,1520): M2M; [1520,1528): L2L
+    std::vector<Slot> hslots;
+    int kt = 8;
+};
+constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
+
+static std::mutex g_plan_mu;
+static std::map<std::tuple<int, int, long long>, std::shared_ptr<LapPlan>> g_plans;
+
+static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Status &st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    long long ekey;
+    memcpy(&ekey, &eps, sizeof ekey);
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto key = std::make_tuple(dev, p, ekey);
+    auto it = g_plans.find(key);
+    if (it != g_plans.end()) return it->second;
+    auto P = std::make_shared<LapPlan>();
+    P->p = p;
+    // direction classes keyed by (rho^2, dz) of a doubled integer vector
+    std::map<std::pair<int, int>, int> cls;
+    std::vector<double> cs;
+    auto class_of = [&](int dx, int dy, int dz) {
+        auto k = std::make_pair(dx * dx + dy * dy, dz);
+        auto f = cls.find(k);
+        if (f != cls.end()) return f->second;
+        double r = sqrt((double)(dx * dx + dy * dy + dz * dz));
+        int id = (int)cls.size();
+        cls[k] = id;
+        cs.push_back(dz / r);
+        cs.push_back(sqrt((double)(dx * dx + dy * dy)) / r);
+        return id;
+    };
+    auto ephi = [](int dx, int dy, double &ex, double &ey) {
+        double rho = sqrt((double)(dx * dx + dy * dy));
+        if (rho == 0) { ex = 1; ey = 0; }
+        else { ex = dx / rho; ey = dy / rho; }
+    };
+    int itab[343];
+    l3dterms_list2(eps, itab);
+    P->hslots.resize(8 * 189 + 16);
+    for (int o = 0; o < 8; o++) {
+        int ob[3] = {o & 1, (o >> 1) & 1, (o >> 2) & 1};
+        int ns = 0;
+        for (int c = 0; c < 27; c++) {
+            int co[3] = {c / 9 - 1, (c / 3) % 3 - 1, c % 3 - 1};
+            for (int d = 0; d < 8; d++) {
+                int db[3] = {d & 1, (d >> 1) & 1, (d >> 2) & 1};
+                int D[3];
+                for (int e = 0; e < 3; e++) D[e] = 2 * co[e] + db[e] - ob[e];
+                if (abs(D[0]) <= 1 && abs(D[1]) <= 1 && abs(D[2]) <= 1) continue;
+                Slot &sl = P->hslots[o * 189 + ns++];
+                sl.coll = c;
+                sl.oct = d;
+                // direction target - source = -D
+                sl.cls = class_of(-2 * D[0], -2 * D[1], -2 * D[2]);
+                ephi(-D[0], -D[1], sl.ex, sl.ey);
+                sl.rt = sqrt((double)(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]));
+                int nt = itab[(D[0] + 3) * 49 + (D[1] + 3) * 7 + (D[2] + 3)];
+                sl.pt = nt < p ? nt : p;
+            }
+        }
+    }
+    for (int d = 0; d < 8; d++) {
+        int b[3] = {d & 1, (d >> 1) & 1, (d >> 2) & 1};
+        // M2M: parent - child = (0.5 - bits) -> doubled (1 - 2 bits)
+        Slot &a = P->hslots[kSlotM2M + d];
+        a.coll = -1; a.oct = d; a.pt = p; a.rt = sqrt(3.0) / 2;
+        a.cls = class_of(1 - 2 * b[0], 1 - 2 * b[1], 1 - 2 * b[2]);
+        ephi(1 - 2 * b[0], 1 - 2 * b[1], a.ex, a.ey);
+        // L2L: child - parent = (bits - 0.5)
+        Slot &l = P->hslots[kSlotL2L + d];
+        l.coll = -1; l.oct = d; l.pt = p; l.rt = sqrt(3.0) / 2;
+        l.cls = class_of(2 * b[0] - 1, 2 * b[1] - 1, 2 * b[2] - 1);
+        ephi(2 * b[0] - 1, 2 * b[1] - 1, l.ex, l.ey);
+    }
+    P->ncls = (int)cls.size();
+    // sqrt of binomial coefficients up to 2p+2
+    P->lddc = 2 * p + 3;
+    std::vector<double> car((size_t)P->lddc * P->lddc, 0.0), dch((size_t)P->lddc * P->lddc, 0.0);
+    for (int n = 0; n < P->lddc; n++) {
+        car[(size_t)n * P->lddc] = 1;
+        for (int k = 1; k <= n; k++)
+            car[(size_t)n * P->lddc + k] = car[(size_t)(n - 1) * P->lddc + k - 1] +
+                                           (k <= n - 1 ? car[(size_t)(n - 1) * P->lddc + k] : 0.0);
+        for (int k = 0; k <= n; k++) dch[(size_t)n * P->lddc + k] = sqrt(car[(size_t)n * P->lddc + k]);
+    }
+    DBuf<double> dcs;
+    P->rot.alloc(rot_class_size(p) * P->ncls, s, st);
+    P->dc.alloc(dch.size(), s, st);
+    P->slots.alloc(P->hslots.size(), s, st);
+    dcs.alloc(cs.size(), s, st);
+    if (!st.ok()) return nullptr;
+    FMM_TRY(st, cudaMemcpyAsync(P->dc.p, dch.data(), sizeof(double) * dch.size(), cudaMemcpyHostToDevice, s));
+    FMM_TRY(st, cudaMemcpyAsync(P->slots.p, P->hslots.data(), sizeof(Slot) * P->hslots.size(),
+                                cudaMemcpyHostToDevice, s));
+    FMM_TRY(st, cudaMemcpyAsync(dcs.p, cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice, s));
+    build_rotations(p, P->ncls, dcs.p, P->rot.p, s, st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) return nullptr;
+    // tile size: three KT x (p+1)^2 complex buffers within ~200 KB of shared memory
+    int NC = (p + 1) * (p + 1);
+    P->kt = 8;
+    while (P->kt > 1 && (size_t)3 * P->kt * NC * 16 > 200 * 1024) P->kt /= 2;
+    // buffers are process-lifetime: detach them from the stream they were made on
+    P->rot.s = nullptr;
+    P->dc.s = nullptr;
+    P->slots.s = nullptr;
+    g_plans[key] = P;
+    return P;
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void k_gather_src(int n, const int *perm, const double *src, const double *q, const double *dq,
+                             const double *dv, int ifc, int ifd, PointsSoA o)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long j = perm[i];
+    o.x[i] = src[3 * j];
+    o.y[i] = src[3 * j + 1];
+    o.z[i] = src[3 * j + 2];
+    if (ifc) o.q[i] = make_double2(q[2 * j], q[2 * j + 1]);
+    if (ifd) {
+        o.dq[i] = make_double2(dq[2 * j], dq[2 * j + 1]);
+        o.vx[i] = dv[3 * j];
+        o.vy[i] = dv[3 * j + 1];
+        o.vz[i] = dv[3 * j + 2];
+    }
+}
+
+__global__ void k_gather_pts(int n, const int *perm, const double *p, double *x, double *y, double *z)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long j = perm[i];
+    x[i] = p[3 * j];
+    y[i] = p[3 * j + 1];
+    z[i] = p[3 * j + 2];
+}
+
+// unsort: l3dpsort / l3dfsort (src/lfmm3drouts.f:583-615)
+__global__ void k_scatter_out(int n, const int *perm, OutSoA o, double *pot, double *fld)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long j = perm ? perm[i] : i;
+    if (pot) { pot[2 * j] = o.pot[i].x; pot[2 * j + 1] = o.pot[i].y; }
+    if (fld) {
+        double2 a = o.fx[i], b = o.fy[i], c = o.fz[i];
+        fld[6 * j] = a.x; fld[6 * j + 1] = a.y;
+        fld[6 * j + 2] = b.x; fld[6 * j + 3] = b.y;
+        fld[6 * j + 4] = c.x; fld[6 * j + 5] = c.y;
+    }
+}
+
+__global__ void k_split_aos(int n, const double *p, double *x, double *y, double *z)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = p[3L * i]; y[i] = p[3L * i + 1]; z[i] = p[3L * i + 2];
+}
+
+__global__ void k_split_c(int n, const double *c, double2 *o)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = make_double2(c[2L * i], c[2L * i + 1]);
+}
+
+// statistics: near-field pairs and far-field pairs
+__global__ void k_stats(int nleaves, const int *leaves, TreeView tv, int do_src, int do_trg,
+                        unsigned long long *acc)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nleaves) return;
+    int b = leaves[t];
+    long ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
+    long ns = tv.nsrc[b];
+    for (int k = tv.l1_start[b]; k < tv.l1_start[b + 1]; k++) ns += tv.nsrc[tv.l1_idx[k]];
+    long self = do_src ? tv.nsrc[b] : 0;
+    atomicAdd(acc, (unsigned long long)(ne * ns - self));
+}
+
+__global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int prune, unsigned long long *hist)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    int b = b0 + t;
+    if (prune && tv.ntrg[b] == 0) return;
+    int P = tv.parent[b];
+    if (P < 0) return;
+    int o = tv.octant[b];
+    for (int s = 0; s < 189; s++) {
+        const Slot &sl = slots[o * 189 + s];
+        int C = tv.coll[27L * P + sl.coll];
+        if (C < 0) continue;
+        int src = tv.child[8L * C + sl.oct];
+        if (src < 0 || tv.nsrc[src] == 0) continue;
+        atomicAdd(&hist[sl.pt], 1ull);
+    }
+}
+
+// ---------------------------------------------------------------- the FMM
+struct Timer {
+    cudaStream_t s;
+    bool on;
+    std::vector<cudaEvent_t> ev;
+    Timer(cudaStream_t s_, bool on_) : s(s_), on(on_) {}
+    void mark()
+    {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        ev.push_back(e);
+    }
+    void finish(std::vector<double> &ms)
+    {
+        ms.clear();
+        if (!on || ev.size() < 2) return;
+        cudaEventSynchronize(ev.back());
+        for (size_t i = 1; i < ev.size(); i++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+            ms.push_back(t);
+        }
+        float t = 0;
+        cudaEventElapsedTime(&t, ev.front(), ev.back());
+        ms.push_back(t);
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+    }
+};
+
+static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
+                          const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
+                          double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
+                          int iffldtarg, double *d_fldtarg, cudaStream_t s)
+{
+    Status st;
+    g_ti.launches = 0;
+    double eps;
+    int nbox;
+    if (ns < 1 || !lap_iprec(iprec, ns, nt, eps, nbox)) return 4;
+    if (nt < 0) nt = 0;
+    if (ifpottarg != 1 && iffldtarg != 1) nt = nt;  // targets still shape the tree, as in the reference
+    lap_init_constants(st);
+    int p = l3dterms(eps);
+    if (p > 72) return 16;
+    auto plan = get_plan(p, eps, s, st);
+    if (!st.ok() || !plan) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    Timer tm(s, g_ti.timing);
+    tm.mark();
+    Tree T;
+    build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
+    tm.mark();
+    const int K = (p + 1) * (p + 1);
+    // sorted point arrays
+    DBuf<double> sx, sy, sz, svx, svy, svz, tx, ty, tz;
+    DBuf<double2> sq, sdq;
+    DBuf<double2> opot, ofx, ofy, ofz, tpot, tfx, tfy, tfz;
+    DBuf<double2> mpole, local;
+    bool ok = sx.alloc(ns, s, st) && sy.alloc(ns, s, st) && sz.alloc(ns, s, st);
+    if (ifcharge == 1) ok = ok && sq.alloc(ns, s, st);
+    if (ifdipole == 1) ok = ok && sdq.alloc(ns, s, st) && svx.alloc(ns, s, st) && svy.alloc(ns, s, st) && svz.alloc(ns, s, st);
+    if (nt) ok = ok && tx.alloc(nt, s, st) && ty.alloc(nt, s, st) && tz.alloc(nt, s, st);
+    int do_src = ifpot == 1 || iffld == 1, do_trg = (ifpottarg == 1 || iffldtarg == 1) && nt > 0;
+    if (ifpot == 1) ok = ok && opot.alloc(ns, s, st);
+    if (iffld == 1) ok = ok && ofx.alloc(ns, s, st) && ofy.alloc(ns, s, st) && ofz.alloc(ns, s, st);
+    if (do_trg && ifpottarg == 1) ok = ok && tpot.alloc(nt, s, st);
+    if (do_trg && iffldtarg == 1) ok = ok && tfx.alloc(nt, s, st) && tfy.alloc(nt, s, st) && tfz.alloc(nt, s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    if (!mpole.alloc((size_t)T.nboxes * K, s, st) || !local.alloc((size_t)T.nboxes * K, s, st)) {
+        g_ti.err = cudaGetErrorString(st.err);
+        return 16;
+    }
+    mpole.zero(st);
+    local.zero(st);
+    PointsSoA P;
+    P.x = sx.p; P.y = sy.p; P.z = sz.p; P.q = sq.p; P.dq = sdq.p; P.vx = svx.p; P.vy = svy.p; P.vz = svz.p;
+    k_gather_src<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, d_q, d_dq, d_dv, ifcharge == 1,
+                                                 ifdipole == 1, P);
+    if (nt) k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p);
+    FMM_LAUNCH_CHECK(st);
+    tm.mark();
+    TreeView tv;
+    tv.level = T.level.p; tv.parent = T.parent.p; tv.octant = T.octant.p; tv.nchild = T.nchild.p;
+    tv.child = T.child.p; tv.coll = T.coll.p; tv.src0 = T.src0.p; tv.nsrc = T.nsrc.p; tv.trg0 = T.trg0.p;
+    tv.ntrg = T.ntrg.p; tv.center = T.center.p; tv.l1_start = T.l1_start.p; tv.l1_idx = T.l1_idx.p;
+    tv.l3_start = T.l3_start.p; tv.l3_idx = T.l3_idx.p; tv.l4_start = T.l4_start.p; tv.l4_idx = T.l4_idx.p;
+    tv.size = T.size;
+    int prune = !(ifpot == 1 || iffld == 1);
+
+    // tiles per (level, octant) group
+    auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot, std::vector<Tile> &out) {
+        for (int o = 0; o < 8; o++) {
+            int g = lev * 8 + o;
+            int a = T.group_start[g], bnd = T.group_start[g + 1];
+            for (int i = a; i < bnd; i += kt) {
+                Tile t;
+                t.first = i;
+                t.count = std::min(kt, bnd - i);
+                t.slot0 = slot0_base + o * per_oct_stride;
+                t.nslot = nslot;
+                out.push_back(t);
+            }
+        }
+    };
+    std::vector<Tile> htiles;
+    std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
+    for (int l = T.nlev - 1; l >= 2; l--) {
+        int a = (int)htiles.size();
+        make_tiles(l, plan->kt, kSlotM2M, 0, 8, htiles);
+        m2m_rng.push_back({a, (int)htiles.size() - a});
+    }
+    int m2l_a = (int)htiles.size();
+    for (int l = 2; l <= T.nlev; l++) make_tiles(l, plan->kt, 0, 189, 189, htiles);
+    int m2l_n = (int)htiles.size() - m2l_a;
+    for (int l = 2; l <= T.nlev - 1; l++) {
+        int a = (int)htiles.size();
+        make_tiles(l + 1, plan->kt, kSlotL2L, 1, 1, htiles);
+        l2l_rng.push_back({a, (int)htiles.size() - a});
+    }
+    DBuf<Tile> dtiles;
+    if (!htiles.empty()) {
+        dtiles.alloc(htiles.size(), s, st);
+        FMM_TRY(st, cudaMemcpyAsync(dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
+    }
+    OutSoA os, ot;
+    os.pot = opot.p; os.fx = ofx.p; os.fy = ofy.p; os.fz = ofz.p;
+    ot.pot = tpot.p; ot.fx = tfx.p; ot.fy = tfy.p; ot.fz = tfz.p;
+
+    // STEP 1: P2M at every childless box
+    launch_p2m(T.leaves.p, T.nleaves, tv, P, ifcharge, ifdipole, p, mpole.p, s, st);
+    tm.mark();
+    // STEP 3: M2M, levels nlev-1 .. 2
+    for (auto &r : m2m_rng)
+        launch_translate(0, dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, mpole.p, mpole.p, prune, plan->kt, s, st);
+    tm.mark();
+    // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
+    launch_p2l(T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, p, local.p, s, st);
+    tm.mark();
+    // STEP 4: M2L over list 2, all levels >= 2
+    launch_translate(1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p, plan->dc.p,
+                     plan->lddc, mpole.p, local.p, prune, plan->kt, s, st);
+    tm.mark();
+    // STEP 5: L2L, levels 2 .. nlev-1
+    for (auto &r : l2l_rng)
+        launch_translate(2, dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, local.p, local.p, prune, plan->kt, s, st);
+    tm.mark();
+    // STEPS 6, 7: M2P from list 3 and L2P (writes the outputs)
+    launch_eval(T.leaves.p, T.nleaves, tv, sx.p, sy.p, sz.p, tx.p, ty.p, tz.p, p, mpole.p, local.p, os, ot,
+                do_src, do_trg, s, st);
+    tm.mark();
+    // STEP 8: P2P over self and list 1 (adds to the outputs)
+    launch_p2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
+               do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+    tm.mark();
+    // unsort into the caller's order
+    if (do_src)
+        k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, os, ifpot == 1 ? d_pot : nullptr,
+                                                      iffld == 1 ? d_fld : nullptr);
+    if (do_trg)
+        k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, ot, ifpottarg == 1 ? d_pottarg : nullptr,
+                                                      iffldtarg == 1 ? d_fldtarg : nullptr);
+    FMM_LAUNCH_CHECK(st);
+    tm.mark();
+    tm.finish(g_ti.ms);
+    // statistics
+    {
+        DBuf<unsigned long long> acc;
+        acc.alloc(1 + 128, s, st);
+        acc.zero(st);
+        if (st.ok()) {
+            k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, tv, do_src, do_trg, acc.p);
+            for (int l = 2; l <= T.nlev; l++)
+                k_m2l_count<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], tv,
+                                                                       plan->slots.p, prune, acc.p + 1);
+            std::vector<unsigned long long> h(129);
+            FMM_TRY(st, cudaMemcpyAsync(h.data(), acc.p, sizeof(unsigned long long) * 129, cudaMemcpyDeviceToHost, s));
+            FMM_TRY(st, cudaStreamSynchronize(s));
+            long long m2l = 0;
+            for (int i = 0; i < 128; i++) m2l += (long long)h[1 + i];
+            g_ti.stats.assign(9 + 128, 0);
+            g_ti.stats[0] = T.nboxes; g_ti.stats[1] = T.nlev; g_ti.stats[2] = T.nleaves; g_ti.stats[3] = p;
+            g_ti.stats[7] = (long long)h[0];
+            g_ti.stats[8] = m2l;
+            for (int i = 0; i < 128; i++) g_ti.stats[9 + i] = (long long)h[1 + i];
+        }
+    }
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+static int lap_direct_device(int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
+                             const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
+                             double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
+                             int iffldtarg, double *d_fldtarg, cudaStream_t s)
+{
+    Status st;
+    DBuf<double> sx, sy, sz, vx, vy, vz, tx, ty, tz;
+    DBuf<double2> q, dq, o0, o1, o2, o3;
+    bool ok = sx.alloc(ns, s, st) && sy.alloc(ns, s, st) && sz.alloc(ns, s, st);
+    if (ifcharge == 1) ok = ok && q.alloc(ns, s, st);
+    if (ifdipole == 1) ok = ok && dq.alloc(ns, s, st) && vx.alloc(ns, s, st) && vy.alloc(ns, s, st) && vz.alloc(ns, s, st);
+    int ne = std::max(ns, nt);
+    ok = ok && o0.alloc(ne, s, st) && o1.alloc(ne, s, st) && o2.alloc(ne, s, st) && o3.alloc(ne, s, st);
+    if (nt > 0) ok = ok && tx.alloc(nt, s, st) && ty.alloc(nt, s, st) && tz.alloc(nt, s, st);
+    if (!ok) return 8;
+    k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_src, sx.p, sy.p, sz.p);
+    if (ifcharge == 1) k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_q, q.p);
+    if (ifdipole == 1) {
+        k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dq, dq.p);
+        k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dv, vx.p, vy.p, vz.p);
+    }
+    OutSoA o;
+    o.pot = o0.p; o.fx = o1.p; o.fy = o2.p; o.fz = o3.p;
+    if (ifpot == 1 || iffld == 1) {
+        launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, ns, sx.p, sy.p, sz.p,
+                      1, o, s, st);
+        k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, nullptr, o, ifpot == 1 ? d_pot : nullptr,
+                                                      iffld == 1 ? d_fld : nullptr);
+    }
+    if (nt > 0 && (ifpottarg == 1 || iffldtarg == 1)) {
+        k_split_aos<<<div_up(nt, 256), 256, 0, s>>>(nt, d_trg, tx.p, ty.p, tz.p);
+        launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, nt, tx.p, ty.p, tz.p,
+                      0, o, s, st);
+        k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, nullptr, o, ifpottarg == 1 ? d_pottarg : nullptr,
+                                                      iffldtarg == 1 ? d_fldtarg : nullptr);
+    }
+    FMM_LAUNCH_CHECK(st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+// ---------------------------------------------------------------- host-array entry points
+// Copies host inputs to the device, runs the device routine and copies the
+// requested outputs back; unrequested outputs are left untouched.
+template <typename F>
+static int with_device_arrays(int ns, const double *source, int ifcharge, const double *charge, int ifdipole,
+                              const double *dipstr, const double *dipvec, int ifpot, double *pot, int iffld,
+                              double *fld, int nt, const double *target, int ifpottarg, double *pottarg,
+                              int iffldtarg, double *fldtarg, F run)
+{
+    cudaStream_t s = thread_stream();
+    Status st;
+    if (ns < 0) ns = 0;
+    if (nt < 0) nt = 0;
+    DBuf<double> dsrc, dq, ddq, ddv, dtrg, dpot, dfld, dpt, dft;
+    bool ok = dsrc.alloc(3L * std::max(ns, 1), s, st);
+    if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
+    if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st) && ddv.alloc(3L * ns, s, st);
+    if (nt) ok = ok && dtrg.alloc(3L * nt, s, st);
+    if (ifpot == 1) ok = ok && dpot.alloc(2L * ns, s, st);
+    if (iffld == 1) ok = ok && dfld.alloc(6L * ns, s, st);
+    if (nt && ifpottarg == 1) ok = ok && dpt.alloc(2L * nt, s, st);
+    if (nt && iffldtarg == 1) ok = ok && dft.alloc(6L * nt, s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    FMM_TRY(st, cudaMemcpyAsync(dsrc.p, source, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+    if (ifcharge == 1) FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
+    if (ifdipole == 1) {
+        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
+        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+    }
+    if (nt) FMM_TRY(st, cudaMemcpyAsync(dtrg.p, target, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
+    if (ier) return ier;
+    if (ifpot == 1) FMM_TRY(st, cudaMemcpyAsync(pot, dpot.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
+    if (iffld == 1) FMM_TRY(st, cudaMemcpyAsync(fld, dfld.p, sizeof(double) * 6 * ns, cudaMemcpyDeviceToHost, s));
+    if (nt && ifpottarg == 1) FMM_TRY(st, cudaMemcpyAsync(pottarg, dpt.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));
+    if (nt && iffldtarg == 1) FMM_TRY(st, cudaMemcpyAsync(fldtarg, dft.p, sizeof(double) * 6 * nt, cudaMemcpyDeviceToHost, s));
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+}  // namespace fmm
+
+using namespace fmm;
+
+extern "C" {
+
+int fmm3d_lfmm3dparttarg_device(int iprec, int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
+                                double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
+                                int ifpottarg, double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return lap_fmm_device(iprec, nsource, d_source, ifcharge, d_charge, ifdipole, d_dipstr, d_dipvec, ifpot, d_pot,
+                          iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
+}
+
+int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                               int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
+                               double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
+                               int ifpottarg, double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return lap_direct_device(nsource, d_source, ifcharge, d_charge, ifdipole, d_dipstr, d_dipvec, ifpot, d_pot,
+                             iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
+}
+
+void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                     const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                     const int *ifpot, double *pot, const int *iffld, double *fld, const int *ntarget,
+                     const double *target, const int *ifpottarg, double *pottarg, const int *iffldtarg,
+                     double *fldtarg)
+{
+    int ns = *nsource, nt = *ntarget, ip = *iprec;
+    *ier = with_device_arrays(
+        ns, source, *ifcharge, charge, *ifdipole, dipstr, dipvec, *ifpot, pot, *iffld, fld, nt, target, *ifpottarg,
+        pottarg, *iffldtarg, fldtarg,
+        [&](const double *s_, const double *q, const double *dq, const double *dv, double *po, double *fo,
+            const double *t_, double *pt, double *ft, cudaStream_t s) {
+            return lap_fmm_device(ip, ns, s_, *ifcharge, q, *ifdipole, dq, dv, *ifpot, po, *iffld, fo, nt, t_,
+                                  *ifpottarg, pt, *iffldtarg, ft, s);
+        });
+}
+
+void lfmm3dpartself_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                     const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                     const int *ifpot, double *pot, const int *iffld, double *fld)
+{
+    int zero = 0;
+    lfmm3dparttarg_(ier, iprec, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, pot, iffld, fld,
+                    &zero, source, &zero, nullptr, &zero, nullptr);
+}
+
+void lfmm3dpart_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                 const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                 const int *ifpot, double *pot, const int *iffld, double *fld)
+{
+    lfmm3dpartself_(ier, iprec, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, pot, iffld, fld);
+}
+
+void l3dpartdirect_(const int *nsource, const double *source, const int *ifcharge, const double *charge,
+                    const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                    const int *iffld, double *fld, const int *ntarget, const double *target,
+                    const int *ifpottarg, double *pottarg, const int *iffldtarg, double *fldtarg)
+{
+    int ns = *nsource, nt = *ntarget;
+    with_device_arrays(ns, source, *ifcharge, charge, *ifdipole, dipstr, dipvec, *ifpot, pot, *iffld, fld, nt, target,
+                       *ifpottarg, pottarg, *iffldtarg, fldtarg,
+                       [&](const double *s_, const double *q, const double *dq, const double *dv, double *po,
+                           double *fo, const double *t_, double *pt, double *ft, cudaStream_t s) {
+                           return lap_direct_device(ns, s_, *ifcharge, q, *ifdipole, dq, dv, *ifpot, po, *iffld,
+                                                    fo, nt, t_, *ifpottarg, pt, *iffldtarg, ft, s);
+                       });
+}
+
+int fmm3d_set_timing(int on)
+{
+    g_ti.timing = on != 0;
+    return 0;
+}
+
+int fmm3d_last_timing(double *ms, int n)
+{
+    int k = std::min(n, (int)g_ti.ms.size());
+    for (int i = 0; i < k; i++) ms[i] = g_ti.ms[i];
+    return k;
+}
+
+int fmm3d_last_stats(long long *out, int n)
+{
+    int k = std::min(n, (int)g_ti.stats.size());
+    for (int i = 0; i < k; i++) out[i] = g_ti.stats[i];
+    return k;
+}
+
+const char *fmm3d_last_error(void) { return g_ti.err.c_str(); }
+
+int fmm3d_last_launches(void) { return g_ti.launches; }
+
+}  // extern "C"

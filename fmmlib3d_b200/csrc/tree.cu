@@ -1,0 +1,521 @@
+// Device octree build and interaction lists (see tree.cuh).
+#include <algorithm>
+
+#include "tree.cuh"
+
+namespace fmm {
+
+namespace {
+
+// ---------------------------------------------------------------- bounding cube
+// d3tallbem (src/d3tstrcr.f:1357-1395): min/max over sources and targets,
+// size = largest extent, center = midpoints.
+__global__ void k_bbox_partial(const double *src, int n, const double *trg, int m, double *part)
+{
+    double mn[3] = {1e308, 1e308, 1e308}, mx[3] = {-1e308, -1e308, -1e308};
+    long tot = (long)n + m;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+        const double *p = i < n ? src + 3 * i : trg + 3 * (i - n);
+        for (int d = 0; d < 3; d++) {
+            double v = p[d];
+            mn[d] = fmin(mn[d], v);
+            mx[d] = fmax(mx[d], v);
+        }
+    }
+    for (int d = 0; d < 3; d++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    }
+    __shared__ double s[32][6];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int d = 0; d < 3; d++) { s[w][d] = mn[d]; s[w][3 + d] = mx[d]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++)
+            for (int d = 0; d < 3; d++) {
+                s[0][d] = fmin(s[0][d], s[ww][d]);
+                s[0][3 + d] = fmax(s[0][3 + d], s[ww][3 + d]);
+            }
+        for (int d = 0; d < 6; d++) part[6 * blockIdx.x + d] = s[0][d];
+    }
+}
+
+__global__ void k_bbox_final(const double *part, int nb, double *geom /* c0x c0y c0z size */)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; d++) { mn[d] = part[d]; mx[d] = part[3 + d]; }
+    for (int b = 1; b < nb; b++)
+        for (int d = 0; d < 3; d++) {
+            mn[d] = fmin(mn[d], part[6 * b + d]);
+            mx[d] = fmax(mx[d], part[6 * b + 3 + d]);
+        }
+    double size = __dsub_rn(mx[0], mn[0]);
+    double sy = __dsub_rn(mx[1], mn[1]), sz = __dsub_rn(mx[2], mn[2]);
+    if (sy > size) size = sy;
+    if (sz > size) size = sz;
+    for (int d = 0; d < 3; d++) geom[d] = __dadd_rn(mn[d], mx[d]) / 2;
+    geom[3] = size;
+}
+
+// ---------------------------------------------------------------- keys
+// Path key of a point: for every level the octant (z,y,x bits) it falls in,
+// decided exactly as d3tsepa0 does (upper half iff coordinate > center) with
+// the center computed as in d3tcentf (src/d3tstrcr.f:1671-1700):
+// x0 + (i-1)*side + side/2, evaluated without contraction.
+__global__ void k_keys(const double *pts, int n, const double *geom, uint64_t *keys, int *idx)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double size = geom[3];
+    double h = size / 2;
+    double x0[3] = {__dsub_rn(geom[0], h), __dsub_rn(geom[1], h), __dsub_rn(geom[2], h)};
+    double p[3] = {pts[3L * i], pts[3L * i + 1], pts[3L * i + 2]};
+    int c[3] = {0, 0, 0};
+    uint64_t key = 0;
+    for (int l = 0; l < kMaxLevel; l++) {
+        double side = size / (double)(1 << l);
+        double side2 = side / 2;
+        int oct = 0;
+        for (int d = 0; d < 3; d++) {
+            double ce = __dadd_rn(__dadd_rn(x0[d], __dmul_rn((double)c[d], side)), side2);
+            int bit = p[d] > ce;
+            c[d] = 2 * c[d] + bit;
+            oct |= bit << d;
+        }
+        key = (key << 3) | (uint64_t)oct;
+    }
+    keys[i] = key;
+    idx[i] = i;
+}
+
+__device__ __forceinline__ int key_digit(uint64_t key, int child_level)
+{
+    return (int)((key >> (3 * (kMaxLevel - child_level))) & 7);
+}
+
+// first index in [lo, hi) whose digit at child_level is >= d
+__device__ int lower_digit(const uint64_t *keys, int lo, int hi, int child_level, int d)
+{
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (key_digit(keys[mid], child_level) < d) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Split decision and child ranges for the boxes of one level
+// (d3tallbem, src/d3tstrcr.f:1458-1578).
+__global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, const int *nsrc, const int *trg0,
+                        const int *ntrg, const uint64_t *ksrc, const uint64_t *ktrg, int *nkids, int *cs0,
+                        int *cns, int *ct0, int *cnt)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    int b = b0 + t;
+    int s0 = src0[b], ns = nsrc[b], q0 = trg0[b], nq = ntrg[b];
+    int k = 0;
+    if (level < kMaxLevel && (ns > nbox || nq > nbox)) {
+        int cl = level + 1;
+        int sb[9], tb[9];
+        sb[0] = s0; sb[8] = s0 + ns;
+        tb[0] = q0; tb[8] = q0 + nq;
+        for (int d = 1; d < 8; d++) {
+            sb[d] = lower_digit(ksrc, sb[d - 1], s0 + ns, cl, d);
+            tb[d] = lower_digit(ktrg, tb[d - 1], q0 + nq, cl, d);
+        }
+        for (int d = 0; d < 8; d++) {
+            cs0[8 * t + d] = sb[d];
+            cns[8 * t + d] = sb[d + 1] - sb[d];
+            ct0[8 * t + d] = tb[d];
+            cnt[8 * t + d] = tb[d + 1] - tb[d];
+            k += (sb[d + 1] > sb[d]) || (tb[d + 1] > tb[d]);
+        }
+    }
+    nkids[t] = k;
+}
+
+__global__ void k_make_children(int b0, int nb, int level, int next0, const int *kbase, const int *nkids,
+                                const int *cs0, const int *cns, const int *ct0, const int *cnt,
+                                const double *geom, int *ijk, int *lev, int *par, int *oct, int *nch,
+                                int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    int b = b0 + t;
+    int id = next0 + kbase[t];
+    nch[b] = nkids[t];
+    if (nkids[t] == 0) return;
+    double size = geom[3], h = size / 2;
+    double side = size / (double)(1 << (level + 1)), side2 = side / 2;
+    for (int d = 0; d < 8; d++) {
+        int ns = cns[8 * t + d], nq = cnt[8 * t + d];
+        if (ns == 0 && nq == 0) continue;
+        int c[3] = {2 * ijk[3 * b] + (d & 1), 2 * ijk[3 * b + 1] + ((d >> 1) & 1), 2 * ijk[3 * b + 2] + ((d >> 2) & 1)};
+        for (int e = 0; e < 3; e++) {
+            ijk[3L * id + e] = c[e];
+            // d3tcentc, src/d3tstrcr.f:1589-1669
+            double x00 = __dsub_rn(geom[e], h);
+            center[3L * id + e] = __dadd_rn(__dadd_rn(x00, __dmul_rn((double)c[e], side)), side2);
+        }
+        lev[id] = level + 1;
+        par[id] = b;
+        oct[id] = d;
+        nch[id] = 0;
+        for (int e = 0; e < 8; e++) child[8L * id + e] = -1;
+        src0[id] = cs0[8 * t + d];
+        nsrc[id] = ns;
+        trg0[id] = ct0[8 * t + d];
+        ntrg[id] = nq;
+        child[8L * b + d] = id;
+        id++;
+    }
+}
+
+__global__ void k_root(int n, int m, const double *geom, int *ijk, int *lev, int *par, int *oct, int *nch,
+                       int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center)
+{
+    if (threadIdx.x != 0) return;
+    for (int e = 0; e < 3; e++) { ijk[e] = 0; center[e] = geom[e]; }
+    lev[0] = 0; par[0] = -1; oct[0] = 0; nch[0] = 0;
+    for (int e = 0; e < 8; e++) child[e] = -1;
+    src0[0] = 0; nsrc[0] = n; trg0[0] = 0; ntrg[0] = m;
+}
+
+// ---------------------------------------------------------------- colleagues (list 5 plus self)
+__global__ void k_colleagues(int b0, int nb, const int *ijk, const int *par, const int *child, int *coll)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb) return;
+    int b = b0 + t;
+    int out[27];
+    for (int s = 0; s < 27; s++) out[s] = -1;
+    int P = par[b];
+    if (P < 0) {
+        out[13] = b;
+    } else {
+        for (int s = 0; s < 27; s++) {
+            int C = coll[27L * P + s];
+            if (C < 0) continue;
+            for (int d = 0; d < 8; d++) {
+                int ch = child[8L * C + d];
+                if (ch < 0) continue;
+                int dx = ijk[3L * ch] - ijk[3L * b], dy = ijk[3L * ch + 1] - ijk[3L * b + 1],
+                    dz = ijk[3L * ch + 2] - ijk[3L * b + 2];
+                if (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1) out[coll_slot(dx, dy, dz)] = ch;
+            }
+        }
+    }
+    for (int s = 0; s < 27; s++) coll[27L * b + s] = out[s];
+}
+
+// Closed boxes on (possibly different) levels intersect or touch: the
+// integer form of d3tifint (src/d3tstrcr.f:1075-1172).
+__device__ __forceinline__ bool touch(const int *ijk, const int *lev, int a, int b)
+{
+    int la = lev[a], lb = lev[b];
+    if (la > lb) { int t = a; a = b; b = t; t = la; la = lb; lb = t; }
+    long sc = 1L << (lb - la);
+    for (int e = 0; e < 3; e++) {
+        long ia = ijk[3L * a + e], ib = ijk[3L * b + e];
+        if (ia * sc > ib + 1 || ib > (ia + 1) * sc) return false;
+    }
+    return true;
+}
+
+// Lists 1 and 3 of a childless non-root box b (d3tlsts/d3tlst31,
+// src/d3tstrcr.f:827-851 and :912-1069).  List 1 = childless boxes that
+// touch b (any level); list 3 = boxes on finer levels that do not touch b
+// but whose parents do.  mode 0 counts, mode 1 writes.
+__global__ void k_lists13(const int *leaves, int nleaves, const int *ijk, const int *lev, const int *par,
+                          const int *nch, const int *child, const int *coll, int mode, int *n1, int *n3,
+                          const int *s1, int *i1, const int *s3, int *i3)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nleaves) return;
+    int b = leaves[t];
+    if (lev[b] == 0) {
+        if (mode == 0) { n1[b] = 0; n3[b] = 0; }
+        return;
+    }
+    int c1 = 0, c3 = 0;
+    int o1 = mode ? s1[b] : 0, o3 = mode ? s3[b] : 0;
+    int stk[8 * kMaxLevel + 8];
+    for (int s = 0; s < 27; s++) {
+        if (s == 13) continue;
+        int C = coll[27L * b + s];
+        if (C < 0) continue;
+        if (nch[C] == 0) {
+            if (mode) i1[o1 + c1] = C;
+            c1++;
+            continue;
+        }
+        int top = 0;
+        for (int d = 7; d >= 0; d--)
+            if (child[8L * C + d] >= 0) stk[top++] = child[8L * C + d];
+        while (top) {
+            int x = stk[--top];
+            if (!touch(ijk, lev, b, x)) {
+                if (mode) i3[o3 + c3] = x;
+                c3++;
+            } else if (nch[x] == 0) {
+                if (mode) i1[o1 + c1] = x;
+                c1++;
+            } else {
+                for (int d = 7; d >= 0; d--)
+                    if (child[8L * x + d] >= 0) stk[top++] = child[8L * x + d];
+            }
+        }
+    }
+    // childless boxes on coarser levels are colleagues of an ancestor of b
+    for (int A = par[b]; A >= 0 && lev[A] >= 1; A = par[A]) {
+        for (int s = 0; s < 27; s++) {
+            if (s == 13) continue;
+            int C = coll[27L * A + s];
+            if (C < 0 || nch[C] != 0) continue;
+            if (touch(ijk, lev, b, C)) {
+                if (mode) i1[o1 + c1] = C;
+                c1++;
+            }
+        }
+    }
+    if (mode == 0) { n1[b] = c1; n3[b] = c3; }
+}
+
+__global__ void k_list4_count(const int *leaves, int nleaves, const int *s3, const int *i3, int *n4)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nleaves) return;
+    int b = leaves[t];
+    for (int k = s3[b]; k < s3[b + 1]; k++) atomicAdd(&n4[i3[k]], 1);
+}
+
+__global__ void k_list4_fill(const int *leaves, int nleaves, const int *s3, const int *i3, int *cursor, int *i4)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nleaves) return;
+    int b = leaves[t];
+    for (int k = s3[b]; k < s3[b + 1]; k++) i4[atomicAdd(&cursor[i3[k]], 1)] = b;
+}
+
+// deterministic order inside each list-4 row
+__global__ void k_sort_rows(int nb, const int *st, int *idx)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    int lo = st[b], hi = st[b + 1];
+    for (int i = lo + 1; i < hi; i++) {
+        int v = idx[i], j = i - 1;
+        while (j >= lo && idx[j] > v) { idx[j + 1] = idx[j]; j--; }
+        idx[j + 1] = v;
+    }
+}
+
+__global__ void k_flag_leaves(int nb, const int *nch, int *flag)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb) flag[b] = nch[b] == 0;
+}
+
+__global__ void k_compact(int nb, const int *flag, const int *pos, int *out)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb && flag[b]) out[pos[b]] = b;
+}
+
+__global__ void k_group_keys(int nb, const int *lev, const int *oct, uint64_t *keys, int *vals)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    keys[b] = (uint64_t)(lev[b] * 8 + oct[b]);
+    vals[b] = b;
+}
+
+__global__ void k_group_bounds(int nb, const uint64_t *keys, int ngroups, int *gstart)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nb) return;
+    int g0 = i == 0 ? 0 : (int)keys[i - 1] + 1;
+    int g1 = i == nb ? ngroups : (int)keys[i];
+    for (int g = g0; g <= g1 && g <= ngroups; g++) gstart[g] = i;
+}
+
+template <typename T>
+bool grow(DBuf<T> &b, size_t need, size_t copy, cudaStream_t s, Status &st)
+{
+    if (b.n >= need) return true;
+    DBuf<T> nb;
+    if (!nb.alloc(need, s, st)) return false;
+    if (copy) FMM_TRY(st, cudaMemcpyAsync(nb.p, b.p, sizeof(T) * copy, cudaMemcpyDeviceToDevice, s));
+    std::swap(b.p, nb.p);
+    std::swap(b.n, nb.n);
+    std::swap(b.s, nb.s);
+    return st.ok();
+}
+
+}  // namespace
+
+void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
+                Status &st)
+{
+    T.n = n;
+    T.m = m;
+    // bounding cube
+    DBuf<double> part, geom;
+    int nbb = std::max(1, std::min(1184, div_up((long)n + m, 256)));
+    part.alloc(6 * nbb, s, st);
+    geom.alloc(4, s, st);
+    if (!st.ok()) return;
+    k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p);
+    k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p);
+    // keys and sort
+    DBuf<uint64_t> ks, kt;
+    ks.alloc(std::max(n, 1), s, st);
+    kt.alloc(std::max(m, 1), s, st);
+    T.perm_src.alloc(std::max(n, 1), s, st);
+    T.perm_trg.alloc(std::max(m, 1), s, st);
+    if (!st.ok()) return;
+    if (n) k_keys<<<div_up(n, 256), 256, 0, s>>>(d_src, n, geom.p, ks.p, T.perm_src.p);
+    if (m) k_keys<<<div_up(m, 256), 256, 0, s>>>(d_trg, m, geom.p, kt.p, T.perm_trg.p);
+    FMM_LAUNCH_CHECK(st);
+    radix_sort_u64(ks.p, T.perm_src.p, n, 3 * kMaxLevel, s, st);
+    radix_sort_u64(kt.p, T.perm_trg.p, m, 3 * kMaxLevel, s, st);
+    double hgeom[4];
+    FMM_TRY(st, cudaMemcpyAsync(hgeom, geom.p, sizeof(hgeom), cudaMemcpyDeviceToHost, s));
+    // boxes
+    int cap = std::max(1024, 2 * (int)(((long)n + m) / std::max(nbox, 1)) + 64);
+    auto ensure = [&](int need, int used) {
+        if (need <= T.cap) return st.ok();
+        int nc = std::max(need, 2 * T.cap);
+        grow(T.ijk, 3L * nc, 3L * used, s, st);
+        grow(T.level, nc, used, s, st);
+        grow(T.parent, nc, used, s, st);
+        grow(T.octant, nc, used, s, st);
+        grow(T.nchild, nc, used, s, st);
+        grow(T.child, 8L * nc, 8L * used, s, st);
+        grow(T.src0, nc, used, s, st);
+        grow(T.nsrc, nc, used, s, st);
+        grow(T.trg0, nc, used, s, st);
+        grow(T.ntrg, nc, used, s, st);
+        grow(T.center, 3L * nc, 3L * used, s, st);
+        T.cap = nc;
+        return st.ok();
+    };
+    T.cap = 0;
+    if (!ensure(cap, 0)) return;
+    k_root<<<1, 32, 0, s>>>(n, m, geom.p, T.ijk.p, T.level.p, T.parent.p, T.octant.p, T.nchild.p, T.child.p,
+                            T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p, T.center.p);
+    T.lev_start.assign(1, 0);
+    T.lev_count.assign(1, 1);
+    int nboxes = 1;
+    DBuf<int> nk, kb, cs0, cns, ct0, cnt;
+    for (int level = 0; level < kMaxLevel; level++) {
+        int b0 = T.lev_start[level], nb = T.lev_count[level];
+        if (!nk.alloc(nb, s, st) || !kb.alloc(nb, s, st) || !cs0.alloc(8L * nb, s, st) ||
+            !cns.alloc(8L * nb, s, st) || !ct0.alloc(8L * nb, s, st) || !cnt.alloc(8L * nb, s, st))
+            return;
+        k_split<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nbox, T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p,
+                                                 ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p, cnt.p);
+        FMM_LAUNCH_CHECK(st);
+        int total = 0;
+        scan_exclusive_int(nk.p, kb.p, nb, s, st, &total);
+        if (!st.ok()) return;
+        if (total > 0 && !ensure(nboxes + total, nboxes)) return;
+        k_make_children<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nboxes, kb.p, nk.p, cs0.p, cns.p, ct0.p,
+                                                         cnt.p, geom.p, T.ijk.p, T.level.p, T.parent.p,
+                                                         T.octant.p, T.nchild.p, T.child.p, T.src0.p, T.nsrc.p,
+                                                         T.trg0.p, T.ntrg.p, T.center.p);
+        FMM_LAUNCH_CHECK(st);
+        if (total == 0) break;
+        T.lev_start.push_back(nboxes);
+        T.lev_count.push_back(total);
+        nboxes += total;
+    }
+    T.nboxes = nboxes;
+    T.nlev = (int)T.lev_start.size() - 1;
+    for (int d = 0; d < 3; d++) T.center0[d] = hgeom[d];
+    T.size = hgeom[3];
+
+    // colleagues, level by level
+    T.coll.alloc(27L * nboxes, s, st);
+    if (!st.ok()) return;
+    for (int l = 0; l <= T.nlev; l++)
+        k_colleagues<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], T.ijk.p,
+                                                                  T.parent.p, T.child.p, T.coll.p);
+    FMM_LAUNCH_CHECK(st);
+
+    // leaves
+    DBuf<int> flag, pos;
+    flag.alloc(nboxes, s, st);
+    pos.alloc(nboxes, s, st);
+    if (!st.ok()) return;
+    k_flag_leaves<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.nchild.p, flag.p);
+    int nleaves = 0;
+    scan_exclusive_int(flag.p, pos.p, nboxes, s, st, &nleaves);
+    T.nleaves = nleaves;
+    T.leaves.alloc(std::max(nleaves, 1), s, st);
+    if (!st.ok()) return;
+    k_compact<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, flag.p, pos.p, T.leaves.p);
+
+    // lists 1 and 3 (count, scan, fill), list 4 as the dual of list 3
+    DBuf<int> n1, n3;
+    n1.alloc(nboxes + 1, s, st);
+    n3.alloc(nboxes + 1, s, st);
+    T.l1_start.alloc(nboxes + 1, s, st);
+    T.l3_start.alloc(nboxes + 1, s, st);
+    T.l4_start.alloc(nboxes + 1, s, st);
+    if (!st.ok()) return;
+    n1.zero(st);
+    n3.zero(st);
+    int lb = std::max(nleaves, 1);
+    k_lists13<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.ijk.p, T.level.p, T.parent.p, T.nchild.p,
+                                              T.child.p, T.coll.p, 0, n1.p, n3.p, nullptr, nullptr, nullptr,
+                                              nullptr);
+    int tot1 = 0, tot3 = 0;
+    scan_exclusive_int(n1.p, T.l1_start.p, nboxes + 1, s, st, &tot1);
+    scan_exclusive_int(n3.p, T.l3_start.p, nboxes + 1, s, st, &tot3);
+    T.l1_idx.alloc(std::max(tot1, 1), s, st);
+    T.l3_idx.alloc(std::max(tot3, 1), s, st);
+    if (!st.ok()) return;
+    k_lists13<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.ijk.p, T.level.p, T.parent.p, T.nchild.p,
+                                              T.child.p, T.coll.p, 1, nullptr, nullptr, T.l1_start.p,
+                                              T.l1_idx.p, T.l3_start.p, T.l3_idx.p);
+    DBuf<int> n4, cur;
+    n4.alloc(nboxes + 1, s, st);
+    cur.alloc(nboxes + 1, s, st);
+    if (!st.ok()) return;
+    n4.zero(st);
+    k_list4_count<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.l3_start.p, T.l3_idx.p, n4.p);
+    int tot4 = 0;
+    scan_exclusive_int(n4.p, T.l4_start.p, nboxes + 1, s, st, &tot4);
+    T.l4_idx.alloc(std::max(tot4, 1), s, st);
+    if (!st.ok()) return;
+    FMM_TRY(st, cudaMemcpyAsync(cur.p, T.l4_start.p, sizeof(int) * (nboxes + 1), cudaMemcpyDeviceToDevice, s));
+    k_list4_fill<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.l3_start.p, T.l3_idx.p, cur.p,
+                                                 T.l4_idx.p);
+    k_sort_rows<<<div_up(nboxes, 128), 128, 0, s>>>(nboxes, T.l4_start.p, T.l4_idx.p);
+    FMM_LAUNCH_CHECK(st);
+
+    // boxes grouped by (level, octant)
+    int ngroups = (T.nlev + 1) * 8;
+    DBuf<uint64_t> gk;
+    DBuf<int> gs;
+    gk.alloc(nboxes, s, st);
+    T.grouped.alloc(nboxes, s, st);
+    gs.alloc(ngroups + 1, s, st);
+    if (!st.ok()) return;
+    k_group_keys<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.level.p, T.octant.p, gk.p, T.grouped.p);
+    int gbits = 8;
+    while ((1 << gbits) < ngroups + 1) gbits += 8;
+    radix_sort_u64(gk.p, T.grouped.p, nboxes, gbits, s, st);
+    k_group_bounds<<<div_up(nboxes + 1, 256), 256, 0, s>>>(nboxes, gk.p, ngroups, gs.p);
+    T.group_start.assign(ngroups + 1, 0);
+    FMM_TRY(st, cudaMemcpyAsync(T.group_start.data(), gs.p, sizeof(int) * (ngroups + 1), cudaMemcpyDeviceToHost, s));
+    FMM_TRY(st, cudaStreamSynchronize(s));
+}
+
+}  // namespace fmm

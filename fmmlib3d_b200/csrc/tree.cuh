@@ -1,0 +1,43 @@
+// Adaptive octree on the device, with the logical structure of FMMLIB3D's
+// d3tstrcr (src/d3tstrcr.f:24-259): the bounding cube of sources and
+// targets, level-by-level refinement of every box that holds more than
+// `nbox` sources or more than `nbox` targets, empty children dropped, boxes
+// of one level contiguous and ordered by (parent, child octant z-y-x), and
+// lists 1-5 with the reference's semantics (src/d3tstrcr.f:695-1069).
+#pragma once
+#include "fmm_common.cuh"
+
+namespace fmm {
+
+struct Tree {
+    int n = 0, m = 0;        // sources, targets
+    int nboxes = 0, nlev = 0;
+    int nleaves = 0;
+    double center0[3] = {0, 0, 0}, size = 0;
+    std::vector<int> lev_start, lev_count;  // host copies, per level 0..nlev
+
+    // per box (device)
+    DBuf<int> ijk;      // 3 per box, 0-based integer coordinates on its level
+    DBuf<int> level, parent, octant, nchild;
+    DBuf<int> child;    // 8 per box, indexed by octant (bit0 x, bit1 y, bit2 z), -1 if absent
+    DBuf<int> src0, nsrc, trg0, ntrg;
+    DBuf<double> center;  // 3 per box
+    DBuf<int> coll;     // 27 per box: same-level boxes at offsets in [-1,1]^3 (self at 13), -1 if absent
+    DBuf<int> leaves;   // ids of childless boxes
+    // lists in CSR form
+    DBuf<int> l1_start, l1_idx, l3_start, l3_idx, l4_start, l4_idx;
+    // sorted position -> original index
+    DBuf<int> perm_src, perm_trg;
+    // boxes grouped by (level, octant), for the translation passes
+    DBuf<int> grouped;                       // box ids
+    std::vector<int> group_start;            // host, (nlev+1)*8 + 1 entries
+    int cap = 0;
+};
+
+// Builds the tree for device arrays src (n x 3, AoS) and trg (m x 3).
+void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
+                Status &st);
+
+__host__ __device__ __forceinline__ int coll_slot(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
+
+}  // namespace fmm

@@ -1,0 +1,85 @@
+/*
+ * fmm3d_b200.h -- C ABI of libfmm3d_b200.so, the B200 (sm_100a) particle FMM.
+ *
+ * The Fortran-callable entry points below have exactly the calling sequences
+ * of FMMLIB3D's particle FMM (all arguments by reference, gfortran name
+ * mangling with one trailing underscore, complex*16 passed as interleaved
+ * (re, im) doubles, source(3,n) as xyz-interleaved doubles, default 32-bit
+ * integers).  A Fortran program linked against this library instead of the
+ * reference's objects runs on the GPU with no source change.
+ *
+ * Ownership and flags follow the reference: the caller allocates every input
+ * and output; the library allocates its own device workspace; an output is
+ * written iff its flag equals 1; inputs are never modified.  ier = 0 on
+ * success, 4 / 8 / 16 when workspace cannot be allocated (here: device
+ * memory), as in src/lfmm3dpart.f:192-197.
+ */
+#ifndef FMM3D_B200_H
+#define FMM3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces lfmm3dpart (src/lfmm3dpart.f:36-80): sources only. */
+void lfmm3dpart_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                 const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                 const int *ifpot, double *pot, const int *iffld, double *fld);
+
+/* Replaces lfmm3dpartself (src/lfmm3dpart.f:87-131). */
+void lfmm3dpartself_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                     const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                     const int *ifpot, double *pot, const int *iffld, double *fld);
+
+/* Replaces lfmm3dparttarg (src/lfmm3dpart.f:138-522). */
+void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                     const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                     const int *ifpot, double *pot, const int *iffld, double *fld, const int *ntarget,
+                     const double *target, const int *ifpottarg, double *pottarg, const int *iffldtarg,
+                     double *fldtarg);
+
+/* Replaces l3dpartdirect (src/lfmm3dpart.f:1391-1523), the O(N^2) sum. */
+void l3dpartdirect_(const int *nsource, const double *source, const int *ifcharge, const double *charge,
+                    const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                    const int *iffld, double *fld, const int *ntarget, const double *target,
+                    const int *ifpottarg, double *pottarg, const int *iffldtarg, double *fldtarg);
+
+/* ---- extensions (no counterpart in the reference) ---------------------- */
+
+/* lfmm3dparttarg on arrays already resident in device memory (same layouts),
+ * enqueued on `stream` (a cudaStream_t, or NULL for the library's own
+ * stream).  Returns ier.  Used by services that keep inputs in HBM. */
+int fmm3d_lfmm3dparttarg_device(int iprec, int nsource, const double *d_source, int ifcharge,
+                                const double *d_charge, int ifdipole, const double *d_dipstr,
+                                const double *d_dipvec, int ifpot, double *d_pot, int iffld, double *d_fld,
+                                int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
+                                int iffldtarg, double *d_fldtarg, void *stream);
+
+/* l3dpartdirect on device-resident arrays (same layouts). */
+int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                               int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
+                               double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
+                               int ifpottarg, double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream);
+
+/* Per-pass device times (ms) of the last FMM call made by this host thread
+ * when timing is on: [tree, sort+gather, P2M, M2M, P2L, M2L, L2L, L2P+M2P,
+ * P2P, scatter, total].  Returns the number of entries written. */
+int fmm3d_set_timing(int on);
+int fmm3d_last_timing(double *ms, int n);
+
+/* Tree statistics of the last call on this thread:
+ * [nboxes, nlev, nleaves, nterms, list1 entries, list3 entries,
+ *  list4 entries, p2p pairs (sum over leaves), m2l pairs]. */
+int fmm3d_last_stats(long long *out, int n);
+
+/* Human-readable description of the last CUDA error on this thread. */
+const char *fmm3d_last_error(void);
+
+/* Number of CUDA kernels launched by the last call on this thread. */
+int fmm3d_last_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMM3D_B200_H */
