@@ -1,0 +1,408 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 particle FMM on the Laplace 2M-source / 2M-target workload.
+
+Workload (one "step" = one lfmm3dparttarg call): N = 2,000,000 sources and
+M = 2,000,000 separate targets, both uniform in the unit cube; complex charges
+and dipole strengths with parts uniform in [-1, 1]; dipole directions uniform on
+the unit sphere; iprec = 1; potential and field at sources and targets, FP64.
+Inputs are seeded synthetic data (no dataset is involved).
+
+  value     points/s = (N + M) * steps / device time, inputs resident in HBM
+            (fmm3d_lfmm3dparttarg_device), max over ranks.
+  e2e       the same metric through the Fortran C ABI (lfmm3dparttarg_) with
+            pinned host arrays: H2D of inputs and D2H of outputs inside the
+            timed region.
+  roofline  the dominant pass of the step, from the library's per-pass CUDA
+            events, against the FP64 peak measured in the same run (cuBLAS
+            DGEMM, float64 8192^3) -- MEASURED_PEAKS.json holds no FP64 figure.
+  errors    relative L2 error vs the FP64 direct sum at 1,000 seeded sources
+            (self excluded) and 1,000 seeded targets, per output.
+  cpu_baseline  the C restatement of the reference (oracle/, OpenMP, all host
+            cores) on a bounded sample (N = M = 500,000 of the same
+            distribution); the Fortran reference cannot be compiled (no
+            Fortran compiler on either machine).
+
+Multi-GPU: an FMM call does not shard; `--gpus N` runs N independent replicas
+(one per rank, scaling "weak"), timed as the max over ranks.
+`--impl reference` times the CPU restatement on the host cores (rank 0 only).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "FMM pts/s at N=2M iprec=1 (FP64 GPU vs mixed), err vs FP64 direct; p50/p99 ms"
+UNIT = "points/s"
+# dipole + charge pair cost of lpotfld3dall_sdp_targ (src/laprouts3d.f:2394-2416),
+# counting sqrt and divide as one flop each
+P2P_FLOPS_PER_PAIR = 62
+P2P_FLOPS_CHARGE = 31
+# DRAM bytes per P2P launch from the committed ncu capture (profiles/), scaled
+# to the full workload by pairs; None until a capture exists.
+P2P_DRAM_BYTES_PER_PAIR = None
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=2_000_000, help="sources (= targets)")
+    ap.add_argument("--iprec", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=500_000, help="sources (= targets) of the CPU sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--err-samples", type=int, default=1000)
+    return ap.parse_args(argv)
+
+
+def make_inputs(n, m, seed):
+    """Seeded inputs of the workload: Fortran layouts as float64 numpy arrays."""
+    rng = np.random.default_rng(seed)
+    src = rng.random((n, 3))
+    trg = rng.random((m, 3))
+    q = rng.uniform(-1, 1, (n, 2))
+    dq = rng.uniform(-1, 1, (n, 2))
+    dv = rng.normal(size=(n, 3))
+    dv /= np.linalg.norm(dv, axis=1)[:, None]
+    return src, q, dq, dv, trg
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(HERE, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_fp64_peak(torch, dev):
+    """FP64 throughput of cuBLAS DGEMM (8192^3, best of 5) in TFLOP/s."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_fmm_sample(n, iprec, seed=11):
+    """One run of the CPU restatement (oracle/) on n sources + n targets; returns (seconds, points)."""
+    import oracle
+    src, q, dq, dv, trg = make_inputs(n, n, seed)
+    t0 = time.perf_counter()
+    ier = oracle.lfmm3dparttarg(iprec, src, q[:, 0] + 1j * q[:, 1], dq[:, 0] + 1j * dq[:, 1], dv, trg)[0]
+    t1 = time.perf_counter()
+    if ier != 0:
+        raise RuntimeError("oracle ier=%d" % ier)
+    return t1 - t0, 2 * n
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    import fmmlib3d_b200 as F
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n = m = args.n
+    src, q, dq, dv, trg = make_inputs(n, m, 2 + rank)
+    g = lambda a: torch.from_numpy(a).to(dev)
+    d_src, d_q, d_dq, d_dv, d_trg = g(src), g(q), g(dq), g(dv), g(trg)
+    d_pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    d_pt = torch.empty((m, 2), dtype=torch.float64, device=dev)
+    d_ft = torch.empty((m, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        ier = F.lfmm3dparttarg_device(args.iprec, d_src, d_q, d_dq, d_dv, d_pot, d_fld, d_trg, d_pt, d_ft,
+                                      stream=stream)
+        if ier != 0:
+            raise RuntimeError("FMM ier=%d: %s" % (ier, F.last_error()))
+
+    F.set_timing(True)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    passes, launches = [], []
+    ev[0].record()
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record()
+        passes.append(F.last_timing())
+        launches.append(F.last_launches())
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = clk.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    stats = F.last_stats()
+    if ws > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # errors vs the FP64 direct sum at seeded sample points (outside the timed region)
+    rng = np.random.default_rng(99)
+    k = min(args.err_samples, n)
+    si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
+    ti = np.sort(rng.choice(m, k, replace=False)).astype(np.int32)
+    errs = {}
+    dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
+    df = torch.empty((k, 6), dtype=torch.float64, device=dev)
+    for name, pts, skip, P, Fd in (("src", d_src[si], torch.from_numpy(si).to(dev), d_pot, d_fld),
+                                   ("targ", d_trg[ti], None, d_pt, d_ft)):
+        ier = F.direct_points_device(d_src, d_q, d_dq, d_dv, pts.contiguous(), skip, dp, df, stream=stream)
+        torch.cuda.synchronize()
+        if ier != 0:
+            raise RuntimeError("direct ier=%d" % ier)
+        idx = torch.from_numpy(si if name == "src" else ti).to(dev).long()
+        ep = torch.linalg.norm(P[idx] - dp) / torch.linalg.norm(dp)
+        ef = torch.linalg.norm(Fd[idx] - df) / torch.linalg.norm(df)
+        key = "pot" if name == "src" else "pottarg"
+        errs[key] = float(ep)
+        errs["fld" if name == "src" else "fldtarg"] = float(ef)
+
+    fp64_peak = measured_fp64_peak(torch, dev)
+    return dict(n=n, m=m, ws=ws, rank=rank, total_ms=total_ms, step_ms=step_ms, passes=passes,
+                launches=launches, stats=stats, clocks=clocks, errs=errs, fp64_peak=fp64_peak, torch=torch,
+                F=F, dist=dist if ws > 1 else None, arrays=(src, q, dq, dv, trg))
+
+
+def run_e2e(args, R):
+    """Same workload through the Fortran C ABI with pinned host arrays (H2D + D2H timed)."""
+    torch, F = R["torch"], R["F"]
+    src, q, dq, dv, trg = R["arrays"]
+    n, m = R["n"], R["m"]
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    h = [pinned(a) for a in (src, q, dq, dv, trg)]
+    outs = [torch.empty(s, dtype=torch.float64, pin_memory=True) for s in ((n, 2), (n, 6), (m, 2), (m, 6))]
+    import ctypes
+    lib = F.lib()
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ier = ctypes.c_int(0)
+
+    def call():
+        lib.lfmm3dparttarg_(ctypes.byref(ier), I(args.iprec), I(n), P(h[0]), I(1), P(h[1]), I(1), P(h[2]), P(h[3]),
+                            I(1), P(outs[0]), I(1), P(outs[1]), I(m), P(h[4]), I(1), P(outs[2]), I(1), P(outs[3]))
+        if ier.value != 0:
+            raise RuntimeError("e2e ier=%d" % ier.value)
+
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    if R["dist"] is not None:
+        R["dist"].barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()  # synchronous: returns after the outputs are in host memory
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    if R["dist"] is not None:
+        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        R["dist"].all_reduce(t, op=R["dist"].ReduceOp.MAX)
+        dt = float(t.item())
+    h2d = n * (24 + 16 + 16 + 24) + m * 24
+    d2h = n * (16 + 48) + m * (16 + 48)
+    return {"value": R["ws"] * (n + m) * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * dt / args.steps, "host_memory": "pinned"}
+
+
+def roofline_of(R):
+    """Roofline of the dominant pass, from the per-pass CUDA events of the timed steps."""
+    keys = [k for k in R["passes"][0] if k not in ("total",)]
+    mean = {k: float(np.mean([p[k] for p in R["passes"]])) for k in keys}
+    top = max(mean, key=mean.get)
+    st = R["stats"]
+    peak = R["fp64_peak"]
+    if top == "p2p":
+        flops = st["p2p_pairs"] * P2P_FLOPS_PER_PAIR
+        traffic = None if P2P_DRAM_BYTES_PER_PAIR is None else P2P_DRAM_BYTES_PER_PAIR * st["p2p_pairs"]
+    elif top == "m2l":
+        flops = sum(cnt * m2l_flops(pt) for pt, cnt in st["m2l_pt_hist"].items())
+        traffic = None
+    else:
+        flops, traffic = None, None
+    out = {"kernel": top, "bound": "fp64", "unit": "TFLOP/s", "peak": round(peak, 2),
+           "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
+           "traffic": traffic, "pass_ms_mean": {k: round(v, 3) for k, v in mean.items()}}
+    if flops is not None:
+        ach = flops / (mean[top] * 1e-3) / 1e12
+        out.update(achieved=round(ach, 3), frac=round(ach / peak, 4), flops_per_launch=float(flops))
+    else:
+        out.update(achieved=None, frac=None)
+    return out
+
+
+def m2l_flops(pt):
+    """Flops of one rotate-shift-rotate M2L at truncation pt, as the reference's scheme counts them:
+    two rotations 2*[4*sum (2n+1)^2], the z-shift 4*sum_n sum_|m|<=n (pt-|m|+1), phases 12(pt+1)^2."""
+    rot = 2 * 4 * sum((2 * n + 1) ** 2 for n in range(pt + 1))
+    z = 4 * sum(pt - abs(mm) + 1 for n in range(pt + 1) for mm in range(-n, n + 1))
+    return rot + z + 12 * (pt + 1) ** 2
+
+
+def run_reference(args):
+    """CPU restatement of the reference (oracle/, OpenMP over all host cores) on a bounded sample."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return None
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+    n = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_fmm_sample(n, args.iprec)
+    times = []
+    for _ in range(args.steps):
+        dt, pts = cpu_fmm_sample(n, args.iprec)
+        times.append(dt)
+    v = 2 * n * len(times) / sum(times)
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    sample = "N=M=%d uniform cube, charges+dipoles, iprec=%d, one lfmm3dparttarg restatement call per step" % (
+        n, args.iprec)
+    return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "p50_ms": 1e3 * float(np.percentile(times, 50)), "p99_ms": 1e3 * float(np.percentile(times, 99)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(args, ws), "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores,
+                                                             "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def config_of(args, ws):
+    return {"workload": "laplace_lfmm3dparttarg_cube_%dM_src_%dM_targ" % (args.n // 10 ** 6, args.n // 10 ** 6),
+            "n_sources": args.n, "n_targets": args.n, "iprec": args.iprec, "charges": True, "dipoles": True,
+            "outputs": "pot+fld at sources and targets", "form": "fp64", "parallelism": "replicas x%d" % ws,
+            "l2_policy": "inputs larger than L2 (%.0f MB per step of inputs vs 126 MB L2)" % (args.n * 104 / 1e6)}
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    ws, rank, _ = dist_env()
+    if args.impl == "reference":
+        line = run_reference(args)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    R = run_b200(args)
+    e2e = None if args.no_e2e else run_e2e(args, R)
+    n, m = R["n"], R["m"]
+    total_s = R["total_ms"] * 1e-3
+    value = ws * (n + m) * args.steps / total_s
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": R["total_ms"] / args.steps,
+            "p50_ms": float(np.percentile(R["step_ms"], 50)), "p99_ms": float(np.percentile(R["step_ms"], 99)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded uniform cube; charges, dipoles)", "config": config_of(args, ws),
+            "errors": {k: float("%.3e" % v) for k, v in R["errs"].items()},
+            "gpu_launches": int(sum(R["launches"])), "clocks": R["clocks"], "e2e": e2e,
+            "roofline": roofline_of(R),
+            "stats": {k: v for k, v in R["stats"].items() if k != "m2l_pt_hist"}}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+        dt, pts = cpu_fmm_sample(args.cpu_sample, args.iprec)
+        line["cpu_baseline"] = {"value": pts / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                "kind": "port",
+                                "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
+                                    args.cpu_sample, args.iprec, dt)}
+    if R["dist"] is not None:
+        R["dist"].barrier()
+        R["dist"].destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -21,7 +21,7 @@ LIBPATH = os.path.join(_HERE, "libfmm3d_b200.so")
 
 if not os.path.exists(LIBPATH):
     raise ImportError(
-        "fmmlib3d_b200: %s is missing; build it with `python -m fmmlib3d_b200.build`" % LIBPATH)
+        "fmmlib3d_b200: %s is missing; build it with `python fmmlib3d_b200/build.py`" % LIBPATH)
 
 _lib = ctypes.CDLL(LIBPATH)
 _P = ctypes.c_void_p
@@ -37,6 +37,9 @@ _lib.fmm3d_lfmm3dparttarg_device.argtypes = [_I, _I, _P, _I, _P, _I, _P, _P, _I,
                                              _I, _P, _P]
 _lib.fmm3d_l3dpartdirect_device.restype = _I
 _lib.fmm3d_l3dpartdirect_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
+_lib.fmm3d_l3ddirect_points_device.restype = _I
+_lib.fmm3d_l3ddirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]
+_lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_last_timing.argtypes = [_P, _I]
 _lib.fmm3d_last_timing.restype = _I
@@ -144,6 +147,21 @@ def lfmm3dparttarg_device(iprec, source, charge, dipstr, dipvec, pot, fld, targe
         iprec, n, ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
         ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m, ptr(target),
         int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
+
+
+def direct_points_device(source, charge, dipstr, dipvec, pts, skip, pot, fld, stream=0):
+    """Direct sum at device points ``pts`` (M,3) with per-point excluded source ``skip``
+    (int32 (M,) or None); ``pot`` (M,2), ``fld`` (M,6) float64 outputs.  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    return _lib.fmm3d_l3ddirect_points_device(
+        source.shape[0], ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
+        ptr(dipvec), pts.shape[0], ptr(pts), ptr(skip), ptr(pot), ptr(fld), _P(stream))
+
+
+def last_launches():
+    """Kernel launches issued by the last library call on this thread."""
+    return _lib.fmm3d_last_launches()
 
 
 def set_timing(on=True):

@@ -1,6 +1,6 @@
 """Build libfmm3d_b200.so (CUDA, sm_100a) in-tree with nvcc.
 
-Usage: python -m fmmlib3d_b200.build   (or fmmlib3d_b200.build.build())
+Usage: python fmmlib3d_b200/build.py   (the package import needs the built library)
 """
 import concurrent.futures as cf
 import os

@@ -27,6 +27,10 @@ struct Status {
 
 #define FMM_LAUNCH_CHECK(st) FMM_TRY(st, cudaGetLastError())
 
+// Kernel launches issued by the current host thread (reported per call).
+extern thread_local int g_launch_count;
+#define FMM_COUNT_LAUNCH() (++::fmm::g_launch_count)
+
 // ---------------------------------------------------------------- complex
 __host__ __device__ __forceinline__ double2 cmk(double a, double b) { return make_double2(a, b); }
 __host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }

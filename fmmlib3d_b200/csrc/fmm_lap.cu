@@ -21,6 +21,8 @@
 
 namespace fmm {
 
+thread_local int g_launch_count = 0;
+
 // ---------------------------------------------------------------- iprec tables
 // src/lfmm3dpart.f:277-300
 static bool lap_iprec(int iprec, int ns, int nt, double &eps, int &nbox)
@@ -351,7 +353,7 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
                           int iffldtarg, double *d_fldtarg, cudaStream_t s)
 {
     Status st;
-    g_ti.launches = 0;
+    g_launch_count = 0;
     double eps;
     int nbox;
     if (ns < 1 || !lap_iprec(iprec, ns, nt, eps, nbox)) return 4;
@@ -393,8 +395,8 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     PointsSoA P;
     P.x = sx.p; P.y = sy.p; P.z = sz.p; P.q = sq.p; P.dq = sdq.p; P.vx = svx.p; P.vy = svy.p; P.vz = svz.p;
     k_gather_src<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, d_q, d_dq, d_dv, ifcharge == 1,
-                                                 ifdipole == 1, P);
-    if (nt) k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p);
+                                                 ifdipole == 1, P); FMM_COUNT_LAUNCH();
+    if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     tm.mark();
     TreeView tv;
@@ -473,12 +475,14 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
                do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
     tm.mark();
     // unsort into the caller's order
-    if (do_src)
+    if (do_src) {
         k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, os, ifpot == 1 ? d_pot : nullptr,
-                                                      iffld == 1 ? d_fld : nullptr);
-    if (do_trg)
+                                                      iffld == 1 ? d_fld : nullptr); FMM_COUNT_LAUNCH();
+    }
+    if (do_trg) {
         k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, ot, ifpottarg == 1 ? d_pottarg : nullptr,
-                                                      iffldtarg == 1 ? d_fldtarg : nullptr);
+                                                      iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
+    }
     FMM_LAUNCH_CHECK(st);
     tm.mark();
     tm.finish(g_ti.ms);
@@ -488,10 +492,11 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
         acc.alloc(1 + 128, s, st);
         acc.zero(st);
         if (st.ok()) {
-            k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, tv, do_src, do_trg, acc.p);
-            for (int l = 2; l <= T.nlev; l++)
+            k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, tv, do_src, do_trg, acc.p); FMM_COUNT_LAUNCH();
+            for (int l = 2; l <= T.nlev; l++) {
                 k_m2l_count<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], tv,
-                                                                       plan->slots.p, prune, acc.p + 1);
+                                                                       plan->slots.p, prune, acc.p + 1); FMM_COUNT_LAUNCH();
+            }
             std::vector<unsigned long long> h(129);
             FMM_TRY(st, cudaMemcpyAsync(h.data(), acc.p, sizeof(unsigned long long) * 129, cudaMemcpyDeviceToHost, s));
             FMM_TRY(st, cudaStreamSynchronize(s));
@@ -524,26 +529,26 @@ static int lap_direct_device(int ns, const double *d_src, int ifcharge, const do
     ok = ok && o0.alloc(ne, s, st) && o1.alloc(ne, s, st) && o2.alloc(ne, s, st) && o3.alloc(ne, s, st);
     if (nt > 0) ok = ok && tx.alloc(nt, s, st) && ty.alloc(nt, s, st) && tz.alloc(nt, s, st);
     if (!ok) return 8;
-    k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_src, sx.p, sy.p, sz.p);
-    if (ifcharge == 1) k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_q, q.p);
+    k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_src, sx.p, sy.p, sz.p); FMM_COUNT_LAUNCH();
+    if (ifcharge == 1) { k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_q, q.p); FMM_COUNT_LAUNCH(); }
     if (ifdipole == 1) {
-        k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dq, dq.p);
-        k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dv, vx.p, vy.p, vz.p);
+        k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dq, dq.p); FMM_COUNT_LAUNCH();
+        k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dv, vx.p, vy.p, vz.p); FMM_COUNT_LAUNCH();
     }
     OutSoA o;
     o.pot = o0.p; o.fx = o1.p; o.fy = o2.p; o.fz = o3.p;
     if (ifpot == 1 || iffld == 1) {
         launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, ns, sx.p, sy.p, sz.p,
-                      1, o, s, st);
+                      nullptr, 1, o, s, st);
         k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, nullptr, o, ifpot == 1 ? d_pot : nullptr,
-                                                      iffld == 1 ? d_fld : nullptr);
+                                                      iffld == 1 ? d_fld : nullptr); FMM_COUNT_LAUNCH();
     }
     if (nt > 0 && (ifpottarg == 1 || iffldtarg == 1)) {
-        k_split_aos<<<div_up(nt, 256), 256, 0, s>>>(nt, d_trg, tx.p, ty.p, tz.p);
+        k_split_aos<<<div_up(nt, 256), 256, 0, s>>>(nt, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH();
         launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, nt, tx.p, ty.p, tz.p,
-                      0, o, s, st);
+                      nullptr, 0, o, s, st);
         k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, nullptr, o, ifpottarg == 1 ? d_pottarg : nullptr,
-                                                      iffldtarg == 1 ? d_fldtarg : nullptr);
+                                                      iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
     }
     FMM_LAUNCH_CHECK(st);
     FMM_TRY(st, cudaStreamSynchronize(s));
@@ -619,6 +624,40 @@ int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge
                              iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
 }
 
+int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                                  int ifdipole, const double *d_dipstr, const double *d_dipvec, int npts,
+                                  const double *d_pts, const int *d_skip, double *d_pot, double *d_fld,
+                                  void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    Status st;
+    int ns = nsource;
+    DBuf<double> sx, sy, sz, vx, vy, vz, px, py, pz;
+    DBuf<double2> q, dq, o0, o1, o2, o3;
+    bool ok = sx.alloc(ns, s, st) && sy.alloc(ns, s, st) && sz.alloc(ns, s, st) && px.alloc(npts, s, st) &&
+              py.alloc(npts, s, st) && pz.alloc(npts, s, st) && o0.alloc(npts, s, st) && o1.alloc(npts, s, st) &&
+              o2.alloc(npts, s, st) && o3.alloc(npts, s, st);
+    if (ifcharge == 1) ok = ok && q.alloc(ns, s, st);
+    if (ifdipole == 1) ok = ok && dq.alloc(ns, s, st) && vx.alloc(ns, s, st) && vy.alloc(ns, s, st) && vz.alloc(ns, s, st);
+    if (!ok) return 8;
+    k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_source, sx.p, sy.p, sz.p); FMM_COUNT_LAUNCH();
+    k_split_aos<<<div_up(npts, 256), 256, 0, s>>>(npts, d_pts, px.p, py.p, pz.p); FMM_COUNT_LAUNCH();
+    if (ifcharge == 1) { k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_charge, q.p); FMM_COUNT_LAUNCH(); }
+    if (ifdipole == 1) {
+        k_split_c<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dipstr, dq.p); FMM_COUNT_LAUNCH();
+        k_split_aos<<<div_up(ns, 256), 256, 0, s>>>(ns, d_dipvec, vx.p, vy.p, vz.p); FMM_COUNT_LAUNCH();
+    }
+    OutSoA o;
+    o.pot = o0.p; o.fx = o1.p; o.fy = o2.p; o.fz = o3.p;
+    launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, npts, px.p, py.p, pz.p,
+                  d_skip, 0, o, s, st);
+    k_scatter_out<<<div_up(npts, 256), 256, 0, s>>>(npts, nullptr, o, d_pot, d_fld); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
 void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
                      const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
                      const int *ifpot, double *pot, const int *iffld, double *fld, const int *ntarget,
@@ -689,6 +728,6 @@ int fmm3d_last_stats(long long *out, int n)
 
 const char *fmm3d_last_error(void) { return g_ti.err.c_str(); }
 
-int fmm3d_last_launches(void) { return g_ti.launches; }
+int fmm3d_last_launches(void) { return g_launch_count; }
 
 }  // extern "C"

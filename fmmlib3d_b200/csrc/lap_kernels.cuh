@@ -77,7 +77,7 @@ __host__ __device__ inline size_t rot_class_size(int p) { return (size_t)(p + 1)
 
 void launch_direct(int nsrc, const double *sx, const double *sy, const double *sz, const double2 *q,
                    const double2 *dq, const double *vx, const double *vy, const double *vz, int ifcharge,
-                   int ifdipole, int neval, const double *ex, const double *ey, const double *ez, int self,
+                   int ifdipole, int neval, const double *ex, const double *ey, const double *ez, const int *skip, int self,
                    OutSoA out, cudaStream_t s, Status &st);
 
 }  // namespace fmm

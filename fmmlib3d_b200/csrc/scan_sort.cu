@@ -110,9 +110,9 @@ void scan_exclusive_int(const int *d_in, int *d_out, int n, cudaStream_t s, Stat
     tiles.alloc(ntiles, s, st);
     tot.alloc(1, s, st);
     if (!st.ok()) return;
-    k_tile_sums<<<ntiles, kScanThreads, 0, s>>>(d_in, n, tiles.p);
-    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tiles.p, ntiles, tot.p);
-    k_scan_apply<<<ntiles, kScanThreads, 0, s>>>(d_in, d_out, n, tiles.p);
+    k_tile_sums<<<ntiles, kScanThreads, 0, s>>>(d_in, n, tiles.p); FMM_COUNT_LAUNCH();
+    k_scan_tiles<<<1, kScanThreads, 0, s>>>(tiles.p, ntiles, tot.p); FMM_COUNT_LAUNCH();
+    k_scan_apply<<<ntiles, kScanThreads, 0, s>>>(d_in, d_out, n, tiles.p); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
     if (h_total) {
         FMM_TRY(st, cudaMemcpyAsync(h_total, tot.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -204,9 +204,9 @@ void radix_sort_u64(uint64_t *d_keys, int *d_vals, int n, int bits, cudaStream_t
     int *va = d_vals, *vb = v2.p;
     int passes = 0;
     for (int shift = 0; shift < bits; shift += kRadixBits) {
-        k_radix_hist<<<ntiles, kSortThreads, 0, s>>>(ka, n, shift, hist.p, ntiles);
+        k_radix_hist<<<ntiles, kSortThreads, 0, s>>>(ka, n, shift, hist.p, ntiles); FMM_COUNT_LAUNCH();
         scan_exclusive_int(hist.p, hist.p, kRadix * ntiles, s, st, nullptr);
-        k_radix_scatter<<<ntiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles);
+        k_radix_scatter<<<ntiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         std::swap(ka, kb);
         std::swap(va, vb);

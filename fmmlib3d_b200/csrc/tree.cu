@@ -370,8 +370,8 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     part.alloc(6 * nbb, s, st);
     geom.alloc(4, s, st);
     if (!st.ok()) return;
-    k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p);
-    k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p);
+    k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p); FMM_COUNT_LAUNCH();
+    k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p); FMM_COUNT_LAUNCH();
     // keys and sort
     DBuf<uint64_t> ks, kt;
     ks.alloc(std::max(n, 1), s, st);
@@ -379,8 +379,8 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     T.perm_src.alloc(std::max(n, 1), s, st);
     T.perm_trg.alloc(std::max(m, 1), s, st);
     if (!st.ok()) return;
-    if (n) k_keys<<<div_up(n, 256), 256, 0, s>>>(d_src, n, geom.p, ks.p, T.perm_src.p);
-    if (m) k_keys<<<div_up(m, 256), 256, 0, s>>>(d_trg, m, geom.p, kt.p, T.perm_trg.p);
+    if (n) { k_keys<<<div_up(n, 256), 256, 0, s>>>(d_src, n, geom.p, ks.p, T.perm_src.p); FMM_COUNT_LAUNCH(); }
+    if (m) { k_keys<<<div_up(m, 256), 256, 0, s>>>(d_trg, m, geom.p, kt.p, T.perm_trg.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     radix_sort_u64(ks.p, T.perm_src.p, n, 3 * kMaxLevel, s, st);
     radix_sort_u64(kt.p, T.perm_trg.p, m, 3 * kMaxLevel, s, st);
@@ -408,7 +408,7 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     T.cap = 0;
     if (!ensure(cap, 0)) return;
     k_root<<<1, 32, 0, s>>>(n, m, geom.p, T.ijk.p, T.level.p, T.parent.p, T.octant.p, T.nchild.p, T.child.p,
-                            T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p, T.center.p);
+                            T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p, T.center.p); FMM_COUNT_LAUNCH();
     T.lev_start.assign(1, 0);
     T.lev_count.assign(1, 1);
     int nboxes = 1;
@@ -419,7 +419,7 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
             !cns.alloc(8L * nb, s, st) || !ct0.alloc(8L * nb, s, st) || !cnt.alloc(8L * nb, s, st))
             return;
         k_split<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nbox, T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p,
-                                                 ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p, cnt.p);
+                                                 ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p, cnt.p); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         int total = 0;
         scan_exclusive_int(nk.p, kb.p, nb, s, st, &total);
@@ -428,7 +428,7 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
         k_make_children<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nboxes, kb.p, nk.p, cs0.p, cns.p, ct0.p,
                                                          cnt.p, geom.p, T.ijk.p, T.level.p, T.parent.p,
                                                          T.octant.p, T.nchild.p, T.child.p, T.src0.p, T.nsrc.p,
-                                                         T.trg0.p, T.ntrg.p, T.center.p);
+                                                         T.trg0.p, T.ntrg.p, T.center.p); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         if (total == 0) break;
         T.lev_start.push_back(nboxes);
@@ -443,9 +443,10 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     // colleagues, level by level
     T.coll.alloc(27L * nboxes, s, st);
     if (!st.ok()) return;
-    for (int l = 0; l <= T.nlev; l++)
+    for (int l = 0; l <= T.nlev; l++) {
         k_colleagues<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], T.ijk.p,
-                                                                  T.parent.p, T.child.p, T.coll.p);
+                                                                  T.parent.p, T.child.p, T.coll.p); FMM_COUNT_LAUNCH();
+    }
     FMM_LAUNCH_CHECK(st);
 
     // leaves
@@ -453,13 +454,13 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     flag.alloc(nboxes, s, st);
     pos.alloc(nboxes, s, st);
     if (!st.ok()) return;
-    k_flag_leaves<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.nchild.p, flag.p);
+    k_flag_leaves<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.nchild.p, flag.p); FMM_COUNT_LAUNCH();
     int nleaves = 0;
     scan_exclusive_int(flag.p, pos.p, nboxes, s, st, &nleaves);
     T.nleaves = nleaves;
     T.leaves.alloc(std::max(nleaves, 1), s, st);
     if (!st.ok()) return;
-    k_compact<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, flag.p, pos.p, T.leaves.p);
+    k_compact<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, flag.p, pos.p, T.leaves.p); FMM_COUNT_LAUNCH();
 
     // lists 1 and 3 (count, scan, fill), list 4 as the dual of list 3
     DBuf<int> n1, n3;
@@ -474,7 +475,7 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     int lb = std::max(nleaves, 1);
     k_lists13<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.ijk.p, T.level.p, T.parent.p, T.nchild.p,
                                               T.child.p, T.coll.p, 0, n1.p, n3.p, nullptr, nullptr, nullptr,
-                                              nullptr);
+                                              nullptr); FMM_COUNT_LAUNCH();
     int tot1 = 0, tot3 = 0;
     scan_exclusive_int(n1.p, T.l1_start.p, nboxes + 1, s, st, &tot1);
     scan_exclusive_int(n3.p, T.l3_start.p, nboxes + 1, s, st, &tot3);
@@ -483,21 +484,21 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     if (!st.ok()) return;
     k_lists13<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.ijk.p, T.level.p, T.parent.p, T.nchild.p,
                                               T.child.p, T.coll.p, 1, nullptr, nullptr, T.l1_start.p,
-                                              T.l1_idx.p, T.l3_start.p, T.l3_idx.p);
+                                              T.l1_idx.p, T.l3_start.p, T.l3_idx.p); FMM_COUNT_LAUNCH();
     DBuf<int> n4, cur;
     n4.alloc(nboxes + 1, s, st);
     cur.alloc(nboxes + 1, s, st);
     if (!st.ok()) return;
     n4.zero(st);
-    k_list4_count<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.l3_start.p, T.l3_idx.p, n4.p);
+    k_list4_count<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.l3_start.p, T.l3_idx.p, n4.p); FMM_COUNT_LAUNCH();
     int tot4 = 0;
     scan_exclusive_int(n4.p, T.l4_start.p, nboxes + 1, s, st, &tot4);
     T.l4_idx.alloc(std::max(tot4, 1), s, st);
     if (!st.ok()) return;
     FMM_TRY(st, cudaMemcpyAsync(cur.p, T.l4_start.p, sizeof(int) * (nboxes + 1), cudaMemcpyDeviceToDevice, s));
     k_list4_fill<<<div_up(lb, 128), 128, 0, s>>>(T.leaves.p, nleaves, T.l3_start.p, T.l3_idx.p, cur.p,
-                                                 T.l4_idx.p);
-    k_sort_rows<<<div_up(nboxes, 128), 128, 0, s>>>(nboxes, T.l4_start.p, T.l4_idx.p);
+                                                 T.l4_idx.p); FMM_COUNT_LAUNCH();
+    k_sort_rows<<<div_up(nboxes, 128), 128, 0, s>>>(nboxes, T.l4_start.p, T.l4_idx.p); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 
     // boxes grouped by (level, octant)
@@ -508,11 +509,11 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
     T.grouped.alloc(nboxes, s, st);
     gs.alloc(ngroups + 1, s, st);
     if (!st.ok()) return;
-    k_group_keys<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.level.p, T.octant.p, gk.p, T.grouped.p);
+    k_group_keys<<<div_up(nboxes, 256), 256, 0, s>>>(nboxes, T.level.p, T.octant.p, gk.p, T.grouped.p); FMM_COUNT_LAUNCH();
     int gbits = 8;
     while ((1 << gbits) < ngroups + 1) gbits += 8;
     radix_sort_u64(gk.p, T.grouped.p, nboxes, gbits, s, st);
-    k_group_bounds<<<div_up(nboxes + 1, 256), 256, 0, s>>>(nboxes, gk.p, ngroups, gs.p);
+    k_group_bounds<<<div_up(nboxes + 1, 256), 256, 0, s>>>(nboxes, gk.p, ngroups, gs.p); FMM_COUNT_LAUNCH();
     T.group_start.assign(ngroups + 1, 0);
     FMM_TRY(st, cudaMemcpyAsync(T.group_start.data(), gs.p, sizeof(int) * (ngroups + 1), cudaMemcpyDeviceToHost, s));
     FMM_TRY(st, cudaStreamSynchronize(s));

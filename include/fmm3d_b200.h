@@ -61,6 +61,16 @@ int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge
                                double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
                                int ifpottarg, double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream);
 
+/* Direct sum at npts arbitrary device-resident points pts(3,npts); skip[k]
+ * (0-based source index, or -1; the array may be NULL) is left out of point
+ * k's sum, which gives the self-excluded values at source points.  Outputs
+ * pot(npts) and fld(3,npts) as complex*16.  The sampled form of
+ * l3dpartdirecttime (src/lfmm3dpart.f:1529-1661). */
+int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                                  int ifdipole, const double *d_dipstr, const double *d_dipvec, int npts,
+                                  const double *d_pts, const int *d_skip, double *d_pot, double *d_fld,
+                                  void *stream);
+
 /* Per-pass device times (ms) of the last FMM call made by this host thread
  * when timing is on: [tree, sort+gather, P2M, M2M, P2L, M2L, L2L, L2P+M2P,
  * P2P, scatter, total].  Returns the number of entries written. */

@@ -1,0 +1,238 @@
+"""GPU parity tests of the Laplace FMM through the C ABI against the oracle.
+
+Tolerances: the GPU FMM and the oracle FMM compute the same tree, lists,
+expansion orders and truncations, so they agree to rounding (relative L2
+difference <= 1e-10 here); against the FP64 direct sum the GPU error must be
+no worse than 2x the oracle's own error (+1e-14) and within the iprec bound.
+"""
+import ctypes
+import os
+import zlib
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import oracle as O  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9}
+TOL_ORACLE = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def geometry(kind, n, rng):
+    if kind == "cube":
+        return rng.random((n, 3))
+    if kind == "sphere":
+        v = rng.normal(size=(n, 3))
+        return v / np.linalg.norm(v, axis=1)[:, None]
+    if kind == "plummer":
+        out = []
+        while sum(len(o) for o in out) < n:
+            u = rng.random(n)
+            r = 0.1 / np.sqrt(u ** (-2 / 3) - 1)
+            v = rng.normal(size=(n, 3))
+            p = r[:, None] * v / np.linalg.norm(v, axis=1)[:, None]
+            out.append(p[r < 1])
+        return np.concatenate(out)[:n]
+    if kind == "ellipsoid":
+        v = rng.normal(size=(n, 3))
+        return v / np.linalg.norm(v, axis=1)[:, None] * np.array([1.0, 0.5, 0.2])
+    if kind == "plane":
+        p = rng.random((n, 3))
+        p[:, 2] = 0.25
+        return p
+    if kind == "two_clusters":
+        p = rng.random((n, 3)) * 1e-3
+        p[n // 2:] += 10.0
+        return p
+    raise ValueError(kind)
+
+
+@pytest.fixture(scope="module")
+def F():
+    import fmmlib3d_b200
+    return fmmlib3d_b200
+
+
+def check_against_oracle(F, iprec, src, trg, q, ds, dv, rng, nsamp=200):
+    n = src.shape[0]
+    ifc, ifd = int(q is not None), int(ds is not None)
+    ier, pot, fld, pt, ft = F.lfmm3dparttarg(iprec, src, ifc, q, ifd, ds, dv, 1, 1, trg, 1, 1)
+    assert ier == 0, F.last_error()
+    oier, opot, ofld, opt, oft = O.lfmm3dparttarg(iprec, src, q, ds, dv, trg)
+    assert oier == 0
+    for a, b in ((pot, opot), (fld, ofld), (pt, opt), (ft, oft)):
+        if b.size:
+            assert rel(a, b) < TOL_ORACLE
+    k = min(nsamp, n)
+    si = rng.choice(n, k, replace=False)
+    dp, df = O.direct_at(src, src[si], si, q, ds, dv)
+    for a, o, d in ((pot[si], opot[si], dp), (fld[si], ofld[si], df)):
+        eg, eo = rel(a, d), rel(o, d)
+        assert eg <= 2 * eo + 1e-14
+        assert eg < EPS[iprec]
+    if trg is not None and len(trg):
+        ti = rng.choice(len(trg), min(nsamp, len(trg)), replace=False)
+        dpt, dft = O.direct_at(src, trg[ti], None, q, ds, dv)
+        for a, o, d in ((pt[ti], opt[ti], dpt), (ft[ti], oft[ti], dft)):
+            assert rel(a, d) <= 2 * rel(o, d) + 1e-14
+    return pot, fld, pt, ft
+
+
+def test_direct_sum_matches_oracle(F):
+    rng = np.random.default_rng(1)
+    n, m = 2500, 700
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    dv = rng.normal(size=(n, 3))
+    g = F.l3dpartdirect(src, 1, q, 1, ds, dv, 1, 1, trg, 1, 1)
+    o = O.l3dpartdirect(src, q, ds, dv, trg)
+    for a, b in zip(g, o):
+        assert rel(a, b) < 1e-13
+
+
+@pytest.mark.parametrize("geom,iprec", [("cube", 0), ("cube", 1), ("cube", 2), ("sphere", 1), ("sphere", -1),
+                                        ("plummer", 1), ("plummer", 0), ("ellipsoid", 2), ("cube", 3),
+                                        ("cube", -2)])
+def test_fmm_parity_charges_dipoles_targets(F, geom, iprec):
+    rng = np.random.default_rng(zlib.crc32(('%s%d' % (geom, iprec)).encode()))
+    n, m = 15000, 6000
+    src = geometry(geom, n, rng)
+    trg = geometry(geom, m, rng) * 1.1
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    dv = rng.normal(size=(n, 3))
+    dv /= np.linalg.norm(dv, axis=1)[:, None]
+    check_against_oracle(F, iprec, src, trg, q, ds, dv, rng)
+
+
+@pytest.mark.parametrize("mode", ["charge", "dipole"])
+def test_fmm_parity_source_kinds(F, mode):
+    rng = np.random.default_rng(7)
+    n = 20000
+    src = geometry("sphere", n, rng)
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n) if mode == "charge" else None
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n) if mode == "dipole" else None
+    dv = rng.normal(size=(n, 3)) if mode == "dipole" else None
+    check_against_oracle(F, 1, src, None, q, ds, dv, rng)
+
+
+def test_reference_driver_inputs(F):
+    from driver_inputs import driver_inputs
+    src, trg, q, ds, dv = driver_inputs(16000)
+    rng = np.random.default_rng(0)
+    check_against_oracle(F, 1, src, trg, q, ds, dv, rng)
+
+
+@pytest.mark.parametrize("geom", ["plane", "two_clusters"])
+def test_degenerate_geometries(F, geom):
+    rng = np.random.default_rng(11)
+    n = 8000
+    src = geometry(geom, n, rng)
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    check_against_oracle(F, 1, src, None, q, None, None, rng)
+
+
+def test_tree_matches_oracle_tree(F):
+    rng = np.random.default_rng(12)
+    n, m = 30000, 10000
+    src = geometry("plummer", n, rng)
+    trg = geometry("cube", m, rng) - 0.5
+    q = rng.uniform(-1, 1, n) + 0j
+    ier = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1, trg, 1, 1)[0]
+    assert ier == 0
+    st = F.last_stats()
+    T = O.Tree(src, trg, 160)
+    nleaves = int(np.sum(T.box[:, 5] < 0))
+    assert (st["nboxes"], st["nlev"], st["nleaves"]) == (T.nboxes, T.nlev, nleaves)
+    # near-field pair count from the oracle's lists 1
+    pairs = 0
+    for b in range(T.nboxes):
+        if T.box[b, 5] >= 0:
+            continue
+        ns = T.box[b, 14] + sum(T.box[c, 14] for c in T.list_of(1, b))
+        pairs += (T.box[b, 14] + T.box[b, 16]) * ns - T.box[b, 14]
+    assert st["p2p_pairs"] == pairs
+
+
+def test_small_and_empty_cases(F):
+    rng = np.random.default_rng(13)
+    # one source: no interactions
+    ier, pot, fld, _, _ = F.lfmm3dparttarg(1, rng.random((1, 3)), 1, np.array([1 + 1j]), 0, None, None, 1, 1)
+    assert ier == 0 and pot[0] == 0 and np.all(fld == 0)
+    # root box only (n <= nbox) equals the direct sum
+    src = rng.random((50, 3))
+    q = rng.normal(size=50) + 0j
+    ier, pot, fld, _, _ = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1)
+    dp, df, _, _ = O.l3dpartdirect(src, q)
+    assert ier == 0 and rel(pot, dp) < 1e-13 and rel(fld, df) < 1e-13
+    # iprec outside -2..6 is rejected
+    assert F.lfmm3dparttarg(9, src, 1, q, 0, None, None, 1, 1)[0] != 0
+
+
+def test_unrequested_outputs_untouched(F):
+    rng = np.random.default_rng(14)
+    n, m = 3000, 1000
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    sentinel = 7.25 + 3.5j
+    pot = np.full(n, sentinel)
+    fld = np.full((n, 3), sentinel)
+    pt = np.full(m, sentinel)
+    ft = np.full((m, 3), sentinel)
+    lib = F.lib()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ier = ctypes.c_int(-1)
+    dummy = np.zeros(2, complex)
+    lib.lfmm3dparttarg_(ctypes.byref(ier), I(1), I(n), P(src), I(1), P(q), I(0), P(dummy), P(src), I(1), P(pot),
+                        I(0), P(fld), I(m), P(trg), I(0), P(pt), I(1), P(ft))
+    assert ier.value == 0
+    assert np.all(fld == sentinel) and np.all(pt == sentinel)
+    assert not np.any(pot == sentinel) and not np.any(ft == sentinel)
+    _, _, opt, oft = O.lfmm3dparttarg(1, src, q, None, None, trg)[1:]
+    assert rel(ft, oft) < TOL_ORACLE
+
+
+def test_repeat_calls_bitwise_identical(F):
+    rng = np.random.default_rng(15)
+    n = 20000
+    src = geometry("sphere", n, rng)
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    a = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1)
+    b = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1)
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
+def test_device_entry_point_matches_host_entry_point(F):
+    import torch
+    rng = np.random.default_rng(16)
+    n, m = 12000, 4000
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.uniform(-1, 1, (n, 2))
+    ds = rng.uniform(-1, 1, (n, 2))
+    dv = rng.normal(size=(n, 3))
+    h = F.lfmm3dparttarg(1, src, 1, q[:, 0] + 1j * q[:, 1], 1, ds[:, 0] + 1j * ds[:, 1], dv, 1, 1, trg, 1, 1)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pot = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+    fld = torch.empty((n, 6), dtype=torch.float64, device="cuda")
+    pt = torch.empty((m, 2), dtype=torch.float64, device="cuda")
+    ft = torch.empty((m, 6), dtype=torch.float64, device="cuda")
+    ier = F.lfmm3dparttarg_device(1, d(src), d(q), d(ds), d(dv), pot, fld, d(trg), pt, ft,
+                                  stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert ier == 0
+    c = lambda t, k: t.cpu().numpy().reshape(-1, 2 * k).view(np.complex128).reshape(-1, k).squeeze()
+    assert np.array_equal(c(pot, 1), h[1]) and np.array_equal(c(fld, 3), h[2])
+    assert np.array_equal(c(pt, 1), h[3]) and np.array_equal(c(ft, 3), h[4])
