@@ -71,6 +71,25 @@ int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcha
                                   const double *d_pts, const int *d_skip, double *d_pot, double *d_fld,
                                   void *stream);
 
+/* l3dpartdirect on device-resident arrays WITHOUT any device allocation.
+ * No counterpart in the reference.  For callers that cannot let the library
+ * allocate: an application whose framework allocator already holds the
+ * GPU's memory, or a latency-bound service loop that forbids cudaMalloc and
+ * cudaFree (which synchronise the device) after start-up.  Scratch lives in
+ * a fixed 11 MB array in the library's device image, present on every GPU
+ * that loads the library until the process exits.  Limit: nsource and
+ * ntarget each at most 65536 (larger sizes return 8 without touching the
+ * GPU).  The first call on a device looks up the array's device address, so
+ * make it before any stream capture.  Calls share the array: calls whose
+ * GPU work overlaps (other streams, other host threads) race; serialise
+ * them.  stream NULL = the legacy default stream.  Returns ier (0 ok, 8 size
+ * limit, 16 CUDA error); fmm3d_noalloc_last_error() describes the failure. */
+int fmm3d_l3dpartdirect_noalloc(int nsource, const double *d_source, int ifcharge, const double *d_charge,
+                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
+                                double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
+                                int ifpottarg, double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream);
+const char *fmm3d_noalloc_last_error(void);
+
 /* Per-pass device times (ms) of the last FMM call made by this host thread
  * when timing is on: [tree, sort+gather, P2M, M2M, P2L, M2L, L2L, L2P+M2P,
  * P2P, scatter, total].  Returns the number of entries written. */
