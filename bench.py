@@ -61,6 +61,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-samples", type=int, default=1000)
+    ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
     return ap.parse_args(argv)
 
 
@@ -200,8 +201,11 @@ def run_b200(args):
             raise RuntimeError("FMM ier=%d: %s" % (ier, F.last_error()))
 
     F.set_timing(True)
-    for _ in range(args.warmup):
+    F.set_m2l_mode(args.m2l_mode)
+    for w in range(args.warmup):
+        F.set_stats(w == args.warmup - 1)   # tree statistics from the last warm-up call only
         step()
+    F.set_stats(False)
     torch.cuda.synchronize()
     clk = ClockSampler(local)
     clk.start()

@@ -41,6 +41,8 @@ _lib.fmm3d_l3ddirect_points_device.restype = _I
 _lib.fmm3d_l3ddirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]
 _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_set_timing.argtypes = [_I]
+_lib.fmm3d_set_stats.argtypes = [_I]
+_lib.fmm3d_set_m2l_mode.argtypes = [_I]
 _lib.fmm3d_last_timing.argtypes = [_P, _I]
 _lib.fmm3d_last_timing.restype = _I
 _lib.fmm3d_last_stats.argtypes = [_P, _I]
@@ -166,6 +168,16 @@ def last_launches():
 
 def set_timing(on=True):
     _lib.fmm3d_set_timing(1 if on else 0)
+
+
+def set_stats(on=True):
+    """Gather tree and interaction statistics on the following calls (last_stats())."""
+    _lib.fmm3d_set_stats(1 if on else 0)
+
+
+def set_m2l_mode(mode):
+    """0 automatic, 1 rotate-shift-rotate, 2 dense per-offset operators (nterms <= 16)."""
+    _lib.fmm3d_set_m2l_mode(int(mode))
 
 
 def last_timing():

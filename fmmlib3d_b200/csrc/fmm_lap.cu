@@ -17,6 +17,7 @@
 
 #include "../../include/fmm3d_b200.h"
 #include "lap_kernels.cuh"
+#include "m2l_dense.cuh"
 #include "tree.cuh"
 
 namespace fmm {
@@ -82,6 +83,7 @@ static void l3dterms_list2(double eps, int *itab)
 // ---------------------------------------------------------------- per-thread state
 struct ThreadInfo {
     bool timing = false;
+    bool want_stats = false;
     std::vector<double> ms;
     std::vector<long long> stats;
     std::string err;
@@ -102,6 +104,22 @@ static cudaStream_t thread_stream()
     return s;
 }
 
+// Keep freed workspace in the device's default memory pool across calls
+// instead of returning it to the driver at every synchronisation.
+static void keep_pool_memory()
+{
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done[dev] = true;
+}
+
 // ---------------------------------------------------------------- operator plan (per device, p, eps)
 // Rotation matrices for every direction class, the slot tables of the three
 // translation kinds and the sqrt-binomial table.  Built once on the device
@@ -114,7 +132,13 @@ struct LapPlan {
     DBuf<Slot> slots;        // [0, 1512): M2L 8 octants x 189; [1512,1520): M2M; [1520,1528): L2L
     std::vector<Slot> hslots;
     int kt = 8;
+    // dense M2L operators (p <= kDenseMaxP): one per list-2 offset, and the
+    // operator offset of every M2L slot
+    bool dense = false;
+    DBuf<double2> T;
+    DBuf<long long> slot_toff;
 };
+static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
 constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
 
 static std::mutex g_plan_mu;
@@ -217,6 +241,45 @@ static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Stat
     int NC = (p + 1) * (p + 1);
     P->kt = 8;
     while (P->kt > 1 && (size_t)3 * P->kt * NC * 16 > 200 * 1024) P->kt /= 2;
+    if (p <= kDenseMaxP) {
+        // unique list-2 offsets and their operators
+        std::map<int, int> uidx;
+        std::vector<M2LOp> uops;
+        std::vector<long long> stoff(8 * 189);
+        long long tot = 0;
+        for (int o = 0; o < 8; o++) {
+            int ob[3] = {o & 1, (o >> 1) & 1, (o >> 2) & 1};
+            for (int si = 0; si < 189; si++) {
+                const Slot &sl = P->hslots[o * 189 + si];
+                int co[3] = {sl.coll / 9 - 1, (sl.coll / 3) % 3 - 1, sl.coll % 3 - 1};
+                int db[3] = {sl.oct & 1, (sl.oct >> 1) & 1, (sl.oct >> 2) & 1};
+                int key = 0;
+                for (int e = 0; e < 3; e++) key = key * 16 + (2 * co[e] + db[e] - ob[e] + 8);
+                auto f = uidx.find(key);
+                if (f == uidx.end()) {
+                    M2LOp op;
+                    op.pt = sl.pt; op.cls = sl.cls; op.ex = sl.ex; op.ey = sl.ey; op.rt = sl.rt; op.toff = tot;
+                    long long R = (long long)(sl.pt + 1) * (sl.pt + 1);
+                    tot += R * R;
+                    f = uidx.emplace(key, (int)uops.size()).first;
+                    uops.push_back(op);
+                }
+                stoff[o * 189 + si] = uops[f->second].toff;
+            }
+        }
+        DBuf<M2LOp> dops;
+        if (dops.alloc(uops.size(), s, st) && P->T.alloc(tot, s, st) && P->slot_toff.alloc(stoff.size(), s, st)) {
+            FMM_TRY(st, cudaMemcpyAsync(dops.p, uops.data(), sizeof(M2LOp) * uops.size(), cudaMemcpyHostToDevice, s));
+            FMM_TRY(st, cudaMemcpyAsync(P->slot_toff.p, stoff.data(), sizeof(long long) * stoff.size(),
+                                        cudaMemcpyHostToDevice, s));
+            build_m2l_ops(p, (int)uops.size(), dops.p, P->rot.p, P->dc.p, P->lddc, P->T.p, s, st);
+            FMM_TRY(st, cudaStreamSynchronize(s));
+        }
+        if (!st.ok()) return nullptr;
+        P->dense = true;
+        P->T.s = nullptr;
+        P->slot_toff.s = nullptr;
+    }
     // buffers are process-lifetime: detach them from the stream they were made on
     P->rot.s = nullptr;
     P->dc.s = nullptr;
@@ -298,21 +361,26 @@ __global__ void k_stats(int nleaves, const int *leaves, TreeView tv, int do_src,
 
 __global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int prune, unsigned long long *hist)
 {
+    __shared__ unsigned int h[128];
+    for (int i = threadIdx.x; i < 128; i += blockDim.x) h[i] = 0;
+    __syncthreads();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nb) return;
     int b = b0 + t;
-    if (prune && tv.ntrg[b] == 0) return;
-    int P = tv.parent[b];
-    if (P < 0) return;
-    int o = tv.octant[b];
-    for (int s = 0; s < 189; s++) {
-        const Slot &sl = slots[o * 189 + s];
-        int C = tv.coll[27L * P + sl.coll];
-        if (C < 0) continue;
-        int src = tv.child[8L * C + sl.oct];
-        if (src < 0 || tv.nsrc[src] == 0) continue;
-        atomicAdd(&hist[sl.pt], 1ull);
+    if (t < nb && !(prune && tv.ntrg[b] == 0) && tv.parent[b] >= 0) {
+        int P = tv.parent[b];
+        int o = tv.octant[b];
+        for (int s = 0; s < 189; s++) {
+            const Slot &sl = slots[o * 189 + s];
+            int C = tv.coll[27L * P + sl.coll];
+            if (C < 0) continue;
+            int src = tv.child[8L * C + sl.oct];
+            if (src < 0 || tv.nsrc[src] == 0) continue;
+            atomicAdd(&h[sl.pt], 1u);
+        }
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 128; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
 }
 
 // ---------------------------------------------------------------- the FMM
@@ -360,6 +428,7 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     if (nt < 0) nt = 0;
     if (ifpottarg != 1 && iffldtarg != 1) nt = nt;  // targets still shape the tree, as in the reference
     lap_init_constants(st);
+    keep_pool_memory();
     int p = l3dterms(eps);
     if (p > 72) return 16;
     auto plan = get_plan(p, eps, s, st);
@@ -429,8 +498,9 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
         make_tiles(l, plan->kt, kSlotM2M, 0, 8, htiles);
         m2m_rng.push_back({a, (int)htiles.size() - a});
     }
+    const bool dense = plan->dense && g_m2l_mode != 1;
     int m2l_a = (int)htiles.size();
-    for (int l = 2; l <= T.nlev; l++) make_tiles(l, plan->kt, 0, 189, 189, htiles);
+    for (int l = 2; l <= T.nlev; l++) make_tiles(l, dense ? kDenseTileTargets : plan->kt, 0, 189, 189, htiles);
     int m2l_n = (int)htiles.size() - m2l_a;
     for (int l = 2; l <= T.nlev - 1; l++) {
         int a = (int)htiles.size();
@@ -458,8 +528,12 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     launch_p2l(T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, p, local.p, s, st);
     tm.mark();
     // STEP 4: M2L over list 2, all levels >= 2
-    launch_translate(1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p, plan->dc.p,
-                     plan->lddc, mpole.p, local.p, prune, plan->kt, s, st);
+    if (dense)
+        launch_m2l_dense(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p, tv, p,
+                         mpole.p, local.p, prune, s, st);
+    else
+        launch_translate(1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p, plan->dc.p,
+                         plan->lddc, mpole.p, local.p, prune, plan->kt, s, st);
     tm.mark();
     // STEP 5: L2L, levels 2 .. nlev-1
     for (auto &r : l2l_rng)
@@ -486,8 +560,8 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     FMM_LAUNCH_CHECK(st);
     tm.mark();
     tm.finish(g_ti.ms);
-    // statistics
-    {
+    // statistics (on request: they cost a few kernels and a device->host read)
+    if (g_ti.want_stats) {
         DBuf<unsigned long long> acc;
         acc.alloc(1 + 128, s, st);
         acc.zero(st);
@@ -649,8 +723,8 @@ int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcha
     }
     OutSoA o;
     o.pot = o0.p; o.fx = o1.p; o.fy = o2.p; o.fz = o3.p;
-    launch_direct(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, npts, px.p, py.p, pz.p,
-                  d_skip, 0, o, s, st);
+    launch_direct_split(ns, sx.p, sy.p, sz.p, q.p, dq.p, vx.p, vy.p, vz.p, ifcharge, ifdipole, npts, px.p, py.p,
+                        pz.p, d_skip, o, s, st);
     k_scatter_out<<<div_up(npts, 256), 256, 0, s>>>(npts, nullptr, o, d_pot, d_fld); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
     FMM_TRY(st, cudaStreamSynchronize(s));
@@ -709,6 +783,18 @@ void l3dpartdirect_(const int *nsource, const double *source, const int *ifcharg
 int fmm3d_set_timing(int on)
 {
     g_ti.timing = on != 0;
+    return 0;
+}
+
+int fmm3d_set_m2l_mode(int mode)
+{
+    g_m2l_mode = mode;
+    return 0;
+}
+
+int fmm3d_set_stats(int on)
+{
+    g_ti.want_stats = on != 0;
     return 0;
 }
 

@@ -80,4 +80,9 @@ void launch_direct(int nsrc, const double *sx, const double *sy, const double *s
                    int ifdipole, int neval, const double *ex, const double *ey, const double *ez, const int *skip, int self,
                    OutSoA out, cudaStream_t s, Status &st);
 
+void launch_direct_split(int nsrc, const double *sx, const double *sy, const double *sz, const double2 *q,
+                         const double2 *dq, const double *vx, const double *vy, const double *vz, int ifcharge,
+                         int ifdipole, int neval, const double *ex, const double *ey, const double *ez,
+                         const int *skip, OutSoA out, cudaStream_t s, Status &st);
+
 }  // namespace fmm

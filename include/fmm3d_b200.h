@@ -96,9 +96,17 @@ const char *fmm3d_noalloc_last_error(void);
 int fmm3d_set_timing(int on);
 int fmm3d_last_timing(double *ms, int n);
 
-/* Tree statistics of the last call on this thread:
+/* Tree statistics of the last call on this thread, gathered only while
+ * fmm3d_set_stats(1) is in effect:
  * [nboxes, nlev, nleaves, nterms, list1 entries, list3 entries,
  *  list4 entries, p2p pairs (sum over leaves), m2l pairs]. */
+int fmm3d_set_stats(int on);
+
+/* M2L form: 0 automatic (dense per-offset operators for nterms <= 16,
+ * rotate-shift-rotate otherwise), 1 always rotate-shift-rotate, 2 dense
+ * where available.  Both give the same results to rounding; the switch
+ * exists for testing and measurement. */
+int fmm3d_set_m2l_mode(int mode);
 int fmm3d_last_stats(long long *out, int n);
 
 /* Human-readable description of the last CUDA error on this thread. */

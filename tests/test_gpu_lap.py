@@ -150,7 +150,9 @@ def test_tree_matches_oracle_tree(F):
     src = geometry("plummer", n, rng)
     trg = geometry("cube", m, rng) - 0.5
     q = rng.uniform(-1, 1, n) + 0j
+    F.set_stats(True)
     ier = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1, trg, 1, 1)[0]
+    F.set_stats(False)
     assert ier == 0
     st = F.last_stats()
     T = O.Tree(src, trg, 160)
@@ -236,3 +238,21 @@ def test_device_entry_point_matches_host_entry_point(F):
     c = lambda t, k: t.cpu().numpy().reshape(-1, 2 * k).view(np.complex128).reshape(-1, k).squeeze()
     assert np.array_equal(c(pot, 1), h[1]) and np.array_equal(c(fld, 3), h[2])
     assert np.array_equal(c(pt, 1), h[3]) and np.array_equal(c(ft, 3), h[4])
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("geom,iprec", [("cube", 1), ("sphere", 0), ("plummer", -1)])
+def test_m2l_forms_agree_with_oracle(F, mode, geom, iprec):
+    """Rotate-shift-rotate (mode 1) and dense per-offset operators (mode 2) both match the oracle."""
+    rng = np.random.default_rng(zlib.crc32(('m2l%s%d%d' % (geom, iprec, mode)).encode()))
+    n, m = 20000, 5000
+    src = geometry(geom, n, rng)
+    trg = geometry(geom, m, rng) * 1.05
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    dv = rng.normal(size=(n, 3))
+    F.set_m2l_mode(mode)
+    try:
+        check_against_oracle(F, iprec, src, trg, q, ds, dv, rng)
+    finally:
+        F.set_m2l_mode(0)
