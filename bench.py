@@ -136,10 +136,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_fp64_peak(torch, dev):
-    """FP64 throughput of cuBLAS DGEMM (8192^3, best of 5) in TFLOP/s."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+def measured_peak(torch, dev, dtype):
+    """cuBLAS GEMM throughput (8192^3, best of 5, TF32 off) in TFLOP/s for dtype."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=dtype, device=dev)
+    b = torch.randn(8192, 8192, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e9
@@ -193,6 +194,7 @@ def run_b200(args):
     d_pt = torch.empty((m, 2), dtype=torch.float64, device=dev)
     d_ft = torch.empty((m, 6), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
+    F.set_m2l_mode(args.m2l_mode)
 
     def step():
         ier = F.lfmm3dparttarg_device(args.iprec, d_src, d_q, d_dq, d_dv, d_pot, d_fld, d_trg, d_pt, d_ft,
@@ -200,63 +202,63 @@ def run_b200(args):
         if ier != 0:
             raise RuntimeError("FMM ier=%d: %s" % (ier, F.last_error()))
 
-    F.set_timing(True)
-    F.set_m2l_mode(args.m2l_mode)
-    for w in range(args.warmup):
-        F.set_stats(w == args.warmup - 1)   # tree statistics from the last warm-up call only
-        step()
-    F.set_stats(False)
-    torch.cuda.synchronize()
-    clk = ClockSampler(local)
-    clk.start()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    passes, launches = [], []
-    ev[0].record()
-    for k in range(args.steps):
-        step()
-        ev[k + 1].record()
-        passes.append(F.last_timing())
-        launches.append(F.last_launches())
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    clocks = clk.stop()
-    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[args.steps])
-    stats = F.last_stats()
-    if ws > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    def errors():
+        rng = np.random.default_rng(99)
+        k = min(args.err_samples, n)
+        si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
+        ti = np.sort(rng.choice(m, k, replace=False)).astype(np.int32)
+        out = {}
+        dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
+        df = torch.empty((k, 6), dtype=torch.float64, device=dev)
+        for name, idx, pts, skip, P, Fd in (("src", si, d_src[si], torch.from_numpy(si).to(dev), d_pot, d_fld),
+                                            ("targ", ti, d_trg[ti], None, d_pt, d_ft)):
+            ier = F.direct_points_device(d_src, d_q, d_dq, d_dv, pts.contiguous(), skip, dp, df, stream=stream)
+            torch.cuda.synchronize()
+            if ier != 0:
+                raise RuntimeError("direct ier=%d" % ier)
+            it = torch.from_numpy(idx).to(dev).long()
+            out["pot" if name == "src" else "pottarg"] = float(torch.linalg.norm(P[it] - dp) / torch.linalg.norm(dp))
+            out["fld" if name == "src" else "fldtarg"] = float(torch.linalg.norm(Fd[it] - df) / torch.linalg.norm(df))
+        return out
 
-    # errors vs the FP64 direct sum at seeded sample points (outside the timed region)
-    rng = np.random.default_rng(99)
-    k = min(args.err_samples, n)
-    si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
-    ti = np.sort(rng.choice(m, k, replace=False)).astype(np.int32)
-    errs = {}
-    dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
-    df = torch.empty((k, 6), dtype=torch.float64, device=dev)
-    for name, pts, skip, P, Fd in (("src", d_src[si], torch.from_numpy(si).to(dev), d_pot, d_fld),
-                                   ("targ", d_trg[ti], None, d_pt, d_ft)):
-        ier = F.direct_points_device(d_src, d_q, d_dq, d_dv, pts.contiguous(), skip, dp, df, stream=stream)
+    def measure(form):
+        F.set_precision(form)
+        F.set_timing(True)
+        for w in range(args.warmup):
+            F.set_stats(w == args.warmup - 1)   # tree statistics from the last warm-up call only
+            step()
+        F.set_stats(False)
         torch.cuda.synchronize()
-        if ier != 0:
-            raise RuntimeError("direct ier=%d" % ier)
-        idx = torch.from_numpy(si if name == "src" else ti).to(dev).long()
-        ep = torch.linalg.norm(P[idx] - dp) / torch.linalg.norm(dp)
-        ef = torch.linalg.norm(Fd[idx] - df) / torch.linalg.norm(df)
-        key = "pot" if name == "src" else "pottarg"
-        errs[key] = float(ep)
-        errs["fld" if name == "src" else "fldtarg"] = float(ef)
+        clk = ClockSampler(local)
+        clk.start()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        passes, launches = [], []
+        ev[0].record()
+        for k in range(args.steps):
+            step()
+            ev[k + 1].record()
+            passes.append(F.last_timing())
+            launches.append(F.last_launches())
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        clocks = clk.stop()
+        step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+        total_ms = ev[0].elapsed_time(ev[args.steps])
+        if ws > 1:
+            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        return dict(total_ms=total_ms, step_ms=step_ms, passes=passes, launches=launches, stats=F.last_stats(),
+                    clocks=clocks, errs=errors())
 
-    fp64_peak = measured_fp64_peak(torch, dev)
-    return dict(n=n, m=m, ws=ws, rank=rank, total_ms=total_ms, step_ms=step_ms, passes=passes,
-                launches=launches, stats=stats, clocks=clocks, errs=errs, fp64_peak=fp64_peak, torch=torch,
-                F=F, dist=dist if ws > 1 else None, arrays=(src, q, dq, dv, trg))
+    forms = {"mixed": measure(1), "fp64": measure(0)}
+    peaks = {"fp64": measured_peak(torch, dev, torch.float64), "fp32": measured_peak(torch, dev, torch.float32)}
+    return dict(n=n, m=m, ws=ws, rank=rank, forms=forms, peaks=peaks, torch=torch, F=F,
+                dist=dist if ws > 1 else None, arrays=(src, q, dq, dv, trg))
 
 
 def run_e2e(args, R):
@@ -304,13 +306,12 @@ def run_e2e(args, R):
             "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * dt / args.steps, "host_memory": "pinned"}
 
 
-def roofline_of(R):
-    """Roofline of the dominant pass, from the per-pass CUDA events of the timed steps."""
-    keys = [k for k in R["passes"][0] if k not in ("total",)]
-    mean = {k: float(np.mean([p[k] for p in R["passes"]])) for k in keys}
+def roofline_of(M, peak, bound):
+    """Roofline of the dominant pass of one form, from the per-pass CUDA events of its timed steps."""
+    keys = [k for k in M["passes"][0] if k not in ("total",)]
+    mean = {k: float(np.mean([p[k] for p in M["passes"]])) for k in keys}
     top = max(mean, key=mean.get)
-    st = R["stats"]
-    peak = R["fp64_peak"]
+    st = M["stats"]
     if top == "p2p":
         flops = st["p2p_pairs"] * P2P_FLOPS_PER_PAIR
         traffic = None if P2P_DRAM_BYTES_PER_PAIR is None else P2P_DRAM_BYTES_PER_PAIR * st["p2p_pairs"]
@@ -319,8 +320,9 @@ def roofline_of(R):
         traffic = None
     else:
         flops, traffic = None, None
-    out = {"kernel": top, "bound": "fp64", "unit": "TFLOP/s", "peak": round(peak, 2),
-           "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
+    out = {"kernel": top, "bound": bound, "unit": "TFLOP/s", "peak": round(peak, 2),
+           "peak_source": "cuBLAS %s GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no %s figure)" % (
+               "DGEMM" if bound == "fp64" else "SGEMM (TF32 off)", bound),
            "traffic": traffic, "pass_ms_mean": {k: round(v, 3) for k, v in mean.items()}}
     if flops is not None:
         ach = flops / (mean[top] * 1e-3) / 1e12
@@ -367,7 +369,8 @@ def run_reference(args):
 def config_of(args, ws):
     return {"workload": "laplace_lfmm3dparttarg_cube_%dM_src_%dM_targ" % (args.n // 10 ** 6, args.n // 10 ** 6),
             "n_sources": args.n, "n_targets": args.n, "iprec": args.iprec, "charges": True, "dipoles": True,
-            "outputs": "pot+fld at sources and targets", "form": "fp64", "parallelism": "replicas x%d" % ws,
+            "outputs": "pot+fld at sources and targets", "forms": "mixed (headline) and fp64",
+            "parallelism": "replicas x%d" % ws,
             "l2_policy": "inputs larger than L2 (%.0f MB per step of inputs vs 126 MB L2)" % (args.n * 104 / 1e6)}
 
 
@@ -380,19 +383,29 @@ def main(argv=None):
             print(json.dumps(line), flush=True)
         return 0
     R = run_b200(args)
+    R["F"].set_precision(1)
     e2e = None if args.no_e2e else run_e2e(args, R)
     n, m = R["n"], R["m"]
-    total_s = R["total_ms"] * 1e-3
-    value = ws * (n + m) * args.steps / total_s
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": R["total_ms"] / args.steps,
-            "p50_ms": float(np.percentile(R["step_ms"], 50)), "p99_ms": float(np.percentile(R["step_ms"], 99)),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+
+    def summary(M):
+        return {"value": ws * (n + m) * args.steps / (M["total_ms"] * 1e-3), "ms_per_step": M["total_ms"] / args.steps,
+                "p50_ms": float(np.percentile(M["step_ms"], 50)), "p99_ms": float(np.percentile(M["step_ms"], 99)),
+                "errors": {k: float("%.3e" % v) for k, v in M["errs"].items()}}
+
+    H = R["forms"]["mixed"]
+    head = summary(H)
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "p50_ms": head["p50_ms"],
+            "p99_ms": head["p99_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 mixed (P2P, M2L in f32; tree, recurrences, other passes f64)",
             "data": "synthetic (seeded uniform cube; charges, dipoles)", "config": config_of(args, ws),
-            "errors": {k: float("%.3e" % v) for k, v in R["errs"].items()},
-            "gpu_launches": int(sum(R["launches"])), "clocks": R["clocks"], "e2e": e2e,
-            "roofline": roofline_of(R),
-            "stats": {k: v for k, v in R["stats"].items() if k != "m2l_pt_hist"}}
+            "errors": head["errors"], "gpu_launches": int(sum(H["launches"])), "clocks": H["clocks"], "e2e": e2e,
+            "roofline": roofline_of(H, R["peaks"]["fp32"], "fp32"),
+            "forms": {"mixed": head, "fp64": dict(summary(R["forms"]["fp64"]),
+                                                  roofline=roofline_of(R["forms"]["fp64"], R["peaks"]["fp64"], "fp64"),
+                                                  gpu_launches=int(sum(R["forms"]["fp64"]["launches"])))},
+            "stats": {k: v for k, v in H["stats"].items() if k != "m2l_pt_hist"}}
+    line["forms"]["mixed_over_fp64"] = round(head["value"] / line["forms"]["fp64"]["value"], 3)
     if rank == 0 and ws == 1 and not args.no_cpu:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         dt, pts = cpu_fmm_sample(args.cpu_sample, args.iprec)

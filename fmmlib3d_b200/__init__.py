@@ -43,6 +43,7 @@ _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
 _lib.fmm3d_set_m2l_mode.argtypes = [_I]
+_lib.fmm3d_set_precision.argtypes = [_I]
 _lib.fmm3d_last_timing.argtypes = [_P, _I]
 _lib.fmm3d_last_timing.restype = _I
 _lib.fmm3d_last_stats.argtypes = [_P, _I]
@@ -178,6 +179,11 @@ def set_stats(on=True):
 def set_m2l_mode(mode):
     """0 automatic, 1 rotate-shift-rotate, 2 dense per-offset operators (nterms <= 16)."""
     _lib.fmm3d_set_m2l_mode(int(mode))
+
+
+def set_precision(mode):
+    """0 FP64 throughout (default), 1 mixed FP32 P2P/M2L for iprec <= 1."""
+    _lib.fmm3d_set_precision(int(mode))
 
 
 def last_timing():

@@ -136,9 +136,11 @@ struct LapPlan {
     // operator offset of every M2L slot
     bool dense = false;
     DBuf<double2> T;
+    DBuf<float2> T32;        // the same operators rounded to FP32 (mixed form)
     DBuf<long long> slot_toff;
 };
 static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
+static int g_precision = 0; // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
 constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
 
 static std::mutex g_plan_mu;
@@ -273,11 +275,13 @@ static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Stat
             FMM_TRY(st, cudaMemcpyAsync(P->slot_toff.p, stoff.data(), sizeof(long long) * stoff.size(),
                                         cudaMemcpyHostToDevice, s));
             build_m2l_ops(p, (int)uops.size(), dops.p, P->rot.p, P->dc.p, P->lddc, P->T.p, s, st);
+            if (P->T32.alloc(tot, s, st)) convert_f32(tot, P->T.p, P->T32.p, s, st);
             FMM_TRY(st, cudaStreamSynchronize(s));
         }
         if (!st.ok()) return nullptr;
         P->dense = true;
         P->T.s = nullptr;
+        P->T32.s = nullptr;
         P->slot_toff.s = nullptr;
     }
     // buffers are process-lifetime: detach them from the stream they were made on
@@ -498,7 +502,8 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
         make_tiles(l, plan->kt, kSlotM2M, 0, 8, htiles);
         m2m_rng.push_back({a, (int)htiles.size() - a});
     }
-    const bool dense = plan->dense && g_m2l_mode != 1;
+    const bool mixed = g_precision == 1 && iprec <= 1 && plan->dense;
+    const bool dense = (plan->dense && g_m2l_mode != 1) || mixed;
     int m2l_a = (int)htiles.size();
     for (int l = 2; l <= T.nlev; l++) make_tiles(l, dense ? kDenseTileTargets : plan->kt, 0, 189, 189, htiles);
     int m2l_n = (int)htiles.size() - m2l_a;
@@ -528,7 +533,10 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     launch_p2l(T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, p, local.p, s, st);
     tm.mark();
     // STEP 4: M2L over list 2, all levels >= 2
-    if (dense)
+    if (mixed)
+        launch_m2l_dense32(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T32.p, tv,
+                           p, mpole.p, local.p, prune, s, st);
+    else if (dense)
         launch_m2l_dense(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p, tv, p,
                          mpole.p, local.p, prune, s, st);
     else
@@ -545,8 +553,12 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
                 do_src, do_trg, s, st);
     tm.mark();
     // STEP 8: P2P over self and list 1 (adds to the outputs)
-    launch_p2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
-               do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+    if (mixed)
+        launch_p2p32(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
+                     do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+    else
+        launch_p2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
+                   do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
     tm.mark();
     // unsort into the caller's order
     if (do_src) {
@@ -783,6 +795,12 @@ void l3dpartdirect_(const int *nsource, const double *source, const int *ifcharg
 int fmm3d_set_timing(int on)
 {
     g_ti.timing = on != 0;
+    return 0;
+}
+
+int fmm3d_set_precision(int mode)
+{
+    g_precision = mode;
     return 0;
 }
 

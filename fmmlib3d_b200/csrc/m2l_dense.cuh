@@ -23,3 +23,17 @@ void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const S
                       double2 *out, int prune, cudaStream_t s, Status &st);
 
 }  // namespace fmm
+
+namespace fmm {
+
+// Mixed-precision form (mixed.cu): FP32 P2P with compensated accumulation
+// and FP32 dense M2L.
+void launch_p2p32(const int *leaves, int nleaves, const TreeView &tv, const PointsSoA &src, const double *tx,
+                  const double *ty, const double *tz, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
+                  int ifpot, int iffld, int ifpottarg, int iffldtarg, cudaStream_t s, Status &st);
+void convert_f32(long long n, const double2 *in, float2 *out, cudaStream_t s, Status &st);
+void launch_m2l_dense32(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
+                        const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const double2 *in,
+                        double2 *out, int prune, cudaStream_t s, Status &st);
+
+}  // namespace fmm

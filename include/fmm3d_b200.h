@@ -107,6 +107,13 @@ int fmm3d_set_stats(int on);
  * where available.  Both give the same results to rounding; the switch
  * exists for testing and measurement. */
 int fmm3d_set_m2l_mode(int mode);
+
+/* Arithmetic form of later calls (process-wide): 0 = FP64 throughout (the
+ * default: the reference's arithmetic), 1 = mixed precision for iprec <= 1:
+ * P2P in FP32 with TwoSum-compensated accumulation and M2L with FP32
+ * operators, FP64 for the tree, geometry, recurrences, rotations and the
+ * other passes.  iprec >= 2 always runs FP64. */
+int fmm3d_set_precision(int mode);
 int fmm3d_last_stats(long long *out, int n);
 
 /* Human-readable description of the last CUDA error on this thread. */

@@ -256,3 +256,32 @@ def test_m2l_forms_agree_with_oracle(F, mode, geom, iprec):
         check_against_oracle(F, iprec, src, trg, q, ds, dv, rng)
     finally:
         F.set_m2l_mode(0)
+
+
+@pytest.mark.parametrize("geom,iprec", [("cube", 1), ("cube", 0), ("sphere", 1), ("plummer", 1)])
+def test_mixed_form_within_twice_reference_error(F, geom, iprec):
+    """Mixed form (FP32 P2P + FP32 M2L operators): error vs the FP64 direct sum at most 2x the oracle's."""
+    rng = np.random.default_rng(zlib.crc32(('mixed%s%d' % (geom, iprec)).encode()))
+    n, m = 40000, 20000
+    src = geometry(geom, n, rng)
+    trg = geometry(geom, m, rng) * 1.05
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    dv = rng.normal(size=(n, 3))
+    dv /= np.linalg.norm(dv, axis=1)[:, None]
+    F.set_precision(1)
+    try:
+        ier, pot, fld, pt, ft = F.lfmm3dparttarg(iprec, src, 1, q, 1, ds, dv, 1, 1, trg, 1, 1)
+    finally:
+        F.set_precision(0)
+    assert ier == 0
+    oier, opot, ofld, opt, oft = O.lfmm3dparttarg(iprec, src, q, ds, dv, trg)
+    k = 400
+    si = rng.choice(n, k, replace=False)
+    ti = rng.choice(m, k, replace=False)
+    dp, df = O.direct_at(src, src[si], si, q, ds, dv)
+    dpt, dft = O.direct_at(src, trg[ti], None, q, ds, dv)
+    for a, o, d in ((pot[si], opot[si], dp), (fld[si], ofld[si], df), (pt[ti], opt[ti], dpt), (ft[ti], oft[ti], dft)):
+        eg, eo = rel(a, d), rel(o, d)
+        assert eg < EPS[iprec]
+        assert eg <= 2 * eo, (eg, eo)
