@@ -54,7 +54,7 @@ __global__ void k_build_m2l_ops(int p, const M2LOp *ops, const double *rot, cons
         double2 en = cmk(1, 0);
         for (int i = 0; i < (m < 0 ? -m : m); i++) en = cmul(en, e1);
         ph = m >= 0 ? cmulc(ph, en) : cmul(ph, en);
-        T[op.toff + (size_t)row * R + col] = cscal(s, ph);
+        T[op.toff + (size_t)col * R + row] = cscal(s, ph);  // column-major
     }
 }
 
@@ -102,19 +102,20 @@ __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tile
         if (!anyv) continue;
         const double2 *Tu = T + slot_toff[tile.slot0 + si];
         for (int k0 = 0; k0 < R; k0 += kTK) {
-            // A tile: rows row0.., cols k0..; each thread loads 4 consecutive columns of one row
+            // A tile: rows row0.., cols k0..; consecutive threads take consecutive
+            // rows of a column (the operators are column-major)
             {
-                int r = threadIdx.x >> 2, c = (threadIdx.x & 3) * 4;
+                int r = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
                 int gr = row0 + r;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     int gc = k0 + c + q;
-                    As[c + q][r] = (gr < R && gc < R) ? Tu[(size_t)gr * R + gc] : cmk(0, 0);
+                    As[c + q][r] = (gr < R && gc < R) ? Tu[(size_t)gc * R + gr] : cmk(0, 0);
                 }
             }
             // B tile: targets j, coefficients k0..; gathered source multipoles
             {
-                int j = threadIdx.x >> 2, c = (threadIdx.x & 3) * 4;
+                int j = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
                 int sb = sv[j];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {

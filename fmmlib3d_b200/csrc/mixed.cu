@@ -31,6 +31,13 @@ __device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float x)
 // centre, and dx = (e.hi - s.hi) + (e.lo - s.lo).  For close pairs the hi
 // difference is exact (Sterbenz), so close-pair differences keep FP64-level
 // accuracy and only r^2, 1/r and the products are FP32.
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <bool CHG, bool DIP>
 __device__ __forceinline__ void pair32(float exh, float eyh, float ezh, float exl, float eyl, float ezl,
                                        float sxh, float syh, float szh, float sxl, float syl, float szl, float2 q,
@@ -38,26 +45,27 @@ __device__ __forceinline__ void pair32(float exh, float eyh, float ezh, float ex
 {
     float dx = (exh - sxh) + (exl - sxl), dy = (eyh - syh) + (eyl - syl), dz = (ezh - szh) + (ezl - szl);
     float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float ri = rsqrtf(r2);
+    float ri = rsqrt_approx(r2);
     float ri2 = ri * ri, ri3 = ri * ri2;
-    if (CHG) {
+    if (CHG && !DIP) {
         a[0] = fmaf(q.x, ri, a[0]);
         a[1] = fmaf(q.y, ri, a[1]);
         float qx = q.x * ri3, qy = q.y * ri3;
         a[2] = fmaf(qx, dx, a[2]); a[3] = fmaf(qy, dx, a[3]);
         a[4] = fmaf(qx, dy, a[4]); a[5] = fmaf(qy, dy, a[5]);
         a[6] = fmaf(qx, dz, a[6]); a[7] = fmaf(qy, dz, a[7]);
-    }
-    if (DIP) {
-        float dot = fmaf(dx, vx, fmaf(dy, vy, dz * vz));
-        float t = dot * ri3;
-        a[0] = fmaf(d.x, t, a[0]);
-        a[1] = fmaf(d.y, t, a[1]);
-        float rt = 3.0f * t * ri2;
-        float gx = fmaf(rt, dx, -ri3 * vx), gy = fmaf(rt, dy, -ri3 * vy), gz = fmaf(rt, dz, -ri3 * vz);
-        a[2] = fmaf(d.x, gx, a[2]); a[3] = fmaf(d.y, gx, a[3]);
-        a[4] = fmaf(d.x, gy, a[4]); a[5] = fmaf(d.y, gy, a[5]);
-        a[6] = fmaf(d.x, gz, a[6]); a[7] = fmaf(d.y, gz, a[7]);
+    } else {
+        // pot = (q + d t) / r with t = (v.dx)/r^2;  fld = [(q + 3 d t) dx - d v] / r^3
+        float t = fmaf(dx, vx, fmaf(dy, vy, dz * vz)) * ri2;
+        float ax = CHG ? fmaf(d.x, t, q.x) : d.x * t, ay = CHG ? fmaf(d.y, t, q.y) : d.y * t;
+        a[0] = fmaf(ax, ri, a[0]);
+        a[1] = fmaf(ay, ri, a[1]);
+        float t3 = 3.0f * t;
+        float bx = (CHG ? fmaf(d.x, t3, q.x) : d.x * t3) * ri3, by = (CHG ? fmaf(d.y, t3, q.y) : d.y * t3) * ri3;
+        float dxr = d.x * ri3, dyr = d.y * ri3;
+        a[2] = fmaf(bx, dx, fmaf(-dxr, vx, a[2])); a[3] = fmaf(by, dx, fmaf(-dyr, vx, a[3]));
+        a[4] = fmaf(bx, dy, fmaf(-dxr, vy, a[4])); a[5] = fmaf(by, dy, fmaf(-dyr, vy, a[5]));
+        a[6] = fmaf(bx, dz, fmaf(-dxr, vz, a[6])); a[7] = fmaf(by, dz, fmaf(-dyr, vz, a[7]));
     }
 }
 
@@ -331,16 +339,16 @@ __global__ void __launch_bounds__(k32Threads, 3) k_m2l_dense32(const Tile *tiles
         const float2 *Tu = T + slot_toff[tile.slot0 + si];
         for (int k0 = 0; k0 < R; k0 += k32TK) {
             {
-                int r = threadIdx.x >> 2, c = (threadIdx.x & 3) * 4;
+                int r = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
                 int gr = row0 + r;
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     int gc = k0 + c + q;
-                    As[c + q][r] = (gr < R && gc < R) ? Tu[(size_t)gr * R + gc] : make_float2(0.f, 0.f);
+                    As[c + q][r] = (gr < R && gc < R) ? Tu[(size_t)gc * R + gr] : make_float2(0.f, 0.f);
                 }
             }
             {
-                int j = threadIdx.x >> 2, c = (threadIdx.x & 3) * 4;
+                int j = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
                 int sb = sv[j];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
