@@ -1264,3 +1264,6 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
     free(mpole); free(local);
     tree_free(&T);
 }
+
+/* The Helmholtz restatement shares the tree, lists and rotations above. */
+#include "hfmm3d_oracle.c"

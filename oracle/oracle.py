@@ -237,3 +237,142 @@ def translate(kind, c_from, c_to, coef, p, nt=None):
                            _p(np.ascontiguousarray(coef, np.complex128)), c_int(p),
                            c_int(p if nt is None else nt), _p(out))
     return out
+
+
+# ---------------------------------------------------------------- Helmholtz
+def h3dall(nterms, z, scale):
+    """Scaled spherical Hankel functions h_n(z) * scale^n and derivatives."""
+    h = _cdouble_arr(nterms + 2); hd = _cdouble_arr(nterms + 2)
+    lib().oracle_h3dall(c_int(nterms), c_dbl(z.real), c_dbl(complex(z).imag), c_dbl(scale), _p(h), _p(hd))
+    return h[:nterms + 1], hd[:nterms + 1]
+
+
+def jfuns3d(nterms, z, scale):
+    """Scaled spherical Bessel functions j_n(z) / scale^n and derivatives."""
+    f = _cdouble_arr(nterms + 2); fd = _cdouble_arr(nterms + 2)
+    L = lib()
+    L.oracle_jfuns3d.restype = c_int
+    ier = L.oracle_jfuns3d(c_int(nterms), c_dbl(z.real), c_dbl(complex(z).imag), c_dbl(scale), _p(f), _p(fd))
+    return ier, f[:nterms + 1], fd[:nterms + 1]
+
+
+def h3dterms(size, zk, eps):
+    L = lib()
+    L.oracle_h3dterms.restype = c_int
+    ier = c_int(0)
+    n = L.oracle_h3dterms(c_dbl(size), c_dbl(complex(zk).real), c_dbl(complex(zk).imag), c_dbl(eps),
+                          ctypes.byref(ier))
+    return n, ier.value
+
+
+def h3dterms_list2(size, zk, eps):
+    t = np.zeros(343, np.int32)
+    ier = c_int(0)
+    lib().oracle_h3dterms_list2(c_dbl(size), c_dbl(complex(zk).real), c_dbl(complex(zk).imag), c_dbl(eps), _p(t),
+                                ctypes.byref(ier))
+    return t.reshape(7, 7, 7)
+
+
+def legewhts(n):
+    x = np.zeros(n); w = np.zeros(n)
+    lib().oracle_legewhts(c_int(n), _p(x), _p(w))
+    return x, w
+
+
+def h3dpartdirect(zk, source, charge=None, dipstr=None, dipvec=None, target=None,
+                  ifpot=1, iffld=1, ifpottarg=1, iffldtarg=1):
+    src = _f64(source, (0, 3)); n = src.shape[0]
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    zk = complex(zk)
+    pot = np.zeros(max(n, 1), np.complex128); fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128); ft = np.zeros((max(m, 1), 3), np.complex128)
+    lib().oracle_h3dpartdirect(
+        c_dbl(zk.real), c_dbl(zk.imag), c_int(n), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+        c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))), c_int(ifpot),
+        _p(pot), c_int(iffld), _p(fld), c_int(m), _p(trg), c_int(ifpottarg if m else 0), _p(pt),
+        c_int(iffldtarg if m else 0), _p(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def hdirect_at(zk, source, pts, skip=None, charge=None, dipstr=None, dipvec=None):
+    """Helmholtz direct pot/fld at arbitrary points; skip[k] = excluded source."""
+    src = _f64(source, (0, 3)); n = src.shape[0]
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    zk = complex(zk)
+    sk = None if skip is None else np.ascontiguousarray(skip, dtype=np.int64)
+    pot = np.zeros(max(k, 1), np.complex128); fld = np.zeros((max(k, 1), 3), np.complex128)
+    lib().oracle_h3ddirect_points(
+        c_dbl(zk.real), c_dbl(zk.imag), c_int(n), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+        c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))), c_int(k), _p(pts),
+        _p(sk), _p(pot), _p(fld))
+    return pot[:k], fld[:k]
+
+
+def hfmm3dparttarg(iprec, zk, source, charge=None, dipstr=None, dipvec=None, target=None,
+                   ifpot=1, iffld=1, ifpottarg=1, iffldtarg=1, timing=False, nterms=False):
+    src = _f64(source, (0, 3)); n = src.shape[0]
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    zk = complex(zk)
+    pot = np.zeros(max(n, 1), np.complex128); fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128); ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = c_int(0)
+    tinfo = np.zeros(8)
+    nt = np.zeros(202, np.int32)
+    lib().oracle_hfmm3dparttarg(
+        ctypes.byref(ier), c_int(iprec), c_dbl(zk.real), c_dbl(zk.imag), c_int(n), _p(src),
+        c_int(int(charge is not None)), _p(_c128(charge, n)), c_int(int(dipstr is not None)), _p(_c128(dipstr, n)),
+        _p(_f64(dipvec, (max(n, 1), 3))), c_int(ifpot), _p(pot), c_int(iffld), _p(fld), c_int(m),
+        _p(trg if m else np.zeros((1, 3))), c_int(ifpottarg if m else 0), _p(pt), c_int(iffldtarg if m else 0),
+        _p(ft), _p(tinfo), _p(nt))
+    out = (ier.value, pot[:n], fld[:n], pt[:m], ft[:m])
+    if timing:
+        out = out + (tinfo,)
+    if nterms:
+        out = out + (nt,)
+    return out
+
+
+def hformmp(zk, rscale, src, c, p, charge=None, dipstr=None, dipvec=None):
+    src = _f64(src, (0, 3)); n = src.shape[0]; zk = complex(zk)
+    mp = _cdouble_arr((p + 1) ** 2)
+    lib().oracle_hformmp(c_dbl(zk.real), c_dbl(zk.imag), c_dbl(rscale), c_int(n), _p(src),
+                         c_int(int(charge is not None)), _p(_c128(charge, n)), c_int(int(dipstr is not None)),
+                         _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))), _p(_f64(c, (3,))), c_int(p), _p(mp))
+    return mp
+
+
+def hformta(zk, rscale, src, c, p, charge=None, dipstr=None, dipvec=None):
+    src = _f64(src, (0, 3)); n = src.shape[0]; zk = complex(zk)
+    lo = _cdouble_arr((p + 1) ** 2)
+    lib().oracle_hformta(c_dbl(zk.real), c_dbl(zk.imag), c_dbl(rscale), c_int(n), _p(src),
+                         c_int(int(charge is not None)), _p(_c128(charge, n)), c_int(int(dipstr is not None)),
+                         _p(_c128(dipstr, n)), _p(_f64(dipvec, (max(n, 1), 3))), _p(_f64(c, (3,))), c_int(p), _p(lo))
+    return lo
+
+
+def hmpeval(zk, rscale, c, mp, p, pts):
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]; zk = complex(zk)
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128)
+    lib().oracle_hmpeval(c_dbl(zk.real), c_dbl(zk.imag), c_dbl(rscale), _p(_f64(c, (3,))),
+                         _p(np.ascontiguousarray(mp, np.complex128)), c_int(p), c_int(k), _p(pts), _p(pot), _p(fld))
+    return pot, fld
+
+
+def htaeval(zk, rscale, c, lo, p, pts):
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]; zk = complex(zk)
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128)
+    lib().oracle_htaeval(c_dbl(zk.real), c_dbl(zk.imag), c_dbl(rscale), _p(_f64(c, (3,))),
+                         _p(np.ascontiguousarray(lo, np.complex128)), c_int(p), c_int(k), _p(pts), _p(pot), _p(fld))
+    return pot, fld
+
+
+def htranslate(kind, zk, c_from, c_to, coef, nin, sc1, nout, sc2, radius, nq):
+    """kind 0 = M2M, 1 = M2L, 2 = L2L by the reference's sphere projection."""
+    zk = complex(zk)
+    out = _cdouble_arr((max(nin, nout) + 1) ** 2)
+    lib().oracle_htranslate(c_int(kind), c_dbl(zk.real), c_dbl(zk.imag), _p(_f64(c_from, (3,))),
+                            _p(_f64(c_to, (3,))), _p(np.ascontiguousarray(coef, np.complex128)), c_int(nin),
+                            c_dbl(sc1), c_int(nout), c_dbl(sc2), c_dbl(radius), c_int(nq), _p(out))
+    return out[:(nout + 1) ** 2]
