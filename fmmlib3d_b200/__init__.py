@@ -1,9 +1,10 @@
 """fmmlib3d_b200 -- FMMLIB3D's particle FMM on one NVIDIA B200 (sm_100a).
 
 Python mirror of the reference calling sequences (the ``cf2py`` interfaces of
-src/lfmm3dpart.f:217-236): ``lfmm3dpartself``, ``lfmm3dparttarg``,
-``lfmm3dpart`` and ``l3dpartdirect`` return ``ier`` and the requested
-outputs.  Every call goes through the C ABI of ``libfmm3d_b200.so``
+src/lfmm3dpart.f:205-226 and src/hfmm3dpart.f:206-227): ``lfmm3dpartself``,
+``lfmm3dparttarg``, ``lfmm3dpart``, ``l3dpartdirect`` and the Helmholtz
+``hfmm3dpartself``, ``hfmm3dparttarg``, ``hfmm3dpart``, ``h3dpartdirect``
+(with ``zk`` after ``iprec``) return ``ier`` and the requested outputs.  Every call goes through the C ABI of ``libfmm3d_b200.so``
 (include/fmm3d_b200.h); there is no CPU path.  Importing this package on a
 machine without the built library raises immediately.
 
@@ -39,6 +40,16 @@ _lib.fmm3d_l3dpartdirect_device.restype = _I
 _lib.fmm3d_l3dpartdirect_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
 _lib.fmm3d_l3ddirect_points_device.restype = _I
 _lib.fmm3d_l3ddirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]
+for _name in ("hfmm3dpart_", "hfmm3dpartself_", "hfmm3dparttarg_", "h3dpartdirect_"):
+    getattr(_lib, _name).restype = None
+_lib.fmm3d_hfmm3dparttarg_device.restype = _I
+_lib.fmm3d_hfmm3dparttarg_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
+                                             _I, _P, _P]
+_lib.fmm3d_h3dpartdirect_device.restype = _I
+_lib.fmm3d_h3dpartdirect_device.argtypes = [_P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P,
+                                            _P]
+_lib.fmm3d_h3ddirect_points_device.restype = _I
+_lib.fmm3d_h3ddirect_points_device.argtypes = [_P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]
 _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
@@ -162,6 +173,93 @@ def direct_points_device(source, charge, dipstr, dipvec, pts, skip, pot, fld, st
         ptr(dipvec), pts.shape[0], ptr(pts), ptr(skip), ptr(pot), ptr(fld), _P(stream))
 
 
+def _zk(zk):
+    z = complex(zk)
+    return np.array([z.real, z.imag], np.float64)
+
+
+def hfmm3dparttarg(iprec, zk, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld,
+                   target=None, ifpottarg=0, iffldtarg=0):
+    """Helmholtz FMM over sources and targets; returns (ier, pot, fld, pottarg, fldtarg).
+
+    Same arguments and outputs as hfmm3dparttarg (src/hfmm3dpart.f:141-539):
+    the kernel is e^{i zk r}/r; unrequested outputs are returned as zeros.
+    """
+    src = _pts(source)
+    n = src.shape[0]
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _cplx(charge, n)
+    ds = _cplx(dipstr, n)
+    dv = _pts(dipvec) if (ifdipole == 1 and dipvec is not None) else np.zeros((max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = ctypes.c_int(0)
+    k = _zk(zk)
+    _lib.hfmm3dparttarg_(ctypes.byref(ier), _iref(iprec), _ptr(k), _iref(n), _ptr(src), _iref(ifcharge), _ptr(q),
+                         _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld),
+                         _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg),
+                         _ptr(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def hfmm3dpartself(iprec, zk, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld):
+    """Helmholtz FMM among sources; returns (ier, pot, fld) as hfmm3dpartself."""
+    ier, pot, fld, _, _ = hfmm3dparttarg(iprec, zk, source, ifcharge, charge, ifdipole, dipstr, dipvec,
+                                         ifpot, iffld)
+    return ier, pot, fld
+
+
+hfmm3dpart = hfmm3dpartself
+
+
+def h3dpartdirect(zk, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld,
+                  target=None, ifpottarg=0, iffldtarg=0):
+    """O(N^2) Helmholtz sum on the GPU; returns (pot, fld, pottarg, fldtarg) as h3dpartdirect."""
+    src = _pts(source)
+    n = src.shape[0]
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _cplx(charge, n)
+    ds = _cplx(dipstr, n)
+    dv = _pts(dipvec) if (ifdipole == 1 and dipvec is not None) else np.zeros((max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    k = _zk(zk)
+    _lib.h3dpartdirect_(_ptr(k), _iref(n), _ptr(src), _iref(ifcharge), _ptr(q), _iref(ifdipole), _ptr(ds), _ptr(dv),
+                        _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld), _iref(m), _ptr(trg if m else src),
+                        _iref(ifpottarg), _ptr(pt), _iref(iffldtarg), _ptr(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def hfmm3dparttarg_device(iprec, zk, source, charge, dipstr, dipvec, pot, fld, target=None, pottarg=None,
+                          fldtarg=None, stream=0):
+    """Helmholtz FMM on device-resident torch tensors (layouts as lfmm3dparttarg_device)."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = source.shape[0]
+    m = 0 if target is None else target.shape[0]
+    k = _zk(zk)
+    return _lib.fmm3d_hfmm3dparttarg_device(
+        iprec, _ptr(k), n, ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
+        ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m, ptr(target),
+        int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
+
+
+def hdirect_points_device(zk, source, charge, dipstr, dipvec, pts, skip, pot, fld, stream=0):
+    """Helmholtz direct sum at device points (as direct_points_device).  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    k = _zk(zk)
+    return _lib.fmm3d_h3ddirect_points_device(
+        _ptr(k), source.shape[0], ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None),
+        ptr(dipstr), ptr(dipvec), pts.shape[0], ptr(pts), ptr(skip), ptr(pot), ptr(fld), _P(stream))
+
+
 def last_launches():
     """Kernel launches issued by the last library call on this thread."""
     return _lib.fmm3d_last_launches()
@@ -194,13 +292,15 @@ def last_timing():
 
 
 def last_stats():
-    out = np.zeros(9 + 128, np.int64)
+    out = np.zeros(9 + 128 + 22, np.int64)
     k = _lib.fmm3d_last_stats(_ptr(out), out.size)
     if k == 0:
         return {}
     names = ["nboxes", "nlev", "nleaves", "nterms", "_l1", "_l3", "_l4", "p2p_pairs", "m2l_pairs"]
     d = {nm: int(out[i]) for i, nm in enumerate(names) if not nm.startswith("_")}
     d["m2l_pt_hist"] = {i: int(out[9 + i]) for i in range(128) if out[9 + i]}
+    if k > 9 + 128:  # Helmholtz: expansion order per level
+        d["nterms_level"] = [int(v) for v in out[9 + 128:k]]
     return d
 
 

@@ -1,0 +1,120 @@
+// Host-side plumbing shared by the Laplace and Helmholtz drivers: per-thread
+// call state (timing, statistics, last error), the per-thread stream, the
+// workspace pool policy, pass timers, the gather/scatter kernels between the
+// caller's AoS arrays and the tree-ordered SoA arrays, and the host-array
+// wrapper of the Fortran-named entry points.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "lap_kernels.cuh"
+#include "tree.cuh"
+
+namespace fmm {
+
+struct ThreadInfo {
+    bool timing = false;
+    bool want_stats = false;
+    std::vector<double> ms;
+    std::vector<long long> stats;
+    std::string err;
+    int launches = 0;
+};
+extern thread_local ThreadInfo g_ti;
+
+cudaStream_t thread_stream();
+void keep_pool_memory();
+
+struct Timer {
+    cudaStream_t s;
+    bool on;
+    std::vector<cudaEvent_t> ev;
+    Timer(cudaStream_t s_, bool on_) : s(s_), on(on_) {}
+    void mark()
+    {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        ev.push_back(e);
+    }
+    void finish(std::vector<double> &ms)
+    {
+        ms.clear();
+        if (!on || ev.size() < 2) return;
+        cudaEventSynchronize(ev.back());
+        for (size_t i = 1; i < ev.size(); i++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
+            ms.push_back(t);
+        }
+        float t = 0;
+        cudaEventElapsedTime(&t, ev.front(), ev.back());
+        ms.push_back(t);
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+    }
+};
+
+// tree order <-> caller order (l3dreorder / l3dpsort / l3dfsort, src/lfmm3drouts.f:583-708)
+__global__ void k_gather_src(int n, const int *perm, const double *src, const double *q, const double *dq,
+                             const double *dv, int ifc, int ifd, PointsSoA o);
+__global__ void k_gather_pts(int n, const int *perm, const double *p, double *x, double *y, double *z);
+__global__ void k_scatter_out(int n, const int *perm, OutSoA o, double *pot, double *fld);
+__global__ void k_split_aos(int n, const double *p, double *x, double *y, double *z);
+__global__ void k_split_c(int n, const double *c, double2 *o);
+
+inline TreeView make_treeview(const Tree &T)
+{
+    TreeView tv;
+    tv.level = T.level.p; tv.parent = T.parent.p; tv.octant = T.octant.p; tv.nchild = T.nchild.p;
+    tv.child = T.child.p; tv.coll = T.coll.p; tv.src0 = T.src0.p; tv.nsrc = T.nsrc.p; tv.trg0 = T.trg0.p;
+    tv.ntrg = T.ntrg.p; tv.center = T.center.p; tv.l1_start = T.l1_start.p; tv.l1_idx = T.l1_idx.p;
+    tv.l3_start = T.l3_start.p; tv.l3_idx = T.l3_idx.p; tv.l4_start = T.l4_start.p; tv.l4_idx = T.l4_idx.p;
+    tv.size = T.size;
+    return tv;
+}
+
+// ---------------------------------------------------------------- host-array entry points
+// Copies host inputs to the device, runs the device routine and copies the
+// requested outputs back; unrequested outputs are left untouched.
+template <typename F>
+inline int with_device_arrays(int ns, const double *source, int ifcharge, const double *charge, int ifdipole,
+                              const double *dipstr, const double *dipvec, int ifpot, double *pot, int iffld,
+                              double *fld, int nt, const double *target, int ifpottarg, double *pottarg,
+                              int iffldtarg, double *fldtarg, F run)
+{
+    cudaStream_t s = thread_stream();
+    Status st;
+    if (ns < 0) ns = 0;
+    if (nt < 0) nt = 0;
+    DBuf<double> dsrc, dq, ddq, ddv, dtrg, dpot, dfld, dpt, dft;
+    bool ok = dsrc.alloc(3L * std::max(ns, 1), s, st);
+    if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
+    if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st) && ddv.alloc(3L * ns, s, st);
+    if (nt) ok = ok && dtrg.alloc(3L * nt, s, st);
+    if (ifpot == 1) ok = ok && dpot.alloc(2L * ns, s, st);
+    if (iffld == 1) ok = ok && dfld.alloc(6L * ns, s, st);
+    if (nt && ifpottarg == 1) ok = ok && dpt.alloc(2L * nt, s, st);
+    if (nt && iffldtarg == 1) ok = ok && dft.alloc(6L * nt, s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    FMM_TRY(st, cudaMemcpyAsync(dsrc.p, source, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+    if (ifcharge == 1) FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
+    if (ifdipole == 1) {
+        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
+        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
+    }
+    if (nt) FMM_TRY(st, cudaMemcpyAsync(dtrg.p, target, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
+    if (ier) return ier;
+    if (ifpot == 1) FMM_TRY(st, cudaMemcpyAsync(pot, dpot.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
+    if (iffld == 1) FMM_TRY(st, cudaMemcpyAsync(fld, dfld.p, sizeof(double) * 6 * ns, cudaMemcpyDeviceToHost, s));
+    if (nt && ifpottarg == 1) FMM_TRY(st, cudaMemcpyAsync(pottarg, dpt.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));
+    if (nt && iffldtarg == 1) FMM_TRY(st, cudaMemcpyAsync(fldtarg, dft.p, sizeof(double) * 6 * nt, cudaMemcpyDeviceToHost, s));
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+}  // namespace fmm

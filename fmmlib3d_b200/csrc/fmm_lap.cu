@@ -19,6 +19,7 @@
 #include "lap_kernels.cuh"
 #include "m2l_dense.cuh"
 #include "tree.cuh"
+#include "driver_common.cuh"
 
 namespace fmm {
 
@@ -81,45 +82,6 @@ static void l3dterms_list2(double eps, int *itab)
 }
 
 // ---------------------------------------------------------------- per-thread state
-struct ThreadInfo {
-    bool timing = false;
-    bool want_stats = false;
-    std::vector<double> ms;
-    std::vector<long long> stats;
-    std::string err;
-    int launches = 0;
-};
-static thread_local ThreadInfo g_ti;
-
-static cudaStream_t thread_stream()
-{
-    static thread_local cudaStream_t s = nullptr;
-    static thread_local int sdev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!s || sdev != dev) {
-        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-        sdev = dev;
-    }
-    return s;
-}
-
-// Keep freed workspace in the device's default memory pool across calls
-// instead of returning it to the driver at every synchronisation.
-static void keep_pool_memory()
-{
-    static bool done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || done[dev]) return;
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = ~0ull;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-    done[dev] = true;
-}
-
 // ---------------------------------------------------------------- operator plan (per device, p, eps)
 // Rotation matrices for every direction class, the slot tables of the three
 // translation kinds and the sqrt-binomial table.  Built once on the device
@@ -293,62 +255,6 @@ static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Stat
 }
 
 // ---------------------------------------------------------------- small kernels
-__global__ void k_gather_src(int n, const int *perm, const double *src, const double *q, const double *dq,
-                             const double *dv, int ifc, int ifd, PointsSoA o)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    long j = perm[i];
-    o.x[i] = src[3 * j];
-    o.y[i] = src[3 * j + 1];
-    o.z[i] = src[3 * j + 2];
-    if (ifc) o.q[i] = make_double2(q[2 * j], q[2 * j + 1]);
-    if (ifd) {
-        o.dq[i] = make_double2(dq[2 * j], dq[2 * j + 1]);
-        o.vx[i] = dv[3 * j];
-        o.vy[i] = dv[3 * j + 1];
-        o.vz[i] = dv[3 * j + 2];
-    }
-}
-
-__global__ void k_gather_pts(int n, const int *perm, const double *p, double *x, double *y, double *z)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    long j = perm[i];
-    x[i] = p[3 * j];
-    y[i] = p[3 * j + 1];
-    z[i] = p[3 * j + 2];
-}
-
-// unsort: l3dpsort / l3dfsort (src/lfmm3drouts.f:583-615)
-__global__ void k_scatter_out(int n, const int *perm, OutSoA o, double *pot, double *fld)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    long j = perm ? perm[i] : i;
-    if (pot) { pot[2 * j] = o.pot[i].x; pot[2 * j + 1] = o.pot[i].y; }
-    if (fld) {
-        double2 a = o.fx[i], b = o.fy[i], c = o.fz[i];
-        fld[6 * j] = a.x; fld[6 * j + 1] = a.y;
-        fld[6 * j + 2] = b.x; fld[6 * j + 3] = b.y;
-        fld[6 * j + 4] = c.x; fld[6 * j + 5] = c.y;
-    }
-}
-
-__global__ void k_split_aos(int n, const double *p, double *x, double *y, double *z)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    x[i] = p[3L * i]; y[i] = p[3L * i + 1]; z[i] = p[3L * i + 2];
-}
-
-__global__ void k_split_c(int n, const double *c, double2 *o)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) o[i] = make_double2(c[2L * i], c[2L * i + 1]);
-}
-
 // statistics: near-field pairs and far-field pairs
 __global__ void k_stats(int nleaves, const int *leaves, TreeView tv, int do_src, int do_trg,
                         unsigned long long *acc)
@@ -388,37 +294,6 @@ __global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int 
 }
 
 // ---------------------------------------------------------------- the FMM
-struct Timer {
-    cudaStream_t s;
-    bool on;
-    std::vector<cudaEvent_t> ev;
-    Timer(cudaStream_t s_, bool on_) : s(s_), on(on_) {}
-    void mark()
-    {
-        if (!on) return;
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        cudaEventRecord(e, s);
-        ev.push_back(e);
-    }
-    void finish(std::vector<double> &ms)
-    {
-        ms.clear();
-        if (!on || ev.size() < 2) return;
-        cudaEventSynchronize(ev.back());
-        for (size_t i = 1; i < ev.size(); i++) {
-            float t = 0;
-            cudaEventElapsedTime(&t, ev[i - 1], ev[i]);
-            ms.push_back(t);
-        }
-        float t = 0;
-        cudaEventElapsedTime(&t, ev.front(), ev.back());
-        ms.push_back(t);
-        for (auto e : ev) cudaEventDestroy(e);
-        ev.clear();
-    }
-};
-
 static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
                           const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
                           double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
@@ -472,12 +347,7 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     tm.mark();
-    TreeView tv;
-    tv.level = T.level.p; tv.parent = T.parent.p; tv.octant = T.octant.p; tv.nchild = T.nchild.p;
-    tv.child = T.child.p; tv.coll = T.coll.p; tv.src0 = T.src0.p; tv.nsrc = T.nsrc.p; tv.trg0 = T.trg0.p;
-    tv.ntrg = T.ntrg.p; tv.center = T.center.p; tv.l1_start = T.l1_start.p; tv.l1_idx = T.l1_idx.p;
-    tv.l3_start = T.l3_start.p; tv.l3_idx = T.l3_idx.p; tv.l4_start = T.l4_start.p; tv.l4_idx = T.l4_idx.p;
-    tv.size = T.size;
+    TreeView tv = make_treeview(T);
     int prune = !(ifpot == 1 || iffld == 1);
 
     // tiles per (level, octant) group
@@ -637,48 +507,6 @@ static int lap_direct_device(int ns, const double *d_src, int ifcharge, const do
                                                       iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
     }
     FMM_LAUNCH_CHECK(st);
-    FMM_TRY(st, cudaStreamSynchronize(s));
-    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
-    return 0;
-}
-
-// ---------------------------------------------------------------- host-array entry points
-// Copies host inputs to the device, runs the device routine and copies the
-// requested outputs back; unrequested outputs are left untouched.
-template <typename F>
-static int with_device_arrays(int ns, const double *source, int ifcharge, const double *charge, int ifdipole,
-                              const double *dipstr, const double *dipvec, int ifpot, double *pot, int iffld,
-                              double *fld, int nt, const double *target, int ifpottarg, double *pottarg,
-                              int iffldtarg, double *fldtarg, F run)
-{
-    cudaStream_t s = thread_stream();
-    Status st;
-    if (ns < 0) ns = 0;
-    if (nt < 0) nt = 0;
-    DBuf<double> dsrc, dq, ddq, ddv, dtrg, dpot, dfld, dpt, dft;
-    bool ok = dsrc.alloc(3L * std::max(ns, 1), s, st);
-    if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
-    if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st) && ddv.alloc(3L * ns, s, st);
-    if (nt) ok = ok && dtrg.alloc(3L * nt, s, st);
-    if (ifpot == 1) ok = ok && dpot.alloc(2L * ns, s, st);
-    if (iffld == 1) ok = ok && dfld.alloc(6L * ns, s, st);
-    if (nt && ifpottarg == 1) ok = ok && dpt.alloc(2L * nt, s, st);
-    if (nt && iffldtarg == 1) ok = ok && dft.alloc(6L * nt, s, st);
-    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    FMM_TRY(st, cudaMemcpyAsync(dsrc.p, source, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
-    if (ifcharge == 1) FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
-    if (ifdipole == 1) {
-        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
-        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
-    }
-    if (nt) FMM_TRY(st, cudaMemcpyAsync(dtrg.p, target, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
-    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
-    if (ier) return ier;
-    if (ifpot == 1) FMM_TRY(st, cudaMemcpyAsync(pot, dpot.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
-    if (iffld == 1) FMM_TRY(st, cudaMemcpyAsync(fld, dfld.p, sizeof(double) * 6 * ns, cudaMemcpyDeviceToHost, s));
-    if (nt && ifpottarg == 1) FMM_TRY(st, cudaMemcpyAsync(pottarg, dpt.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));
-    if (nt && iffldtarg == 1) FMM_TRY(st, cudaMemcpyAsync(fldtarg, dft.p, sizeof(double) * 6 * nt, cudaMemcpyDeviceToHost, s));
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     return 0;

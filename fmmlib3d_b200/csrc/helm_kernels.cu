@@ -1,0 +1,1124 @@
+// Helmholtz FMM kernels (FP64): special functions, P2M/P2L, L2P/M2P,
+// z-shift operators, rotate-shift-rotate translations, P2P and the direct sum.
+#include "helm_kernels.cuh"
+
+namespace fmm {
+
+// ================================================================ complex helpers
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b)
+{
+    // Smith's algorithm
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    }
+    double r = b.x / b.y, d = b.x * r + b.y;
+    return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double cabsd(double2 a) { return hypot(a.x, a.y); }
+// e^{i z}
+__device__ __forceinline__ double2 cexpi(double2 z)
+{
+    double s, c;
+    sincos(z.x, &s, &c);
+    double e = exp(-z.y);
+    return make_double2(e * c, e * s);
+}
+
+// ================================================================ special functions
+// Scaled spherical Hankel functions h_n(z) scale^n, n = 0..nt, and (if hd)
+// their derivatives: h3dall (src/helmrouts3d.f:709-809).  Needs nt >= 1.
+__device__ void hank_dev(int nt, double2 z, double scale, double2 *h, double2 *hd)
+{
+    if (cabsd(z) < 1.0e-15) {
+        for (int i = 0; i <= nt; i++) { h[i] = cmk(0, 0); if (hd) hd[i] = cmk(0, 0); }
+        return;
+    }
+    // h0 = e^{iz} / (iz), h1 = h0 (1/z - i)   (h3d01, :666-704)
+    double2 iz = cmk(-z.y, z.x);
+    double2 h0 = cdiv(cexpi(z), iz);
+    double2 zi = cdiv(cmk(1, 0), z);
+    double2 h1 = cmul(h0, cmk(zi.x, zi.y - 1.0));
+    h[0] = h0;
+    h[1] = cscal(scale, h1);
+    double s2 = scale * scale;
+    double2 zs = cscal(scale, zi);
+    for (int i = 1; i <= nt - 1; i++) {
+        double2 t = cscal(2 * i + 1.0, zs);
+        h[i + 1] = csub(cmul(t, h[i]), cscal(s2, h[i - 1]));
+    }
+    if (hd) {
+        hd[0] = cscal(-1.0 / scale, h[1]);
+        for (int i = 1; i <= nt; i++) hd[i] = csub(cscal(scale, h[i - 1]), cmul(cscal(i + 1.0, zi), h[i]));
+    }
+}
+
+// Scaled spherical Bessel functions j_n(z) / scale^n, n = 0..nt+1, by the
+// backward recurrence of jfuns3d (src/cdjseval3d.f:15-197): the upward
+// sweep from n = nt finds the start ntop (first |f|^2 > 1e40, at most
+// nt + 1000 terms), the downward sweep rescales by 1e-40 when it grows past
+// that bound, and the values are normalized against sin z / z or its
+// successor.  Only entries 0..nt+1 are stored.  fd (optional) receives the
+// derivatives of entries 0..nt.  Returns 8 if the upward sweep never grew.
+__device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd)
+{
+    const double ub = 1.0e40, ubinv = 1.0e-40;
+    if (cabsd(z) < 1.0e-200) {
+        f[0] = cmk(1, 0);
+        for (int i = 1; i <= nt + 1; i++) f[i] = cmk(0, 0);
+        if (fd) {
+            for (int i = 0; i <= nt; i++) fd[i] = cmk(0, 0);
+            if (nt >= 1) fd[1] = cmk(1.0 / (3 * scale), 0);
+        }
+        return 0;
+    }
+    double2 zi = cdiv(cmk(1, 0), z);
+    int ntop = 0;
+    {
+        double2 fm = cmk(0, 0), fc = cmk(1, 0);
+        for (int i = nt; i <= nt + 1000; i++) {
+            double2 fn = csub(cmul(cscal(2 * i + 1.0, zi), fc), fm);
+            if (cabs2(fn) > ub) { ntop = i + 1; break; }
+            fm = fc;
+            fc = fn;
+        }
+    }
+    if (ntop == 0) return 8;
+    unsigned long long fl[2] = {0ull, 0ull};  // rescale events at index i <= 127
+    if (ntop <= nt + 1) f[ntop] = cmk(0, 0);
+    double2 a = cmk(0, 0), b = cmk(1, 0);    // f(i+1), f(i)
+    for (int i = ntop - 1; i >= 1; i--) {
+        double2 c = csub(cmul(cscal(2 * i + 1.0, zi), b), a);
+        if (cabs2(c) > ub) {
+            b = cscal(ubinv, b);
+            c = cscal(ubinv, c);
+            if (i < 128) fl[i >> 6] |= 1ull << (i & 63);
+        }
+        if (i <= nt + 1) f[i] = b;
+        a = b;
+        b = c;
+    }
+    f[0] = b;
+    double sinv = 1.0 / scale, sct = 1.0;
+    for (int i = 1; i <= nt + 1; i++) {
+        sct *= sinv;
+        int k = i - 1;
+        if ((fl[k >> 6] >> (k & 63)) & 1ull) sct *= ubinv;
+        f[i] = cscal(sct, f[i]);
+    }
+    // sin z / z and (sin z / z - cos z) / z
+    double sx, cx;
+    sincos(z.x, &sx, &cx);
+    double ch = cosh(z.y), sh = sinh(z.y);
+    double2 sz = cmk(sx * ch, cx * sh), cz = cmk(cx * ch, -sx * sh);
+    double2 j0 = cmul(sz, zi);
+    double2 j1 = csub(cmul(j0, zi), cmul(cz, zi));
+    double2 zs = cabsd(j1) > cabsd(j0) ? cdiv(j1, cscal(scale, f[1])) : cdiv(j0, f[0]);
+    for (int i = 0; i <= nt + 1; i++) f[i] = cmul(f[i], zs);
+    if (fd) {
+        fd[0] = cscal(-scale, f[1]);
+        for (int i = 1; i <= nt; i++) {
+            double d1 = i / (2 * i + 1.0), d2 = 1.0 - d1;
+            fd[i] = csub(cscal(d1 * sinv, f[i - 1]), cscal(d2 * scale, f[i + 1]));
+        }
+    }
+    return 0;
+}
+
+// Column m of the Legendre functions with the sqrt(2n+1) factor at x, for
+// n = m..nmax, in the scaled form of ylgndr2s (src/yrecursion.f:298-385):
+// y[n] = Y_n^m / sin(theta) and d[n] = -dY_n^m/dtheta for m >= 1, and
+// y[n] = Y_n^0, d[n] = dY_n^0/dx for m = 0.  Arrays are indexed by n - m.
+// `regular` multiplies y by sin(theta) (giving Y_n^m) and turns d into
+// dY/dtheta for every m.  d may be null.
+__device__ void legendre_col(int m, int nmax, double x, double *y, double *d, bool regular)
+{
+    double u2 = (1 - x) * (1 + x), st = sqrt(u2), u = -st;
+    double ym, dm;
+    if (m == 0) { ym = 1; dm = 0; }
+    else {
+        ym = -sqrt(0.5);
+        for (int k = 2; k <= m; k++) ym *= u * sqrt((2 * k - 1.0) / (2 * k));
+        dm = ym * (-m) * x;
+    }
+    const double w = m == 0 ? 1.0 : u2;
+    double y1 = 0, d1 = 0, y2 = 0, d2 = 0;  // values at n-1 and n-2
+    for (int n = m; n <= nmax; n++) {
+        double yn, dn;
+        if (n == m) { yn = ym; dn = dm; }
+        else if (n == m + 1) {
+            yn = x * y1 * sqrt(2 * m + 1.0);
+            dn = (x * d1 + w * y1) * sqrt(2 * m + 1.0);
+        } else {
+            double a = sqrt((n + m - 1.0) * (n - m - 1.0)), b = sqrt((n - m + 0.0) * (n + m));
+            yn = ((2 * n - 1) * x * y1 - a * y2) / b;
+            dn = ((2 * n - 1) * (x * d1 + w * y1) - a * d2) / b;
+        }
+        y[n - m] = yn;
+        if (d) d[n - m] = dn;
+        y2 = y1; d2 = d1;
+        y1 = yn; d1 = dn;
+    }
+    for (int n = m; n <= nmax; n++) {
+        double s = sqrt(2 * n + 1.0);
+        y[n - m] *= s;
+        if (regular && m > 0) y[n - m] *= st;
+        if (d) {
+            d[n - m] *= s;
+            if (regular) d[n - m] = m == 0 ? -st * d[n - m] : -d[n - m];
+        }
+    }
+}
+
+// ================================================================ z-shift operators
+// For one block (kind, degrees nin -> nout, shift zshift along z, sphere
+// radius, quadrature x_j, w_j of nq Gauss-Legendre nodes) the reference
+// evaluates the rotated source expansion at the nodes of the target sphere
+// (h3dmpevalspherenm_fast / h3dmpevalspherenmstab_fast /
+// h3dlocevalspherestab_fast, src/projections.f:1611, 1917, 901), projects
+// on Y_l^m (h3dprojlocnmsep_fast / h3dprojlocsepstab_fast, :1277, 2292) and
+// rescales (h3drescalemp / h3drescalestab, :556, 679).  The composition is
+// linear and diagonal in m, depends on |m| only, and is built here entry by
+// entry:
+//   A[l][n] = sum_j w_j/2 Y_l^m(x_j) f_n(k r_j) Y_n^m(cos t_j)
+//   B[l][n] = sum_j w_j/2 Y_l^m(x_j) (k f'_n(k r_j) rn_j Y_n^m + f_n thn_j dY_n^m/dtheta)
+// with f = h (M2M, M2L) or j (L2L) scaled by sc1, and
+//   M2M:   Z = A / h_l(k R)                 (scaled by sc2)
+//   stab:  Z = (j_l A + k j'_l B) / (j_l^2 + (k j'_l)^2)   at k R, scaled by sc2.
+__device__ __forceinline__ void hz_node(const HZBlock &B, const double *xw, int j, double &ctj, double &stj,
+                                        double &rn, double &thn, double &rj)
+{
+    double ct = xw[2 * (B.qoff + j)], st = sqrt(1.0 - ct * ct);
+    double a = B.zshift + B.radius * ct, c = B.radius * st;
+    rj = sqrt(a * a + c * c);
+    ctj = a / rj;
+    stj = sqrt(1.0 - ctj * ctj);
+    rn = stj * st + ctj * ct;
+    thn = (ctj * st - ct * stj) / rj;
+}
+
+__global__ void k_hz_radial(const HZBlock *blk, const double *xw, double2 zk, int pmax, double2 *rad)
+{
+    const HZBlock B = blk[blockIdx.x];
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j > B.nq) return;
+    const int W = pmax + 2;
+    double2 *R = rad + B.roff + (size_t)j * 2 * W, *Rd = R + W;
+    if (j < B.nq) {
+        double ctj, stj, rn, thn, rj;
+        hz_node(B, xw, j, ctj, stj, rn, thn, rj);
+        double2 z = cscal(rj, zk);
+        int nt = B.nin > 1 ? B.nin : 1;
+        if (B.kind == 2) {
+            if (bess_dev(nt, z, B.sc1, R, Rd))
+                for (int i = 0; i <= nt + 1; i++) { R[i] = cmk(0, 0); Rd[i] = cmk(0, 0); }
+        } else {
+            hank_dev(nt, z, B.sc1, R, B.kind == 1 ? Rd : nullptr);
+        }
+        if (B.kind != 0)
+            for (int i = 0; i <= nt; i++) Rd[i] = cmul(Rd[i], zk);
+    } else {
+        double2 z = cscal(B.radius, zk);
+        int nt = B.nout > 1 ? B.nout : 1;
+        if (B.kind == 0) hank_dev(nt, z, B.sc2, R, nullptr);
+        else {
+            if (bess_dev(nt, z, B.sc2, R, Rd))
+                for (int i = 0; i <= nt + 1; i++) { R[i] = cmk(0, 0); Rd[i] = cmk(0, 0); }
+            for (int i = 0; i <= nt; i++) Rd[i] = cmul(Rd[i], zk);
+        }
+    }
+}
+
+constexpr int kHzThreads = 256, kHzNodes = 32, kHzPer = 4;
+
+__global__ void __launch_bounds__(kHzThreads) k_hz_build(const HZBlock *blk, const double *xw, int pmax,
+                                                         const double2 *rad, double2 *Z)
+{
+    extern __shared__ double hzs[];
+    const HZBlock B = blk[blockIdx.x];
+    const int m = blockIdx.y;
+    const int mmax = B.nin < B.nout ? B.nin : B.nout;
+    if (m > mmax) return;
+    const int W = pmax + 2, LD = pmax + 1;
+    double *Yt = hzs;                          // [node][l - m]
+    double *Ys = Yt + kHzNodes * LD;           // [node][n - m]
+    double *dYs = Ys + kHzNodes * LD;
+    double *gw = dYs + kHzNodes * LD;          // w/2, rn, thn per node
+    const int nr = B.nout + 1 - m, ncol = B.nin + 1 - m, ne = nr * ncol;
+    long long mo = 0;
+    for (int k = 0; k < m; k++) mo += (long long)(B.nout + 1 - k) * (B.nin + 1 - k);
+    double2 *Zm = Z + B.zoff + mo;
+    const double2 *Rt = rad + B.roff + (size_t)B.nq * 2 * W, *Rtd = Rt + W;
+    for (int e0 = 0; e0 < ne; e0 += kHzThreads * kHzPer) {
+        double2 A[kHzPer], Bv[kHzPer];
+#pragma unroll
+        for (int q = 0; q < kHzPer; q++) { A[q] = cmk(0, 0); Bv[q] = cmk(0, 0); }
+        for (int j0 = 0; j0 < B.nq; j0 += kHzNodes) {
+            const int nj = min(kHzNodes, B.nq - j0);
+            __syncthreads();
+            if (threadIdx.x < nj) {
+                int j = j0 + threadIdx.x;
+                double ctj, stj, rn, thn, rj;
+                hz_node(B, xw, j, ctj, stj, rn, thn, rj);
+                legendre_col(m, B.nin, ctj, Ys + threadIdx.x * LD, B.kind == 0 ? nullptr : dYs + threadIdx.x * LD,
+                             true);
+                gw[3 * threadIdx.x] = 0.5 * xw[2 * (B.qoff + j) + 1];
+                gw[3 * threadIdx.x + 1] = rn;
+                gw[3 * threadIdx.x + 2] = thn;
+            } else if (threadIdx.x >= 32 && threadIdx.x < 32 + nj) {
+                int t = threadIdx.x - 32;
+                legendre_col(m, B.nout, xw[2 * (B.qoff + j0 + t)], Yt + t * LD, nullptr, true);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < kHzPer; q++) {
+                int e = e0 + q * kHzThreads + threadIdx.x;
+                if (e >= ne) continue;
+                int li = e / ncol, ni = e % ncol, n = ni + m;
+                for (int jj = 0; jj < nj; jj++) {
+                    const double2 *R = rad + B.roff + (size_t)(j0 + jj) * 2 * W;
+                    double wt = gw[3 * jj] * Yt[jj * LD + li];
+                    double ys = Ys[jj * LD + ni];
+                    crfma(A[q], wt * ys, R[n]);
+                    if (B.kind != 0) {
+                        crfma(Bv[q], wt * ys * gw[3 * jj + 1], R[W + n]);
+                        crfma(Bv[q], wt * dYs[jj * LD + ni] * gw[3 * jj + 2], R[n]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kHzPer; q++) {
+            int e = e0 + q * kHzThreads + threadIdx.x;
+            if (e >= ne) continue;
+            int l = e / ncol + m;
+            double2 v;
+            if (B.kind == 0) v = cdiv(A[q], Rt[l]);
+            else {
+                double2 zh = Rt[l], zhn = Rtd[l];
+                double2 zm = cadd(cmul(zh, zh), cmul(zhn, zhn));
+                v = cdiv(cadd(cmul(zh, A[q]), cmul(zhn, Bv[q])), zm);
+            }
+            Zm[e] = v;
+        }
+    }
+}
+
+void build_hz(int nblk, const HZBlock *d_blk, const HZBlock *h_blk, const double *d_xw, double2 zk, int pmax,
+              double2 *rad, double2 *Z, cudaStream_t s, Status &st)
+{
+    if (!st.ok() || nblk == 0) return;
+    int maxq = 0;
+    for (int b = 0; b < nblk; b++) maxq = std::max(maxq, h_blk[b].nq + 1);
+    dim3 g1(nblk, div_up(maxq, 64));
+    k_hz_radial<<<g1, 64, 0, s>>>(d_blk, d_xw, zk, pmax, rad); FMM_COUNT_LAUNCH();
+    size_t sm = sizeof(double) * (3 * kHzNodes * (pmax + 1) + 3 * kHzNodes);
+    FMM_TRY(st, cudaFuncSetAttribute(k_hz_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 g2(nblk, pmax + 1);
+    k_hz_build<<<g2, kHzThreads, sm, s>>>(d_blk, d_xw, pmax, rad, Z); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// ================================================================ translations
+// h3dmpmpquad0 (M2M), h3dmplocquad_trunc0 (M2L) and h3dloclocquad0 (L2L)
+// (src/h3dtrans.f:211, 1229, 1998), batched as the Laplace translations: a
+// CTA owns up to KT targets of one (level, octant) group; per source slot it
+// gathers the sources, applies e^{i m phi}, the rotation D(theta), the
+// z-shift operator of the slot (per |m| dense block), D(theta)^T and
+// e^{-i m phi}, and accumulates in shared memory.
+constexpr int kHTransThreads = 256;
+
+__device__ __forceinline__ int hsrc_of(int kind, const TreeView &tv, int t, const HSlot &sl)
+{
+    if (kind == 0) return tv.child[8L * t + sl.oct];
+    if (kind == 2) return tv.parent[t];
+    int P = tv.parent[t];
+    if (P < 0) return -1;
+    int C = tv.coll[27L * P + sl.coll];
+    if (C < 0) return -1;
+    return tv.child[8L * C + sl.oct];
+}
+
+__device__ __forceinline__ int deg_of(int e)
+{
+    int n = (int)sqrtf((float)e);
+    while (n * n > e) n--;
+    while ((n + 1) * (n + 1) <= e) n++;
+    return n;
+}
+
+template <int KIND, int KT>
+__global__ void __launch_bounds__(kHTransThreads) k_htranslate(const Tile *tiles, const int *grouped,
+                                                               const HSlot *slots, TreeView tv, int pmax,
+                                                               const double *rot, const double2 *Z,
+                                                               const double2 *in, double2 *out, int prune)
+{
+    extern __shared__ double2 sm[];
+    const int NC = (pmax + 1) * (pmax + 1);
+    double2 *acc = sm;
+    double2 *bA = acc + (size_t)KT * NC;
+    double2 *bB = bA + (size_t)KT * NC;
+    double2 *eph = bB + (size_t)KT * NC;  // e^{i m phi}, m = 0..pmax
+    __shared__ int tg[8], sv[8];
+    __shared__ int anyv;
+    const Tile tile = tiles[blockIdx.x];
+    if (threadIdx.x < 8) {
+        int t = threadIdx.x < tile.count ? grouped[tile.first + threadIdx.x] : -1;
+        if (t >= 0 && KIND == 0 && tv.nchild[t] == 0) t = -1;
+        if (t >= 0 && KIND == 0 && tv.nsrc[t] == 0) t = -1;  // sourceless boxes keep a zero multipole
+        tg[threadIdx.x] = t;
+    }
+    for (int i = threadIdx.x; i < KT * NC; i += kHTransThreads) acc[i] = cmk(0, 0);
+    const size_t csz = rot_class_size(pmax);
+    for (int si = 0; si < tile.nslot; si++) {
+        const HSlot sl = slots[tile.slot0 + si];
+        __syncthreads();
+        if (threadIdx.x == 0) anyv = 0;
+        __syncthreads();
+        if (threadIdx.x < KT) {
+            int t = tg[threadIdx.x];
+            int sb = -1;
+            if (t >= 0) {
+                sb = hsrc_of(KIND, tv, t, sl);
+                if (sb >= 0 && KIND != 2 && tv.nsrc[sb] == 0) sb = -1;
+                if (KIND == 1 && prune && tv.ntrg[t] == 0) sb = -1;
+            }
+            sv[threadIdx.x] = sb;
+            if (sb >= 0) atomicOr(&anyv, 1);
+        }
+        if (threadIdx.x == 32) {
+            double2 e1 = cmk(sl.ex, sl.ey), e = cmk(1, 0);
+            for (int m = 0; m <= pmax; m++) { eph[m] = e; e = cmul(e, e1); }
+        }
+        __syncthreads();
+        if (!anyv) continue;
+        const int nin = sl.nin, nout = sl.nout, mmax = sl.mmax;
+        const int Rin = (nin + 1) * (nin + 1), Rout = (nout + 1) * (nout + 1);
+        // phase 1: gather, times e^{i m phi}
+        for (int i = threadIdx.x; i < KT * Rin; i += kHTransThreads) {
+            int k = i / Rin, e = i % Rin;
+            int sb = sv[k];
+            double2 v = cmk(0, 0);
+            if (sb >= 0) {
+                int n = deg_of(e), m = e - n * n - n;
+                double2 ph = m >= 0 ? eph[m] : cconj(eph[-m]);
+                v = cmul(in[(size_t)sb * NC + e], ph);
+            }
+            bA[(size_t)k * NC + e] = v;
+        }
+        __syncthreads();
+        const double *R = rot + csz * sl.cls;
+        // phase 2: bB[n][m'] = sum_m bA[n][m] D^n[m][m']
+        for (int row = threadIdx.x; row < Rin; row += kHTransThreads) {
+            int n = deg_of(row), mp = row - n * n - n;
+            const double *Dn = R + (size_t)n * (4 * n * n - 1) / 3;
+            int w = 2 * n + 1;
+            double2 a[KT];
+            _Pragma("unroll") for (int k = 0; k < KT; k++) a[k] = cmk(0, 0);
+            for (int m = -n; m <= n; m++) {
+                double d = Dn[(m + n) * w + (mp + n)];
+                _Pragma("unroll") for (int k = 0; k < KT; k++) crfma(a[k], d, bA[(size_t)k * NC + eidx(n, m)]);
+            }
+            _Pragma("unroll") for (int k = 0; k < KT; k++) bB[(size_t)k * NC + row] = a[k];
+        }
+        __syncthreads();
+        // phase 3: z-shift, bA[l][m] = sum_n Z_|m|[l][n] bB[n][m]
+        const double2 *Zb = Z + sl.zoff;
+        for (int row = threadIdx.x; row < Rout; row += kHTransThreads) {
+            int l = deg_of(row), m = row - l * l - l, am = m < 0 ? -m : m;
+            double2 a[KT];
+            _Pragma("unroll") for (int k = 0; k < KT; k++) a[k] = cmk(0, 0);
+            if (am <= mmax) {
+                long long mo = 0;
+                for (int q = 0; q < am; q++) mo += (long long)(nout + 1 - q) * (nin + 1 - q);
+                const double2 *zr = Zb + mo + (long long)(l - am) * (nin + 1 - am) - am;
+                for (int n = am; n <= nin; n++) {
+                    double2 z = zr[n];
+                    _Pragma("unroll") for (int k = 0; k < KT; k++) cfma(a[k], z, bB[(size_t)k * NC + eidx(n, m)]);
+                }
+            }
+            _Pragma("unroll") for (int k = 0; k < KT; k++) bA[(size_t)k * NC + row] = a[k];
+        }
+        __syncthreads();
+        // phase 4: back rotation, times e^{-i m phi}, accumulate
+        for (int row = threadIdx.x; row < Rout; row += kHTransThreads) {
+            int n = deg_of(row), m = row - n * n - n;
+            const double *Dn = R + (size_t)n * (4 * n * n - 1) / 3 + (size_t)(m + n) * (2 * n + 1);
+            double2 a[KT];
+            _Pragma("unroll") for (int k = 0; k < KT; k++) a[k] = cmk(0, 0);
+            for (int mp = -n; mp <= n; mp++) {
+                double d = Dn[mp + n];
+                _Pragma("unroll") for (int k = 0; k < KT; k++) crfma(a[k], d, bA[(size_t)k * NC + eidx(n, mp)]);
+            }
+            double2 ph = m >= 0 ? cconj(eph[m]) : eph[-m];
+            _Pragma("unroll") for (int k = 0; k < KT; k++)
+                if (sv[k] >= 0) acc[(size_t)k * NC + row] = cadd(acc[(size_t)k * NC + row], cmul(a[k], ph));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < KT * NC; i += kHTransThreads) {
+        int k = i / NC, e = i % NC;
+        int t = tg[k];
+        if (t < 0) continue;
+        double2 *o = out + (size_t)t * NC + e;
+        if (KIND == 0) *o = acc[i];
+        else *o = cadd(*o, acc[i]);
+    }
+}
+
+template <int KIND>
+static void launch_htranslate_kind(const Tile *tiles, int ntiles, const int *grouped, const HSlot *slots,
+                                   const TreeView &tv, int pmax, const double *rot, const double2 *Z,
+                                   const double2 *in, double2 *out, int prune, int kt, size_t sm, cudaStream_t s,
+                                   Status &st)
+{
+#define FMM_HTR(KTV)                                                                                           \
+    do {                                                                                                       \
+        FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)sm));                                                            \
+        k_htranslate<KIND, KTV><<<ntiles, kHTransThreads, sm, s>>>(tiles, grouped, slots, tv, pmax, rot, Z, in, \
+                                                                   out, prune);                                \
+        FMM_COUNT_LAUNCH();                                                                                    \
+    } while (0)
+    if (kt == 8) FMM_HTR(8);
+    else if (kt == 4) FMM_HTR(4);
+    else if (kt == 2) FMM_HTR(2);
+    else FMM_HTR(1);
+#undef FMM_HTR
+}
+
+void launch_htranslate(int kind, const Tile *tiles, int ntiles, const int *grouped, const HSlot *slots,
+                       const TreeView &tv, int pmax, const double *rot, const double2 *Z, const double2 *in,
+                       double2 *out, int prune, int kt, cudaStream_t s, Status &st)
+{
+    if (ntiles == 0 || !st.ok()) return;
+    int NC = (pmax + 1) * (pmax + 1);
+    size_t sm = (size_t)3 * kt * NC * sizeof(double2) + (pmax + 1) * sizeof(double2);
+    if (kind == 0) launch_htranslate_kind<0>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
+    else if (kind == 1) launch_htranslate_kind<1>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
+    else launch_htranslate_kind<2>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
+    FMM_LAUNCH_CHECK(st);
+}
+
+// ================================================================ point operators
+// Legendre recurrence coefficients for the column recurrences in registers:
+// g_ha[n][m] = sqrt((n+m-1)(n-m-1)), g_hb[n][m] = 1/sqrt((n-m)(n+m)),
+// g_hs[n] = sqrt(2n+1).
+constexpr int kHTab = kHelmMaxP + 3;
+__device__ double g_ha[kHTab * kHTab], g_hb[kHTab * kHTab], g_hs[kHTab];
+
+__global__ void k_htab_init()
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kHTab) g_hs[i] = sqrt(2 * i + 1.0);
+    if (i >= kHTab * kHTab) return;
+    int n = i / kHTab, m = i % kHTab;
+    g_ha[i] = (n >= m + 2) ? sqrt((n + m - 1.0) * (n - m - 1.0)) : 0.0;
+    g_hb[i] = (n > m) ? 1.0 / sqrt((n - m + 0.0) * (n + m)) : 0.0;
+}
+
+static void htab_init(cudaStream_t s, Status &st)
+{
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    k_htab_init<<<div_up(kHTab * kHTab, 256), 256, 0, s>>>(); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    if (st.ok() && dev >= 0 && dev < 64) done[dev] = true;
+}
+
+// One step of the scaled column recurrence (2s form, src/yrecursion.f:298):
+// y1, d1 hold degree n-1 and y2, d2 degree n-2 of column m.
+struct LegCol {
+    double x, w, y1, d1, y2, d2;
+    int m;
+    __device__ __forceinline__ void start(int m_, double x_, double u)
+    {
+        m = m_;
+        x = x_;
+        w = m == 0 ? 1.0 : u * u;
+        double y;
+        if (m == 0) y = 1;
+        else {
+            y = -sqrt(0.5);
+            for (int k = 2; k <= m; k++) y *= u * sqrt((2 * k - 1.0) / (2 * k));
+        }
+        y1 = y;
+        d1 = m == 0 ? 0.0 : y * (-m) * x;
+        y2 = 0;
+        d2 = 0;
+    }
+    // advance from degree n-1 to n (n > m)
+    __device__ __forceinline__ void step(int n)
+    {
+        double yn, dn;
+        if (n == m + 1) {
+            double s = __ldg(&g_hs[m]);
+            yn = x * y1 * s;
+            dn = (x * d1 + w * y1) * s;
+        } else {
+            double a = __ldg(&g_ha[n * kHTab + m]), b = __ldg(&g_hb[n * kHTab + m]);
+            yn = ((2 * n - 1) * x * y1 - a * y2) * b;
+            dn = ((2 * n - 1) * (x * d1 + w * y1) - a * d2) * b;
+        }
+        y2 = y1; d2 = d1;
+        y1 = yn; d1 = dn;
+    }
+};
+
+// Geometry of one point relative to an expansion center (cart2polar,
+// src/helmrouts3d.f:627-662).
+struct PtGeo {
+    double r, ct, st, cp, sp;
+};
+__device__ __forceinline__ PtGeo pt_geo(double dx, double dy, double dz)
+{
+    PtGeo g;
+    g.r = sqrt(dx * dx + dy * dy + dz * dz);
+    double proj = sqrt(dx * dx + dy * dy);
+    double th = atan2(proj, dz);
+    g.ct = cos(th);
+    g.st = sqrt(1.0 - g.ct * g.ct);
+    double ph = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
+    sincos(ph, &g.sp, &g.cp);
+    return g;
+}
+
+constexpr int kHWarps = 4;
+
+// P2M / P2L.  CTA per receiving box; per source batch of 32, lane j computes
+// the radial functions of source j, then the warp walks the batch with lane
+// per order m, accumulating column m of the expansion in its warp's shared
+// accumulator.  The warp accumulators are summed and multiplied by ik at
+// the end (h3dformmp_add_trunc / h3dformta_add_trunc, src/helmrouts3d.f:2972,
+// 3299; dipoles :3580, 3978).
+template <bool IRREG, bool CHG, bool DIP>
+__global__ void __launch_bounds__(kHWarps * 32) k_hform(const int *boxes, TreeView tv, PointsSoA src, HLevels lv,
+                                                       int NC, double2 zk, double2 *exps)
+{
+    extern __shared__ double2 hsm[];
+    const int b = boxes[blockIdx.x];
+    const int lev = tv.level[b];
+    if (lev < 2) return;
+    if (!IRREG && (tv.nchild[b] != 0 || tv.nsrc[b] == 0)) return;
+    if (IRREG && tv.l4_start[b + 1] == tv.l4_start[b]) return;
+    const int p = lv.p[lev];
+    const double sc = lv.sc[lev];
+    const int W = p + 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int K = (p + 1) * (p + 1);
+    double2 *acc = hsm + (size_t)warp * K;
+    double2 *F = hsm + (size_t)kHWarps * K + (size_t)warp * 32 * W;
+    double *geo = (double *)(hsm + (size_t)kHWarps * K + (size_t)kHWarps * 32 * W) + warp * 32 * 12;
+    for (int i = lane; i < K; i += 32) acc[i] = cmk(0, 0);
+    const double *c = tv.center + 3L * b;
+    const int nsb = IRREG ? tv.l4_start[b + 1] - tv.l4_start[b] : 1;
+    for (int si = 0; si < nsb; si++) {
+        const int sb = IRREG ? tv.l4_idx[tv.l4_start[b] + si] : b;
+        const int s0 = tv.src0[sb], ns = tv.nsrc[sb];
+        for (int c0 = warp * 32; c0 < ns; c0 += kHWarps * 32) {
+            const int nb = min(32, ns - c0);
+            __syncwarp();
+            if (lane < nb) {
+                int i = s0 + c0 + lane;
+                PtGeo g = pt_geo(src.x[i] - c[0], src.y[i] - c[1], src.z[i] - c[2]);
+                double2 *f = F + lane * W;
+                double2 z = cscal(g.r, zk);
+                bool ok = true;
+                if (IRREG) {
+                    if (cabsd(z) < 1.0e-15) ok = false;
+                    else hank_dev(p > 1 ? p : 1, z, sc, f, nullptr);
+                } else {
+                    ok = bess_dev(p > 1 ? p : 1, z, sc, f, nullptr) == 0;
+                }
+                if (!ok)  // the reference skips such a source (ier 4 / 16)
+                    for (int n = 0; n < W; n++) f[n] = cmk(0, 0);
+                double *gg = geo + lane * 12;
+                gg[0] = g.r; gg[1] = g.ct; gg[2] = g.st; gg[3] = g.cp; gg[4] = g.sp;
+                double2 q = (CHG && ok) ? src.q[i] : cmk(0, 0), d = (DIP && ok) ? src.dq[i] : cmk(0, 0);
+                gg[5] = q.x; gg[6] = q.y; gg[7] = d.x; gg[8] = d.y;
+                if (DIP) {
+                    double vx = src.vx[i], vy = src.vy[i], vz = src.vz[i];
+                    gg[9] = vx * g.st * g.cp + vy * g.st * g.sp + vz * g.ct;     // v . r-hat
+                    gg[10] = vx * g.ct * g.cp + vy * g.ct * g.sp - vz * g.st;    // v . theta-hat
+                    gg[11] = -vx * g.sp + vy * g.cp;                             // v . phi-hat
+                }
+            }
+            __syncwarp();
+            for (int j = 0; j < nb; j++) {
+                const double *gg = geo + j * 12;
+                const double2 *f = F + j * W;
+                const double ct = gg[1], st = gg[2];
+                const double2 q = cmk(gg[5], gg[6]), ds = cmk(gg[7], gg[8]);
+                const double phi = atan2(gg[4], gg[3]);
+                double2 zi = cmk(0, 0);
+                if (IRREG && DIP) zi = cdiv(cmk(1, 0), cscal(gg[0], zk));
+                for (int m = lane; m <= p; m += 32) {
+                    double es, ec;
+                    sincos(m * phi, &es, &ec);
+                    const double2 em = cmk(ec, -es);  // e^{-i m phi}
+                    LegCol L;
+                    L.start(m, ct, -st);
+                    for (int n = m; n <= p; n++) {
+                        if (n > m) L.step(n);
+                        const double sn = __ldg(&g_hs[n]);
+                        const double y = L.y1 * sn, dd = L.d1 * sn;  // 2s form
+                        double2 vm = cmk(0, 0), vp = cmk(0, 0);      // to (n, m) and (n, -m)
+                        if (CHG) {
+                            double yr = m == 0 ? y : y * st;
+                            double2 v = cmul(q, cscal(yr, f[n]));
+                            vm = cmul(v, em);
+                            vp = cmul(v, cconj(em));
+                        }
+                        if (DIP) {
+                            // radial derivative and the 1/r angular factor
+                            double2 fd, fu;
+                            if (IRREG) {
+                                fd = n == 0 ? cscal(-1.0 / sc, f[1])
+                                            : csub(cscal(sc, f[n - 1]), cmul(cscal(n + 1.0, zi), f[n]));
+                                fu = cscal(1.0 / gg[0], f[n]);
+                            } else {
+                                double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
+                                fd = n == 0 ? cscal(-sc, f[1])
+                                            : csub(cscal(d1 / sc, f[n - 1]), cscal(d2 * sc, f[n + 1]));
+                                double2 t = n == 0 ? cmk(0, 0) : cadd(cscal(sc, f[n + 1]), cscal(1.0 / sc, f[n - 1]));
+                                fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, t));
+                            }
+                            fd = cmul(fd, zk);
+                            double2 A, B = cmk(0, 0);
+                            if (m == 0) A = csub(cscal(y * gg[9], fd), cscal(dd * st * gg[10], fu));
+                            else {
+                                A = csub(cscal(y * st * gg[9], fd), cscal(dd * gg[10], fu));
+                                B = cscal(m * y * gg[11], fu);
+                            }
+                            double2 Ad = cmul(ds, A), Bd = cmul(ds, B);
+                            // (n, m): ds E (A - iB); (n, -m): ds conj(E) (A + iB)
+                            vm = cadd(vm, cmul(em, cmk(Ad.x + Bd.y, Ad.y - Bd.x)));
+                            vp = cadd(vp, cmul(cconj(em), cmk(Ad.x - Bd.y, Ad.y + Bd.x)));
+                        }
+                        acc[eidx(n, m)] = cadd(acc[eidx(n, m)], vm);
+                        if (m > 0) acc[eidx(n, -m)] = cadd(acc[eidx(n, -m)], vp);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double2 *o = exps + (size_t)b * NC;
+    const double2 ik = cmk(-zk.y, zk.x);
+    for (int e = threadIdx.x; e < K; e += blockDim.x) {
+        double2 t = hsm[e];
+        for (int w = 1; w < kHWarps; w++) t = cadd(t, hsm[(size_t)w * K + e]);
+        o[e] = cadd(o[e], cmul(t, ik));
+    }
+}
+
+static size_t hform_smem(int p)
+{
+    int K = (p + 1) * (p + 1), W = p + 2;
+    return sizeof(double2) * ((size_t)kHWarps * K + (size_t)kHWarps * 32 * W) + sizeof(double) * kHWarps * 32 * 12;
+}
+
+__host__ __device__ static int max_p(const HLevels &lv)
+{
+    int pm = 1;
+    for (int l = 0; l <= kMaxLevel; l++) pm = lv.p[l] > pm ? lv.p[l] : pm;
+    return pm;
+}
+
+void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, const PointsSoA &src,
+                  int ifcharge, int ifdipole, HLevels lv, int NC, double2 zk, double2 *exps, cudaStream_t s,
+                  Status &st)
+{
+    if (nboxes == 0 || !st.ok()) return;
+    bool c = ifcharge == 1, d = ifdipole == 1;
+    if (!c && !d) return;
+    htab_init(s, st);
+    size_t sm = hform_smem(max_p(lv));
+#define FMM_HF(IR, C, D)                                                                                       \
+    do {                                                                                                       \
+        FMM_TRY(st, cudaFuncSetAttribute(k_hform<IR, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        k_hform<IR, C, D><<<nboxes, kHWarps * 32, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);                   \
+        FMM_COUNT_LAUNCH();                                                                                    \
+    } while (0)
+    if (irreg) {
+        if (c && d) FMM_HF(true, true, true);
+        else if (c) FMM_HF(true, true, false);
+        else FMM_HF(true, false, true);
+    } else {
+        if (c && d) FMM_HF(false, true, true);
+        else if (c) FMM_HF(false, true, false);
+        else FMM_HF(false, false, true);
+    }
+#undef FMM_HF
+    FMM_LAUNCH_CHECK(st);
+}
+
+// L2P (h3dtaeval_trunc0, src/helmrouts3d.f:2732) at the leaf's own local
+// expansion when its level is >= 2, and M2P (h3dmpeval_trunc0, :2405) of the
+// multipoles of its list-3 boxes, at the leaf's sources and targets.  CTA per
+// leaf; per expansion the coefficients are staged in shared memory; per batch
+// of 32 points, lane j computes the radial functions of point j, then the
+// warp walks the batch with lane per order m and reduces pot, d/dr, d/dtheta
+// and d/dphi across lanes.
+__global__ void __launch_bounds__(kHWarps * 32) k_heval(const int *leaves, TreeView tv, const double *sx,
+                                                       const double *sy, const double *sz, const double *tx,
+                                                       const double *ty, const double *tz, HLevels lv, int NC,
+                                                       double2 zk, const double2 *mpole, const double2 *local,
+                                                       OutSoA outs, OutSoA outt, int do_src, int do_trg)
+{
+    extern __shared__ double2 hsm[];
+    const int b = leaves[blockIdx.x];
+    const int blev = tv.level[b];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
+    if (ne == 0) return;
+    const int pm = max_p(lv);
+    const int KM = (pm + 1) * (pm + 1), W = pm + 2;
+    double2 *E = hsm;
+    double2 *F = hsm + KM + (size_t)warp * 32 * W;
+    double *geo = (double *)(hsm + KM + (size_t)kHWarps * 32 * W) + warp * 32 * 6;
+    const int l3a = tv.l3_start[b], nl3 = tv.l3_start[b + 1] - l3a;
+    for (int xi = -1; xi < nl3; xi++) {
+        int eb;
+        const bool isloc = xi < 0;
+        if (isloc) {
+            if (blev < 2) continue;
+            eb = b;
+        } else {
+            eb = tv.l3_idx[l3a + xi];
+            if (tv.nsrc[eb] == 0) continue;
+        }
+        const int lev = tv.level[eb], p = lv.p[lev];
+        const double sc = lv.sc[lev];
+        const int K = (p + 1) * (p + 1);
+        const double2 *ex = (isloc ? local : mpole) + (size_t)eb * NC;
+        __syncthreads();
+        for (int i = threadIdx.x; i < K; i += blockDim.x) E[i] = ex[i];
+        __syncthreads();
+        const double *c = tv.center + 3L * eb;
+        for (int c0 = warp * 32; c0 < ne; c0 += kHWarps * 32) {
+            const int nb = min(32, ne - c0);
+            __syncwarp();
+            if (lane < nb) {
+                int e = c0 + lane;
+                double px, py, pz;
+                if (e < ns) { int i = tv.src0[b] + e; px = sx[i]; py = sy[i]; pz = sz[i]; }
+                else { int i = tv.trg0[b] + e - ns; px = tx[i]; py = ty[i]; pz = tz[i]; }
+                PtGeo g = pt_geo(px - c[0], py - c[1], pz - c[2]);
+                double2 *f = F + lane * W;
+                double2 z = cscal(g.r, zk);
+                bool ok;
+                if (isloc) ok = bess_dev(p > 1 ? p : 1, z, sc, f, nullptr) == 0;
+                else {
+                    ok = cabsd(z) >= 1.0e-15;
+                    if (ok) hank_dev(p > 1 ? p : 1, z, sc, f, nullptr);
+                }
+                double *gg = geo + lane * 6;
+                gg[0] = ok ? g.r : -1.0; gg[1] = g.ct; gg[2] = g.st; gg[3] = g.cp; gg[4] = g.sp;
+            }
+            __syncwarp();
+            for (int j = 0; j < nb; j++) {
+                const double *gg = geo + j * 6;
+                if (gg[0] < 0) continue;  // uniform over the warp
+                const double2 *f = F + j * W;
+                const double r = gg[0], ct = gg[1], st = gg[2], cp = gg[3], sp = gg[4];
+                const double2 zi = cdiv(cmk(1, 0), cscal(r, zk));
+                const double phi = atan2(sp, cp);
+                double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
+                for (int m = lane; m <= p; m += 32) {
+                    double es, ec;
+                    sincos(m * phi, &es, &ec);
+                    const double2 ep = cmk(ec, es);  // e^{i m phi}
+                    LegCol L;
+                    L.start(m, ct, -st);
+                    for (int n = m; n <= p; n++) {
+                        if (n > m) L.step(n);
+                        const double sn = __ldg(&g_hs[n]);
+                        const double y = L.y1 * sn, dd = L.d1 * sn;
+                        double2 fd, fu;
+                        if (isloc) {
+                            double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
+                            fd = n == 0 ? cscal(-sc, f[1]) : csub(cscal(d1 / sc, f[n - 1]), cscal(d2 * sc, f[n + 1]));
+                            double2 t = n == 0 ? cmk(0, 0) : cadd(cscal(sc, f[n + 1]), cscal(1.0 / sc, f[n - 1]));
+                            fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, t));
+                        } else {
+                            fd = n == 0 ? cscal(-1.0 / sc, f[1]) : csub(cscal(sc, f[n - 1]), cmul(cscal(n + 1.0, zi), f[n]));
+                            fu = cscal(1.0 / r, f[n]);
+                        }
+                        fd = cmul(fd, zk);
+                        if (m == 0) {
+                            double2 a = E[eidx(n, 0)];
+                            cfma(pot, f[n], cscal(y, a));
+                            cfma(ur, fd, cscal(y, a));
+                            cfma(ut, fu, cscal(-dd * st, a));
+                        } else {
+                            double2 z2 = cmul(E[eidx(n, m)], ep), z3 = cmul(E[eidx(n, -m)], cconj(ep));
+                            double2 zs = cadd(z2, z3), zd = csub(z2, z3);
+                            cfma(pot, f[n], cscal(y * st, zs));
+                            cfma(ur, fd, cscal(y * st, zs));
+                            cfma(ut, fu, cscal(-dd, zs));
+                            cfma(up, fu, cscal(y * m, cmk(-zd.y, zd.x)));  // i m (z2 - z3)
+                        }
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    pot.x += __shfl_xor_sync(0xffffffffu, pot.x, o);
+                    pot.y += __shfl_xor_sync(0xffffffffu, pot.y, o);
+                    ur.x += __shfl_xor_sync(0xffffffffu, ur.x, o);
+                    ur.y += __shfl_xor_sync(0xffffffffu, ur.y, o);
+                    ut.x += __shfl_xor_sync(0xffffffffu, ut.x, o);
+                    ut.y += __shfl_xor_sync(0xffffffffu, ut.y, o);
+                    up.x += __shfl_xor_sync(0xffffffffu, up.x, o);
+                    up.y += __shfl_xor_sync(0xffffffffu, up.y, o);
+                }
+                if (lane == 0) {
+                    // fld = -(ur r-hat + ut theta-hat + up phi-hat)
+                    double2 fx = cadd(cadd(cscal(st * cp, ur), cscal(ct * cp, ut)), cscal(-sp, up));
+                    double2 fy = cadd(cadd(cscal(st * sp, ur), cscal(ct * sp, ut)), cscal(cp, up));
+                    double2 fz = csub(cscal(ct, ur), cscal(st, ut));
+                    int e = c0 + j;
+                    const bool is_src = e < ns;
+                    double2 *po = is_src ? outs.pot : outt.pot;
+                    double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy;
+                    double2 *oz = is_src ? outs.fz : outt.fz;
+                    int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
+                    if (po) po[i] = cadd(po[i], pot);
+                    if (ox) {
+                        ox[i] = csub(ox[i], fx);
+                        oy[i] = csub(oy[i], fy);
+                        oz[i] = csub(oz[i], fz);
+                    }
+                }
+            }
+        }
+    }
+}
+
+void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const double *sx, const double *sy,
+                  const double *sz, const double *tx, const double *ty, const double *tz, HLevels lv, int NC,
+                  double2 zk, const double2 *mpole, const double2 *local, OutSoA outs, OutSoA outt, int do_src,
+                  int do_trg, cudaStream_t s, Status &st)
+{
+    if (nleaves == 0 || !st.ok() || (!do_src && !do_trg)) return;
+    htab_init(s, st);
+    int pm = max_p(lv);
+    size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)kHWarps * 32 * (pm + 2)) +
+                sizeof(double) * kHWarps * 32 * 6;
+    FMM_TRY(st, cudaFuncSetAttribute(k_heval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_heval<<<nleaves, kHWarps * 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
+                                              outt, do_src, do_trg); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// ================================================================ near field
+// One source at one evaluation point: hpotfld3d (src/helmrouts3d.f:1335-1417)
+// and hpotfld3d_dp (:1844-1924) in closed form,
+//   g = e^{ikr}/r,  charge: pot q g,  fld q g (1 - ikr) / r^2 (x - y)
+//   dipole: pot d (1 - ikr) g / r^2 (v . (x - y)),
+//           fld -d [g (3ik/r^2 + k^2/r - 3/r^3)/r (v . (x - y)) (x - y) + (1 - ikr) g / r^2 v]
+template <bool CHG, bool DIP>
+__device__ __forceinline__ void hpair(double dx, double dy, double dz, double2 zk, double2 k2, double2 q, double2 ds,
+                                      double vx, double vy, double vz, double2 &pot, double2 &fx, double2 &fy,
+                                      double2 &fz)
+{
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double r = sqrt(r2), ri = 1.0 / r, ri2 = ri * ri;
+    double s, c;
+    sincos(zk.x * r, &s, &c);
+    double ee = zk.y == 0.0 ? ri : exp(-zk.y * r) * ri;
+    double2 g = cmk(c * ee, s * ee);
+    // (1 - ikr) g / r^2
+    double2 h = cscal(ri2, cmul(cmk(1.0 + zk.y * r, -zk.x * r), g));
+    if (CHG) {
+        cfma(pot, q, g);
+        double2 qh = cmul(q, h);
+        crfma(fx, dx, qh);
+        crfma(fy, dy, qh);
+        crfma(fz, dz, qh);
+    }
+    if (DIP) {
+        double dot = dx * vx + dy * vy + dz * vz;
+        double2 dh = cmul(ds, h);
+        crfma(pot, dot, dh);
+        // 3ik/r^2 + k^2/r - 3/r^3
+        double2 t = cadd(cscal(3 * ri2, cmk(-zk.y, zk.x)), cscal(ri, k2));
+        t.x -= 3 * ri2 * ri;
+        double2 F = cscal(ri * dot, cmul(cmul(ds, g), t));
+        fx = csub(fx, cadd(cscal(dx, F), cscal(vx, dh)));
+        fy = csub(fy, cadd(cscal(dy, F), cscal(vy, dh)));
+        fz = csub(fz, cadd(cscal(dz, F), cscal(vz, dh)));
+    }
+}
+
+constexpr int kHP2PThreads = 128;
+
+// P2P: hfmm3dpart_direct_self / _targ (src/hfmm3dpart.f:1092-1262).  CTA per
+// leaf, one evaluation point (sources, then targets) per thread, source boxes
+// self and list 1 staged through shared memory, the self pair skipped by index.
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kHP2PThreads) k_hp2p(const int *leaves, TreeView tv, PointsSoA src,
+                                                      const double *tx, const double *ty, const double *tz,
+                                                      double2 zk, OutSoA outs, OutSoA outt, int do_src, int do_trg)
+{
+    __shared__ double sx[kHP2PThreads], sy[kHP2PThreads], sz[kHP2PThreads];
+    __shared__ double2 sq[kHP2PThreads], sd[kHP2PThreads];
+    __shared__ double svx[kHP2PThreads], svy[kHP2PThreads], svz[kHP2PThreads];
+    const int b = leaves[blockIdx.x];
+    const int s0 = tv.src0[b], ns = do_src ? tv.nsrc[b] : 0;
+    const int t0 = tv.trg0[b], nt = do_trg ? tv.ntrg[b] : 0;
+    const int ne = ns + nt;
+    const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
+    const double2 k2 = cmul(zk, zk);
+    for (int e0 = 0; e0 < ne; e0 += kHP2PThreads) {
+        const int e = e0 + threadIdx.x;
+        const bool act = e < ne;
+        const bool is_src = e < ns;
+        double ex = 0, ey = 0, ez = 0;
+        int self = -1;
+        if (act) {
+            if (is_src) { int i = s0 + e; ex = src.x[i]; ey = src.y[i]; ez = src.z[i]; self = i; }
+            else { int i = t0 + e - ns; ex = tx[i]; ey = ty[i]; ez = tz[i]; }
+        }
+        double2 pot = cmk(0, 0), fx = cmk(0, 0), fy = cmk(0, 0), fz = cmk(0, 0);
+        for (int j = 0; j < nl; j++) {
+            const int jb = j == 0 ? b : tv.l1_idx[l1a + j - 1];
+            const int js0 = tv.src0[jb], jn = tv.nsrc[jb];
+            for (int c0 = 0; c0 < jn; c0 += kHP2PThreads) {
+                const int cn = min(kHP2PThreads, jn - c0);
+                __syncthreads();
+                if (threadIdx.x < cn) {
+                    int i = js0 + c0 + threadIdx.x;
+                    sx[threadIdx.x] = src.x[i]; sy[threadIdx.x] = src.y[i]; sz[threadIdx.x] = src.z[i];
+                    if (CHG) sq[threadIdx.x] = src.q[i];
+                    if (DIP) {
+                        sd[threadIdx.x] = src.dq[i];
+                        svx[threadIdx.x] = src.vx[i]; svy[threadIdx.x] = src.vy[i]; svz[threadIdx.x] = src.vz[i];
+                    }
+                }
+                __syncthreads();
+                if (!act) continue;
+                const int selfk = self - (js0 + c0);
+                for (int k = 0; k < cn; k++) {
+                    if (k == selfk) continue;
+                    hpair<CHG, DIP>(ex - sx[k], ey - sy[k], ez - sz[k], zk, k2, CHG ? sq[k] : cmk(0, 0),
+                                    DIP ? sd[k] : cmk(0, 0), DIP ? svx[k] : 0.0, DIP ? svy[k] : 0.0,
+                                    DIP ? svz[k] : 0.0, pot, fx, fy, fz);
+                }
+            }
+        }
+        if (act) {
+            double2 *po = is_src ? outs.pot : outt.pot;
+            double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy, *oz = is_src ? outs.fz : outt.fz;
+            int i = is_src ? s0 + e : t0 + e - ns;
+            if (po) po[i] = cadd(po[i], pot);
+            if (ox) {
+                ox[i] = cadd(ox[i], fx);
+                oy[i] = cadd(oy[i], fy);
+                oz[i] = cadd(oz[i], fz);
+            }
+        }
+    }
+}
+
+void launch_hp2p(const int *leaves, int nleaves, const TreeView &tv, const PointsSoA &src, const double *tx,
+                 const double *ty, const double *tz, double2 zk, OutSoA outs, OutSoA outt, int ifcharge,
+                 int ifdipole, int ifpot, int iffld, int ifpottarg, int iffldtarg, cudaStream_t s, Status &st)
+{
+    if (nleaves == 0 || !st.ok()) return;
+    int do_src = (ifpot == 1 || iffld == 1), do_trg = (ifpottarg == 1 || iffldtarg == 1);
+    bool c = ifcharge == 1, d = ifdipole == 1;
+    if (!c && !d) return;
+    if (c && d) k_hp2p<true, true><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    else if (c) k_hp2p<true, false><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    else k_hp2p<false, true><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// Direct sum (h3dpartdirect, src/hfmm3dpart.f:1268-1401): blockIdx.x tiles
+// the evaluation points, blockIdx.y the sources; partial sums per source chunk
+// go to scratch and are reduced in chunk order.
+constexpr int kHDirThreads = 128;
+
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kHDirThreads) k_hdirect(int nsrc, PointsSoA src, int neval, const double *ex,
+                                                         const double *ey, const double *ez, const int *skip,
+                                                         int self, double2 zk, int chunk, double2 *part)
+{
+    __shared__ double sx[kHDirThreads], sy[kHDirThreads], sz[kHDirThreads];
+    __shared__ double2 sq[kHDirThreads], sd[kHDirThreads];
+    __shared__ double svx[kHDirThreads], svy[kHDirThreads], svz[kHDirThreads];
+    const int e = blockIdx.x * kHDirThreads + threadIdx.x;
+    const bool act = e < neval;
+    const int j0 = blockIdx.y * chunk, j1 = min(nsrc, j0 + chunk);
+    double px = act ? ex[e] : 0, py = act ? ey[e] : 0, pz = act ? ez[e] : 0;
+    int sk = act ? (skip ? skip[e] : (self ? e : -1)) : -1;
+    const double2 k2 = cmul(zk, zk);
+    double2 pot = cmk(0, 0), fx = cmk(0, 0), fy = cmk(0, 0), fz = cmk(0, 0);
+    for (int c0 = j0; c0 < j1; c0 += kHDirThreads) {
+        const int cn = min(kHDirThreads, j1 - c0);
+        __syncthreads();
+        if (threadIdx.x < cn) {
+            int i = c0 + threadIdx.x;
+            sx[threadIdx.x] = src.x[i]; sy[threadIdx.x] = src.y[i]; sz[threadIdx.x] = src.z[i];
+            if (CHG) sq[threadIdx.x] = src.q[i];
+            if (DIP) {
+                sd[threadIdx.x] = src.dq[i];
+                svx[threadIdx.x] = src.vx[i]; svy[threadIdx.x] = src.vy[i]; svz[threadIdx.x] = src.vz[i];
+            }
+        }
+        __syncthreads();
+        if (!act) continue;
+        for (int k = 0; k < cn; k++) {
+            if (c0 + k == sk) continue;
+            hpair<CHG, DIP>(px - sx[k], py - sy[k], pz - sz[k], zk, k2, CHG ? sq[k] : cmk(0, 0),
+                            DIP ? sd[k] : cmk(0, 0), DIP ? svx[k] : 0.0, DIP ? svy[k] : 0.0, DIP ? svz[k] : 0.0,
+                            pot, fx, fy, fz);
+        }
+    }
+    if (act) {
+        double2 *o = part + ((size_t)blockIdx.y * neval + e) * 4;
+        o[0] = pot; o[1] = fx; o[2] = fy; o[3] = fz;
+    }
+}
+
+__global__ void k_hdirect_reduce(int neval, int nchunk, const double2 *part, OutSoA out)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= neval) return;
+    double2 a[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    for (int c = 0; c < nchunk; c++)
+        for (int q = 0; q < 4; q++) a[q] = cadd(a[q], part[((size_t)c * neval + e) * 4 + q]);
+    if (out.pot) out.pot[e] = a[0];
+    if (out.fx) { out.fx[e] = a[1]; out.fy[e] = a[2]; out.fz[e] = a[3]; }
+}
+
+void launch_hdirect(int nsrc, const PointsSoA &src, int ifcharge, int ifdipole, int neval, const double *ex,
+                    const double *ey, const double *ez, const int *skip, int self, double2 zk, OutSoA out,
+                    cudaStream_t s, Status &st)
+{
+    if (neval == 0 || !st.ok()) return;
+    bool c = ifcharge == 1, d = ifdipole == 1;
+    int gx = div_up(neval, kHDirThreads);
+    // enough source chunks to fill the GPU (about 4 CTAs per SM), at least 1024 sources each
+    int nchunk = std::max(1, std::min(div_up(std::max(nsrc, 1), 1024), div_up(148 * 4, gx)));
+    int chunk = div_up(std::max(nsrc, 1), nchunk);
+    nchunk = div_up(std::max(nsrc, 1), chunk);
+    DBuf<double2> part;
+    if (!part.alloc((size_t)nchunk * neval * 4, s, st)) return;
+    if ((!c && !d) || nsrc == 0) part.zero(st);
+    dim3 g(gx, nchunk);
+    if (nsrc > 0) {
+        if (c && d) { k_hdirect<true, true><<<g, kHDirThreads, 0, s>>>(nsrc, src, neval, ex, ey, ez, skip, self, zk, chunk, part.p); FMM_COUNT_LAUNCH(); }
+        else if (c) { k_hdirect<true, false><<<g, kHDirThreads, 0, s>>>(nsrc, src, neval, ex, ey, ez, skip, self, zk, chunk, part.p); FMM_COUNT_LAUNCH(); }
+        else if (d) { k_hdirect<false, true><<<g, kHDirThreads, 0, s>>>(nsrc, src, neval, ex, ey, ez, skip, self, zk, chunk, part.p); FMM_COUNT_LAUNCH(); }
+    }
+    k_hdirect_reduce<<<div_up(neval, 256), 256, 0, s>>>(neval, nchunk, part.p, out); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+}  // namespace fmm

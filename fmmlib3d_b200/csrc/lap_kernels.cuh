@@ -70,6 +70,9 @@ void launch_translate(int kind, const Tile *tiles, int ntiles, const int *groupe
                       const TreeView &tv, int p, const double *rot, const double *dc, int lddc,
                       const double2 *in, double2 *out, int prune, int kt, cudaStream_t s, Status &st);
 
+// Gauss-Legendre nodes and weights on [-1, 1] (host).
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w);
+
 // Rotation matrices about the y axis for each class (cos, sin of theta).
 void build_rotations(int p, int ncls, const double *d_cs, double *d_rot, cudaStream_t s, Status &st);
 

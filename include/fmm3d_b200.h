@@ -44,6 +44,33 @@ void l3dpartdirect_(const int *nsource, const double *source, const int *ifcharg
                     const int *iffld, double *fld, const int *ntarget, const double *target,
                     const int *ifpottarg, double *pottarg, const int *iffldtarg, double *fldtarg);
 
+/* Replaces hfmm3dparttarg (src/hfmm3dpart.f:141-539): Helmholtz potential
+ * e^{ik r}/r and field at sources and targets.  zk is complex*16 (two
+ * doubles, re and im) passed after iprec; every other argument as for
+ * lfmm3dparttarg_. */
+void hfmm3dparttarg_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *source,
+                     const int *ifcharge, const double *charge, const int *ifdipole, const double *dipstr,
+                     const double *dipvec, const int *ifpot, double *pot, const int *iffld, double *fld,
+                     const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
+                     const int *iffldtarg, double *fldtarg);
+
+/* Replaces hfmm3dpartself (src/hfmm3dpart.f:90-131): sources only. */
+void hfmm3dpartself_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *source,
+                     const int *ifcharge, const double *charge, const int *ifdipole, const double *dipstr,
+                     const double *dipvec, const int *ifpot, double *pot, const int *iffld, double *fld);
+
+/* Replaces hfmm3dpart (src/hfmm3dpart.f:39-84), the older name of hfmm3dpartself. */
+void hfmm3dpart_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *source,
+                 const int *ifcharge, const double *charge, const int *ifdipole, const double *dipstr,
+                 const double *dipvec, const int *ifpot, double *pot, const int *iffld, double *fld);
+
+/* Replaces h3dpartdirect (src/hfmm3dpart.f:1268-1401), the O(N^2) Helmholtz sum. */
+void h3dpartdirect_(const double *zk, const int *nsource, const double *source, const int *ifcharge,
+                    const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                    const int *ifpot, double *pot, const int *iffld, double *fld, const int *ntarget,
+                    const double *target, const int *ifpottarg, double *pottarg, const int *iffldtarg,
+                    double *fldtarg);
+
 /* ---- extensions (no counterpart in the reference) ---------------------- */
 
 /* lfmm3dparttarg on arrays already resident in device memory (same layouts),
@@ -70,6 +97,23 @@ int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcha
                                   int ifdipole, const double *d_dipstr, const double *d_dipvec, int npts,
                                   const double *d_pts, const int *d_skip, double *d_pot, double *d_fld,
                                   void *stream);
+
+/* hfmm3dparttarg, h3dpartdirect and the sampled Helmholtz direct sum on
+ * device-resident arrays (layouts as above; zk = two doubles on the host). */
+int fmm3d_hfmm3dparttarg_device(int iprec, const double *zk, int nsource, const double *d_source, int ifcharge,
+                                const double *d_charge, int ifdipole, const double *d_dipstr, const double *d_dipvec,
+                                int ifpot, double *d_pot, int iffld, double *d_fld, int ntarget,
+                                const double *d_target, int ifpottarg, double *d_pottarg, int iffldtarg,
+                                double *d_fldtarg, void *stream);
+int fmm3d_h3dpartdirect_device(const double *zk, int nsource, const double *d_source, int ifcharge,
+                               const double *d_charge, int ifdipole, const double *d_dipstr, const double *d_dipvec,
+                               int ifpot, double *d_pot, int iffld, double *d_fld, int ntarget,
+                               const double *d_target, int ifpottarg, double *d_pottarg, int iffldtarg,
+                               double *d_fldtarg, void *stream);
+int fmm3d_h3ddirect_points_device(const double *zk, int nsource, const double *d_source, int ifcharge,
+                                  const double *d_charge, int ifdipole, const double *d_dipstr,
+                                  const double *d_dipvec, int npts, const double *d_pts, const int *d_skip,
+                                  double *d_pot, double *d_fld, void *stream);
 
 /* l3dpartdirect on device-resident arrays WITHOUT any device allocation.
  * No counterpart in the reference.  For callers that cannot let the library
@@ -99,7 +143,11 @@ int fmm3d_last_timing(double *ms, int n);
 /* Tree statistics of the last call on this thread, gathered only while
  * fmm3d_set_stats(1) is in effect:
  * [nboxes, nlev, nleaves, nterms, list1 entries, list3 entries,
- *  list4 entries, p2p pairs (sum over leaves), m2l pairs]. */
+ *  list4 entries, p2p pairs (sum over leaves), m2l pairs, then 128 counts of
+ *  M2L pairs by truncation order]; Helmholtz calls append the expansion
+ *  order of levels 0..21 (0 where a level carries no expansions) and report
+ *  the largest order as nterms.  For Helmholtz the "sort+gather" timing entry
+ *  also holds the construction of that call's z-shift operators. */
 int fmm3d_set_stats(int on);
 
 /* M2L form: 0 automatic (dense per-offset operators for nterms <= 16,
