@@ -28,11 +28,12 @@ __device__ __forceinline__ double2 cexpi(double2 z)
 
 // ================================================================ special functions
 // Scaled spherical Hankel functions h_n(z) scale^n, n = 0..nt, and (if hd)
-// their derivatives: h3dall (src/helmrouts3d.f:709-809).  Needs nt >= 1.
-__device__ void hank_dev(int nt, double2 z, double scale, double2 *h, double2 *hd)
+// their derivatives: h3dall (src/helmrouts3d.f:709-809), stored with stride
+// hs.  Needs nt >= 1.
+__device__ void hank_dev(int nt, double2 z, double scale, double2 *h, double2 *hd, int hs = 1)
 {
     if (cabsd(z) < 1.0e-15) {
-        for (int i = 0; i <= nt; i++) { h[i] = cmk(0, 0); if (hd) hd[i] = cmk(0, 0); }
+        for (int i = 0; i <= nt; i++) { h[i * hs] = cmk(0, 0); if (hd) hd[i * hs] = cmk(0, 0); }
         return;
     }
     // h0 = e^{iz} / (iz), h1 = h0 (1/z - i)   (h3d01, :666-704)
@@ -41,16 +42,16 @@ __device__ void hank_dev(int nt, double2 z, double scale, double2 *h, double2 *h
     double2 zi = cdiv(cmk(1, 0), z);
     double2 h1 = cmul(h0, cmk(zi.x, zi.y - 1.0));
     h[0] = h0;
-    h[1] = cscal(scale, h1);
+    h[hs] = cscal(scale, h1);
     double s2 = scale * scale;
     double2 zs = cscal(scale, zi);
     for (int i = 1; i <= nt - 1; i++) {
         double2 t = cscal(2 * i + 1.0, zs);
-        h[i + 1] = csub(cmul(t, h[i]), cscal(s2, h[i - 1]));
+        h[(i + 1) * hs] = csub(cmul(t, h[i * hs]), cscal(s2, h[(i - 1) * hs]));
     }
     if (hd) {
-        hd[0] = cscal(-1.0 / scale, h[1]);
-        for (int i = 1; i <= nt; i++) hd[i] = csub(cscal(scale, h[i - 1]), cmul(cscal(i + 1.0, zi), h[i]));
+        hd[0] = cscal(-1.0 / scale, h[hs]);
+        for (int i = 1; i <= nt; i++) hd[i * hs] = csub(cscal(scale, h[(i - 1) * hs]), cmul(cscal(i + 1.0, zi), h[i * hs]));
     }
 }
 
@@ -59,17 +60,18 @@ __device__ void hank_dev(int nt, double2 z, double scale, double2 *h, double2 *h
 // sweep from n = nt finds the start ntop (first |f|^2 > 1e40, at most
 // nt + 1000 terms), the downward sweep rescales by 1e-40 when it grows past
 // that bound, and the values are normalized against sin z / z or its
-// successor.  Only entries 0..nt+1 are stored.  fd (optional) receives the
-// derivatives of entries 0..nt.  Returns 8 if the upward sweep never grew.
-__device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd)
+// successor.  Only entries 0..nt+1 are stored (with stride fs).  fd
+// (optional) receives the derivatives of entries 0..nt.  Returns 8 if the
+// upward sweep never grew.
+__device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd, int fs = 1)
 {
     const double ub = 1.0e40, ubinv = 1.0e-40;
     if (cabsd(z) < 1.0e-200) {
         f[0] = cmk(1, 0);
-        for (int i = 1; i <= nt + 1; i++) f[i] = cmk(0, 0);
+        for (int i = 1; i <= nt + 1; i++) f[i * fs] = cmk(0, 0);
         if (fd) {
-            for (int i = 0; i <= nt; i++) fd[i] = cmk(0, 0);
-            if (nt >= 1) fd[1] = cmk(1.0 / (3 * scale), 0);
+            for (int i = 0; i <= nt; i++) fd[i * fs] = cmk(0, 0);
+            if (nt >= 1) fd[fs] = cmk(1.0 / (3 * scale), 0);
         }
         return 0;
     }
@@ -86,7 +88,7 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
     }
     if (ntop == 0) return 8;
     unsigned long long fl[2] = {0ull, 0ull};  // rescale events at index i <= 127
-    if (ntop <= nt + 1) f[ntop] = cmk(0, 0);
+    if (ntop <= nt + 1) f[ntop * fs] = cmk(0, 0);
     double2 a = cmk(0, 0), b = cmk(1, 0);    // f(i+1), f(i)
     for (int i = ntop - 1; i >= 1; i--) {
         double2 c = csub(cmul(cscal(2 * i + 1.0, zi), b), a);
@@ -95,7 +97,7 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
             c = cscal(ubinv, c);
             if (i < 128) fl[i >> 6] |= 1ull << (i & 63);
         }
-        if (i <= nt + 1) f[i] = b;
+        if (i <= nt + 1) f[i * fs] = b;
         a = b;
         b = c;
     }
@@ -105,7 +107,7 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
         sct *= sinv;
         int k = i - 1;
         if ((fl[k >> 6] >> (k & 63)) & 1ull) sct *= ubinv;
-        f[i] = cscal(sct, f[i]);
+        f[i * fs] = cscal(sct, f[i * fs]);
     }
     // sin z / z and (sin z / z - cos z) / z
     double sx, cx;
@@ -114,13 +116,13 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
     double2 sz = cmk(sx * ch, cx * sh), cz = cmk(cx * ch, -sx * sh);
     double2 j0 = cmul(sz, zi);
     double2 j1 = csub(cmul(j0, zi), cmul(cz, zi));
-    double2 zs = cabsd(j1) > cabsd(j0) ? cdiv(j1, cscal(scale, f[1])) : cdiv(j0, f[0]);
-    for (int i = 0; i <= nt + 1; i++) f[i] = cmul(f[i], zs);
+    double2 zs = cabsd(j1) > cabsd(j0) ? cdiv(j1, cscal(scale, f[fs])) : cdiv(j0, f[0]);
+    for (int i = 0; i <= nt + 1; i++) f[i * fs] = cmul(f[i * fs], zs);
     if (fd) {
-        fd[0] = cscal(-scale, f[1]);
+        fd[0] = cscal(-scale, f[fs]);
         for (int i = 1; i <= nt; i++) {
             double d1 = i / (2 * i + 1.0), d2 = 1.0 - d1;
-            fd[i] = csub(cscal(d1 * sinv, f[i - 1]), cscal(d2 * scale, f[i + 1]));
+            fd[i * fs] = csub(cscal(d1 * sinv, f[(i - 1) * fs]), cscal(d2 * scale, f[(i + 1) * fs]));
         }
     }
     return 0;
@@ -504,14 +506,17 @@ void launch_htranslate(int kind, const Tile *tiles, int ntiles, const int *group
 // ================================================================ point operators
 // Legendre recurrence coefficients for the column recurrences in registers:
 // g_ha[n][m] = sqrt((n+m-1)(n-m-1)), g_hb[n][m] = 1/sqrt((n-m)(n+m)),
-// g_hs[n] = sqrt(2n+1).
+// g_hs[n] = sqrt(2n+1), g_hc[m] = sqrt((2m-1)/(2m)).
 constexpr int kHTab = kHelmMaxP + 3;
-__device__ double g_ha[kHTab * kHTab], g_hb[kHTab * kHTab], g_hs[kHTab];
+__device__ double g_ha[kHTab * kHTab], g_hb[kHTab * kHTab], g_hs[kHTab], g_hc[kHTab];
 
 __global__ void k_htab_init()
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < kHTab) g_hs[i] = sqrt(2 * i + 1.0);
+    if (i < kHTab) {
+        g_hs[i] = sqrt(2 * i + 1.0);
+        g_hc[i] = i > 0 ? sqrt((2 * i - 1.0) / (2 * i)) : 0.0;
+    }
     if (i >= kHTab * kHTab) return;
     int n = i / kHTab, m = i % kHTab;
     g_ha[i] = (n >= m + 2) ? sqrt((n + m - 1.0) * (n - m - 1.0)) : 0.0;
@@ -586,19 +591,33 @@ __device__ __forceinline__ PtGeo pt_geo(double dx, double dy, double dz)
     return g;
 }
 
-constexpr int kHWarps = 4;
+// P2M / P2L.  CTA per receiving box and range of 1024 coefficients, each
+// thread owning up to kHFormPer coefficients in registers.  Sources are taken in chunks of CH: per chunk
+// the sources' radial functions, e^{-i m phi} powers, diagonal Legendre
+// values and full Legendre tables (2s form, one column per (source, m) task)
+// are built in shared memory, then every thread adds the chunk's
+// contributions to its coefficients.  The sum is multiplied by ik at the end
+// (h3dformmp_add_trunc / h3dformta_add_trunc, src/helmrouts3d.f:2972, 3299;
+// dipoles h3dformmp_dp_add_trunc :3580, h3dformta_dp_add_trunc :3978).
+constexpr int kHFormThreads = 256, kHFormPer = 4;
 
-// P2M / P2L.  CTA per receiving box; per source batch of 32, lane j computes
-// the radial functions of source j, then the warp walks the batch with lane
-// per order m, accumulating column m of the expansion in its warp's shared
-// accumulator.  The warp accumulators are summed and multiplied by ik at
-// the end (h3dformmp_add_trunc / h3dformta_add_trunc, src/helmrouts3d.f:2972,
-// 3299; dipoles :3580, 3978).
-template <bool IRREG, bool CHG, bool DIP>
-__global__ void __launch_bounds__(kHWarps * 32) k_hform(const int *boxes, TreeView tv, PointsSoA src, HLevels lv,
-                                                       int NC, double2 zk, double2 *exps)
+template <int CH, bool DIP>
+struct HFormSmem {
+    // sizes in doubles for expansion order p
+    static __host__ __device__ size_t doubles(int p)
+    {
+        size_t W = p + 2, T = (size_t)(p + 1) * (p + 2) / 2;
+        size_t d = CH * (2 * W + 2 * (p + 1) + (p + 1) + T + 16);  // f, e^{-im phi}, diagonal, Y, scalars
+        if (DIP) d += CH * (T + 4 * (p + 1));                        // D, fd, fu
+        return d;
+    }
+};
+
+template <bool IRREG, bool CHG, bool DIP, int CH>
+__global__ void __launch_bounds__(kHFormThreads) k_hform(const int *boxes, TreeView tv, PointsSoA src, HLevels lv,
+                                                        int NC, double2 zk, double2 *exps)
 {
-    extern __shared__ double2 hsm[];
+    extern __shared__ double hsd[];
     const int b = boxes[blockIdx.x];
     const int lev = tv.level[b];
     if (lev < 2) return;
@@ -606,26 +625,42 @@ __global__ void __launch_bounds__(kHWarps * 32) k_hform(const int *boxes, TreeVi
     if (IRREG && tv.l4_start[b + 1] == tv.l4_start[b]) return;
     const int p = lv.p[lev];
     const double sc = lv.sc[lev];
-    const int W = p + 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int K = (p + 1) * (p + 1);
-    double2 *acc = hsm + (size_t)warp * K;
-    double2 *F = hsm + (size_t)kHWarps * K + (size_t)warp * 32 * W;
-    double *geo = (double *)(hsm + (size_t)kHWarps * K + (size_t)kHWarps * 32 * W) + warp * 32 * 12;
-    for (int i = lane; i < K; i += 32) acc[i] = cmk(0, 0);
+    const int W = p + 2, P1 = p + 1, TS = (p + 1) * (p + 2) / 2, K = (p + 1) * (p + 1);
+    double2 *F = (double2 *)hsd;            // [CH][W]
+    double2 *Em = F + CH * W;               // [CH][P1]   e^{-i m phi}
+    double *Dg = (double *)(Em + CH * P1);  // [CH][P1]   diagonal Y_m^m (2s form)
+    double *Y = Dg + CH * P1;               // [CH][TS]
+    double *Sc = Y + CH * TS;               // [CH][16]   per-source scalars
+    double *D = Sc + CH * 16;               // [CH][TS]   (dipoles)
+    double2 *Fd = (double2 *)(D + (DIP ? CH * TS : 0));  // [CH][P1]
+    double2 *Fu = Fd + (DIP ? CH * P1 : 0);              // [CH][P1]
+    const int e0 = blockIdx.y * kHFormThreads * kHFormPer;  // this CTA's coefficient range
+    if (e0 >= K) return;
+    double2 acc[kHFormPer];
+    int en[kHFormPer], em_[kHFormPer];
+#pragma unroll
+    for (int q = 0; q < kHFormPer; q++) {
+        acc[q] = cmk(0, 0);
+        int e = e0 + threadIdx.x + q * kHFormThreads;
+        int n = 0;
+        while ((n + 1) * (n + 1) <= e) n++;
+        en[q] = e < K ? n : -1;
+        em_[q] = e - n * n - n;
+    }
     const double *c = tv.center + 3L * b;
     const int nsb = IRREG ? tv.l4_start[b + 1] - tv.l4_start[b] : 1;
     for (int si = 0; si < nsb; si++) {
         const int sb = IRREG ? tv.l4_idx[tv.l4_start[b] + si] : b;
         const int s0 = tv.src0[sb], ns = tv.nsrc[sb];
-        for (int c0 = warp * 32; c0 < ns; c0 += kHWarps * 32) {
-            const int nb = min(32, ns - c0);
-            __syncwarp();
-            if (lane < nb) {
-                int i = s0 + c0 + lane;
-                PtGeo g = pt_geo(src.x[i] - c[0], src.y[i] - c[1], src.z[i] - c[2]);
-                double2 *f = F + lane * W;
-                double2 z = cscal(g.r, zk);
+        for (int c0 = 0; c0 < ns; c0 += CH) {
+            const int nb = min(CH, ns - c0);
+            __syncthreads();
+            // phase A: per source, radial functions, phases, diagonal, scalars
+            if (threadIdx.x < nb) {
+                const int j = threadIdx.x, i = s0 + c0 + j;
+                const PtGeo g = pt_geo(src.x[i] - c[0], src.y[i] - c[1], src.z[i] - c[2]);
+                double2 *f = F + j * W;
+                const double2 z = cscal(g.r, zk);
                 bool ok = true;
                 if (IRREG) {
                     if (cabsd(z) < 1.0e-15) ok = false;
@@ -635,90 +670,101 @@ __global__ void __launch_bounds__(kHWarps * 32) k_hform(const int *boxes, TreeVi
                 }
                 if (!ok)  // the reference skips such a source (ier 4 / 16)
                     for (int n = 0; n < W; n++) f[n] = cmk(0, 0);
-                double *gg = geo + lane * 12;
-                gg[0] = g.r; gg[1] = g.ct; gg[2] = g.st; gg[3] = g.cp; gg[4] = g.sp;
-                double2 q = (CHG && ok) ? src.q[i] : cmk(0, 0), d = (DIP && ok) ? src.dq[i] : cmk(0, 0);
-                gg[5] = q.x; gg[6] = q.y; gg[7] = d.x; gg[8] = d.y;
+                const double2 e1 = cmk(g.cp, -g.sp);  // e^{-i phi}
+                double2 e = cmk(1, 0);
+                double dg = 1.0;
+                const double u = -g.st;
+                for (int m = 0; m <= p; m++) {
+                    if (m > 0) e = cmul(e, e1);
+                    if (m == 1) dg = -sqrt(0.5);
+                    else if (m > 1) dg *= u * __ldg(&g_hc[m]);
+                    Em[j * P1 + m] = e;
+                    Dg[j * P1 + m] = dg;
+                }
+                double *S = Sc + j * 16;
+                const double2 qv = (CHG && ok) ? src.q[i] : cmk(0, 0), dv = (DIP && ok) ? src.dq[i] : cmk(0, 0);
+                S[0] = g.ct; S[1] = g.st; S[2] = qv.x; S[3] = qv.y; S[4] = dv.x; S[5] = dv.y;
                 if (DIP) {
-                    double vx = src.vx[i], vy = src.vy[i], vz = src.vz[i];
-                    gg[9] = vx * g.st * g.cp + vy * g.st * g.sp + vz * g.ct;     // v . r-hat
-                    gg[10] = vx * g.ct * g.cp + vy * g.ct * g.sp - vz * g.st;    // v . theta-hat
-                    gg[11] = -vx * g.sp + vy * g.cp;                             // v . phi-hat
+                    const double vx = src.vx[i], vy = src.vy[i], vz = src.vz[i];
+                    S[6] = vx * g.st * g.cp + vy * g.st * g.sp + vz * g.ct;  // v . r-hat
+                    S[7] = vx * g.ct * g.cp + vy * g.ct * g.sp - vz * g.st;  // v . theta-hat
+                    S[8] = -vx * g.sp + vy * g.cp;                           // v . phi-hat
+                    // radial derivative (times k) and the 1/r angular radial factor
+                    const double2 zi = IRREG && ok ? cdiv(cmk(1, 0), z) : cmk(0, 0);
+                    for (int n = 0; n <= p; n++) {
+                        double2 fd, fu;
+                        if (IRREG) {
+                            fd = n == 0 ? cscal(-1.0 / sc, f[1]) : csub(cscal(sc, f[n - 1]), cmul(cscal(n + 1.0, zi), f[n]));
+                            fu = ok ? cscal(1.0 / g.r, f[n]) : cmk(0, 0);
+                        } else {
+                            double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
+                            fd = n == 0 ? cscal(-sc, f[1]) : csub(cscal(d1 / sc, f[n - 1]), cscal(d2 * sc, f[n + 1]));
+                            fu = n == 0 ? cmk(0, 0)
+                                        : cscal(1.0 / (2 * n + 1.0), cmul(zk, cadd(cscal(sc, f[n + 1]), cscal(1.0 / sc, f[n - 1]))));
+                        }
+                        Fd[j * P1 + n] = cmul(fd, zk);
+                        Fu[j * P1 + n] = fu;
+                    }
                 }
             }
-            __syncwarp();
-            for (int j = 0; j < nb; j++) {
-                const double *gg = geo + j * 12;
-                const double2 *f = F + j * W;
-                const double ct = gg[1], st = gg[2];
-                const double2 q = cmk(gg[5], gg[6]), ds = cmk(gg[7], gg[8]);
-                const double phi = atan2(gg[4], gg[3]);
-                double2 zi = cmk(0, 0);
-                if (IRREG && DIP) zi = cdiv(cmk(1, 0), cscal(gg[0], zk));
-                for (int m = lane; m <= p; m += 32) {
-                    double es, ec;
-                    sincos(m * phi, &es, &ec);
-                    const double2 em = cmk(ec, -es);  // e^{-i m phi}
-                    LegCol L;
-                    L.start(m, ct, -st);
-                    for (int n = m; n <= p; n++) {
-                        if (n > m) L.step(n);
-                        const double sn = __ldg(&g_hs[n]);
-                        const double y = L.y1 * sn, dd = L.d1 * sn;  // 2s form
-                        double2 vm = cmk(0, 0), vp = cmk(0, 0);      // to (n, m) and (n, -m)
-                        if (CHG) {
-                            double yr = m == 0 ? y : y * st;
-                            double2 v = cmul(q, cscal(yr, f[n]));
-                            vm = cmul(v, em);
-                            vp = cmul(v, cconj(em));
+            __syncthreads();
+            // phase B: Legendre columns, one (source, m) task per thread
+            for (int task = threadIdx.x; task < nb * P1; task += kHFormThreads) {
+                const int j = task / P1, m = task % P1;
+                const double x = Sc[j * 16], u = -Sc[j * 16 + 1];
+                LegCol L;
+                L.x = x; L.m = m; L.w = m == 0 ? 1.0 : u * u;
+                L.y1 = Dg[j * P1 + m];
+                L.d1 = m == 0 ? 0.0 : L.y1 * (-m) * x;
+                L.y2 = 0; L.d2 = 0;
+                for (int n = m; n <= p; n++) {
+                    if (n > m) L.step(n);
+                    const double sn = __ldg(&g_hs[n]);
+                    Y[j * TS + tidx(n, m)] = L.y1 * sn;
+                    if (DIP) D[j * TS + tidx(n, m)] = L.d1 * sn;
+                }
+            }
+            __syncthreads();
+            // phase C: accumulate into this thread's coefficients
+#pragma unroll
+            for (int q = 0; q < kHFormPer; q++) {
+                const int n = en[q];
+                if (n < 0) continue;
+                const int m = em_[q], am = m < 0 ? -m : m, ti = tidx(n, am);
+                for (int j = 0; j < nb; j++) {
+                    const double *S = Sc + j * 16;
+                    const double st = S[1];
+                    double2 E = Em[j * P1 + am];
+                    if (m < 0) E = cconj(E);
+                    const double ys = Y[j * TS + ti];
+                    if (CHG) {
+                        const double yr = am == 0 ? ys : ys * st;
+                        cfma(acc[q], cmul(cmk(S[2], S[3]), cscal(yr, F[j * W + n])), E);
+                    }
+                    if (DIP) {
+                        const double dd = D[j * TS + ti];
+                        const double2 fd = Fd[j * P1 + n], fu = Fu[j * P1 + n];
+                        double2 A, B = cmk(0, 0);
+                        if (am == 0) A = csub(cscal(ys * S[6], fd), cscal(dd * st * S[7], fu));
+                        else {
+                            A = csub(cscal(ys * st * S[6], fd), cscal(dd * S[7], fu));
+                            B = cscal((m > 0 ? am : -am) * ys * S[8], fu);
                         }
-                        if (DIP) {
-                            // radial derivative and the 1/r angular factor
-                            double2 fd, fu;
-                            if (IRREG) {
-                                fd = n == 0 ? cscal(-1.0 / sc, f[1])
-                                            : csub(cscal(sc, f[n - 1]), cmul(cscal(n + 1.0, zi), f[n]));
-                                fu = cscal(1.0 / gg[0], f[n]);
-                            } else {
-                                double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
-                                fd = n == 0 ? cscal(-sc, f[1])
-                                            : csub(cscal(d1 / sc, f[n - 1]), cscal(d2 * sc, f[n + 1]));
-                                double2 t = n == 0 ? cmk(0, 0) : cadd(cscal(sc, f[n + 1]), cscal(1.0 / sc, f[n - 1]));
-                                fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, t));
-                            }
-                            fd = cmul(fd, zk);
-                            double2 A, B = cmk(0, 0);
-                            if (m == 0) A = csub(cscal(y * gg[9], fd), cscal(dd * st * gg[10], fu));
-                            else {
-                                A = csub(cscal(y * st * gg[9], fd), cscal(dd * gg[10], fu));
-                                B = cscal(m * y * gg[11], fu);
-                            }
-                            double2 Ad = cmul(ds, A), Bd = cmul(ds, B);
-                            // (n, m): ds E (A - iB); (n, -m): ds conj(E) (A + iB)
-                            vm = cadd(vm, cmul(em, cmk(Ad.x + Bd.y, Ad.y - Bd.x)));
-                            vp = cadd(vp, cmul(cconj(em), cmk(Ad.x - Bd.y, Ad.y + Bd.x)));
-                        }
-                        acc[eidx(n, m)] = cadd(acc[eidx(n, m)], vm);
-                        if (m > 0) acc[eidx(n, -m)] = cadd(acc[eidx(n, -m)], vp);
+                        // ds E (A - i sgn(m) B)
+                        const double2 AB = cmk(A.x + B.y, A.y - B.x);
+                        cfma(acc[q], cmul(cmk(S[4], S[5]), AB), E);
                     }
                 }
             }
         }
     }
-    __syncthreads();
     double2 *o = exps + (size_t)b * NC;
     const double2 ik = cmk(-zk.y, zk.x);
-    for (int e = threadIdx.x; e < K; e += blockDim.x) {
-        double2 t = hsm[e];
-        for (int w = 1; w < kHWarps; w++) t = cadd(t, hsm[(size_t)w * K + e]);
-        o[e] = cadd(o[e], cmul(t, ik));
+#pragma unroll
+    for (int q = 0; q < kHFormPer; q++) {
+        const int e = e0 + threadIdx.x + q * kHFormThreads;
+        if (e < K) o[e] = cadd(o[e], cmul(acc[q], ik));
     }
-}
-
-static size_t hform_smem(int p)
-{
-    int K = (p + 1) * (p + 1), W = p + 2;
-    return sizeof(double2) * ((size_t)kHWarps * K + (size_t)kHWarps * 32 * W) + sizeof(double) * kHWarps * 32 * 12;
 }
 
 __host__ __device__ static int max_p(const HLevels &lv)
@@ -736,21 +782,24 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
     bool c = ifcharge == 1, d = ifdipole == 1;
     if (!c && !d) return;
     htab_init(s, st);
-    size_t sm = hform_smem(max_p(lv));
-#define FMM_HF(IR, C, D)                                                                                       \
-    do {                                                                                                       \
-        FMM_TRY(st, cudaFuncSetAttribute(k_hform<IR, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-        k_hform<IR, C, D><<<nboxes, kHWarps * 32, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);                   \
-        FMM_COUNT_LAUNCH();                                                                                    \
+    const int pm = max_p(lv);
+    const dim3 grid(nboxes, div_up((pm + 1) * (pm + 1), kHFormThreads * kHFormPer));
+#define FMM_HF(IR, C, D, CHV)                                                                                 \
+    do {                                                                                                      \
+        size_t sm = sizeof(double) * HFormSmem<CHV, D>::doubles(pm);                                         \
+        FMM_TRY(st, cudaFuncSetAttribute(k_hform<IR, C, D, CHV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)sm));                                                           \
+        k_hform<IR, C, D, CHV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);           \
+        FMM_COUNT_LAUNCH();                                                                                   \
     } while (0)
     if (irreg) {
-        if (c && d) FMM_HF(true, true, true);
-        else if (c) FMM_HF(true, true, false);
-        else FMM_HF(true, false, true);
+        if (c && d) FMM_HF(true, true, true, 8);
+        else if (c) FMM_HF(true, true, false, 16);
+        else FMM_HF(true, false, true, 8);
     } else {
-        if (c && d) FMM_HF(false, true, true);
-        else if (c) FMM_HF(false, true, false);
-        else FMM_HF(false, false, true);
+        if (c && d) FMM_HF(false, true, true, 8);
+        else if (c) FMM_HF(false, true, false, 16);
+        else FMM_HF(false, false, true, 8);
     }
 #undef FMM_HF
     FMM_LAUNCH_CHECK(st);
@@ -759,27 +808,30 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
 // L2P (h3dtaeval_trunc0, src/helmrouts3d.f:2732) at the leaf's own local
 // expansion when its level is >= 2, and M2P (h3dmpeval_trunc0, :2405) of the
 // multipoles of its list-3 boxes, at the leaf's sources and targets.  CTA per
-// leaf; per expansion the coefficients are staged in shared memory; per batch
-// of 32 points, lane j computes the radial functions of point j, then the
-// warp walks the batch with lane per order m and reduces pot, d/dr, d/dtheta
-// and d/dphi across lanes.
-__global__ void __launch_bounds__(kHWarps * 32) k_heval(const int *leaves, TreeView tv, const double *sx,
-                                                       const double *sy, const double *sz, const double *tx,
-                                                       const double *ty, const double *tz, HLevels lv, int NC,
-                                                       double2 zk, const double2 *mpole, const double2 *local,
-                                                       OutSoA outs, OutSoA outt, int do_src, int do_trg)
+// leaf, one evaluation point per thread; per expansion the coefficients are
+// staged in shared memory and read by all threads of a warp at once
+// (broadcast), each thread keeps its point's radial functions in a shared
+// column, and walks the orders m (outer) and degrees n (inner) with the
+// Legendre column recurrence in registers.
+constexpr int kHEvalThreads = 128;
+
+__global__ void __launch_bounds__(kHEvalThreads) k_heval(const int *leaves, TreeView tv, const double *sx,
+                                                        const double *sy, const double *sz, const double *tx,
+                                                        const double *ty, const double *tz, HLevels lv, int NC,
+                                                        double2 zk, const double2 *mpole, const double2 *local,
+                                                        OutSoA outs, OutSoA outt, int do_src, int do_trg)
 {
     extern __shared__ double2 hsm[];
+    constexpr int T = kHEvalThreads;
     const int b = leaves[blockIdx.x];
     const int blev = tv.level[b];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
     if (ne == 0) return;
     const int pm = max_p(lv);
-    const int KM = (pm + 1) * (pm + 1), W = pm + 2;
+    const int KM = (pm + 1) * (pm + 1);
     double2 *E = hsm;
-    double2 *F = hsm + KM + (size_t)warp * 32 * W;
-    double *geo = (double *)(hsm + KM + (size_t)kHWarps * 32 * W) + warp * 32 * 6;
+    double2 *Fs = hsm + KM;  // radial functions, [n][thread]
+    const int t = threadIdx.x;
     const int l3a = tv.l3_start[b], nl3 = tv.l3_start[b + 1] - l3a;
     for (int xi = -1; xi < nl3; xi++) {
         int eb;
@@ -796,103 +848,87 @@ __global__ void __launch_bounds__(kHWarps * 32) k_heval(const int *leaves, TreeV
         const int K = (p + 1) * (p + 1);
         const double2 *ex = (isloc ? local : mpole) + (size_t)eb * NC;
         __syncthreads();
-        for (int i = threadIdx.x; i < K; i += blockDim.x) E[i] = ex[i];
+        for (int i = t; i < K; i += T) E[i] = ex[i];
         __syncthreads();
         const double *c = tv.center + 3L * eb;
-        for (int c0 = warp * 32; c0 < ne; c0 += kHWarps * 32) {
-            const int nb = min(32, ne - c0);
-            __syncwarp();
-            if (lane < nb) {
-                int e = c0 + lane;
-                double px, py, pz;
-                if (e < ns) { int i = tv.src0[b] + e; px = sx[i]; py = sy[i]; pz = sz[i]; }
-                else { int i = tv.trg0[b] + e - ns; px = tx[i]; py = ty[i]; pz = tz[i]; }
-                PtGeo g = pt_geo(px - c[0], py - c[1], pz - c[2]);
-                double2 *f = F + lane * W;
-                double2 z = cscal(g.r, zk);
-                bool ok;
-                if (isloc) ok = bess_dev(p > 1 ? p : 1, z, sc, f, nullptr) == 0;
-                else {
-                    ok = cabsd(z) >= 1.0e-15;
-                    if (ok) hank_dev(p > 1 ? p : 1, z, sc, f, nullptr);
-                }
-                double *gg = geo + lane * 6;
-                gg[0] = ok ? g.r : -1.0; gg[1] = g.ct; gg[2] = g.st; gg[3] = g.cp; gg[4] = g.sp;
+        for (int c0 = 0; c0 < ne; c0 += T) {
+            const int e = c0 + t;
+            if (e >= ne) continue;
+            const bool is_src = e < ns;
+            const int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
+            double px = is_src ? sx[i] : tx[i], py = is_src ? sy[i] : ty[i], pz = is_src ? sz[i] : tz[i];
+            const PtGeo g = pt_geo(px - c[0], py - c[1], pz - c[2]);
+            double2 *f = Fs + t;
+            const double2 z = cscal(g.r, zk);
+            if (isloc) {
+                if (bess_dev(p > 1 ? p : 1, z, sc, f, nullptr, T)) continue;
+            } else {
+                if (cabsd(z) < 1.0e-15) continue;
+                hank_dev(p > 1 ? p : 1, z, sc, f, nullptr, T);
             }
-            __syncwarp();
-            for (int j = 0; j < nb; j++) {
-                const double *gg = geo + j * 6;
-                if (gg[0] < 0) continue;  // uniform over the warp
-                const double2 *f = F + j * W;
-                const double r = gg[0], ct = gg[1], st = gg[2], cp = gg[3], sp = gg[4];
-                const double2 zi = cdiv(cmk(1, 0), cscal(r, zk));
-                const double phi = atan2(sp, cp);
-                double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
-                for (int m = lane; m <= p; m += 32) {
-                    double es, ec;
-                    sincos(m * phi, &es, &ec);
-                    const double2 ep = cmk(ec, es);  // e^{i m phi}
-                    LegCol L;
-                    L.start(m, ct, -st);
-                    for (int n = m; n <= p; n++) {
-                        if (n > m) L.step(n);
-                        const double sn = __ldg(&g_hs[n]);
-                        const double y = L.y1 * sn, dd = L.d1 * sn;
-                        double2 fd, fu;
-                        if (isloc) {
-                            double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
-                            fd = n == 0 ? cscal(-sc, f[1]) : csub(cscal(d1 / sc, f[n - 1]), cscal(d2 * sc, f[n + 1]));
-                            double2 t = n == 0 ? cmk(0, 0) : cadd(cscal(sc, f[n + 1]), cscal(1.0 / sc, f[n - 1]));
-                            fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, t));
-                        } else {
-                            fd = n == 0 ? cscal(-1.0 / sc, f[1]) : csub(cscal(sc, f[n - 1]), cmul(cscal(n + 1.0, zi), f[n]));
-                            fu = cscal(1.0 / r, f[n]);
+            const double r = g.r, ct = g.ct, st = g.st, u = -st;
+            const double2 zi = cdiv(cmk(1, 0), z), e1 = cmk(g.cp, g.sp);
+            double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
+            double2 em = cmk(1, 0);
+            double ymm = 1.0;
+            for (int m = 0; m <= p; m++) {
+                if (m == 1) ymm = -sqrt(0.5);
+                else if (m > 1) ymm *= u * __ldg(&g_hc[m]);
+                if (m > 0) em = cmul(em, e1);
+                LegCol L;
+                L.x = ct;
+                L.m = m;
+                L.w = m == 0 ? 1.0 : u * u;
+                L.y1 = ymm;
+                L.d1 = m == 0 ? 0.0 : ymm * (-m) * ct;
+                L.y2 = 0;
+                L.d2 = 0;
+                for (int n = m; n <= p; n++) {
+                    if (n > m) L.step(n);
+                    const double sn = __ldg(&g_hs[n]);
+                    const double y = L.y1 * sn, dd = L.d1 * sn;
+                    const double2 fn = f[n * T];
+                    double2 fd, fu;
+                    if (isloc) {
+                        if (n == 0) { fd = cscal(-sc, f[T]); fu = cmk(0, 0); }
+                        else {
+                            const double2 fm = f[(n - 1) * T], fp = f[(n + 1) * T];
+                            const double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
+                            fd = csub(cscal(d1 / sc, fm), cscal(d2 * sc, fp));
+                            fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, cadd(cscal(sc, fp), cscal(1.0 / sc, fm))));
                         }
-                        fd = cmul(fd, zk);
-                        if (m == 0) {
-                            double2 a = E[eidx(n, 0)];
-                            cfma(pot, f[n], cscal(y, a));
-                            cfma(ur, fd, cscal(y, a));
-                            cfma(ut, fu, cscal(-dd * st, a));
-                        } else {
-                            double2 z2 = cmul(E[eidx(n, m)], ep), z3 = cmul(E[eidx(n, -m)], cconj(ep));
-                            double2 zs = cadd(z2, z3), zd = csub(z2, z3);
-                            cfma(pot, f[n], cscal(y * st, zs));
-                            cfma(ur, fd, cscal(y * st, zs));
-                            cfma(ut, fu, cscal(-dd, zs));
-                            cfma(up, fu, cscal(y * m, cmk(-zd.y, zd.x)));  // i m (z2 - z3)
-                        }
+                    } else {
+                        fd = n == 0 ? cscal(-1.0 / sc, f[T]) : csub(cscal(sc, f[(n - 1) * T]), cmul(cscal(n + 1.0, zi), fn));
+                        fu = cscal(1.0 / r, fn);
+                    }
+                    fd = cmul(fd, zk);
+                    if (m == 0) {
+                        const double2 a = E[eidx(n, 0)];
+                        cfma(pot, fn, cscal(y, a));
+                        cfma(ur, fd, cscal(y, a));
+                        cfma(ut, fu, cscal(-dd * st, a));
+                    } else {
+                        const double2 z2 = cmul(E[eidx(n, m)], em), z3 = cmul(E[eidx(n, -m)], cconj(em));
+                        const double2 zs = cadd(z2, z3), zd = csub(z2, z3);
+                        cfma(pot, fn, cscal(y * st, zs));
+                        cfma(ur, fd, cscal(y * st, zs));
+                        cfma(ut, fu, cscal(-dd, zs));
+                        cfma(up, fu, cscal(y * m, cmk(-zd.y, zd.x)));  // i m (z2 - z3)
                     }
                 }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    pot.x += __shfl_xor_sync(0xffffffffu, pot.x, o);
-                    pot.y += __shfl_xor_sync(0xffffffffu, pot.y, o);
-                    ur.x += __shfl_xor_sync(0xffffffffu, ur.x, o);
-                    ur.y += __shfl_xor_sync(0xffffffffu, ur.y, o);
-                    ut.x += __shfl_xor_sync(0xffffffffu, ut.x, o);
-                    ut.y += __shfl_xor_sync(0xffffffffu, ut.y, o);
-                    up.x += __shfl_xor_sync(0xffffffffu, up.x, o);
-                    up.y += __shfl_xor_sync(0xffffffffu, up.y, o);
-                }
-                if (lane == 0) {
-                    // fld = -(ur r-hat + ut theta-hat + up phi-hat)
-                    double2 fx = cadd(cadd(cscal(st * cp, ur), cscal(ct * cp, ut)), cscal(-sp, up));
-                    double2 fy = cadd(cadd(cscal(st * sp, ur), cscal(ct * sp, ut)), cscal(cp, up));
-                    double2 fz = csub(cscal(ct, ur), cscal(st, ut));
-                    int e = c0 + j;
-                    const bool is_src = e < ns;
-                    double2 *po = is_src ? outs.pot : outt.pot;
-                    double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy;
-                    double2 *oz = is_src ? outs.fz : outt.fz;
-                    int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
-                    if (po) po[i] = cadd(po[i], pot);
-                    if (ox) {
-                        ox[i] = csub(ox[i], fx);
-                        oy[i] = csub(oy[i], fy);
-                        oz[i] = csub(oz[i], fz);
-                    }
-                }
+            }
+            // fld = -(ur r-hat + ut theta-hat + up phi-hat)
+            const double cp = g.cp, sp = g.sp;
+            const double2 fx = cadd(cadd(cscal(st * cp, ur), cscal(ct * cp, ut)), cscal(-sp, up));
+            const double2 fy = cadd(cadd(cscal(st * sp, ur), cscal(ct * sp, ut)), cscal(cp, up));
+            const double2 fz = csub(cscal(ct, ur), cscal(st, ut));
+            double2 *po = is_src ? outs.pot : outt.pot;
+            double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy, *oz = is_src ? outs.fz : outt.fz;
+            if (po) po[i] = cadd(po[i], pot);
+            if (ox) {
+                ox[i] = csub(ox[i], fx);
+                oy[i] = csub(oy[i], fy);
+                oz[i] = csub(oz[i], fz);
             }
         }
     }
@@ -906,11 +942,10 @@ void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const doub
     if (nleaves == 0 || !st.ok() || (!do_src && !do_trg)) return;
     htab_init(s, st);
     int pm = max_p(lv);
-    size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)kHWarps * 32 * (pm + 2)) +
-                sizeof(double) * kHWarps * 32 * 6;
+    size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * kHEvalThreads);
     FMM_TRY(st, cudaFuncSetAttribute(k_heval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_heval<<<nleaves, kHWarps * 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
-                                              outt, do_src, do_trg); FMM_COUNT_LAUNCH();
+    k_heval<<<nleaves, kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
+                                               outt, do_src, do_trg); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
 
