@@ -4,23 +4,33 @@
 Workload (one "step" = one lfmm3dparttarg call): N = 2,000,000 sources and
 M = 2,000,000 separate targets, both uniform in the unit cube; complex charges
 and dipole strengths with parts uniform in [-1, 1]; dipole directions uniform on
-the unit sphere; iprec = 1; potential and field at sources and targets, FP64.
-Inputs are seeded synthetic data (no dataset is involved).
+the unit sphere; iprec = 1; potential and field at sources and targets.
+Inputs are seeded synthetic data (no dataset is involved).  The step runs in
+two arithmetic forms: "mixed" (FP32 compensated P2P and FP32 M2L operators,
+FP64 elsewhere; the headline) and "fp64" (the reference's arithmetic
+throughout), both reported.
 
-  value     points/s = (N + M) * steps / device time, inputs resident in HBM
-            (fmm3d_lfmm3dparttarg_device), max over ranks.
+  value     points/s = (N + M) * steps / device time of the mixed form, inputs
+            resident in HBM (fmm3d_lfmm3dparttarg_device), max over ranks.
   e2e       the same metric through the Fortran C ABI (lfmm3dparttarg_) with
             pinned host arrays: H2D of inputs and D2H of outputs inside the
             timed region.
   roofline  the dominant pass of the step, from the library's per-pass CUDA
-            events, against the FP64 peak measured in the same run (cuBLAS
-            DGEMM, float64 8192^3) -- MEASURED_PEAKS.json holds no FP64 figure.
+            events, against the FP32 (mixed) or FP64 (fp64 form) GEMM rate
+            measured in the same run (cuBLAS 8192^3) -- MEASURED_PEAKS.json
+            holds only HBM and bf16 figures, and the dominant passes are
+            CUDA-core arithmetic.
   errors    relative L2 error vs the FP64 direct sum at 1,000 seeded sources
             (self excluded) and 1,000 seeded targets, per output.
   cpu_baseline  the C restatement of the reference (oracle/, OpenMP, all host
             cores) on a bounded sample (N = M = 500,000 of the same
             distribution); the Fortran reference cannot be compiled (no
             Fortran compiler on either machine).
+  helmholtz the Helmholtz workload measured in the same run (not the
+            headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
+            unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
+            FP64, with its errors, per-pass times and a CPU sample of the
+            restatement (100,000 sources).
 
 Multi-GPU: an FMM call does not shard; `--gpus N` runs N independent replicas
 (one per rank, scaling "weak"), timed as the max over ranks.
@@ -62,6 +72,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-samples", type=int, default=1000)
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
+    ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
+    ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
     return ap.parse_args(argv)
 
 
@@ -75,6 +87,32 @@ def make_inputs(n, m, seed):
     dv = rng.normal(size=(n, 3))
     dv /= np.linalg.norm(dv, axis=1)[:, None]
     return src, q, dq, dv, trg
+
+
+HELM_ZK = 8 * np.pi
+HELM_IPREC = 2
+
+
+def helm_inputs(n, seed=3):
+    """Sphere of radius 1 (normalized Gaussian directions), charges uniform in the unit disk."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    src = v / np.linalg.norm(v, axis=1)[:, None]
+    r, a = np.sqrt(rng.random(n)), rng.random(n) * 2 * np.pi
+    q = np.stack([r * np.cos(a), r * np.sin(a)], -1)
+    return src, q
+
+
+def cpu_helm_sample(n):
+    """One hfmm3dpartself restatement call on the sphere workload with n sources; returns seconds."""
+    import oracle
+    src, q = helm_inputs(n, seed=5)
+    t0 = time.perf_counter()
+    ier = oracle.hfmm3dparttarg(HELM_IPREC, HELM_ZK, src, q[:, 0] + 1j * q[:, 1])[0]
+    t1 = time.perf_counter()
+    if ier != 0:
+        raise RuntimeError("oracle ier=%d" % ier)
+    return t1 - t0
 
 
 def dist_env():
@@ -306,6 +344,70 @@ def run_e2e(args, R):
             "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * dt / args.steps, "host_memory": "pinned"}
 
 
+def run_helm(args, R):
+    """The Helmholtz sphere workload on the device (hfmm3dpartself, FP64)."""
+    torch, F = R["torch"], R["F"]
+    n = args.helm_n
+    src, q = helm_inputs(n, seed=3 + R["rank"])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_src, d_q = torch.from_numpy(src).to(dev), torch.from_numpy(q).to(dev)
+    d_pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        ier = F.hfmm3dparttarg_device(HELM_IPREC, HELM_ZK, d_src, d_q, None, None, d_pot, d_fld, stream=stream)
+        if ier != 0:
+            raise RuntimeError("Helmholtz FMM ier=%d: %s" % (ier, F.last_error()))
+
+    F.set_timing(True)
+    for w in range(args.warmup):
+        F.set_stats(w == args.warmup - 1)
+        step()
+    F.set_stats(False)
+    stats = F.last_stats()
+    torch.cuda.synchronize()
+    if R["dist"] is not None:
+        R["dist"].barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    passes = []
+    ev[0].record()
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record()
+        passes.append(F.last_timing())
+    torch.cuda.synchronize()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    if R["dist"] is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        R["dist"].all_reduce(t, op=R["dist"].ReduceOp.MAX)
+        total_ms = float(t.item())
+    # errors at 1,000 seeded sources against the FP64 direct sum
+    rng = np.random.default_rng(98)
+    k = min(args.err_samples, n)
+    si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
+    dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
+    df = torch.empty((k, 6), dtype=torch.float64, device=dev)
+    it = torch.from_numpy(si).to(dev)
+    ier = F.hdirect_points_device(HELM_ZK, d_src, d_q, None, None, d_src[it.long()].contiguous(), it, dp, df,
+                                  stream=stream)
+    torch.cuda.synchronize()
+    if ier != 0:
+        raise RuntimeError("Helmholtz direct ier=%d" % ier)
+    errs = {"pot": float(torch.linalg.norm(d_pot[it.long()] - dp) / torch.linalg.norm(dp)),
+            "fld": float(torch.linalg.norm(d_fld[it.long()] - df) / torch.linalg.norm(df))}
+    mean = {kk: round(float(np.mean([p[kk] for p in passes])), 3) for kk in passes[0]}
+    out = {"workload": "helmholtz_hfmm3dpartself_sphere_%dk_zk_8pi_iprec2" % (n // 1000), "n_sources": n,
+           "zk": "8*pi", "iprec": HELM_IPREC, "dtype": "f64",
+           "value": R["ws"] * n * args.steps / (total_ms * 1e-3), "unit": UNIT,
+           "ms_per_step": total_ms / args.steps, "p50_ms": float(np.percentile(step_ms, 50)),
+           "p99_ms": float(np.percentile(step_ms, 99)), "errors": {kk: float("%.3e" % v) for kk, v in errs.items()},
+           "pass_ms_mean": mean, "stats": {kk: v for kk, v in stats.items() if kk != "m2l_pt_hist"},
+           "p2p_pairs_per_s": stats.get("p2p_pairs", 0) / (mean["p2p"] * 1e-3) if mean.get("p2p") else None}
+    return out
+
+
 def roofline_of(M, peak, bound):
     """Roofline of the dominant pass of one form, from the per-pass CUDA events of its timed steps."""
     keys = [k for k in M["passes"][0] if k not in ("total",)]
@@ -355,6 +457,11 @@ def run_reference(args):
         times.append(dt)
     v = 2 * n * len(times) / sum(times)
     cores = int(os.environ["OMP_NUM_THREADS"])
+    helm = None
+    if args.helm_n > 0 and args.helm_cpu_sample > 0:
+        dt = cpu_helm_sample(args.helm_cpu_sample)
+        helm = {"workload": "helmholtz_hfmm3dpartself_sphere_zk_8pi_iprec2", "value": args.helm_cpu_sample / dt,
+                "unit": UNIT, "sample": "%d sources, one call (%.1f s)" % (args.helm_cpu_sample, dt)}
     sample = "N=M=%d uniform cube, charges+dipoles, iprec=%d, one lfmm3dparttarg restatement call per step" % (
         n, args.iprec)
     return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
@@ -363,7 +470,8 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(args, ws), "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores,
                                                              "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "helmholtz": helm}
 
 
 def config_of(args, ws):
@@ -406,13 +514,22 @@ def main(argv=None):
                                                   gpu_launches=int(sum(R["forms"]["fp64"]["launches"])))},
             "stats": {k: v for k, v in H["stats"].items() if k != "m2l_pt_hist"}}
     line["forms"]["mixed_over_fp64"] = round(head["value"] / line["forms"]["fp64"]["value"], 3)
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
     if rank == 0 and ws == 1 and not args.no_cpu:
-        os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         dt, pts = cpu_fmm_sample(args.cpu_sample, args.iprec)
         line["cpu_baseline"] = {"value": pts / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
                                 "kind": "port",
                                 "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
                                     args.cpu_sample, args.iprec, dt)}
+    if args.helm_n > 0:
+        H2 = run_helm(args, R)
+        if rank == 0 and ws == 1 and not args.no_cpu and args.helm_cpu_sample > 0:
+            dt = cpu_helm_sample(args.helm_cpu_sample)
+            H2["cpu_baseline"] = {"value": args.helm_cpu_sample / dt, "unit": UNIT,
+                                  "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+                                  "sample": "%d sources, same distribution, one call (%.1f s)" % (
+                                      args.helm_cpu_sample, dt)}
+        line["helmholtz"] = H2
     if R["dist"] is not None:
         R["dist"].barrier()
         R["dist"].destroy_process_group()
