@@ -122,6 +122,16 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_max(dist, value, device):
+    """Max of a per-rank float over all ranks (the replicas' device time); plain value on one rank."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
 
@@ -286,10 +296,7 @@ def run_b200(args):
         clocks = clk.stop()
         step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
         total_ms = ev[0].elapsed_time(ev[args.steps])
-        if ws > 1:
-            t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = reduce_max(dist if ws > 1 else None, total_ms, dev)
         return dict(total_ms=total_ms, step_ms=step_ms, passes=passes, launches=launches, stats=F.last_stats(),
                     clocks=clocks, errs=errors())
 
@@ -334,10 +341,7 @@ def run_e2e(args, R):
         call()  # synchronous: returns after the outputs are in host memory
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    if R["dist"] is not None:
-        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        R["dist"].all_reduce(t, op=R["dist"].ReduceOp.MAX)
-        dt = float(t.item())
+    dt = reduce_max(R["dist"], dt, "cuda")
     h2d = n * (24 + 16 + 16 + 24) + m * 24
     d2h = n * (16 + 48) + m * (16 + 48)
     return {"value": R["ws"] * (n + m) * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -379,10 +383,7 @@ def run_helm(args, R):
     torch.cuda.synchronize()
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[args.steps])
-    if R["dist"] is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        R["dist"].all_reduce(t, op=R["dist"].ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_max(R["dist"], total_ms, dev)
     # errors at 1,000 seeded sources against the FP64 direct sum
     rng = np.random.default_rng(98)
     k = min(args.err_samples, n)
