@@ -74,6 +74,9 @@ def parse_args(argv=None):
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
     ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
     ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
+    ap.add_argument("--workload", choices=["all", "laplace", "helmholtz"], default="all",
+                    help="all: the Laplace headline line with the Helmholtz object (default); "
+                         "laplace / helmholtz: one workload only (profiling runs)")
     return ap.parse_args(argv)
 
 
@@ -491,6 +494,18 @@ def main(argv=None):
         if line is not None:
             print(json.dumps(line), flush=True)
         return 0
+    if args.workload == "helmholtz":
+        import torch
+        import fmmlib3d_b200 as F
+        torch.cuda.set_device(dist_env()[2])
+        R = dict(torch=torch, F=F, rank=rank, ws=1, dist=None)
+        out = run_helm(args, R)
+        print(json.dumps({"metric": "Helmholtz FMM pts/s (sphere, zk=8pi, iprec=2)", "value": out["value"],
+                          "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                          "helmholtz": out}), flush=True)
+        return 0
+    if args.workload == "laplace":
+        args.helm_n = 0
     R = run_b200(args)
     R["F"].set_precision(1)
     e2e = None if args.no_e2e else run_e2e(args, R)
