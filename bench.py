@@ -26,6 +26,16 @@ throughout), both reported.
             cores) on a bounded sample (N = M = 500,000 of the same
             distribution); the Fortran reference cannot be compiled (no
             Fortran compiler on either machine).
+  laplace_sphere  the CPU-runnable Laplace workload measured in the same run:
+            lfmm3dpartself on 100,000 sources on the unit sphere (seed 1),
+            charges only, iprec = 1, FP64, with the CPU restatement timed on
+            the same input.
+  serving   the request loop of fmmlib3d_b200.serving (4 slots, admission by
+            projected HBM footprint) on a seeded stream of requests (70%
+            Laplace, 30% Helmholtz with zk uniform in [1, 20], N log-uniform in
+            [1e3, 1e6], iprec in {0, 1, 2}, cube / Plummer / ellipsoid
+            geometries), Poisson arrivals at swept rates: p50/p99 latency and
+            points/s per rate (host arrays in and out, copies included).
   helmholtz the Helmholtz workload measured in the same run (not the
             headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
             unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
@@ -74,6 +84,8 @@ def parse_args(argv=None):
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
     ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
     ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
+    ap.add_argument("--serve-requests", type=int, default=40, help="requests per serving rate (0: skip)")
+    ap.add_argument("--serve-rates", default="10,40,inf", help="Poisson arrival rates (requests/s)")
     ap.add_argument("--workload", choices=["all", "laplace", "helmholtz"], default="all",
                     help="all: the Laplace headline line with the Helmholtz object (default); "
                          "laplace / helmholtz: one workload only (profiling runs)")
@@ -104,6 +116,81 @@ def helm_inputs(n, seed=3):
     r, a = np.sqrt(rng.random(n)), rng.random(n) * 2 * np.pi
     q = np.stack([r * np.cos(a), r * np.sin(a)], -1)
     return src, q
+
+
+def sphere_inputs(n, seed=1):
+    """Unit-sphere surface (normalized Gaussian directions), charges with parts uniform in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    src = v / np.linalg.norm(v, axis=1)[:, None]
+    return src, rng.uniform(-1, 1, (n, 2))
+
+
+def run_laplace_sphere(args, R, n=100_000):
+    """lfmm3dpartself on the sphere workload: device time (FP64 form), errors, CPU restatement time."""
+    torch, F = R["torch"], R["F"]
+    src, q = sphere_inputs(n)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_src, d_q = torch.from_numpy(src).to(dev), torch.from_numpy(q).to(dev)
+    d_pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    F.set_precision(0)
+
+    def step():
+        ier = F.lfmm3dparttarg_device(1, d_src, d_q, None, None, d_pot, d_fld, stream=stream)
+        if ier != 0:
+            raise RuntimeError("sphere FMM ier=%d: %s" % (ier, F.last_error()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(args.steps):
+        step()
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    rng = np.random.default_rng(97)
+    k = min(args.err_samples, n)
+    si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
+    it = torch.from_numpy(si).to(dev)
+    dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
+    df = torch.empty((k, 6), dtype=torch.float64, device=dev)
+    F.direct_points_device(d_src, d_q, None, None, d_src[it.long()].contiguous(), it, dp, df, stream=stream)
+    torch.cuda.synchronize()
+    out = {"workload": "laplace_lfmm3dpartself_sphere_100k_iprec1", "n_sources": n, "iprec": 1, "dtype": "f64",
+           "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "errors": {"pot": float("%.3e" % float(torch.linalg.norm(d_pot[it.long()] - dp) / torch.linalg.norm(dp))),
+                      "fld": float("%.3e" % float(torch.linalg.norm(d_fld[it.long()] - df) / torch.linalg.norm(df)))}}
+    if R["rank"] == 0 and not args.no_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        oracle.lfmm3dparttarg(1, src, q[:, 0] + 1j * q[:, 1])
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
+                               "kind": "port", "sample": "the whole workload, one call (%.2f s)" % dt}
+    return out
+
+
+def run_serving(args):
+    """Swept-rate serving measurement (one warm-up pass over the same requests first)."""
+    from fmmlib3d_b200.serving import FMMServer, make_request_stream, run_stream
+    reqs = make_request_stream(args.serve_requests, seed=7)
+    srv = FMMServer(slots=4)
+    out = {"slots": 4, "requests_per_rate": len(reqs), "mean_n": float(np.mean([len(r.source) for r in reqs])),
+           "laplace_fraction": float(np.mean([r.kernel == "laplace" for r in reqs])), "rates": []}
+    try:
+        run_stream(srv, reqs, float("inf"))  # warm-up: plans, pools
+        for rate in [float(x) for x in args.serve_rates.split(",")]:
+            st, _ = run_stream(srv, reqs, rate, seed=int(rate) if rate != float("inf") else 0)
+            st["rate_hz"] = None if rate == float("inf") else rate
+            out["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()})
+        out["max_on_gpu"] = srv.max_running
+    finally:
+        srv.close()
+    return out
 
 
 def cpu_helm_sample(n):
@@ -537,6 +624,9 @@ def main(argv=None):
                                 "kind": "port",
                                 "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
                                     args.cpu_sample, args.iprec, dt)}
+    line["laplace_sphere"] = run_laplace_sphere(args, R)
+    if args.serve_requests > 0 and ws == 1:
+        line["serving"] = run_serving(args)
     if args.helm_n > 0:
         H2 = run_helm(args, R)
         if rank == 0 and ws == 1 and not args.no_cpu and args.helm_cpu_sample > 0:

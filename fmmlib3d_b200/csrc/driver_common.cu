@@ -1,4 +1,6 @@
 // Definitions for driver_common.cuh.
+#include <mutex>
+
 #include "driver_common.cuh"
 
 namespace fmm {
@@ -22,6 +24,8 @@ cudaStream_t thread_stream()
 // instead of returning it to the driver at every synchronisation.
 void keep_pool_memory()
 {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
     static bool done[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);

@@ -1,5 +1,7 @@
 // Helmholtz FMM kernels (FP64): special functions, P2M/P2L, L2P/M2P,
 // z-shift operators, rotate-shift-rotate translations, P2P and the direct sum.
+#include <mutex>
+
 #include "helm_kernels.cuh"
 
 namespace fmm {
@@ -525,12 +527,15 @@ __global__ void k_htab_init()
 
 static void htab_init(cudaStream_t s, Status &st)
 {
+    static std::mutex mu;  // several host threads may make their first call at once
+    std::lock_guard<std::mutex> lk(mu);
     static bool done[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && done[dev]) return;
     k_htab_init<<<div_up(kHTab * kHTab, 256), 256, 0, s>>>(); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
+    FMM_TRY(st, cudaStreamSynchronize(s));  // other threads' streams may read the tables next
     if (st.ok() && dev >= 0 && dev < 64) done[dev] = true;
 }
 
