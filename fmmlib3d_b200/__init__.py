@@ -50,6 +50,9 @@ _lib.fmm3d_h3dpartdirect_device.argtypes = [_P, _I, _P, _I, _P, _I, _P, _P, _I, 
                                             _P]
 _lib.fmm3d_h3ddirect_points_device.restype = _I
 _lib.fmm3d_h3ddirect_points_device.argtypes = [_P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _P]
+_lib.fmm3d_lfmm3dparttarg_batched_device.restype = _I
+_lib.fmm3d_lfmm3dparttarg_batched_device.argtypes = [_I, _I, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _I,
+                                                     _P, _I, _P, _P]
 _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
@@ -171,6 +174,26 @@ def direct_points_device(source, charge, dipstr, dipvec, pts, skip, pot, fld, st
     return _lib.fmm3d_l3ddirect_points_device(
         source.shape[0], ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
         ptr(dipvec), pts.shape[0], ptr(pts), ptr(skip), ptr(pot), ptr(fld), _P(stream))
+
+
+def lfmm3dparttarg_batched_device(iprec, src_offsets, source, charge, dipstr, dipvec, pot, fld, trg_offsets=None,
+                                  target=None, pottarg=None, fldtarg=None, stream=0):
+    """Many independent Laplace FMMs in one call on device-resident torch tensors.
+
+    ``src_offsets`` (ninst+1 ints, from 0): instance i owns rows
+    src_offsets[i]:src_offsets[i+1] of the concatenated ``source``/``charge``/...
+    arrays (layouts as lfmm3dparttarg_device); ``trg_offsets`` likewise for
+    ``target``.  Outputs are written in the concatenated order.  Returns ier.
+    """
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    so = np.ascontiguousarray(src_offsets, dtype=np.int32)
+    to = None if trg_offsets is None else np.ascontiguousarray(trg_offsets, dtype=np.int32)
+    return _lib.fmm3d_lfmm3dparttarg_batched_device(
+        iprec, len(so) - 1, _ptr(so), ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None),
+        ptr(dipstr), ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld),
+        None if to is None else _ptr(to), ptr(target), int(pottarg is not None), ptr(pottarg),
+        int(fldtarg is not None), ptr(fldtarg), _P(stream))
 
 
 def _zk(zk):

@@ -72,6 +72,10 @@ inline TreeView make_treeview(const Tree &T)
     tv.ntrg = T.ntrg.p; tv.center = T.center.p; tv.l1_start = T.l1_start.p; tv.l1_idx = T.l1_idx.p;
     tv.l3_start = T.l3_start.p; tv.l3_idx = T.l3_idx.p; tv.l4_start = T.l4_start.p; tv.l4_idx = T.l4_idx.p;
     tv.size = T.size;
+    if (T.ninst > 1) {
+        tv.binst = T.binst.p;
+        tv.inst_geom = T.inst_geom.p;
+    }
     return tv;
 }
 

@@ -294,10 +294,13 @@ __global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int 
 }
 
 // ---------------------------------------------------------------- the FMM
+// so / to (optional): instance offsets of a batch, each instance an
+// independent FMM over its own sources and targets (a forest, one root each).
 static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
                           const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
                           double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
-                          int iffldtarg, double *d_fldtarg, cudaStream_t s)
+                          int iffldtarg, double *d_fldtarg, cudaStream_t s, const std::vector<int> *so = nullptr,
+                          const std::vector<int> *to = nullptr)
 {
     Status st;
     g_launch_count = 0;
@@ -315,7 +318,8 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     Timer tm(s, g_ti.timing);
     tm.mark();
     Tree T;
-    build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
+    if (so) build_forest(T, d_src, *so, d_trg, *to, nbox, s, st);
+    else build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
     tm.mark();
     const int K = (p + 1) * (p + 1);
@@ -570,6 +574,23 @@ int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcha
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     return 0;
+}
+
+int fmm3d_lfmm3dparttarg_batched_device(int iprec, int ninst, const int *src_offsets, const double *d_source,
+                                        int ifcharge, const double *d_charge, int ifdipole, const double *d_dipstr,
+                                        const double *d_dipvec, int ifpot, double *d_pot, int iffld, double *d_fld,
+                                        const int *trg_offsets, const double *d_target, int ifpottarg,
+                                        double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream)
+{
+    if (ninst < 1 || !src_offsets) return 4;
+    std::vector<int> so(src_offsets, src_offsets + ninst + 1), to(ninst + 1, 0);
+    if (trg_offsets) to.assign(trg_offsets, trg_offsets + ninst + 1);
+    for (int i = 0; i < ninst; i++)
+        if (so[i + 1] < so[i] || to[i + 1] < to[i] || so[i] < 0 || to[i] < 0) return 4;
+    if (so[0] != 0 || to[0] != 0) return 4;
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return lap_fmm_device(iprec, so[ninst], d_source, ifcharge, d_charge, ifdipole, d_dipstr, d_dipvec, ifpot, d_pot,
+                          iffld, d_fld, to[ninst], d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s, &so, &to);
 }
 
 void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,

@@ -28,6 +28,10 @@ struct TreeView {
     const double *center;
     const int *l1_start, *l1_idx, *l3_start, *l3_idx, *l4_start, *l4_idx;
     double size;  // side of the level-0 box
+    // forests (several instances): the instance of every box and, per
+    // instance, its bounding cube (center x, y, z, side); null for one tree
+    const int *binst = nullptr;
+    const double *inst_geom = nullptr;
 };
 
 // One source slot of a translation: where the source box is relative to the

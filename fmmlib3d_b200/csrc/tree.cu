@@ -61,15 +61,61 @@ __global__ void k_bbox_final(const double *part, int nb, double *geom /* c0x c0y
     geom[3] = size;
 }
 
+// Bounding cube of every instance of a forest: CTA per instance over its
+// source range [so[i], so[i+1]) and target range [to[i], to[i+1]).
+__global__ void k_bbox_inst(const double *src, const int *so, const double *trg, const int *to, double *geom)
+{
+    const int inst = blockIdx.x;
+    double mn[3] = {1e308, 1e308, 1e308}, mx[3] = {-1e308, -1e308, -1e308};
+    const long a = so[inst], ns = so[inst + 1] - a, b = to[inst], nt = to[inst + 1] - b;
+    for (long i = threadIdx.x; i < ns + nt; i += blockDim.x) {
+        const double *p = i < ns ? src + 3 * (a + i) : trg + 3 * (b + i - ns);
+        for (int d = 0; d < 3; d++) {
+            mn[d] = fmin(mn[d], p[d]);
+            mx[d] = fmax(mx[d], p[d]);
+        }
+    }
+    for (int d = 0; d < 3; d++)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    __shared__ double sh[32][6];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int d = 0; d < 3; d++) { sh[w][d] = mn[d]; sh[w][3 + d] = mx[d]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++)
+            for (int d = 0; d < 3; d++) {
+                sh[0][d] = fmin(sh[0][d], sh[ww][d]);
+                sh[0][3 + d] = fmax(sh[0][3 + d], sh[ww][3 + d]);
+            }
+        double size = __dsub_rn(sh[0][3], sh[0][0]);
+        double sy = __dsub_rn(sh[0][4], sh[0][1]), sz = __dsub_rn(sh[0][5], sh[0][2]);
+        if (sy > size) size = sy;
+        if (sz > size) size = sz;
+        for (int d = 0; d < 3; d++) geom[4 * inst + d] = __dadd_rn(sh[0][d], sh[0][3 + d]) / 2;
+        geom[4 * inst + 3] = size;
+    }
+}
+
+// instance id of every point of the concatenated arrays
+__global__ void k_point_inst(const int *off, int *pinst)
+{
+    for (int i = off[blockIdx.x] + threadIdx.x; i < off[blockIdx.x + 1]; i += blockDim.x) pinst[i] = blockIdx.x;
+}
+
 // ---------------------------------------------------------------- keys
 // Path key of a point: for every level the octant (z,y,x bits) it falls in,
 // decided exactly as d3tsepa0 does (upper half iff coordinate > center) with
 // the center computed as in d3tcentf (src/d3tstrcr.f:1671-1700):
 // x0 + (i-1)*side + side/2, evaluated without contraction.
-__global__ void k_keys(const double *pts, int n, const double *geom, uint64_t *keys, int *idx)
+__global__ void k_keys(const double *pts, int n, const double *geom_all, const int *pinst, uint64_t *keys, int *idx)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const double *geom = geom_all + (pinst ? 4 * pinst[i] : 0);
     double size = geom[3];
     double h = size / 2;
     double x0[3] = {__dsub_rn(geom[0], h), __dsub_rn(geom[1], h), __dsub_rn(geom[2], h)};
@@ -141,8 +187,8 @@ __global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, co
 
 __global__ void k_make_children(int b0, int nb, int level, int next0, const int *kbase, const int *nkids,
                                 const int *cs0, const int *cns, const int *ct0, const int *cnt,
-                                const double *geom, int *ijk, int *lev, int *par, int *oct, int *nch,
-                                int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center)
+                                const double *geom_all, int *ijk, int *lev, int *par, int *oct, int *nch,
+                                int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center, int *binst)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nb) return;
@@ -150,6 +196,8 @@ __global__ void k_make_children(int b0, int nb, int level, int next0, const int 
     int id = next0 + kbase[t];
     nch[b] = nkids[t];
     if (nkids[t] == 0) return;
+    const int inst = binst[b];
+    const double *geom = geom_all + 4 * inst;
     double size = geom[3], h = size / 2;
     double side = size / (double)(1 << (level + 1)), side2 = side / 2;
     for (int d = 0; d < 8; d++) {
@@ -163,6 +211,7 @@ __global__ void k_make_children(int b0, int nb, int level, int next0, const int 
             center[3L * id + e] = __dadd_rn(__dadd_rn(x00, __dmul_rn((double)c[e], side)), side2);
         }
         lev[id] = level + 1;
+        binst[id] = inst;
         par[id] = b;
         oct[id] = d;
         nch[id] = 0;
@@ -176,14 +225,17 @@ __global__ void k_make_children(int b0, int nb, int level, int next0, const int 
     }
 }
 
-__global__ void k_root(int n, int m, const double *geom, int *ijk, int *lev, int *par, int *oct, int *nch,
-                       int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center)
+// Root box of every instance (box id = instance id).
+__global__ void k_root(int ninst, const int *so, const int *to, const double *geom, int *ijk, int *lev, int *par,
+                       int *oct, int *nch, int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center,
+                       int *binst)
 {
-    if (threadIdx.x != 0) return;
-    for (int e = 0; e < 3; e++) { ijk[e] = 0; center[e] = geom[e]; }
-    lev[0] = 0; par[0] = -1; oct[0] = 0; nch[0] = 0;
-    for (int e = 0; e < 8; e++) child[e] = -1;
-    src0[0] = 0; nsrc[0] = n; trg0[0] = 0; ntrg[0] = m;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= ninst) return;
+    for (int e = 0; e < 3; e++) { ijk[3 * r + e] = 0; center[3 * r + e] = geom[4 * r + e]; }
+    lev[r] = 0; par[r] = -1; oct[r] = 0; nch[r] = 0; binst[r] = r;
+    for (int e = 0; e < 8; e++) child[8 * r + e] = -1;
+    src0[r] = so[r]; nsrc[r] = so[r + 1] - so[r]; trg0[r] = to[r]; ntrg[r] = to[r + 1] - to[r];
 }
 
 // ---------------------------------------------------------------- colleagues (list 5 plus self)
@@ -357,37 +409,102 @@ bool grow(DBuf<T> &b, size_t need, size_t copy, cudaStream_t s, Status &st)
     return st.ok();
 }
 
+// Stable reorder of (key, perm) into instance-major order: sort by the
+// instance of each point (gathered through perm), carrying the position,
+// then gather keys and perm by the resulting order.
+__global__ void k_gather_inst(int n, const int *perm, const int *pinst, uint64_t *ikey, int *pos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ikey[i] = (uint64_t)pinst[perm[i]];
+    pos[i] = i;
+}
+
+__global__ void k_apply_pos(int n, const int *pos, const uint64_t *kin, const int *pin, uint64_t *kout, int *pout)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    kout[i] = kin[pos[i]];
+    pout[i] = pin[pos[i]];
+}
+
+void instance_major(DBuf<uint64_t> &keys, DBuf<int> &perm, const DBuf<int> &pinst, int n, int ibits,
+                    cudaStream_t s, Status &st)
+{
+    if (n == 0 || !st.ok()) return;
+    DBuf<uint64_t> ik, k2;
+    DBuf<int> pos, p2;
+    if (!ik.alloc(n, s, st) || !pos.alloc(n, s, st) || !k2.alloc(n, s, st) || !p2.alloc(n, s, st)) return;
+    k_gather_inst<<<div_up(n, 256), 256, 0, s>>>(n, perm.p, pinst.p, ik.p, pos.p); FMM_COUNT_LAUNCH();
+    radix_sort_u64(ik.p, pos.p, n, ibits, s, st);
+    k_apply_pos<<<div_up(n, 256), 256, 0, s>>>(n, pos.p, keys.p, perm.p, k2.p, p2.p); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    std::swap(keys.p, k2.p);
+    std::swap(keys.n, k2.n);
+    std::swap(perm.p, p2.p);
+    std::swap(perm.n, p2.n);
+}
+
 }  // namespace
 
 void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
                 Status &st)
 {
+    std::vector<int> so = {0, n}, to = {0, m};
+    build_forest(T, d_src, so, d_trg, to, nbox, s, st);
+}
+
+void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, const double *d_trg,
+                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st)
+{
+    const int ninst = (int)so.size() - 1;
+    const int n = so[ninst], m = to[ninst];
     T.n = n;
     T.m = m;
-    // bounding cube
-    DBuf<double> part, geom;
-    int nbb = std::max(1, std::min(1184, div_up((long)n + m, 256)));
-    part.alloc(6 * nbb, s, st);
-    geom.alloc(4, s, st);
+    T.ninst = ninst;
+    // bounding cube of every instance
+    DBuf<double> part, &geom = T.inst_geom;
+    DBuf<int> dso, dto, pis, pit;
+    geom.alloc(4L * ninst, s, st);
     if (!st.ok()) return;
-    k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p); FMM_COUNT_LAUNCH();
-    k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p); FMM_COUNT_LAUNCH();
-    // keys and sort
+    if (ninst == 1) {
+        int nbb = std::max(1, std::min(1184, div_up((long)n + m, 256)));
+        part.alloc(6 * nbb, s, st);
+        if (!st.ok()) return;
+        k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p); FMM_COUNT_LAUNCH();
+        k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p); FMM_COUNT_LAUNCH();
+    } else {
+        if (!dso.alloc(ninst + 1, s, st) || !dto.alloc(ninst + 1, s, st) || !pis.alloc(std::max(n, 1), s, st) ||
+            !pit.alloc(std::max(m, 1), s, st))
+            return;
+        FMM_TRY(st, cudaMemcpyAsync(dso.p, so.data(), sizeof(int) * (ninst + 1), cudaMemcpyHostToDevice, s));
+        FMM_TRY(st, cudaMemcpyAsync(dto.p, to.data(), sizeof(int) * (ninst + 1), cudaMemcpyHostToDevice, s));
+        k_bbox_inst<<<ninst, 256, 0, s>>>(d_src, dso.p, d_trg, dto.p, geom.p); FMM_COUNT_LAUNCH();
+        k_point_inst<<<ninst, 256, 0, s>>>(dso.p, pis.p); FMM_COUNT_LAUNCH();
+        k_point_inst<<<ninst, 256, 0, s>>>(dto.p, pit.p); FMM_COUNT_LAUNCH();
+    }
+    // keys and sort: by path key, then (forests) stably by instance
     DBuf<uint64_t> ks, kt;
     ks.alloc(std::max(n, 1), s, st);
     kt.alloc(std::max(m, 1), s, st);
     T.perm_src.alloc(std::max(n, 1), s, st);
     T.perm_trg.alloc(std::max(m, 1), s, st);
     if (!st.ok()) return;
-    if (n) { k_keys<<<div_up(n, 256), 256, 0, s>>>(d_src, n, geom.p, ks.p, T.perm_src.p); FMM_COUNT_LAUNCH(); }
-    if (m) { k_keys<<<div_up(m, 256), 256, 0, s>>>(d_trg, m, geom.p, kt.p, T.perm_trg.p); FMM_COUNT_LAUNCH(); }
+    if (n) { k_keys<<<div_up(n, 256), 256, 0, s>>>(d_src, n, geom.p, ninst > 1 ? pis.p : nullptr, ks.p, T.perm_src.p); FMM_COUNT_LAUNCH(); }
+    if (m) { k_keys<<<div_up(m, 256), 256, 0, s>>>(d_trg, m, geom.p, ninst > 1 ? pit.p : nullptr, kt.p, T.perm_trg.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     radix_sort_u64(ks.p, T.perm_src.p, n, 3 * kMaxLevel, s, st);
     radix_sort_u64(kt.p, T.perm_trg.p, m, 3 * kMaxLevel, s, st);
+    if (ninst > 1) {
+        int ibits = 8;
+        while ((1L << ibits) < ninst) ibits += 8;
+        instance_major(ks, T.perm_src, pis, n, ibits, s, st);
+        instance_major(kt, T.perm_trg, pit, m, ibits, s, st);
+    }
     double hgeom[4];
     FMM_TRY(st, cudaMemcpyAsync(hgeom, geom.p, sizeof(hgeom), cudaMemcpyDeviceToHost, s));
     // boxes
-    int cap = std::max(1024, 2 * (int)(((long)n + m) / std::max(nbox, 1)) + 64);
+    int cap = std::max(1024, 2 * (int)(((long)n + m) / std::max(nbox, 1)) + 64 + 2 * ninst);
     auto ensure = [&](int need, int used) {
         if (need <= T.cap) return st.ok();
         int nc = std::max(need, 2 * T.cap);
@@ -402,16 +519,26 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
         grow(T.trg0, nc, used, s, st);
         grow(T.ntrg, nc, used, s, st);
         grow(T.center, 3L * nc, 3L * used, s, st);
+        grow(T.binst, nc, used, s, st);
         T.cap = nc;
         return st.ok();
     };
     T.cap = 0;
     if (!ensure(cap, 0)) return;
-    k_root<<<1, 32, 0, s>>>(n, m, geom.p, T.ijk.p, T.level.p, T.parent.p, T.octant.p, T.nchild.p, T.child.p,
-                            T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p, T.center.p); FMM_COUNT_LAUNCH();
+    {
+        DBuf<int> rso, rto;
+        if (!rso.alloc(ninst + 1, s, st) || !rto.alloc(ninst + 1, s, st)) return;
+        // root ranges in sorted order: instances are contiguous and in order
+        FMM_TRY(st, cudaMemcpyAsync(rso.p, so.data(), sizeof(int) * (ninst + 1), cudaMemcpyHostToDevice, s));
+        FMM_TRY(st, cudaMemcpyAsync(rto.p, to.data(), sizeof(int) * (ninst + 1), cudaMemcpyHostToDevice, s));
+        k_root<<<div_up(ninst, 128), 128, 0, s>>>(ninst, rso.p, rto.p, geom.p, T.ijk.p, T.level.p, T.parent.p,
+                                                  T.octant.p, T.nchild.p, T.child.p, T.src0.p, T.nsrc.p, T.trg0.p,
+                                                  T.ntrg.p, T.center.p, T.binst.p); FMM_COUNT_LAUNCH();
+        FMM_TRY(st, cudaStreamSynchronize(s));  // the host range vectors are read by the copies above
+    }
     T.lev_start.assign(1, 0);
-    T.lev_count.assign(1, 1);
-    int nboxes = 1;
+    T.lev_count.assign(1, ninst);
+    int nboxes = ninst;
     DBuf<int> nk, kb, cs0, cns, ct0, cnt;
     for (int level = 0; level < kMaxLevel; level++) {
         int b0 = T.lev_start[level], nb = T.lev_count[level];
@@ -428,7 +555,7 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
         k_make_children<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nboxes, kb.p, nk.p, cs0.p, cns.p, ct0.p,
                                                          cnt.p, geom.p, T.ijk.p, T.level.p, T.parent.p,
                                                          T.octant.p, T.nchild.p, T.child.p, T.src0.p, T.nsrc.p,
-                                                         T.trg0.p, T.ntrg.p, T.center.p); FMM_COUNT_LAUNCH();
+                                                         T.trg0.p, T.ntrg.p, T.center.p, T.binst.p); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         if (total == 0) break;
         T.lev_start.push_back(nboxes);

@@ -11,6 +11,8 @@ namespace fmm {
 
 struct Tree {
     int n = 0, m = 0;        // sources, targets
+    int ninst = 1;           // instances of a forest (one root each, boxes 0..ninst-1)
+    DBuf<double> inst_geom;  // 4 per instance: center of the bounding cube, side
     int nboxes = 0, nlev = 0;
     int nleaves = 0;
     double center0[3] = {0, 0, 0}, size = 0;
@@ -22,6 +24,7 @@ struct Tree {
     DBuf<int> child;    // 8 per box, indexed by octant (bit0 x, bit1 y, bit2 z), -1 if absent
     DBuf<int> src0, nsrc, trg0, ntrg;
     DBuf<double> center;  // 3 per box
+    DBuf<int> binst;      // instance of every box
     DBuf<int> coll;     // 27 per box: same-level boxes at offsets in [-1,1]^3 (self at 13), -1 if absent
     DBuf<int> leaves;   // ids of childless boxes
     // lists in CSR form
@@ -37,6 +40,14 @@ struct Tree {
 // Builds the tree for device arrays src (n x 3, AoS) and trg (m x 3).
 void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
                 Status &st);
+
+// A forest of independent trees, one per instance: instance i owns sources
+// so[i]..so[i+1]-1 and targets to[i]..to[i+1]-1 of the concatenated arrays
+// (host offsets).  Every instance gets its own bounding cube and the same
+// refinement rule; points are sorted instance-major, boxes of one level of all
+// instances are contiguous, and lists never cross instances.
+void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, const double *d_trg,
+                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st);
 
 __host__ __device__ __forceinline__ int coll_slot(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
 

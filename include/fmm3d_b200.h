@@ -98,6 +98,21 @@ int fmm3d_l3ddirect_points_device(int nsource, const double *d_source, int ifcha
                                   const double *d_pts, const int *d_skip, double *d_pot, double *d_fld,
                                   void *stream);
 
+/* Batched lfmm3dparttarg on device arrays: ninst independent FMMs in one
+ * call.  No counterpart in the reference (it has one FMM per call).  Instance
+ * i owns sources src_offsets[i]..src_offsets[i+1]-1 and targets
+ * trg_offsets[i]..trg_offsets[i+1]-1 of the concatenated arrays (host offset
+ * arrays of ninst+1 entries starting at 0; trg_offsets may be NULL for no
+ * targets); outputs are written in the same concatenated order.  Each
+ * instance gets its own octree (bounding cube, lists, expansions) exactly as a
+ * single call would build it, so its results equal those of a single call; all
+ * instances share every pass (one kernel launch per pass for the batch). */
+int fmm3d_lfmm3dparttarg_batched_device(int iprec, int ninst, const int *src_offsets, const double *d_source,
+                                        int ifcharge, const double *d_charge, int ifdipole, const double *d_dipstr,
+                                        const double *d_dipvec, int ifpot, double *d_pot, int iffld, double *d_fld,
+                                        const int *trg_offsets, const double *d_target, int ifpottarg,
+                                        double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream);
+
 /* hfmm3dparttarg, h3dpartdirect and the sampled Helmholtz direct sum on
  * device-resident arrays (layouts as above; zk = two doubles on the host). */
 int fmm3d_hfmm3dparttarg_device(int iprec, const double *zk, int nsource, const double *d_source, int ifcharge,
