@@ -30,6 +30,13 @@ throughout), both reported.
             lfmm3dpartself on 100,000 sources on the unit sphere (seed 1),
             charges only, iprec = 1, FP64, with the CPU restatement timed on
             the same input.
+  batched   4,096 independent Laplace instances in one batched call
+            (fmm3d_lfmm3dparttarg_batched_device, one launch per pass): N per
+            instance floor(10^U[3, log10 2e5]) (seed 4), geometry per instance
+            uniformly a unit cube, a Plummer sphere (scale 0.1, r <= 1) or an
+            ellipsoid surface with semi-axes U[0.2, 1]; charges in [-1, 1]^2;
+            iprec = 1, mixed form; points/s over all instances and errors at
+            sampled points of sampled instances.
   serving   the request loop of fmmlib3d_b200.serving (4 slots, admission by
             projected HBM footprint) on a seeded stream of requests (70%
             Laplace, 30% Helmholtz with zk uniform in [1, 20], N log-uniform in
@@ -84,11 +91,12 @@ def parse_args(argv=None):
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
     ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
     ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
+    ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests per serving rate (0: skip)")
     ap.add_argument("--serve-rates", default="10,40,inf", help="Poisson arrival rates (requests/s)")
-    ap.add_argument("--workload", choices=["all", "laplace", "helmholtz"], default="all",
-                    help="all: the Laplace headline line with the Helmholtz object (default); "
-                         "laplace / helmholtz: one workload only (profiling runs)")
+    ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched"], default="all",
+                    help="all: the Laplace headline line with the other workloads' objects (default); "
+                         "laplace / helmholtz / batched: one workload only (profiling runs)")
     return ap.parse_args(argv)
 
 
@@ -172,6 +180,91 @@ def run_laplace_sphere(args, R, n=100_000):
         out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
                                "kind": "port", "sample": "the whole workload, one call (%.2f s)" % dt}
     return out
+
+
+def batched_inputs(k, seed=4):
+    """The batched workload's instances, concatenated: (sources, charges, offsets)."""
+    rng = np.random.default_rng(seed)
+    srcs, qs = [], []
+    for _ in range(k):
+        n = int(10 ** rng.uniform(3, np.log10(2e5)))
+        g = int(rng.integers(3))
+        if g == 0:
+            src = rng.random((n, 3))
+        elif g == 1:
+            parts, have = [], 0
+            while have < n:
+                u = rng.random(n)
+                r = 0.1 / np.sqrt(np.maximum(u ** (-2 / 3) - 1, 1e-300))
+                v = rng.normal(size=(n, 3))
+                keep = r <= 1
+                p = v[keep] / np.linalg.norm(v[keep], axis=1)[:, None] * r[keep][:, None]
+                parts.append(p)
+                have += len(p)
+            src = np.concatenate(parts)[:n]
+        else:
+            v = rng.normal(size=(n, 3))
+            src = v / np.linalg.norm(v, axis=1)[:, None] * rng.uniform(0.2, 1, 3)
+        srcs.append(src)
+        qs.append(rng.uniform(-1, 1, (n, 2)))
+    off = np.concatenate([[0], np.cumsum([len(x) for x in srcs])]).astype(np.int32)
+    return np.concatenate(srcs), np.concatenate(qs), off
+
+
+def run_batched(args, R):
+    torch, F = R["torch"], R["F"]
+    src, q, off = batched_inputs(args.batch_instances)
+    n = int(off[-1])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_src, d_q = torch.from_numpy(src).to(dev), torch.from_numpy(q).to(dev)
+    d_pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    F.set_precision(1)
+    F.set_timing(True)
+
+    def step():
+        ier = F.lfmm3dparttarg_batched_device(1, off, d_src, d_q, None, None, d_pot, d_fld, stream=stream)
+        if ier != 0:
+            raise RuntimeError("batched FMM ier=%d: %s" % (ier, F.last_error()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    steps = max(1, min(args.steps, 3))
+    passes, launches = [], []
+    ev[0].record()
+    for _ in range(steps):
+        step()
+        passes.append(F.last_timing())
+        launches.append(F.last_launches())
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    # errors: 50 points of each of 20 seeded instances against the FP64 direct sum
+    rng = np.random.default_rng(96)
+    num = {"pot": 0.0, "fld": 0.0}
+    den = {"pot": 0.0, "fld": 0.0}
+    for i in rng.choice(args.batch_instances, min(20, args.batch_instances), replace=False):
+        a, b = int(off[i]), int(off[i + 1])
+        k = min(50, b - a)
+        idx = np.sort(rng.choice(b - a, k, replace=False)).astype(np.int32)
+        it = torch.from_numpy(idx).to(dev)
+        dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
+        df = torch.empty((k, 6), dtype=torch.float64, device=dev)
+        F.direct_points_device(d_src[a:b], d_q[a:b], None, None, d_src[a:b][it.long()].contiguous(), it, dp, df,
+                               stream=stream)
+        torch.cuda.synchronize()
+        gp, gf = d_pot[a:b][it.long()], d_fld[a:b][it.long()]
+        num["pot"] += float(torch.sum((gp - dp) ** 2)); den["pot"] += float(torch.sum(dp ** 2))
+        num["fld"] += float(torch.sum((gf - df) ** 2)); den["fld"] += float(torch.sum(df ** 2))
+    F.set_precision(0)
+    mean = {kk: round(float(np.mean([p[kk] for p in passes])), 3) for kk in passes[0]}
+    return {"workload": "laplace_batched_%d_instances_logN_1e3_2e5_iprec1_mixed" % args.batch_instances,
+            "instances": args.batch_instances, "n_total": n, "value": n / (ms * 1e-3), "unit": UNIT,
+            "ms_per_step": ms, "steps": steps, "gpu_launches_per_step": int(np.mean(launches)),
+            "errors": {kk: float("%.3e" % np.sqrt(num[kk] / den[kk])) for kk in num}, "pass_ms_mean": mean}
 
 
 def run_serving(args):
@@ -591,8 +684,17 @@ def main(argv=None):
                           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                           "helmholtz": out}), flush=True)
         return 0
+    if args.workload == "batched":
+        import torch
+        import fmmlib3d_b200 as F
+        torch.cuda.set_device(dist_env()[2])
+        out = run_batched(args, dict(torch=torch, F=F, rank=rank, ws=1, dist=None))
+        print(json.dumps({"metric": "batched Laplace FMM pts/s", "value": out["value"], "unit": UNIT,
+                          "n_gpus": 1, "steps": out["steps"], "warmup": args.warmup, "batched": out}), flush=True)
+        return 0
     if args.workload == "laplace":
         args.helm_n = 0
+        args.batch_instances = 0
     R = run_b200(args)
     R["F"].set_precision(1)
     e2e = None if args.no_e2e else run_e2e(args, R)
@@ -625,6 +727,8 @@ def main(argv=None):
                                 "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
                                     args.cpu_sample, args.iprec, dt)}
     line["laplace_sphere"] = run_laplace_sphere(args, R)
+    if args.batch_instances > 0:
+        line["batched"] = run_batched(args, R)
     if args.serve_requests > 0 and ws == 1:
         line["serving"] = run_serving(args)
     if args.helm_n > 0:
