@@ -89,6 +89,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-samples", type=int, default=1000)
     ap.add_argument("--m2l-mode", type=int, default=0, help="0 auto, 1 rotate-shift-rotate, 2 dense operators")
+    ap.add_argument("--tensor-m2l", type=int, default=1,
+                    help="mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (tcgen05 split TF32)")
     ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
     ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched workload (0: skip)")
@@ -221,6 +223,7 @@ def run_batched(args, R):
     d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
     F.set_precision(1)
+    F.set_tensor_m2l(args.tensor_m2l)
     F.set_timing(True)
 
     def step():
@@ -426,6 +429,7 @@ def run_b200(args):
     d_ft = torch.empty((m, 6), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
     F.set_m2l_mode(args.m2l_mode)
+    F.set_tensor_m2l(args.tensor_m2l)
 
     def step():
         ier = F.lfmm3dparttarg_device(args.iprec, d_src, d_q, d_dq, d_dv, d_pot, d_fld, d_trg, d_pt, d_ft,

@@ -58,6 +58,12 @@ _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
 _lib.fmm3d_set_m2l_mode.argtypes = [_I]
 _lib.fmm3d_set_precision.argtypes = [_I]
+_lib.fmm3d_set_tensor_m2l.argtypes = [_I]
+_lib.fmm3d_set_tensor_m2l.restype = _I
+_lib.fmm3d_set_tensor_m2l_group.argtypes = [_I]
+_lib.fmm3d_set_tensor_m2l_group.restype = _I
+_lib.fmm3d_tc_selftest.argtypes = [_I, _I, _P, _P, _P, _I]
+_lib.fmm3d_tc_selftest.restype = _I
 _lib.fmm3d_last_timing.argtypes = [_P, _I]
 _lib.fmm3d_last_timing.restype = _I
 _lib.fmm3d_last_stats.argtypes = [_P, _I]
@@ -305,6 +311,27 @@ def set_m2l_mode(mode):
 def set_precision(mode):
     """0 FP64 throughout (default), 1 mixed FP32 P2P/M2L for iprec <= 1."""
     _lib.fmm3d_set_precision(int(mode))
+
+
+def set_tensor_m2l(mode):
+    """Mixed-form M2L: 0 FP32 CUDA cores, 1 (default) / 2 tensor cores (tcgen05, split TF32; staging variants)."""
+    if _lib.fmm3d_set_tensor_m2l(int(mode)) != 0:
+        raise ValueError("unknown tensor M2L mode %r" % (mode,))
+
+
+def set_tensor_m2l_group(slots):
+    """Tensor-core M2L: list-2 slots per TMEM sum before it is added into FP32 registers (0: one per tile)."""
+    if _lib.fmm3d_set_tensor_m2l_group(int(slots)) != 0:
+        raise ValueError("bad group %r" % (slots,))
+
+
+def tc_selftest(A, B, nprod=3):
+    """D = A @ B.T on the tensor cores (A: 128 x K, B: N x K float32).  Returns (status, D)."""
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    D = np.zeros((128, B.shape[0]), np.float32)
+    st = _lib.fmm3d_tc_selftest(B.shape[0], A.shape[1], _ptr(A), _ptr(B), _ptr(D), int(nprod))
+    return st, D
 
 
 def last_timing():

@@ -103,6 +103,8 @@ struct LapPlan {
 };
 static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
 static int g_precision = 0; // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
+static int g_tc_m2l = 1;    // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
+static int g_tc_group = 1;  // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
 constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
 
 static std::mutex g_plan_mu;
@@ -379,7 +381,9 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     const bool mixed = g_precision == 1 && iprec <= 1 && plan->dense;
     const bool dense = (plan->dense && g_m2l_mode != 1) || mixed;
     int m2l_a = (int)htiles.size();
-    for (int l = 2; l <= T.nlev; l++) make_tiles(l, dense ? kDenseTileTargets : plan->kt, 0, 189, 189, htiles);
+    const bool tcm2l = mixed && g_tc_m2l > 0;
+    const int m2l_kt = tcm2l ? kTcTileTargets : dense ? kDenseTileTargets : plan->kt;
+    for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
     int m2l_n = (int)htiles.size() - m2l_a;
     for (int l = 2; l <= T.nlev - 1; l++) {
         int a = (int)htiles.size();
@@ -407,7 +411,19 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     launch_p2l(T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, p, local.p, s, st);
     tm.mark();
     // STEP 4: M2L over list 2, all levels >= 2
-    if (mixed)
+    DBuf<float2> mp32;
+    DBuf<int> tcerr;
+    const int ldm = K + (K & 1);
+    if (tcm2l) {
+        if (!mp32.alloc((size_t)T.nboxes * ldm, s, st) || !tcerr.alloc(1, s, st)) {
+            g_ti.err = cudaGetErrorString(st.err);
+            return 16;
+        }
+        tcerr.zero(st);
+        convert_mp_f32(T.nboxes, K, ldm, mpole.p, mp32.p, s, st);
+        launch_m2l_tc(g_tc_m2l - 1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+                      plan->T32.p, tv, p, mp32.p, ldm, local.p, prune, 3, g_tc_group, tcerr.p, s, st);
+    } else if (mixed)
         launch_m2l_dense32(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T32.p, tv,
                            p, mpole.p, local.p, prune, s, st);
     else if (dense)
@@ -469,8 +485,11 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
             for (int i = 0; i < 128; i++) g_ti.stats[9 + i] = (long long)h[1 + i];
         }
     }
+    int herr = 0;
+    if (tcm2l) FMM_TRY(st, cudaMemcpyAsync(&herr, tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    if (herr) { g_ti.err = "tensor-core M2L: a wait expired"; return 16; }
     return 0;
 }
 
@@ -650,6 +669,20 @@ int fmm3d_set_timing(int on)
 int fmm3d_set_precision(int mode)
 {
     g_precision = mode;
+    return 0;
+}
+
+int fmm3d_set_tensor_m2l(int mode)
+{
+    if (mode < 0 || mode > 2) return 1;
+    g_tc_m2l = mode;
+    return 0;
+}
+
+int fmm3d_set_tensor_m2l_group(int slots)
+{
+    if (slots < 0) return 1;
+    g_tc_group = slots;
     return 0;
 }
 

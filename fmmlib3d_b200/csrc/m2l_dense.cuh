@@ -32,6 +32,17 @@ void launch_p2p32(const int *leaves, int nleaves, const TreeView &tv, const Poin
                   const double *ty, const double *tz, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
                   int ifpot, int iffld, int ifpottarg, int iffldtarg, cudaStream_t s, Status &st);
 void convert_f32(long long n, const double2 *in, float2 *out, cudaStream_t s, Status &st);
+// Tensor-core (tcgen05, split TF32) form of the FP32 dense M2L (tc_m2l.cu):
+// tiles of up to 128 targets, FP32 multipoles with an even row stride ldm;
+// the TMEM sum is added into FP32 registers every `group` slots (0: once, at
+// the end); *err is set on an expired wait.  variant 0: K stage 16, 3
+// stages; 1: K stage 32, 2 stages.
+void launch_m2l_tc(int variant, const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
+                   const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
+                   int ldm, double2 *out, int prune, int nprod, int group, int *err, cudaStream_t s, Status &st);
+void convert_mp_f32(long long nboxes, int nc, int ldm, const double2 *in, float2 *out, cudaStream_t s, Status &st);
+constexpr int kTcTileTargets = 128;
+
 void launch_m2l_dense32(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                         const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const double2 *in,
                         double2 *out, int prune, cudaStream_t s, Status &st);

@@ -1,0 +1,407 @@
+// M2L on the Blackwell tensor cores (mixed form, nterms <= 16).
+//
+// The dense per-offset operators T_D (m2l_dense.cu) applied to gathered source
+// multipoles are products of complex matrices.  Here each CTA owns 64 complex
+// rows of the local expansions of a tile of up to 128 target boxes and
+// streams the tile's 189 list-2 slots:
+//   D[r, t] += sum_k A[r, k] B[t, k]
+// with the complex product embedded in real arithmetic:
+//   A rows 0..63   (real parts):      [Re T, -Im T] interleaved per column,
+//   A rows 64..127 (imaginary parts): [Im T,  Re T],
+//   B (per target): [Re M, Im M] interleaved per coefficient.
+// A and B are rounded to FP32, split into TF32 pairs x = hi + lo (both
+// rounded to nearest, so hi + lo is x to about 2^-24), and
+// D += A_hi B_hi + A_hi B_lo + A_lo B_hi + A_lo B_lo is issued as
+// tcgen05.mma kind::tf32 (M = 128, N = targets, K = 8) by one thread, with D
+// in TMEM (FP32).
+// Operands are staged in shared memory by all threads (gather of the source
+// multipoles, split, K-major no-swizzle layout) in a ring of S stages; each
+// stage is released by a tcgen05.commit on its mbarrier.  The tensor cores
+// accumulate a group of slots (TMEM columns 0..127); the group's sum is then
+// added by the CUDA cores, with round-to-nearest FP32 additions, into a
+// running sum held in TMEM columns 128..255: long tensor-core accumulations
+// lose accuracy, groups of a few slots keep the FP32 CUDA-core form's error.
+// At the end every warp reads its TMEM lane quarter of the running sum and
+// adds the tile into the FP64 locals.
+// Every wait is bounded: on expiry the kernel records an error, waits (again
+// bounded) for its own MMAs, frees its TMEM and returns.
+#include "lap_kernels.cuh"
+#include "m2l_dense.cuh"
+#include "tc_common.cuh"
+
+namespace fmm {
+
+constexpr int kTcThreads = 256;
+constexpr uint32_t kTcLBO = 128 * 16 + 16;           // K-block stride (bytes): 128 rows + 16 B pad
+constexpr long long kTcWaitCycles = 2000000000LL;    // ~1 s at 2 GHz
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *mbar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_wait(mbar, parity, 64))
+        if (clock64() - t0 > kTcWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l)
+{
+    split_tf32(v.x, h.x, l.x);
+    split_tf32(v.y, h.y, l.y);
+    split_tf32(v.z, h.z, l.z);
+    split_tf32(v.w, h.w, l.w);
+}
+
+// Issue the MMAs of one stage: K = KC in steps of 8; per step the product of
+// the high parts and, for nprod >= 3, the two cross products, for nprod >= 4
+// also the product of the low parts (then the sum is the exact product of
+// hi + lo, i.e. of the operands to within about 2^-24 each).
+template <int KC>
+__device__ __forceinline__ void issue_stage(uint32_t base, uint32_t tm, uint32_t idesc, bool first, int nprod)
+{
+    constexpr uint32_t OPB = (KC / 4) * kTcLBO;
+#pragma unroll
+    for (int s = 0; s < KC / 8; s++) {
+        const uint32_t o = 2 * s * kTcLBO;
+        const uint64_t ah = tc_desc(base + o, kTcLBO, 128), al = tc_desc(base + OPB + o, kTcLBO, 128);
+        const uint64_t bh = tc_desc(base + 2 * OPB + o, kTcLBO, 128), bl = tc_desc(base + 3 * OPB + o, kTcLBO, 128);
+        tc_mma_tf32(tm, ah, bh, idesc, (first && s == 0) ? 0u : 1u);
+        if (nprod >= 3) {
+            tc_mma_tf32(tm, ah, bl, idesc, 1u);
+            tc_mma_tf32(tm, al, bh, idesc, 1u);
+        }
+        if (nprod >= 4) tc_mma_tf32(tm, al, bl, idesc, 1u);
+    }
+}
+
+template <int KC, int S>
+__global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, const int *grouped, const Slot *slots,
+                                                        const long long *slot_toff, const float2 *T, TreeView tv,
+                                                        int p, const float2 *mp, int ldm, double2 *out, int prune,
+                                                        int nprod, int group, int *err)
+{
+    constexpr int KB = KC / 4;                 // 16-byte K blocks per stage
+    constexpr uint32_t OPB = KB * kTcLBO;      // one operand buffer
+    constexpr uint32_t STB = 4 * OPB;          // A_hi, A_lo, B_hi, B_lo
+    constexpr int TPP = kTcThreads / KB;       // targets staged per pass
+    constexpr int NPASS = 128 / TPP;
+    extern __shared__ unsigned char tc_smraw[];
+    unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smraw + 127) & ~(uintptr_t)127);
+    __shared__ uint64_t mbar[S];
+    __shared__ uint32_t tbase;
+    __shared__ int tg[128];
+    const Tile tile = tiles[blockIdx.x];
+    const int row0 = 64 * blockIdx.y;          // first complex row of this CTA
+    const int NC = (p + 1) * (p + 1);
+    const int N = max(16, (tile.count + 15) & ~15);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid < 128) tg[tid] = tid < tile.count ? grouped[tile.first + tid] : -1;
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) mbar_init(&mbar[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(&tbase, 256);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = tbase;
+    const uint32_t idesc = tc_idesc_tf32(128, N);
+    const uint32_t sbase = smem_u32(sm);
+    const int q = warp & 3, h = warp >> 2;     // TMEM lane quarter and column half of this warp
+    const uint32_t tD = tm + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * h);   // tensor-core sum (columns 0..127)
+    const uint32_t tA = tD + 128;                                                // FP32 running sum (128..255)
+    int it = 0;
+    bool aborted = false, fresh = true;        // fresh: the next MMA starts a new TMEM sum
+    bool have_acc = false;                     // the running sum holds flushed groups
+    // Add the tensor-core sum of the group that ends with item it - 1 into the running sum.
+    auto flush = [&]() {
+        const int last = it - 1;
+        const bool done = mbar_wait_bounded(&mbar[last % S], (last / S) & 1);
+        if (__syncthreads_or(!done)) { aborted = true; return; }
+        tc_fence_after();
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            if (64 * h + c0 < N) {
+                float v[16], a[16];
+                tmem_ld16(tD + c0, v);
+                if (have_acc) {
+                    tmem_ld16(tA + c0, a);
+#pragma unroll
+                    for (int u = 0; u < 16; u++) v[u] += a[u];
+                }
+                tmem_st16(tA + c0, v);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        fresh = true;
+        have_acc = true;
+    };
+    for (int si = 0; si < tile.nslot && !aborted; si++) {
+        do {  // one slot; break = nothing to add for it
+            const Slot sl = slots[tile.slot0 + si];
+            const int R = (sl.pt + 1) * (sl.pt + 1);
+            if (row0 >= R) break;
+            int sbr[NPASS];
+            int have = 0;
+#pragma unroll
+            for (int j = 0; j < NPASS; j++) {
+                const int n = tid / KB + TPP * j;
+                const int t = n < tile.count ? tg[n] : -1;
+                int sb = -1;
+                if (t >= 0 && !(prune && tv.ntrg[t] == 0)) {
+                    const int P = tv.parent[t];
+                    const int C = P >= 0 ? tv.coll[27L * P + sl.coll] : -1;
+                    sb = C >= 0 ? tv.child[8L * C + sl.oct] : -1;
+                    if (sb >= 0 && tv.nsrc[sb] == 0) sb = -1;
+                }
+                sbr[j] = sb;
+                have |= sb >= 0;
+            }
+            if (!__syncthreads_or(have)) break;
+            const float2 *Tu = T + slot_toff[tile.slot0 + si];
+            const int nk = (2 * R + KC - 1) / KC;
+            for (int kc = 0; kc < nk; kc++, it++) {
+                const int st = it % S;
+                unsigned char *base = sm + st * STB;
+                int late = 0;
+                if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
+                const int jb = kc * (KC / 2);      // first complex column of this stage
+                // A: operator rows row0 .. row0 + 63, columns jb .. jb + KC/2 - 1 (column-major T)
+                for (int task = tid; task < 64 * KB; task += kTcThreads) {
+                    const int i = task & 63, kb = task >> 6;
+                    const int row = row0 + i, j0 = jb + 2 * kb;
+                    float2 v0 = make_float2(0.f, 0.f), v1 = v0;
+                    if (row < R) {
+                        if (j0 < R) v0 = Tu[(size_t)j0 * R + row];
+                        if (j0 + 1 < R) v1 = Tu[(size_t)(j0 + 1) * R + row];
+                    }
+                    float4 h, l;
+                    unsigned char *ah = base + kb * kTcLBO, *al = base + OPB + kb * kTcLBO;
+                    split4(make_float4(v0.x, -v0.y, v1.x, -v1.y), h, l);
+                    *(float4 *)(ah + i * 16) = h;
+                    *(float4 *)(al + i * 16) = l;
+                    split4(make_float4(v0.y, v0.x, v1.y, v1.x), h, l);
+                    *(float4 *)(ah + (64 + i) * 16) = h;
+                    *(float4 *)(al + (64 + i) * 16) = l;
+                }
+                // B: the gathered source multipoles, coefficients jb .. jb + KC/2 - 1
+#pragma unroll
+                for (int j = 0; j < NPASS; j++) {
+                    const int n = tid / KB + TPP * j, kb = tid % KB;
+                    if (n >= N) continue;
+                    const int sb = sbr[j], j0 = jb + 2 * kb;
+                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (sb >= 0 && j0 < R) {
+                        v = *(const float4 *)(mp + (size_t)sb * ldm + j0);
+                        if (j0 + 1 >= R) { v.z = 0.f; v.w = 0.f; }
+                    }
+                    float4 h, l;
+                    split4(v, h, l);
+                    *(float4 *)(base + 2 * OPB + kb * kTcLBO + n * 16) = h;
+                    *(float4 *)(base + 3 * OPB + kb * kTcLBO + n * 16) = l;
+                }
+                fence_async_smem();
+                if (__syncthreads_or(late)) { aborted = true; break; }
+                if (tid == 0) {
+                    tc_fence_after();
+                    issue_stage<KC>(sbase + st * STB, tm, idesc, fresh && kc == 0, nprod);
+                    tc_commit(&mbar[st]);
+                }
+                fresh = false;
+            }
+        } while (0);
+        // group boundaries at fixed slot indices, so a target's sums do not
+        // depend on which other targets share its tile
+        if (!aborted && group > 0 && (si + 1) % group == 0 && !fresh) flush();
+    }
+    if (!aborted && !fresh) flush();
+    int bad = aborted ? 1 : 0;
+    if (!bad && have_acc) {
+        tc_fence_after();
+        const int L = 32 * q + lane, ci = L & 63, part = L >> 6, row = row0 + ci;
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            if (64 * h + c0 < N) {
+                float v[16];
+                tmem_ld16(tA + c0, v);
+                if (row < NC) {
+#pragma unroll
+                    for (int u = 0; u < 16; u++) {
+                        const int n = 64 * h + c0 + u;
+                        const int t = n < tile.count ? tg[n] : -1;
+                        if (t >= 0) {
+                            double *o = (double *)(out + (size_t)t * NC + row) + part;
+                            *o += (double)v[u];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (aborted && it > 0) {
+        // let this CTA's own MMAs finish (bounded) before its TMEM is released
+        const int last = it - 1;
+        mbar_wait_bounded(&mbar[last % S], (last / S) & 1);
+    }
+    if (bad && tid == 0) atomicExch(err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tm, 256);
+}
+
+template <int KC, int S>
+static void launch_tc_t(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
+                        const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
+                        int ldm, double2 *out, int prune, int nprod, int group, int *err, cudaStream_t s,
+                        Status &st)
+{
+    const size_t sm = (size_t)S * 4 * (KC / 4) * kTcLBO + 128;
+    FMM_TRY(st, cudaFuncSetAttribute(k_m2l_tc<KC, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 g(ntiles, div_up((p + 1) * (p + 1), 64));
+    k_m2l_tc<KC, S><<<g, kTcThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod,
+                                              group, err); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+void launch_m2l_tc(int variant, const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
+                   const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
+                   int ldm, double2 *out, int prune, int nprod, int group, int *err, cudaStream_t s, Status &st)
+{
+    if (!st.ok() || ntiles == 0) return;
+    if (variant == 1)
+        launch_tc_t<32, 2>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
+    else
+        launch_tc_t<16, 3>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
+}
+
+// FP32 copy of the multipoles with an even row stride (16-byte aligned pairs).
+__global__ void k_mp_f32(long long nb, int nc, int ldm, const double2 *in, float2 *out)
+{
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nb * ldm) return;
+    long long b = i / ldm;
+    int c = (int)(i - b * ldm);
+    double2 v = c < nc ? in[b * nc + c] : make_double2(0.0, 0.0);
+    out[i] = make_float2((float)v.x, (float)v.y);
+}
+
+void convert_mp_f32(long long nboxes, int nc, int ldm, const double2 *in, float2 *out, cudaStream_t s, Status &st)
+{
+    if (!st.ok() || nboxes == 0) return;
+    long long n = nboxes * ldm;
+    k_mp_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(nboxes, nc, ldm, in, out); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// ---------------------------------------------------------------- self-test
+// D (128 x N) = A (128 x K) B^T (N x K), row-major FP32 inputs, through the
+// same staging layout, descriptors, split products, commit/wait and TMEM
+// loads as the M2L kernel (one CTA, K a multiple of 32; nprod 1, 3 or 4).
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc_selftest(int N, int K, const float *A, const float *B,
+                                                               float *D, int nprod, int *err)
+{
+    constexpr int KC = 32, S = 2, KB = KC / 4;
+    constexpr uint32_t OPB = KB * kTcLBO, STB = 4 * OPB;
+    extern __shared__ unsigned char tc_smraw[];
+    unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smraw + 127) & ~(uintptr_t)127);
+    __shared__ uint64_t mbar[S];
+    __shared__ uint32_t tbase;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) mbar_init(&mbar[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(&tbase, 128);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = tbase, idesc = tc_idesc_tf32(128, N), sbase = smem_u32(sm);
+    int it = 0;
+    bool aborted = false;
+    for (int kc = 0; kc < K / KC; kc++, it++) {
+        const int st = it % S;
+        unsigned char *base = sm + st * STB;
+        int late = 0;
+        if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
+        for (int task = tid; task < 128 * KB; task += kTcThreads) {
+            const int r = task & 127, kb = task >> 7;
+            float4 h, l;
+            split4(*(const float4 *)(A + (size_t)r * K + kc * KC + 4 * kb), h, l);
+            *(float4 *)(base + kb * kTcLBO + r * 16) = h;
+            *(float4 *)(base + OPB + kb * kTcLBO + r * 16) = l;
+        }
+        for (int task = tid; task < N * KB; task += kTcThreads) {
+            const int n = task / KB, kb = task % KB;
+            float4 h, l;
+            split4(*(const float4 *)(B + (size_t)n * K + kc * KC + 4 * kb), h, l);
+            *(float4 *)(base + 2 * OPB + kb * kTcLBO + n * 16) = h;
+            *(float4 *)(base + 3 * OPB + kb * kTcLBO + n * 16) = l;
+        }
+        fence_async_smem();
+        if (__syncthreads_or(late)) { aborted = true; break; }
+        if (tid == 0) {
+            tc_fence_after();
+            issue_stage<KC>(sbase + st * STB, tm, idesc, it == 0, nprod);
+            tc_commit(&mbar[st]);
+        }
+    }
+    int bad = aborted ? 1 : 0;
+    if (it > 0) {
+        const int last = it - 1;
+        const bool done = mbar_wait_bounded(&mbar[last % S], (last / S) & 1);
+        if (__syncthreads_or(!done)) bad = 1;
+        tc_fence_after();
+        if (!bad) {
+            const int q = warp & 3, h = warp >> 2, r = 32 * q + lane;
+            for (int c0 = 0; c0 < 64; c0 += 16) {
+                const int col = 64 * h + c0;
+                if (col >= N) break;
+                float v[16];
+                tmem_ld16(tm + ((uint32_t)(32 * q) << 16) + (uint32_t)col, v);
+#pragma unroll
+                for (int u = 0; u < 16; u++) D[(size_t)r * N + col + u] = v[u];
+            }
+        }
+    }
+    if (bad && tid == 0) atomicExch(err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tm, 128);
+}
+
+}  // namespace fmm
+
+using namespace fmm;
+
+// Runs the tensor-core self-test on the current device: D (128 x N) from
+// A (128 x K) and B (N x K), host arrays.  N in 16..128 (multiple of 16), K a
+// multiple of 32, nprod 1 (hi products only) or 3 (split products).
+// Returns 0, 1 on a bad argument, 2 on a CUDA error, 3 on a wait that expired.
+extern "C" int fmm3d_tc_selftest(int N, int K, const float *A, const float *B, float *D, int nprod)
+{
+    if (N < 16 || N > 128 || N % 16 || K < 32 || K % 32) return 1;
+    float *dA = nullptr, *dB = nullptr, *dD = nullptr;
+    int *derr = nullptr, herr = 0;
+    cudaError_t e = cudaSuccess;
+    const size_t sm = 2 * 4 * (32 / 4) * kTcLBO + 128;
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
+    if (ok(cudaMalloc(&dA, sizeof(float) * 128 * K)) && ok(cudaMalloc(&dB, sizeof(float) * N * K)) &&
+        ok(cudaMalloc(&dD, sizeof(float) * 128 * N)) && ok(cudaMalloc(&derr, sizeof(int))) &&
+        ok(cudaMemcpy(dA, A, sizeof(float) * 128 * K, cudaMemcpyHostToDevice)) &&
+        ok(cudaMemcpy(dB, B, sizeof(float) * N * K, cudaMemcpyHostToDevice)) && ok(cudaMemset(derr, 0, sizeof(int))) &&
+        ok(cudaMemset(dD, 0, sizeof(float) * 128 * N)) &&
+        ok(cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) {
+        k_tc_selftest<<<1, kTcThreads, sm>>>(N, K, dA, dB, dD, nprod, derr);
+        if (ok(cudaGetLastError()) && ok(cudaDeviceSynchronize()))
+            if (ok(cudaMemcpy(D, dD, sizeof(float) * 128 * N, cudaMemcpyDeviceToHost)))
+                ok(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dD);
+    cudaFree(derr);
+    if (e != cudaSuccess) return 2;
+    return herr ? 3 : 0;
+}

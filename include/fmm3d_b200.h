@@ -177,6 +177,30 @@ int fmm3d_set_m2l_mode(int mode);
  * operators, FP64 for the tree, geometry, recurrences, rotations and the
  * other passes.  iprec >= 2 always runs FP64. */
 int fmm3d_set_precision(int mode);
+
+/* M2L of the mixed form (iprec <= 1, nterms <= 16) on the tensor cores:
+ * 0 = FP32 CUDA cores, 1 or 2 = tcgen05 kind::tf32 with operands split into
+ * TF32 pairs (three products per step, FP32 accumulation in TMEM; the
+ * default is 1); 1 and 2 differ only in the shared-memory staging (K stage
+ * 16 with three stages, K stage 32 with two).  No counterpart in the reference.  Returns 1 for an
+ * unknown mode. */
+int fmm3d_set_tensor_m2l(int mode);
+
+/* Tensor-core M2L: number of list-2 slots summed in the tensor-core (TMEM)
+ * accumulator before the sum is added, with round-to-nearest FP32 additions,
+ * into the tile's running sum (default 1; 0 = one tensor-core sum per tile).
+ * Smaller groups bound the accumulation error of the tensor cores: on
+ * adaptive trees one slot per group is more accurate than the FP32 CUDA-core
+ * form, four per group is not.  No counterpart in the reference.  Returns 1 if negative. */
+int fmm3d_set_tensor_m2l_group(int slots);
+
+/* Self-test of the tensor-core path on the current device: D (128 x N, row
+ * major) = A (128 x K) B^T (B is N x K), FP32 host arrays, through the same
+ * staging, descriptors and TMEM reads as the M2L kernel.  N in 16..128 (a
+ * multiple of 16), K a multiple of 32; nprod 1 = TF32 high parts only,
+ * 3 = high and cross products, 4 = all four split products.  Returns 0, 1 on a bad argument, 2 on a CUDA error,
+ * 3 when a bounded wait expired.  No counterpart in the reference. */
+int fmm3d_tc_selftest(int N, int K, const float *A, const float *B, float *D, int nprod);
 int fmm3d_last_stats(long long *out, int n);
 
 /* Human-readable description of the last CUDA error on this thread. */
