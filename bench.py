@@ -699,6 +699,7 @@ def main(argv=None):
     if args.workload == "laplace":
         args.helm_n = 0
         args.batch_instances = 0
+        args.serve_requests = 0
     R = run_b200(args)
     R["F"].set_precision(1)
     e2e = None if args.no_e2e else run_e2e(args, R)

@@ -105,73 +105,96 @@ __device__ __forceinline__ void pair64(double dx, double dy, double dz, double2 
     }
 }
 
-// Warp-synchronous mixed-precision near field.  A CTA of two warps serves
-// one childless box; each lane owns two evaluation points (e, e+32 of its
-// warp's 64).  The box's own sources, which carry the largest and most
-// cancellation-prone terms, are summed in FP64 straight from global memory
-// (L1 broadcast); the sources of list 1 are streamed through a per-warp
-// 32-entry shared buffer in double-float coordinates and summed in FP32
-// with TwoSum-compensated accumulation across chunks, the next chunk being
-// prefetched into registers.  No block-wide barrier is needed.
-constexpr int kP2P32Threads = 64, kP2P32Warps = kP2P32Threads / 32, kEPT = 2;
+// Warp-synchronous mixed-precision near field.  A CTA is one warp and serves
+// one childless box in passes of 32, 64 or 128 evaluation points (one, two or
+// four per lane: e, e+32, e+64, e+96), chosen from the points left.  First the box's own sources, which carry
+// the largest and most cancellation-prone terms, are summed in FP64 straight
+// from global memory (L1 broadcast) and added to the outputs; their
+// accumulators are then dead.  The sources of list 1 follow in FP32: they
+// are streamed through a 32-entry shared buffer of float4 records (double-
+// float coordinates relative to the box centre, charge, dipole), the next
+// chunk being fetched into registers while the current one is used, each
+// chunk is summed in FP32 and folded into an FP32 (value, error) pair with
+// TwoSum (the pairs live in shared memory, one slot per lane, to keep the
+// register count at 128), and the result is added to the outputs.
+constexpr int kP2P32Threads = 32, kEPT = 4;   // at most four evaluation points per lane
 
-template <bool CHG, bool DIP>
-__global__ void __launch_bounds__(kP2P32Threads) k_p2p32(const int *leaves, TreeView tv, PointsSoA src,
-                                                          const double *tx, const double *ty, const double *tz,
-                                                          OutSoA outs, OutSoA outt, int do_src, int do_trg,
-                                                          int want_fs, int want_ft, int want_ps, int want_pt)
+template <bool CHG, bool DIP, int kEPT>
+__device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, const PointsSoA &src,
+                                           const double *tx, const double *ty, const double *tz, OutSoA &outs,
+                                           OutSoA &outt, int do_src, int do_trg, int want_fs, int want_ft,
+                                           int want_ps, int want_pt, float4 *wA, float4 *wB, float4 *wC,
+                                           float *wD, float (*whi)[32], float (*wlo)[32])
 {
-    __shared__ float wp[kP2P32Warps][6][32];
-    __shared__ float2 wq[kP2P32Warps][2][32];
-    __shared__ float wv[kP2P32Warps][3][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int b = leaves[blockIdx.x];
+    const int lane = threadIdx.x;
     const double cx = tv.center[3L * b], cy = tv.center[3L * b + 1], cz = tv.center[3L * b + 2];
     const int s0 = tv.src0[b], nsb = tv.nsrc[b], ns = do_src ? nsb : 0;
     const int t0 = tv.trg0[b], nt = do_trg ? tv.ntrg[b] : 0;
     const int ne = ns + nt;
     const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
-    for (int e0 = w * 32 * kEPT; e0 < ne; e0 += kP2P32Threads * kEPT) {
-        bool act[kEPT];
-        int self[kEPT];
-        double ed[kEPT][3];
-        float eh[kEPT][3], el[kEPT][3];
-        float hi[kEPT][8], lo[kEPT][8];
-#pragma unroll
-        for (int u = 0; u < kEPT; u++) {
-            const int e = e0 + lane + 32 * u;
-            act[u] = e < ne;
-            self[u] = -1;
-            double x = 0, y = 0, z = 0;
-            if (act[u]) {
-                if (e < ns) { int i = s0 + e; x = src.x[i]; y = src.y[i]; z = src.z[i]; self[u] = i; }
-                else { int i = t0 + e - ns; x = tx[i]; y = ty[i]; z = tz[i]; }
+    auto add_out = [&](int e, const double *r) {
+        if (e < ns) {
+            int i = s0 + e;
+            if (want_ps) outs.pot[i] = cadd(outs.pot[i], cmk(r[0], r[1]));
+            if (want_fs) {
+                outs.fx[i] = cadd(outs.fx[i], cmk(r[2], r[3]));
+                outs.fy[i] = cadd(outs.fy[i], cmk(r[4], r[5]));
+                outs.fz[i] = cadd(outs.fz[i], cmk(r[6], r[7]));
             }
-            ed[u][0] = x - cx; ed[u][1] = y - cy; ed[u][2] = z - cz;
-#pragma unroll
-            for (int c = 0; c < 3; c++) split_df(ed[u][c], eh[u][c], el[u][c]);
-#pragma unroll
-            for (int c = 0; c < 8; c++) { hi[u][c] = 0.f; lo[u][c] = 0.f; }
+        } else {
+            int i = t0 + e - ns;
+            if (want_pt) outt.pot[i] = cadd(outt.pot[i], cmk(r[0], r[1]));
+            if (want_ft) {
+                outt.fx[i] = cadd(outt.fx[i], cmk(r[2], r[3]));
+                outt.fy[i] = cadd(outt.fy[i], cmk(r[4], r[5]));
+                outt.fz[i] = cadd(outt.fz[i], cmk(r[6], r[7]));
+            }
         }
-        // the box's own sources in FP64
-        double a64[kEPT][8];
+    };
+    {
+        bool act[kEPT];
+        float eh[kEPT][3], el[kEPT][3];
+        {
+            // the box's own sources in FP64
+            int self[kEPT];
+            double ed[kEPT][3], a64[kEPT][8];
 #pragma unroll
-        for (int u = 0; u < kEPT; u++)
+            for (int u = 0; u < kEPT; u++) {
+                const int e = e0 + lane + 32 * u;
+                act[u] = e < ne;
+                self[u] = -1;
+                double x = 0, y = 0, z = 0;
+                if (act[u]) {
+                    if (e < ns) { int i = s0 + e; x = src.x[i]; y = src.y[i]; z = src.z[i]; self[u] = i; }
+                    else { int i = t0 + e - ns; x = tx[i]; y = ty[i]; z = tz[i]; }
+                }
+                ed[u][0] = x - cx; ed[u][1] = y - cy; ed[u][2] = z - cz;
 #pragma unroll
-            for (int c = 0; c < 8; c++) a64[u][c] = 0.0;
-        for (int k = 0; k < nsb; k++) {
-            const int i = s0 + k;
-            const double sx = src.x[i] - cx, sy = src.y[i] - cy, sz = src.z[i] - cz;
-            const double2 q = CHG ? src.q[i] : cmk(0, 0), d = DIP ? src.dq[i] : cmk(0, 0);
-            const double vx = DIP ? src.vx[i] : 0, vy = DIP ? src.vy[i] : 0, vz = DIP ? src.vz[i] : 0;
+                for (int c = 0; c < 8; c++) a64[u][c] = 0.0;
+            }
+            for (int k = 0; k < nsb; k++) {
+                const int i = s0 + k;
+                const double sx = src.x[i] - cx, sy = src.y[i] - cy, sz = src.z[i] - cz;
+                const double2 q = CHG ? src.q[i] : cmk(0, 0), d = DIP ? src.dq[i] : cmk(0, 0);
+                const double vx = DIP ? src.vx[i] : 0, vy = DIP ? src.vy[i] : 0, vz = DIP ? src.vz[i] : 0;
 #pragma unroll
-            for (int u = 0; u < kEPT; u++)
-                if (act[u] && i != self[u])
-                    pair64<CHG, DIP>(ed[u][0] - sx, ed[u][1] - sy, ed[u][2] - sz, q, d, vx, vy, vz, a64[u]);
+                for (int u = 0; u < kEPT; u++)
+                    if (act[u] && i != self[u])
+                        pair64<CHG, DIP>(ed[u][0] - sx, ed[u][1] - sy, ed[u][2] - sz, q, d, vx, vy, vz, a64[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < kEPT; u++) {
+                if (act[u]) add_out(e0 + lane + 32 * u, a64[u]);
+#pragma unroll
+                for (int c = 0; c < 3; c++) split_df(ed[u][c], eh[u][c], el[u][c]);
+            }
         }
+        if (nl <= 1) return;
         // list-1 sources in FP32, streamed per warp
+#pragma unroll
+        for (int c = 0; c < kEPT * 8; c++) { whi[c][lane] = 0.f; wlo[c][lane] = 0.f; }
         int j = 1, c0 = 0, js0 = 0, jn = 0;
-        if (nl > 1) { int jb = tv.l1_idx[l1a]; js0 = tv.src0[jb]; jn = tv.nsrc[jb]; }
+        { int jb = tv.l1_idx[l1a]; js0 = tv.src0[jb]; jn = tv.nsrc[jb]; }
         auto advance = [&]() {
             while (j < nl && c0 >= jn) {
                 j++;
@@ -180,15 +203,27 @@ __global__ void __launch_bounds__(kP2P32Threads) k_p2p32(const int *leaves, Tree
             }
         };
         advance();
-        double px = 0, py = 0, pz = 0, vxx = 0, vyy = 0, vzz = 0;
-        double2 pq = cmk(0, 0), pd = cmk(0, 0);
+        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pc = pa;
+        float pdz = 0.f;
         auto fetch = [&]() {
             int i = c0 + lane;
             if (j < nl && i < jn) {
                 i += js0;
-                px = src.x[i]; py = src.y[i]; pz = src.z[i];
-                if (CHG) pq = src.q[i];
-                if (DIP) { pd = src.dq[i]; vxx = src.vx[i]; vyy = src.vy[i]; vzz = src.vz[i]; }
+                split_df(src.x[i] - cx, pa.x, pb.x);
+                split_df(src.y[i] - cy, pa.y, pb.y);
+                split_df(src.z[i] - cz, pa.z, pb.z);
+                if (DIP) {
+                    pa.w = (float)src.vx[i];
+                    pb.w = (float)src.vy[i];
+                    pdz = (float)src.vz[i];
+                    const double2 d = src.dq[i];
+                    const double2 q = CHG ? src.q[i] : cmk(0, 0);
+                    pc = make_float4((float)q.x, (float)q.y, (float)d.x, (float)d.y);
+                } else {
+                    const double2 q = src.q[i];
+                    pa.w = (float)q.x;
+                    pb.w = (float)q.y;
+                }
             }
         };
         fetch();
@@ -196,14 +231,9 @@ __global__ void __launch_bounds__(kP2P32Threads) k_p2p32(const int *leaves, Tree
             const int cn = min(32, jn - c0);
             __syncwarp();
             if (lane < cn) {
-                split_df(px - cx, wp[w][0][lane], wp[w][3][lane]);
-                split_df(py - cy, wp[w][1][lane], wp[w][4][lane]);
-                split_df(pz - cz, wp[w][2][lane], wp[w][5][lane]);
-                if (CHG) wq[w][0][lane] = make_float2((float)pq.x, (float)pq.y);
-                if (DIP) {
-                    wq[w][1][lane] = make_float2((float)pd.x, (float)pd.y);
-                    wv[w][0][lane] = (float)vxx; wv[w][1][lane] = (float)vyy; wv[w][2][lane] = (float)vzz;
-                }
+                wA[lane] = pa;
+                wB[lane] = pb;
+                if (DIP) { wC[lane] = pc; wD[lane] = pdz; }
             }
             __syncwarp();
             c0 += 32;
@@ -216,45 +246,72 @@ __global__ void __launch_bounds__(kP2P32Threads) k_p2p32(const int *leaves, Tree
                 for (int c = 0; c < 8; c++) a[u][c] = 0.f;
 #pragma unroll 2
             for (int k = 0; k < cn; k++) {
-                const float sxh = wp[w][0][k], syh = wp[w][1][k], szh = wp[w][2][k];
-                const float sxl = wp[w][3][k], syl = wp[w][4][k], szl = wp[w][5][k];
-                const float2 q = CHG ? wq[w][0][k] : make_float2(0.f, 0.f);
-                const float2 d = DIP ? wq[w][1][k] : make_float2(0.f, 0.f);
-                const float vx = DIP ? wv[w][0][k] : 0.f, vy = DIP ? wv[w][1][k] : 0.f, vz = DIP ? wv[w][2][k] : 0.f;
+                const float4 A = wA[k], B = wB[k];
+                float2 q, d;
+                float vx = 0.f, vy = 0.f, vz = 0.f;
+                if (DIP) {
+                    const float4 C = wC[k];
+                    q = make_float2(C.x, C.y);
+                    d = make_float2(C.z, C.w);
+                    vx = A.w; vy = B.w; vz = wD[k];
+                } else {
+                    q = make_float2(A.w, B.w);
+                    d = make_float2(0.f, 0.f);
+                }
 #pragma unroll
                 for (int u = 0; u < kEPT; u++)
-                    pair32<CHG, DIP>(eh[u][0], eh[u][1], eh[u][2], el[u][0], el[u][1], el[u][2], sxh, syh, szh,
-                                     sxl, syl, szl, q, d, vx, vy, vz, a[u]);
+                    pair32<CHG, DIP>(eh[u][0], eh[u][1], eh[u][2], el[u][0], el[u][1], el[u][2], A.x, A.y, A.z,
+                                     B.x, B.y, B.z, q, d, vx, vy, vz, a[u]);
             }
 #pragma unroll
             for (int u = 0; u < kEPT; u++)
 #pragma unroll
-                for (int c = 0; c < 8; c++) two_sum_acc(hi[u][c], lo[u][c], a[u][c]);
+                for (int c = 0; c < 8; c++) {
+                    float h = whi[8 * u + c][lane], l = wlo[8 * u + c][lane];
+                    two_sum_acc(h, l, a[u][c]);
+                    whi[8 * u + c][lane] = h;
+                    wlo[8 * u + c][lane] = l;
+                }
         }
 #pragma unroll
         for (int u = 0; u < kEPT; u++) {
             if (!act[u]) continue;
-            const int e = e0 + lane + 32 * u;
             double r[8];
 #pragma unroll
-            for (int c = 0; c < 8; c++) r[c] = a64[u][c] + ((double)hi[u][c] + (double)lo[u][c]);
-            if (e < ns) {
-                int i = s0 + e;
-                if (want_ps) outs.pot[i] = cadd(outs.pot[i], cmk(r[0], r[1]));
-                if (want_fs) {
-                    outs.fx[i] = cadd(outs.fx[i], cmk(r[2], r[3]));
-                    outs.fy[i] = cadd(outs.fy[i], cmk(r[4], r[5]));
-                    outs.fz[i] = cadd(outs.fz[i], cmk(r[6], r[7]));
-                }
-            } else {
-                int i = t0 + e - ns;
-                if (want_pt) outt.pot[i] = cadd(outt.pot[i], cmk(r[0], r[1]));
-                if (want_ft) {
-                    outt.fx[i] = cadd(outt.fx[i], cmk(r[2], r[3]));
-                    outt.fy[i] = cadd(outt.fy[i], cmk(r[4], r[5]));
-                    outt.fz[i] = cadd(outt.fz[i], cmk(r[6], r[7]));
-                }
-            }
+            for (int c = 0; c < 8; c++) r[c] = (double)whi[8 * u + c][lane] + (double)wlo[8 * u + c][lane];
+            add_out(e0 + lane + 32 * u, r);
+        }
+    }
+}
+
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, TreeView tv, PointsSoA src,
+                                                          const double *tx, const double *ty, const double *tz,
+                                                          OutSoA outs, OutSoA outt, int do_src, int do_trg,
+                                                          int want_fs, int want_ft, int want_ps, int want_pt)
+{
+    // per source: A = (x hi, y hi, z hi, charge re | vx), B = (x lo, y lo, z lo, charge im | vy),
+    // C = (charge re, charge im, dipstr re, dipstr im), D = vz   (C, D with dipoles only)
+    __shared__ float4 wA[32], wB[32], wC[32];
+    __shared__ float wD[32];
+    __shared__ float whi[kEPT * 8][32], wlo[kEPT * 8][32];   // TwoSum pairs, [component][lane]
+    const int b = leaves[blockIdx.x];
+    const int ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
+    // passes of 32, 64 or 128 evaluation points (one, two or four per lane)
+    for (int e0 = 0; e0 < ne;) {
+        const int left = ne - e0;
+        if (left <= 32) {
+            p2p32_pass<CHG, DIP, 1>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+            e0 += 32;
+        } else if (left <= 64) {
+            p2p32_pass<CHG, DIP, 2>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+            e0 += 64;
+        } else {
+            p2p32_pass<CHG, DIP, 4>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+            e0 += 128;
         }
     }
 }
