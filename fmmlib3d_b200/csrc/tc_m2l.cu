@@ -84,6 +84,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
     constexpr uint32_t STB = 4 * OPB;          // A_hi, A_lo, B_hi, B_lo
     constexpr int TPP = kTcThreads / KB;       // targets staged per pass
     constexpr int NPASS = 128 / TPP;
+    constexpr int NA = 64 * KB / kTcThreads;   // operator pairs staged per thread
+    static_assert(64 * KB % kTcThreads == 0, "stage tasks must divide evenly");
     extern __shared__ unsigned char tc_smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smraw + 127) & ~(uintptr_t)127);
     __shared__ uint64_t mbar[S];
@@ -161,21 +163,36 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
             if (!__syncthreads_or(have)) break;
             const float2 *Tu = T + slot_toff[tile.slot0 + si];
             const int nk = (2 * R + KC - 1) / KC;
-            for (int kc = 0; kc < nk; kc++, it++) {
-                const int st = it % S;
-                unsigned char *base = sm + st * STB;
-                int late = 0;
-                if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
-                const int jb = kc * (KC / 2);      // first complex column of this stage
-                // A: operator rows row0 .. row0 + 63, columns jb .. jb + KC/2 - 1 (column-major T)
-                for (int task = tid; task < 64 * KB; task += kTcThreads) {
-                    const int i = task & 63, kb = task >> 6;
+            // registers of one stage: operator pairs (A) and multipole pairs (B)
+            float2 ra0[NA], ra1[NA];
+            float4 rb[NPASS];
+            // A: operator rows row0 .. row0 + 63, columns jb .. jb + KC/2 - 1 (column-major T);
+            // B: the gathered source multipoles, coefficients jb .. jb + KC/2 - 1
+            auto load = [&](int kc) {
+                const int jb = kc * (KC / 2);
+#pragma unroll
+                for (int a = 0; a < NA; a++) {
+                    const int task = tid + a * kTcThreads, i = task & 63, kb = task >> 6;
                     const int row = row0 + i, j0 = jb + 2 * kb;
-                    float2 v0 = make_float2(0.f, 0.f), v1 = v0;
-                    if (row < R) {
-                        if (j0 < R) v0 = Tu[(size_t)j0 * R + row];
-                        if (j0 + 1 < R) v1 = Tu[(size_t)(j0 + 1) * R + row];
+                    ra0[a] = (row < R && j0 < R) ? Tu[(size_t)j0 * R + row] : make_float2(0.f, 0.f);
+                    ra1[a] = (row < R && j0 + 1 < R) ? Tu[(size_t)(j0 + 1) * R + row] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int j = 0; j < NPASS; j++) {
+                    const int n = tid / KB + TPP * j, kb = tid % KB, j0 = jb + 2 * kb;
+                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (n < N && sbr[j] >= 0 && j0 < R) {
+                        v = *(const float4 *)(mp + (size_t)sbr[j] * ldm + j0);
+                        if (j0 + 1 >= R) { v.z = 0.f; v.w = 0.f; }
                     }
+                    rb[j] = v;
+                }
+            };
+            auto store = [&](unsigned char *base) {
+#pragma unroll
+                for (int a = 0; a < NA; a++) {
+                    const int task = tid + a * kTcThreads, i = task & 63, kb = task >> 6;
+                    const float2 v0 = ra0[a], v1 = ra1[a];
                     float4 h, l;
                     unsigned char *ah = base + kb * kTcLBO, *al = base + OPB + kb * kTcLBO;
                     split4(make_float4(v0.x, -v0.y, v1.x, -v1.y), h, l);
@@ -185,22 +202,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
                     *(float4 *)(ah + (64 + i) * 16) = h;
                     *(float4 *)(al + (64 + i) * 16) = l;
                 }
-                // B: the gathered source multipoles, coefficients jb .. jb + KC/2 - 1
 #pragma unroll
                 for (int j = 0; j < NPASS; j++) {
                     const int n = tid / KB + TPP * j, kb = tid % KB;
                     if (n >= N) continue;
-                    const int sb = sbr[j], j0 = jb + 2 * kb;
-                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (sb >= 0 && j0 < R) {
-                        v = *(const float4 *)(mp + (size_t)sb * ldm + j0);
-                        if (j0 + 1 >= R) { v.z = 0.f; v.w = 0.f; }
-                    }
                     float4 h, l;
-                    split4(v, h, l);
+                    split4(rb[j], h, l);
                     *(float4 *)(base + 2 * OPB + kb * kTcLBO + n * 16) = h;
                     *(float4 *)(base + 3 * OPB + kb * kTcLBO + n * 16) = l;
                 }
+            };
+            load(0);
+            for (int kc = 0; kc < nk; kc++, it++) {
+                const int st = it % S;
+                int late = 0;
+                if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
+                store(sm + st * STB);
+                if (kc + 1 < nk) load(kc + 1);     // next stage's loads in flight during this one's MMAs
                 fence_async_smem();
                 if (__syncthreads_or(late)) { aborted = true; break; }
                 if (tid == 0) {
