@@ -71,9 +71,9 @@ UNIT = "points/s"
 # counting sqrt and divide as one flop each
 P2P_FLOPS_PER_PAIR = 62
 P2P_FLOPS_CHARGE = 31
-# DRAM bytes per P2P launch from the committed ncu capture (profiles/), scaled
-# to the full workload by pairs; None until a capture exists.
-P2P_DRAM_BYTES_PER_PAIR = None
+# DRAM bytes per evaluation point of one mixed-form P2P launch (k_p2p32), from the
+# committed ncu capture (profiles/); traffic scales with the points, not the pairs.
+P2P_DRAM_BYTES_PER_POINT = 208.6   # 834.6 MB per launch at N = M = 2,000,000 (4M evaluation points)
 
 
 def parse_args(argv=None):
@@ -370,9 +370,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_peak(torch, dev, dtype):
-    """cuBLAS GEMM throughput (8192^3, best of 5, TF32 off) in TFLOP/s for dtype."""
-    torch.backends.cuda.matmul.allow_tf32 = False
+def measured_peak(torch, dev, dtype, tf32=False):
+    """cuBLAS GEMM throughput (8192^3, best of 5) in TFLOP/s for dtype; FP32 inputs run on the
+    CUDA cores (TF32 off) or, with tf32=True, on the tensor cores in TF32."""
+    torch.backends.cuda.matmul.allow_tf32 = bool(tf32)
     a = torch.randn(8192, 8192, dtype=dtype, device=dev)
     b = torch.randn(8192, 8192, dtype=dtype, device=dev)
     torch.matmul(a, b)
@@ -386,6 +387,7 @@ def measured_peak(torch, dev, dtype):
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
     del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
     return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
@@ -485,10 +487,11 @@ def run_b200(args):
         total_ms = ev[0].elapsed_time(ev[args.steps])
         total_ms = reduce_max(dist if ws > 1 else None, total_ms, dev)
         return dict(total_ms=total_ms, step_ms=step_ms, passes=passes, launches=launches, stats=F.last_stats(),
-                    clocks=clocks, errs=errors())
+                    clocks=clocks, errs=errors(), points=n + m)
 
     forms = {"mixed": measure(1), "fp64": measure(0)}
-    peaks = {"fp64": measured_peak(torch, dev, torch.float64), "fp32": measured_peak(torch, dev, torch.float32)}
+    peaks = {"fp64": measured_peak(torch, dev, torch.float64), "fp32": measured_peak(torch, dev, torch.float32),
+             "tf32": measured_peak(torch, dev, torch.float32, tf32=True)}
     return dict(n=n, m=m, ws=ws, rank=rank, forms=forms, peaks=peaks, torch=torch, F=F,
                 dist=dist if ws > 1 else None, arrays=(src, q, dq, dv, trg))
 
@@ -596,29 +599,34 @@ def run_helm(args, R):
     return out
 
 
-def roofline_of(M, peak, bound):
-    """Roofline of the dominant pass of one form, from the per-pass CUDA events of its timed steps."""
+PEAK_SOURCE = {"fp64": "cuBLAS DGEMM 8192^3", "fp32": "cuBLAS SGEMM 8192^3 (TF32 off, CUDA cores)",
+               "tf32": "cuBLAS SGEMM 8192^3 with TF32 (tensor cores)"}
+
+
+def roofline_of(M, peaks, form, tensor_m2l=False):
+    """Roofline of the dominant pass (and of P2P and M2L separately) of one form, from the per-pass
+    CUDA events of its timed steps.  P2P and M2L are compute passes: P2P on the CUDA cores (FP32 in
+    the mixed form, FP64 otherwise), M2L on the tensor cores (TF32) when the mixed form runs it there.
+    Peaks are cuBLAS GEMM rates measured in the same run (MEASURED_PEAKS.json holds HBM and bf16
+    figures only)."""
     keys = [k for k in M["passes"][0] if k not in ("total",)]
     mean = {k: float(np.mean([p[k] for p in M["passes"]])) for k in keys}
     top = max(mean, key=mean.get)
     st = M["stats"]
-    if top == "p2p":
-        flops = st["p2p_pairs"] * P2P_FLOPS_PER_PAIR
-        traffic = None if P2P_DRAM_BYTES_PER_PAIR is None else P2P_DRAM_BYTES_PER_PAIR * st["p2p_pairs"]
-    elif top == "m2l":
-        flops = sum(cnt * m2l_flops(pt) for pt, cnt in st["m2l_pt_hist"].items())
-        traffic = None
-    else:
-        flops, traffic = None, None
-    out = {"kernel": top, "bound": bound, "unit": "TFLOP/s", "peak": round(peak, 2),
-           "peak_source": "cuBLAS %s GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no %s figure)" % (
-               "DGEMM" if bound == "fp64" else "SGEMM (TF32 off)", bound),
-           "traffic": traffic, "pass_ms_mean": {k: round(v, 3) for k, v in mean.items()}}
-    if flops is not None:
-        ach = flops / (mean[top] * 1e-3) / 1e12
-        out.update(achieved=round(ach, 3), frac=round(ach / peak, 4), flops_per_launch=float(flops))
-    else:
-        out.update(achieved=None, frac=None)
+    cuda = "fp32" if form == "mixed" else "fp64"
+    per = {}
+    p2p_flops = st["p2p_pairs"] * P2P_FLOPS_PER_PAIR
+    m2l_fl = sum(cnt * m2l_flops(pt) for pt, cnt in st["m2l_pt_hist"].items())
+    for name, flops, bound in (("p2p", p2p_flops, cuda), ("m2l", m2l_fl, "tf32" if tensor_m2l else cuda)):
+        ach = flops / (mean[name] * 1e-3) / 1e12
+        per[name] = {"bound": "tensor" if bound == "tf32" else bound + " CUDA cores", "achieved": round(ach, 3),
+                     "peak": round(peaks[bound], 2), "unit": "TFLOP/s", "frac": round(ach / peaks[bound], 4),
+                     "peak_source": PEAK_SOURCE[bound] + ", measured in this run", "flops_per_launch": float(flops),
+                     "ms": round(mean[name], 3)}
+    per["p2p"]["traffic"] = None if P2P_DRAM_BYTES_PER_POINT is None else P2P_DRAM_BYTES_PER_POINT * M["points"]
+    out = dict(per.get(top, {"bound": None, "achieved": None, "peak": None, "unit": None, "frac": None}))
+    out.setdefault("traffic", None)
+    out.update(kernel=top, pass_ms_mean={k: round(v, 3) for k, v in mean.items()}, passes=per)
     return out
 
 
@@ -718,9 +726,9 @@ def main(argv=None):
             "dtype": "f32/f64 mixed (P2P, M2L in f32; tree, recurrences, other passes f64)",
             "data": "synthetic (seeded uniform cube; charges, dipoles)", "config": config_of(args, ws),
             "errors": head["errors"], "gpu_launches": int(sum(H["launches"])), "clocks": H["clocks"], "e2e": e2e,
-            "roofline": roofline_of(H, R["peaks"]["fp32"], "fp32"),
+            "roofline": roofline_of(H, R["peaks"], "mixed", tensor_m2l=args.tensor_m2l > 0),
             "forms": {"mixed": head, "fp64": dict(summary(R["forms"]["fp64"]),
-                                                  roofline=roofline_of(R["forms"]["fp64"], R["peaks"]["fp64"], "fp64"),
+                                                  roofline=roofline_of(R["forms"]["fp64"], R["peaks"], "fp64"),
                                                   gpu_launches=int(sum(R["forms"]["fp64"]["launches"])))},
             "stats": {k: v for k, v in H["stats"].items() if k != "m2l_pt_hist"}}
     line["forms"]["mixed_over_fp64"] = round(head["value"] / line["forms"]["fp64"]["value"], 3)
