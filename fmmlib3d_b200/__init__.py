@@ -64,6 +64,18 @@ _lib.fmm3d_set_tensor_m2l_group.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l_group.restype = _I
 _lib.fmm3d_tc_selftest.argtypes = [_I, _I, _P, _P, _P, _I]
 _lib.fmm3d_tc_selftest.restype = _I
+_lib.fmm3d_lfmm3d_plan_create.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, ctypes.POINTER(_P)]
+_lib.fmm3d_lfmm3d_plan_create.restype = _I
+_lib.fmm3d_lfmm3d_plan_execute.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P]
+_lib.fmm3d_lfmm3d_plan_execute.restype = _I
+_lib.fmm3d_lfmm3d_plan_destroy.argtypes = [_P]
+_lib.fmm3d_lfmm3d_plan_destroy.restype = _I
+_lib.fmm3d_lfmm3d_plan_info.argtypes = [_P, _P, _I]
+_lib.fmm3d_lfmm3d_plan_info.restype = _I
+_lib.fmm3d_lfmm3d_plan_getb.argtypes = [_P, _I, _P, _P, _P]
+_lib.fmm3d_lfmm3d_plan_getb.restype = _I
+_lib.fmm3d_lfmm3d_plan_getl.argtypes = [_P, _I, _I, _P, ctypes.POINTER(_I)]
+_lib.fmm3d_lfmm3d_plan_getl.restype = _I
 _lib.fmm3d_last_timing.argtypes = [_P, _I]
 _lib.fmm3d_last_timing.restype = _I
 _lib.fmm3d_last_stats.argtypes = [_P, _I]
@@ -200,6 +212,64 @@ def lfmm3dparttarg_batched_device(iprec, src_offsets, source, charge, dipstr, di
         ptr(dipstr), ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld),
         None if to is None else _ptr(to), ptr(target), int(pottarg is not None), ptr(pottarg),
         int(fldtarg is not None), ptr(fldtarg), _P(stream))
+
+
+class LaplacePlan:
+    """A Laplace FMM geometry kept on the device: build once for fixed sources and
+    targets (device tensors, layouts as lfmm3dparttarg_device), then ``execute`` for
+    new charges / dipoles.  ``use_graph`` replays a CUDA graph of the passes.
+    ``getb`` / ``getl`` answer d3tgetb / d3tgetl queries (1-based boxes)."""
+
+    def __init__(self, iprec, source, ifcharge=1, ifdipole=0, ifpot=1, iffld=1, target=None, ifpottarg=0,
+                 iffldtarg=0, stream=0):
+        h = _P()
+        m = 0 if target is None else target.shape[0]
+        ier = _lib.fmm3d_lfmm3d_plan_create(
+            iprec, source.shape[0], _P(source.data_ptr()), ifcharge, ifdipole, ifpot, iffld, m,
+            None if target is None else _P(target.data_ptr()), ifpottarg, iffldtarg, _P(stream), ctypes.byref(h))
+        if ier != 0:
+            raise RuntimeError("plan creation failed, ier=%d: %s" % (ier, last_error()))
+        self._h = h
+
+    def execute(self, charge=None, dipstr=None, dipvec=None, pot=None, fld=None, pottarg=None, fldtarg=None,
+                use_graph=True, stream=0):
+        def ptr(t):
+            return None if t is None else _P(t.data_ptr())
+        return _lib.fmm3d_lfmm3d_plan_execute(self._h, ptr(charge), ptr(dipstr), ptr(dipvec), ptr(pot), ptr(fld),
+                                              ptr(pottarg), ptr(fldtarg), int(bool(use_graph)), _P(stream))
+
+    def info(self):
+        out = np.zeros(10)
+        _lib.fmm3d_lfmm3d_plan_info(self._h, _ptr(out), 10)
+        keys = ["nboxes", "nlev", "nleaves", "nterms", "nsource", "ntarget"]
+        d = {k: int(out[i]) for i, k in enumerate(keys)}
+        d["center"], d["size"] = out[6:9].copy(), float(out[9])
+        return d
+
+    def getb(self, ibox):
+        box = np.zeros(20, np.int32)
+        c = np.zeros(3)
+        corners = np.zeros((8, 3))
+        ier = _lib.fmm3d_lfmm3d_plan_getb(self._h, int(ibox), _ptr(box), _ptr(c), _ptr(corners))
+        return ier, box, c, corners
+
+    def getl(self, ibox, itype):
+        n = _I(0)
+        _lib.fmm3d_lfmm3d_plan_getl(self._h, int(ibox), int(itype), None, ctypes.byref(n))
+        lst = np.zeros(max(n.value, 1), np.int32)
+        ier = _lib.fmm3d_lfmm3d_plan_getl(self._h, int(ibox), int(itype), _ptr(lst), ctypes.byref(n))
+        return ier, lst[:n.value]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fmm3d_lfmm3d_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 -- interpreter shutdown
+            pass
 
 
 def _zk(zk):

@@ -295,66 +295,101 @@ __global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int 
         if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
 }
 
-// ---------------------------------------------------------------- the FMM
-// so / to (optional): instance offsets of a batch, each instance an
-// independent FMM over its own sources and targets (a forest, one root each).
-static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
-                          const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
-                          double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
-                          int iffldtarg, double *d_fldtarg, cudaStream_t s, const std::vector<int> *so = nullptr,
-                          const std::vector<int> *to = nullptr)
+// ---------------------------------------------------------------- one evaluation geometry
+// Device state of a Laplace evaluation for fixed sources and targets: tree and
+// lists, tree-ordered coordinates, expansion and output workspace, translation
+// tiles.  A single call builds it and runs the passes once; a plan
+// (fmm3d_lfmm3d_plan_*) keeps it and runs the passes for new charges.
+struct LapSetup {
+    int iprec = 0, p = 0, K = 0, ns = 0, nt = 0, ldm = 0;
+    int ifcharge = 0, ifdipole = 0, ifpot = 0, iffld = 0, ifpottarg = 0, iffldtarg = 0;
+    int do_src = 0, do_trg = 0, prune = 0;
+    bool mixed = false, dense = false, tcm2l = false;
+    std::shared_ptr<LapPlan> plan;
+    Tree T;
+    TreeView tv;
+    DBuf<double> sx, sy, sz, svx, svy, svz, tx, ty, tz;
+    DBuf<double2> sq, sdq, opot, ofx, ofy, ofz, tpot, tfx, tfy, tfz, mpole, local;
+    DBuf<float2> mp32;
+    DBuf<int> tcerr;
+    DBuf<Tile> dtiles;
+    std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
+    int m2l_a = 0, m2l_n = 0;
+    PointsSoA P;
+    OutSoA os, ot;
+};
+
+// charges and dipoles into tree order (l3dreorder, src/lfmm3drouts.f:667-691)
+__global__ void k_gather_q(int n, const int *perm, const double *q, const double *dq, const double *dv, int ifc,
+                           int ifd, PointsSoA o)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long j = perm[i];
+    if (ifc) o.q[i] = make_double2(q[2 * j], q[2 * j + 1]);
+    if (ifd) {
+        o.dq[i] = make_double2(dq[2 * j], dq[2 * j + 1]);
+        o.vx[i] = dv[3 * j];
+        o.vy[i] = dv[3 * j + 1];
+        o.vz[i] = dv[3 * j + 2];
+    }
+}
+
+// Geometry-dependent part: operator plan, tree and lists, sorted coordinates,
+// workspace and tiles.  so / to (optional): instance offsets of a batch, each
+// instance an independent FMM over its own sources and targets (a forest).
+static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int ifcharge, int ifdipole, int ifpot,
+                     int iffld, int nt, const double *d_trg, int ifpottarg, int iffldtarg, cudaStream_t s, Timer &tm,
+                     const std::vector<int> *so = nullptr, const std::vector<int> *to = nullptr)
 {
     Status st;
-    g_launch_count = 0;
     double eps;
     int nbox;
     if (ns < 1 || !lap_iprec(iprec, ns, nt, eps, nbox)) return 4;
     if (nt < 0) nt = 0;
-    if (ifpottarg != 1 && iffldtarg != 1) nt = nt;  // targets still shape the tree, as in the reference
     lap_init_constants(st);
     keep_pool_memory();
-    int p = l3dterms(eps);
+    const int p = l3dterms(eps);
     if (p > 72) return 16;
-    auto plan = get_plan(p, eps, s, st);
-    if (!st.ok() || !plan) { g_ti.err = cudaGetErrorString(st.err); return 16; }
-    Timer tm(s, g_ti.timing);
+    S.plan = get_plan(p, eps, s, st);
+    if (!st.ok() || !S.plan) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    auto &plan = S.plan;
+    S.iprec = iprec; S.p = p; S.K = (p + 1) * (p + 1); S.ns = ns; S.nt = nt;
+    S.ifcharge = ifcharge; S.ifdipole = ifdipole; S.ifpot = ifpot; S.iffld = iffld;
+    S.ifpottarg = ifpottarg; S.iffldtarg = iffldtarg;
     tm.mark();
-    Tree T;
+    Tree &T = S.T;
     if (so) build_forest(T, d_src, *so, d_trg, *to, nbox, s, st);
     else build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
     tm.mark();
-    const int K = (p + 1) * (p + 1);
-    // sorted point arrays
-    DBuf<double> sx, sy, sz, svx, svy, svz, tx, ty, tz;
-    DBuf<double2> sq, sdq;
-    DBuf<double2> opot, ofx, ofy, ofz, tpot, tfx, tfy, tfz;
-    DBuf<double2> mpole, local;
-    bool ok = sx.alloc(ns, s, st) && sy.alloc(ns, s, st) && sz.alloc(ns, s, st);
-    if (ifcharge == 1) ok = ok && sq.alloc(ns, s, st);
-    if (ifdipole == 1) ok = ok && sdq.alloc(ns, s, st) && svx.alloc(ns, s, st) && svy.alloc(ns, s, st) && svz.alloc(ns, s, st);
-    if (nt) ok = ok && tx.alloc(nt, s, st) && ty.alloc(nt, s, st) && tz.alloc(nt, s, st);
-    int do_src = ifpot == 1 || iffld == 1, do_trg = (ifpottarg == 1 || iffldtarg == 1) && nt > 0;
-    if (ifpot == 1) ok = ok && opot.alloc(ns, s, st);
-    if (iffld == 1) ok = ok && ofx.alloc(ns, s, st) && ofy.alloc(ns, s, st) && ofz.alloc(ns, s, st);
-    if (do_trg && ifpottarg == 1) ok = ok && tpot.alloc(nt, s, st);
-    if (do_trg && iffldtarg == 1) ok = ok && tfx.alloc(nt, s, st) && tfy.alloc(nt, s, st) && tfz.alloc(nt, s, st);
+    const int K = S.K;
+    bool ok = S.sx.alloc(ns, s, st) && S.sy.alloc(ns, s, st) && S.sz.alloc(ns, s, st);
+    if (ifcharge == 1) ok = ok && S.sq.alloc(ns, s, st);
+    if (ifdipole == 1)
+        ok = ok && S.sdq.alloc(ns, s, st) && S.svx.alloc(ns, s, st) && S.svy.alloc(ns, s, st) && S.svz.alloc(ns, s, st);
+    if (nt) ok = ok && S.tx.alloc(nt, s, st) && S.ty.alloc(nt, s, st) && S.tz.alloc(nt, s, st);
+    S.do_src = ifpot == 1 || iffld == 1;
+    S.do_trg = (ifpottarg == 1 || iffldtarg == 1) && nt > 0;
+    if (ifpot == 1) ok = ok && S.opot.alloc(ns, s, st);
+    if (iffld == 1) ok = ok && S.ofx.alloc(ns, s, st) && S.ofy.alloc(ns, s, st) && S.ofz.alloc(ns, s, st);
+    if (S.do_trg && ifpottarg == 1) ok = ok && S.tpot.alloc(nt, s, st);
+    if (S.do_trg && iffldtarg == 1) ok = ok && S.tfx.alloc(nt, s, st) && S.tfy.alloc(nt, s, st) && S.tfz.alloc(nt, s, st);
     if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    if (!mpole.alloc((size_t)T.nboxes * K, s, st) || !local.alloc((size_t)T.nboxes * K, s, st)) {
+    if (!S.mpole.alloc((size_t)T.nboxes * K, s, st) || !S.local.alloc((size_t)T.nboxes * K, s, st)) {
         g_ti.err = cudaGetErrorString(st.err);
         return 16;
     }
-    mpole.zero(st);
-    local.zero(st);
-    PointsSoA P;
-    P.x = sx.p; P.y = sy.p; P.z = sz.p; P.q = sq.p; P.dq = sdq.p; P.vx = svx.p; P.vy = svy.p; P.vz = svz.p;
-    k_gather_src<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, d_q, d_dq, d_dv, ifcharge == 1,
-                                                 ifdipole == 1, P); FMM_COUNT_LAUNCH();
-    if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }
+    PointsSoA &P = S.P;
+    P.x = S.sx.p; P.y = S.sy.p; P.z = S.sz.p; P.q = S.sq.p; P.dq = S.sdq.p;
+    P.vx = S.svx.p; P.vy = S.svy.p; P.vz = S.svz.p;
+    k_gather_pts<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, S.sx.p, S.sy.p, S.sz.p); FMM_COUNT_LAUNCH();
+    if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, S.tx.p, S.ty.p, S.tz.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
-    tm.mark();
-    TreeView tv = make_treeview(T);
-    int prune = !(ifpot == 1 || iffld == 1);
+    S.tv = make_treeview(T);
+    S.prune = !(ifpot == 1 || iffld == 1);
+    S.os.pot = S.opot.p; S.os.fx = S.ofx.p; S.os.fy = S.ofy.p; S.os.fz = S.ofz.p;
+    S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
     // tiles per (level, octant) group
     auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot, std::vector<Tile> &out) {
@@ -372,126 +407,417 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
         }
     };
     std::vector<Tile> htiles;
-    std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
     for (int l = T.nlev - 1; l >= 2; l--) {
         int a = (int)htiles.size();
         make_tiles(l, plan->kt, kSlotM2M, 0, 8, htiles);
-        m2m_rng.push_back({a, (int)htiles.size() - a});
+        S.m2m_rng.push_back({a, (int)htiles.size() - a});
     }
-    const bool mixed = g_precision == 1 && iprec <= 1 && plan->dense;
-    const bool dense = (plan->dense && g_m2l_mode != 1) || mixed;
-    int m2l_a = (int)htiles.size();
-    const bool tcm2l = mixed && g_tc_m2l > 0;
-    const int m2l_kt = tcm2l ? kTcTileTargets : dense ? kDenseTileTargets : plan->kt;
+    S.mixed = g_precision == 1 && iprec <= 1 && plan->dense;
+    S.dense = (plan->dense && g_m2l_mode != 1) || S.mixed;
+    S.tcm2l = S.mixed && g_tc_m2l > 0;
+    const int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt;
+    S.m2l_a = (int)htiles.size();
     for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
-    int m2l_n = (int)htiles.size() - m2l_a;
+    S.m2l_n = (int)htiles.size() - S.m2l_a;
     for (int l = 2; l <= T.nlev - 1; l++) {
         int a = (int)htiles.size();
         make_tiles(l + 1, plan->kt, kSlotL2L, 1, 1, htiles);
-        l2l_rng.push_back({a, (int)htiles.size() - a});
+        S.l2l_rng.push_back({a, (int)htiles.size() - a});
     }
-    DBuf<Tile> dtiles;
     if (!htiles.empty()) {
-        dtiles.alloc(htiles.size(), s, st);
-        FMM_TRY(st, cudaMemcpyAsync(dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
+        S.dtiles.alloc(htiles.size(), s, st);
+        FMM_TRY(st, cudaMemcpyAsync(S.dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
     }
-    OutSoA os, ot;
-    os.pot = opot.p; os.fx = ofx.p; os.fy = ofy.p; os.fz = ofz.p;
-    ot.pot = tpot.p; ot.fx = tfx.p; ot.fy = tfy.p; ot.fz = tfz.p;
+    S.ldm = K + (K & 1);
+    if (S.tcm2l && (!S.mp32.alloc((size_t)T.nboxes * S.ldm, s, st) || !S.tcerr.alloc(1, s, st))) {
+        g_ti.err = cudaGetErrorString(st.err);
+        return 16;
+    }
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
 
+// Charge-dependent part: charges into tree order, the eight passes of
+// lfmm3dparttargmain (src/lfmm3dpart.f:528-1169) and the scatter back into the
+// caller's order.  Stream work only (no host synchronisation, no allocation),
+// so a plan captures it in a CUDA graph.
+static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const double *d_dv, double *d_pot,
+                       double *d_fld, double *d_pottarg, double *d_fldtarg, cudaStream_t s, Timer &tm, Status &st)
+{
+    Tree &T = S.T;
+    auto &plan = S.plan;
+    const int p = S.p, K = S.K, ns = S.ns, nt = S.nt;
+    const TreeView &tv = S.tv;
+    const PointsSoA &P = S.P;
+    const int prune = S.prune;
+    if (S.ifcharge == 1 || S.ifdipole == 1) {
+        k_gather_q<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_q, d_dq, d_dv, S.ifcharge == 1,
+                                                   S.ifdipole == 1, P); FMM_COUNT_LAUNCH();
+    }
+    FMM_TRY(st, cudaMemsetAsync(S.mpole.p, 0, sizeof(double2) * S.mpole.n, s));
+    FMM_TRY(st, cudaMemsetAsync(S.local.p, 0, sizeof(double2) * S.local.n, s));
+    FMM_LAUNCH_CHECK(st);
+    tm.mark();
     // STEP 1: P2M at every childless box
-    launch_p2m(T.leaves.p, T.nleaves, tv, P, ifcharge, ifdipole, p, mpole.p, s, st);
+    launch_p2m(T.leaves.p, T.nleaves, tv, P, S.ifcharge, S.ifdipole, p, S.mpole.p, s, st);
     tm.mark();
     // STEP 3: M2M, levels nlev-1 .. 2
-    for (auto &r : m2m_rng)
-        launch_translate(0, dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, mpole.p, mpole.p, prune, plan->kt, s, st);
+    for (auto &r : S.m2m_rng)
+        launch_translate(0, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, plan->kt, s, st);
     tm.mark();
     // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
-    launch_p2l(T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, p, local.p, s, st);
+    launch_p2l(T.grouped.p, T.nboxes, tv, P, S.ifcharge, S.ifdipole, p, S.local.p, s, st);
     tm.mark();
     // STEP 4: M2L over list 2, all levels >= 2
-    DBuf<float2> mp32;
-    DBuf<int> tcerr;
-    const int ldm = K + (K & 1);
-    if (tcm2l) {
-        if (!mp32.alloc((size_t)T.nboxes * ldm, s, st) || !tcerr.alloc(1, s, st)) {
-            g_ti.err = cudaGetErrorString(st.err);
-            return 16;
-        }
-        tcerr.zero(st);
-        convert_mp_f32(T.nboxes, K, ldm, mpole.p, mp32.p, s, st);
-        launch_m2l_tc(g_tc_m2l - 1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
-                      plan->T32.p, tv, p, mp32.p, ldm, local.p, prune, 3, g_tc_group, tcerr.p, s, st);
-    } else if (mixed)
-        launch_m2l_dense32(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T32.p, tv,
-                           p, mpole.p, local.p, prune, s, st);
-    else if (dense)
-        launch_m2l_dense(dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p, tv, p,
-                         mpole.p, local.p, prune, s, st);
+    if (S.tcm2l) {
+        FMM_TRY(st, cudaMemsetAsync(S.tcerr.p, 0, sizeof(int), s));
+        convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, s, st);
+        launch_m2l_tc(g_tc_m2l - 1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, s, st);
+    } else if (S.mixed)
+        launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+                           plan->T32.p, tv, p, S.mpole.p, S.local.p, prune, s, st);
+    else if (S.dense)
+        launch_m2l_dense(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p,
+                         tv, p, S.mpole.p, S.local.p, prune, s, st);
     else
-        launch_translate(1, dtiles.p + m2l_a, m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p, plan->dc.p,
-                         plan->lddc, mpole.p, local.p, prune, plan->kt, s, st);
+        launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt, s, st);
     tm.mark();
     // STEP 5: L2L, levels 2 .. nlev-1
-    for (auto &r : l2l_rng)
-        launch_translate(2, dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, local.p, local.p, prune, plan->kt, s, st);
+    for (auto &r : S.l2l_rng)
+        launch_translate(2, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, plan->kt, s, st);
     tm.mark();
     // STEPS 6, 7: M2P from list 3 and L2P (writes the outputs)
-    launch_eval(T.leaves.p, T.nleaves, tv, sx.p, sy.p, sz.p, tx.p, ty.p, tz.p, p, mpole.p, local.p, os, ot,
-                do_src, do_trg, s, st);
+    launch_eval(T.leaves.p, T.nleaves, tv, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
+                S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
     tm.mark();
     // STEP 8: P2P over self and list 1 (adds to the outputs)
-    if (mixed)
-        launch_p2p32(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
-                     do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+    const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
+    if (S.mixed)
+        launch_p2p32(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
+                     S.ifpot, S.iffld, ppt, pft, s, st);
     else
-        launch_p2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, os, ot, ifcharge, ifdipole, ifpot, iffld,
-                   do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+        launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
+                   S.ifpot, S.iffld, ppt, pft, s, st);
     tm.mark();
     // unsort into the caller's order
-    if (do_src) {
-        k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, os, ifpot == 1 ? d_pot : nullptr,
-                                                      iffld == 1 ? d_fld : nullptr); FMM_COUNT_LAUNCH();
+    if (S.do_src) {
+        k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, S.os, S.ifpot == 1 ? d_pot : nullptr,
+                                                      S.iffld == 1 ? d_fld : nullptr); FMM_COUNT_LAUNCH();
     }
-    if (do_trg) {
-        k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, ot, ifpottarg == 1 ? d_pottarg : nullptr,
-                                                      iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
+    if (S.do_trg) {
+        k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, S.ot, S.ifpottarg == 1 ? d_pottarg : nullptr,
+                                                      S.iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
     }
     FMM_LAUNCH_CHECK(st);
     tm.mark();
-    tm.finish(g_ti.ms);
-    // statistics (on request: they cost a few kernels and a device->host read)
-    if (g_ti.want_stats) {
-        DBuf<unsigned long long> acc;
-        acc.alloc(1 + 128, s, st);
-        acc.zero(st);
-        if (st.ok()) {
-            k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, tv, do_src, do_trg, acc.p); FMM_COUNT_LAUNCH();
-            for (int l = 2; l <= T.nlev; l++) {
-                k_m2l_count<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], tv,
-                                                                       plan->slots.p, prune, acc.p + 1); FMM_COUNT_LAUNCH();
-            }
-            std::vector<unsigned long long> h(129);
-            FMM_TRY(st, cudaMemcpyAsync(h.data(), acc.p, sizeof(unsigned long long) * 129, cudaMemcpyDeviceToHost, s));
-            FMM_TRY(st, cudaStreamSynchronize(s));
-            long long m2l = 0;
-            for (int i = 0; i < 128; i++) m2l += (long long)h[1 + i];
-            g_ti.stats.assign(9 + 128, 0);
-            g_ti.stats[0] = T.nboxes; g_ti.stats[1] = T.nlev; g_ti.stats[2] = T.nleaves; g_ti.stats[3] = p;
-            g_ti.stats[7] = (long long)h[0];
-            g_ti.stats[8] = m2l;
-            for (int i = 0; i < 128; i++) g_ti.stats[9 + i] = (long long)h[1 + i];
-        }
+}
+
+// tree and interaction statistics of the last call (on request: a few kernels and a device->host read)
+static void lap_stats(LapSetup &S, cudaStream_t s, Status &st)
+{
+    Tree &T = S.T;
+    DBuf<unsigned long long> acc;
+    acc.alloc(1 + 128, s, st);
+    acc.zero(st);
+    if (!st.ok()) return;
+    k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, S.tv, S.do_src, S.do_trg,
+                                                                acc.p); FMM_COUNT_LAUNCH();
+    for (int l = 2; l <= T.nlev; l++) {
+        k_m2l_count<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], S.tv,
+                                                               S.plan->slots.p, S.prune, acc.p + 1); FMM_COUNT_LAUNCH();
     }
+    std::vector<unsigned long long> h(129);
+    FMM_TRY(st, cudaMemcpyAsync(h.data(), acc.p, sizeof(unsigned long long) * 129, cudaMemcpyDeviceToHost, s));
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    long long m2l = 0;
+    for (int i = 0; i < 128; i++) m2l += (long long)h[1 + i];
+    g_ti.stats.assign(9 + 128, 0);
+    g_ti.stats[0] = T.nboxes; g_ti.stats[1] = T.nlev; g_ti.stats[2] = T.nleaves; g_ti.stats[3] = S.p;
+    g_ti.stats[7] = (long long)h[0];
+    g_ti.stats[8] = m2l;
+    for (int i = 0; i < 128; i++) g_ti.stats[9 + i] = (long long)h[1 + i];
+}
+
+// Waits for the stream and turns launch errors and the tensor-core wait flag into ier.
+static int lap_finish(LapSetup &S, cudaStream_t s, Status &st)
+{
     int herr = 0;
-    if (tcm2l) FMM_TRY(st, cudaMemcpyAsync(&herr, tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (S.tcm2l) FMM_TRY(st, cudaMemcpyAsync(&herr, S.tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
     if (herr) { g_ti.err = "tensor-core M2L: a wait expired"; return 16; }
     return 0;
 }
+
+// ---------------------------------------------------------------- the FMM, one call
+static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
+                          const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
+                          double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
+                          int iffldtarg, double *d_fldtarg, cudaStream_t s, const std::vector<int> *so = nullptr,
+                          const std::vector<int> *to = nullptr)
+{
+    g_launch_count = 0;
+    Timer tm(s, g_ti.timing);
+    LapSetup S;
+    int ier = lap_setup(S, iprec, ns, d_src, ifcharge, ifdipole, ifpot, iffld, nt, d_trg, ifpottarg, iffldtarg, s, tm,
+                        so, to);
+    if (ier) return ier;
+    Status st;
+    lap_passes(S, d_q, d_dq, d_dv, d_pot, d_fld, d_pottarg, d_fldtarg, s, tm, st);
+    tm.finish(g_ti.ms);
+    if (g_ti.want_stats && st.ok()) lap_stats(S, s, st);
+    return lap_finish(S, s, st);
+}
+
+// ---------------------------------------------------------------- plans: fixed geometry, new charges
+// A plan keeps one evaluation geometry on the device (tree, lists, sorted
+// coordinates, workspace) and runs the charge-dependent passes for any number
+// of charge vectors.  The passes are captured once per set of caller pointers
+// and stream into a CUDA graph and replayed (one launch instead of ~150).
+// Tree queries mirror d3tgetb / d3tgetl (src/d3tstrcr.f:576-665).
+struct LapPlanExec {
+    LapSetup S;
+    std::mutex mu;
+    cudaStream_t made_on = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void *key[8] = {};
+    int graph_launches = 0;
+    std::vector<cudaStream_t> used;
+    // host copy of the tree for the queries (filled on first use)
+    bool host = false;
+    std::vector<int> level, ijk, parent, child, src0, nsrc, trg0, ntrg, coll;
+    std::vector<int> lst[6], lidx[6];   // CSR of lists 1, 3, 4 (index = list type)
+    std::vector<double> center, geom;   // geom: 4 per instance (centre, side)
+    std::vector<int> binst;
+};
+
+static void plan_host_tree(LapPlanExec &E, Status &st)
+{
+    if (E.host) return;
+    Tree &T = E.S.T;
+    const int nb = T.nboxes;
+    auto get = [&](std::vector<int> &h, const DBuf<int> &d, size_t n) {
+        h.resize(n);
+        if (n) FMM_TRY(st, cudaMemcpy(h.data(), d.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    };
+    get(E.level, T.level, nb); get(E.ijk, T.ijk, 3L * nb); get(E.parent, T.parent, nb); get(E.child, T.child, 8L * nb);
+    get(E.src0, T.src0, nb); get(E.nsrc, T.nsrc, nb); get(E.trg0, T.trg0, nb); get(E.ntrg, T.ntrg, nb);
+    get(E.coll, T.coll, 27L * nb);
+    const DBuf<int> *cs[6] = {nullptr, &T.l1_start, nullptr, &T.l3_start, &T.l4_start, nullptr};
+    const DBuf<int> *ci[6] = {nullptr, &T.l1_idx, nullptr, &T.l3_idx, &T.l4_idx, nullptr};
+    for (int ty : {1, 3, 4}) {
+        get(E.lst[ty], *cs[ty], nb + 1);
+        get(E.lidx[ty], *ci[ty], st.ok() && nb ? (size_t)E.lst[ty][nb] : 0);
+    }
+    E.center.resize(3L * nb);
+    if (nb) FMM_TRY(st, cudaMemcpy(E.center.data(), T.center.p, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost));
+    if (T.ninst > 1) {
+        get(E.binst, T.binst, nb);
+        E.geom.resize(4L * T.ninst);
+        FMM_TRY(st, cudaMemcpy(E.geom.data(), T.inst_geom.p, sizeof(double) * 4 * T.ninst, cudaMemcpyDeviceToHost));
+    }
+    E.host = st.ok();
+}
+
+}  // namespace fmm
+
+using namespace fmm;
+
+extern "C" {
+
+int fmm3d_lfmm3d_plan_create(int iprec, int nsource, const double *d_source, int ifcharge, int ifdipole, int ifpot,
+                             int iffld, int ntarget, const double *d_target, int ifpottarg, int iffldtarg,
+                             void *stream, void **plan)
+{
+    if (!plan) return 1;
+    *plan = nullptr;
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    g_launch_count = 0;
+    auto *E = new LapPlanExec;
+    Timer tm(s, false);
+    int ier = lap_setup(E->S, iprec, nsource, d_source, ifcharge, ifdipole, ifpot, iffld, ntarget, d_target,
+                        ifpottarg, iffldtarg, s, tm);
+    Status st;
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!ier && !st.ok()) { g_ti.err = cudaGetErrorString(st.err); ier = 16; }
+    if (ier) {
+        delete E;
+        return ier;
+    }
+    E->made_on = s;
+    E->used.push_back(s);
+    *plan = E;
+    return 0;
+}
+
+int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *d_dipstr, const double *d_dipvec,
+                              double *d_pot, double *d_fld, double *d_pottarg, double *d_fldtarg, int use_graph,
+                              void *stream)
+{
+    if (!plan) return 1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    if (std::find(E->used.begin(), E->used.end(), s) == E->used.end()) {
+        // the plan's buffers were made on another stream: order this one after it
+        cudaStreamSynchronize(E->made_on);
+        E->used.push_back(s);
+    }
+    Status st;
+    g_launch_count = 0;
+    if (use_graph) {
+        const void *key[8] = {d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, (const void *)s};
+        if (!E->exec || memcmp(key, E->key, sizeof key) != 0) {
+            if (E->exec) cudaGraphExecDestroy(E->exec);
+            E->exec = nullptr;
+            cudaGraph_t g = nullptr;
+            Timer off(s, false);
+            FMM_TRY(st, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            if (st.ok()) lap_passes(E->S, d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, s, off, st);
+            cudaError_t ce = cudaStreamEndCapture(s, &g);
+            if (st.ok() && ce != cudaSuccess) { st.err = ce; st.where = "cudaStreamEndCapture"; }
+            if (st.ok()) FMM_TRY(st, cudaGraphInstantiate(&E->exec, g, 0));
+            if (g) cudaGraphDestroy(g);
+            if (!st.ok()) {
+                E->exec = nullptr;
+                g_ti.err = std::string("graph capture: ") + cudaGetErrorString(st.err);
+                return 16;
+            }
+            memcpy(E->key, key, sizeof key);
+            E->graph_launches = g_launch_count;
+        }
+        FMM_TRY(st, cudaGraphLaunch(E->exec, s));
+        g_launch_count = E->graph_launches;
+        g_ti.ms.clear();
+    } else {
+        Timer tm(s, g_ti.timing);
+        tm.mark();
+        tm.mark();   // no tree work in an execute: the "tree" interval is empty
+        lap_passes(E->S, d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, s, tm, st);
+        tm.finish(g_ti.ms);
+    }
+    return lap_finish(E->S, s, st);
+}
+
+int fmm3d_lfmm3d_plan_destroy(void *plan)
+{
+    if (!plan) return 0;
+    auto *E = (LapPlanExec *)plan;
+    {
+        std::lock_guard<std::mutex> lk(E->mu);
+        for (auto s : E->used) cudaStreamSynchronize(s);
+        if (E->exec) cudaGraphExecDestroy(E->exec);
+        E->exec = nullptr;
+    }
+    delete E;
+    return 0;
+}
+
+// out[0..9] = nboxes, nlev, nleaves, nterms, nsource, ntarget, centre x, y, z, side of the root cube
+// (of the first instance for a batch)
+int fmm3d_lfmm3d_plan_info(void *plan, double *out, int n)
+{
+    if (!plan || !out) return 1;
+    auto *E = (LapPlanExec *)plan;
+    Tree &T = E->S.T;
+    const double v[10] = {(double)T.nboxes, (double)T.nlev, (double)T.nleaves, (double)E->S.p, (double)E->S.ns,
+                          (double)E->S.nt, T.center0[0], T.center0[1], T.center0[2], T.size};
+    for (int i = 0; i < n && i < 10; i++) out[i] = v[i];
+    return 0;
+}
+
+// d3tgetb: box(20), centre(3) and corners(3,8) of box ibox (1-based).  ier 2 for a bad ibox.
+int fmm3d_lfmm3d_plan_getb(void *plan, int ibox, int *box, double *center, double *corners)
+{
+    if (!plan) return 1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    Status st;
+    plan_host_tree(*E, st);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    const int nb = E->S.T.nboxes;
+    if (ibox < 1 || ibox > nb) return 2;
+    const int b = ibox - 1;
+    if (box) {
+        int nk = 0;
+        box[0] = E->level[b];
+        for (int k = 0; k < 3; k++) box[1 + k] = E->ijk[3L * b + k] + 1;
+        box[4] = E->parent[b] + 1;
+        for (int k = 0; k < 8; k++) box[5 + k] = 0;
+        for (int k = 0; k < 8; k++)
+            if (E->child[8L * b + k] >= 0) box[5 + nk++] = E->child[8L * b + k] + 1;
+        box[13] = E->src0[b] + 1;
+        box[14] = E->nsrc[b];
+        box[15] = E->trg0[b] + 1;
+        box[16] = E->ntrg[b];
+        box[17] = E->nsrc[b] == 0 ? 0 : (nk == 0 ? 1 : 2);
+        box[18] = E->ntrg[b] == 0 ? 0 : (nk == 0 ? 1 : 2);
+        box[19] = 0;
+    }
+    const double side = (E->binst.empty() ? E->S.T.size : E->geom[4L * E->binst[b] + 3]) / (double)(1L << E->level[b]);
+    const double *c = &E->center[3L * b];
+    if (center)
+        for (int k = 0; k < 3; k++) center[k] = c[k];
+    if (corners)
+        for (int q = 0; q < 8; q++) {
+            corners[3 * q] = c[0] + ((q >> 2) ? 0.5 : -0.5) * side;
+            corners[3 * q + 1] = c[1] + (((q >> 1) & 1) ? 0.5 : -0.5) * side;
+            corners[3 * q + 2] = c[2] + ((q & 1) ? 0.5 : -0.5) * side;
+        }
+    return 0;
+}
+
+// d3tgetl: list itype (1..5) of box ibox (1-based boxes in list[]); ier 4 when
+// the list is empty, 2 for a bad ibox or itype.  list must hold the list
+// (lists 2 and 5 at most 189 and 26 boxes; fmm3d_lfmm3d_plan_getl with
+// list = NULL returns the length in *nlist).
+int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlist)
+{
+    if (!plan || !nlist) return 1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    Status st;
+    plan_host_tree(*E, st);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    const int nb = E->S.T.nboxes;
+    *nlist = 0;
+    if (ibox < 1 || ibox > nb || itype < 1 || itype > 5) return 2;
+    const int b = ibox - 1;
+    std::vector<int> out;
+    if (itype == 1 || itype == 3 || itype == 4) {
+        for (int k = E->lst[itype][b]; k < E->lst[itype][b + 1]; k++) out.push_back(E->lidx[itype][k]);
+    } else if (itype == 5) {
+        for (int k = 0; k < 27; k++)
+            if (k != 13 && E->coll[27L * b + k] >= 0) out.push_back(E->coll[27L * b + k]);
+    } else {
+        // list 2: children of the parent's colleagues that do not touch b
+        const int P = E->parent[b];
+        if (P >= 0)
+            for (int k = 0; k < 27; k++) {
+                const int C = E->coll[27L * P + k];
+                if (C < 0) continue;
+                for (int o = 0; o < 8; o++) {
+                    const int c = E->child[8L * C + o];
+                    if (c < 0 || c == b) continue;
+                    bool touch = true;
+                    for (int d = 0; d < 3; d++) touch = touch && std::abs(E->ijk[3L * c + d] - E->ijk[3L * b + d]) <= 1;
+                    if (!touch) out.push_back(c);
+                }
+            }
+    }
+    *nlist = (int)out.size();
+    if (list)
+        for (size_t i = 0; i < out.size(); i++) list[i] = out[i] + 1;
+    return out.empty() ? 4 : 0;
+}
+
+}  // extern "C"
+
+namespace fmm {
 
 static int lap_direct_device(int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
                              const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,

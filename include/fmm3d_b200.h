@@ -203,6 +203,35 @@ int fmm3d_set_tensor_m2l_group(int slots);
 int fmm3d_tc_selftest(int N, int K, const float *A, const float *B, float *D, int nprod);
 int fmm3d_last_stats(long long *out, int n);
 
+/* ---- Plans: one geometry, many charge vectors (no counterpart in the reference's
+ * particle API; the tree queries mirror d3tgetb / d3tgetl, src/d3tstrcr.f:576-665).
+ * fmm3d_lfmm3d_plan_create builds the tree, lists, tree-ordered coordinates and
+ * all workspace for device arrays source(3,nsource) and target(3,ntarget) and the
+ * given output flags (the arithmetic form, fmm3d_set_precision, is fixed at
+ * creation).  fmm3d_lfmm3d_plan_execute runs the passes for device charge /
+ * dipole arrays (NULL where the plan's flag is off) and writes the requested
+ * outputs; with use_graph = 1 the passes are captured into a CUDA graph once
+ * per set of pointers and stream and replayed.  Results equal those of
+ * lfmm3dparttarg on the same inputs bitwise.  Calls on one plan are serialised.
+ * Returns ier as lfmm3dparttarg (1: NULL plan). */
+int fmm3d_lfmm3d_plan_create(int iprec, int nsource, const double *d_source, int ifcharge, int ifdipole, int ifpot,
+                             int iffld, int ntarget, const double *d_target, int ifpottarg, int iffldtarg,
+                             void *stream, void **plan);
+int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *d_dipstr, const double *d_dipvec,
+                              double *d_pot, double *d_fld, double *d_pottarg, double *d_fldtarg, int use_graph,
+                              void *stream);
+int fmm3d_lfmm3d_plan_destroy(void *plan);
+/* out[0..9]: nboxes, nlev, nleaves, nterms, nsource, ntarget, root centre (3), root side. */
+int fmm3d_lfmm3d_plan_info(void *plan, double *out, int n);
+/* d3tgetb: box(20) (level; i, j, k; parent; children; first source (1-based in tree
+ * order), count; first target, count; source and target type 0 empty / 1 leaf /
+ * 2 subdivided; 0), centre(3) and corners(3,8) of box ibox (1-based); ier 2 for a
+ * bad ibox. */
+int fmm3d_lfmm3d_plan_getb(void *plan, int ibox, int *box, double *center, double *corners);
+/* d3tgetl: list itype (1..5) of box ibox as 1-based box numbers; ier 4 when empty,
+ * 2 for a bad ibox or itype; list = NULL returns only the length in *nlist. */
+int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlist);
+
 /* Human-readable description of the last CUDA error on this thread. */
 const char *fmm3d_last_error(void);
 
