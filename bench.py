@@ -30,6 +30,9 @@ throughout), both reported.
             lfmm3dpartself on 100,000 sources on the unit sphere (seed 1),
             charges only, iprec = 1, FP64, with the CPU restatement timed on
             the same input.
+  plans     repeated solves on a fixed geometry: single calls vs plan executes (tree built
+            once) vs plan executes replaying a CUDA graph of the passes (sphere 100k and
+            10k, FP64; the batched workload as a plan, mixed form).
   batched   4,096 independent Laplace instances in one batched call
             (fmm3d_lfmm3dparttarg_batched_device, one launch per pass): N per
             instance floor(10^U[3, log10 2e5]) (seed 4), geometry per instance
@@ -184,6 +187,61 @@ def run_laplace_sphere(args, R, n=100_000):
     return out
 
 
+def run_plans(args, R, batch=None):
+    """Repeated solves on a fixed geometry: single calls vs plan executes (tree built once) vs plan
+    executes replaying a CUDA graph of the passes.  Sphere workloads (FP64) of 100k (cfg1) and 10k
+    sources, and, when given, the batched workload (mixed form) as a plan."""
+    torch, F = R["torch"], R["F"]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream().cuda_stream
+    out = {}
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    F.set_precision(0)
+    for n in (100_000, 10_000):
+        src, q = sphere_inputs(n)
+        d_src, d_q = torch.from_numpy(src).to(dev), torch.from_numpy(q).to(dev)
+        pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+        fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+        single = timed(lambda: F.lfmm3dparttarg_device(1, d_src, d_q, None, None, pot, fld, stream=stream), 20)
+        t0 = time.perf_counter()
+        plan = F.LaplacePlan(1, d_src, 1, 0, 1, 1, stream=stream)
+        create = 1e3 * (time.perf_counter() - t0)
+        plain = timed(lambda: plan.execute(d_q, None, None, pot, fld, use_graph=False, stream=stream), 20)
+        graph = timed(lambda: plan.execute(d_q, None, None, pot, fld, use_graph=True, stream=stream), 20)
+        out["sphere_%dk" % (n // 1000)] = {
+            "n_sources": n, "dtype": "f64", "single_call_ms": round(single, 3), "plan_create_ms": round(create, 3),
+            "plan_execute_ms": round(plain, 3), "plan_graph_execute_ms": round(graph, 3),
+            "kernels_per_execute": F.last_launches(), "graph_points_per_s": n / (graph * 1e-3)}
+        plan.close()
+    if batch is not None:
+        d_src, d_q, off, pot, fld = batch
+        F.set_precision(1)
+        F.set_tensor_m2l(args.tensor_m2l)
+        t0 = time.perf_counter()
+        plan = F.LaplacePlan(1, d_src, 1, 0, 1, 1, stream=stream, src_offsets=off)
+        create = 1e3 * (time.perf_counter() - t0)
+        graph = timed(lambda: plan.execute(d_q, None, None, pot, fld, use_graph=True, stream=stream), 2)
+        n = int(off[-1])
+        out["batched"] = {"instances": len(off) - 1, "n_total": n, "dtype": "mixed", "plan_create_ms": round(create, 1),
+                          "plan_graph_execute_ms": round(graph, 1), "kernels_per_execute": F.last_launches(),
+                          "graph_points_per_s": n / (graph * 1e-3)}
+        plan.close()
+        F.set_precision(0)
+    return out
+
+
 def batched_inputs(k, seed=4):
     """The batched workload's instances, concatenated: (sources, charges, offsets)."""
     rng = np.random.default_rng(seed)
@@ -263,6 +321,7 @@ def run_batched(args, R):
         num["pot"] += float(torch.sum((gp - dp) ** 2)); den["pot"] += float(torch.sum(dp ** 2))
         num["fld"] += float(torch.sum((gf - df) ** 2)); den["fld"] += float(torch.sum(df ** 2))
     F.set_precision(0)
+    R["batch_arrays"] = (d_src, d_q, off, d_pot, d_fld)
     mean = {kk: round(float(np.mean([p[kk] for p in passes])), 3) for kk in passes[0]}
     return {"workload": "laplace_batched_%d_instances_logN_1e3_2e5_iprec1_mixed" % args.batch_instances,
             "instances": args.batch_instances, "n_total": n, "value": n / (ms * 1e-3), "unit": UNIT,
@@ -700,9 +759,12 @@ def main(argv=None):
         import torch
         import fmmlib3d_b200 as F
         torch.cuda.set_device(dist_env()[2])
-        out = run_batched(args, dict(torch=torch, F=F, rank=rank, ws=1, dist=None))
+        R = dict(torch=torch, F=F, rank=rank, ws=1, dist=None)
+        out = run_batched(args, R)
+        plans = run_plans(args, R, R.pop("batch_arrays", None))
         print(json.dumps({"metric": "batched Laplace FMM pts/s", "value": out["value"], "unit": UNIT,
-                          "n_gpus": 1, "steps": out["steps"], "warmup": args.warmup, "batched": out}), flush=True)
+                          "n_gpus": 1, "steps": out["steps"], "warmup": args.warmup, "batched": out,
+                          "plans": plans}), flush=True)
         return 0
     if args.workload == "laplace":
         args.helm_n = 0
@@ -742,6 +804,7 @@ def main(argv=None):
     line["laplace_sphere"] = run_laplace_sphere(args, R)
     if args.batch_instances > 0:
         line["batched"] = run_batched(args, R)
+    line["plans"] = run_plans(args, R, R.pop("batch_arrays", None))
     if args.serve_requests > 0 and ws == 1:
         line["serving"] = run_serving(args)
     if args.helm_n > 0:

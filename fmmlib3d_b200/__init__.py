@@ -66,6 +66,9 @@ _lib.fmm3d_tc_selftest.argtypes = [_I, _I, _P, _P, _P, _I]
 _lib.fmm3d_tc_selftest.restype = _I
 _lib.fmm3d_lfmm3d_plan_create.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, ctypes.POINTER(_P)]
 _lib.fmm3d_lfmm3d_plan_create.restype = _I
+_lib.fmm3d_lfmm3d_plan_create_batched.argtypes = [_I, _I, _P, _P, _I, _I, _I, _I, _P, _P, _I, _I, _P,
+                                                  ctypes.POINTER(_P)]
+_lib.fmm3d_lfmm3d_plan_create_batched.restype = _I
 _lib.fmm3d_lfmm3d_plan_execute.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P]
 _lib.fmm3d_lfmm3d_plan_execute.restype = _I
 _lib.fmm3d_lfmm3d_plan_destroy.argtypes = [_P]
@@ -221,12 +224,21 @@ class LaplacePlan:
     ``getb`` / ``getl`` answer d3tgetb / d3tgetl queries (1-based boxes)."""
 
     def __init__(self, iprec, source, ifcharge=1, ifdipole=0, ifpot=1, iffld=1, target=None, ifpottarg=0,
-                 iffldtarg=0, stream=0):
+                 iffldtarg=0, stream=0, src_offsets=None, trg_offsets=None):
+        """``src_offsets`` / ``trg_offsets`` (ninst+1 ints): a batch of independent instances."""
         h = _P()
         m = 0 if target is None else target.shape[0]
-        ier = _lib.fmm3d_lfmm3d_plan_create(
-            iprec, source.shape[0], _P(source.data_ptr()), ifcharge, ifdipole, ifpot, iffld, m,
-            None if target is None else _P(target.data_ptr()), ifpottarg, iffldtarg, _P(stream), ctypes.byref(h))
+        tp = None if target is None else _P(target.data_ptr())
+        if src_offsets is None:
+            ier = _lib.fmm3d_lfmm3d_plan_create(
+                iprec, source.shape[0], _P(source.data_ptr()), ifcharge, ifdipole, ifpot, iffld, m, tp, ifpottarg,
+                iffldtarg, _P(stream), ctypes.byref(h))
+        else:
+            so = np.ascontiguousarray(src_offsets, dtype=np.int32)
+            to = None if trg_offsets is None else np.ascontiguousarray(trg_offsets, dtype=np.int32)
+            ier = _lib.fmm3d_lfmm3d_plan_create_batched(
+                iprec, len(so) - 1, _ptr(so), _P(source.data_ptr()), ifcharge, ifdipole, ifpot, iffld,
+                None if to is None else _ptr(to), tp, ifpottarg, iffldtarg, _P(stream), ctypes.byref(h))
         if ier != 0:
             raise RuntimeError("plan creation failed, ier=%d: %s" % (ier, last_error()))
         self._h = h

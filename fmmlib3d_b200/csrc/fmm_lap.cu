@@ -295,6 +295,14 @@ __global__ void k_m2l_count(int b0, int nb, TreeView tv, const Slot *slots, int 
         if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
 }
 
+static int device_sms()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
 // ---------------------------------------------------------------- one evaluation geometry
 // Device state of a Laplace evaluation for fixed sources and targets: tree and
 // lists, tree-ordered coordinates, expansion and output workspace, translation
@@ -314,7 +322,7 @@ struct LapSetup {
     DBuf<int> tcerr;
     DBuf<Tile> dtiles;
     std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
-    int m2l_a = 0, m2l_n = 0;
+    int m2l_a = 0, m2l_n = 0, m2l_kt = 0;
     PointsSoA P;
     OutSoA os, ot;
 };
@@ -415,7 +423,21 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.mixed = g_precision == 1 && iprec <= 1 && plan->dense;
     S.dense = (plan->dense && g_m2l_mode != 1) || S.mixed;
     S.tcm2l = S.mixed && g_tc_m2l > 0;
-    const int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt;
+    // M2L tile size: the largest whose tile count fills the GPU (two CTAs per SM per
+    // 64-row block); smaller tiles only add CTAs, every target's sums are unchanged
+    int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt;
+    if (S.dense && !(S.mixed && !S.tcm2l)) {
+        const int rows = div_up(K, 64), want = 2 * device_sms();
+        auto ntiles = [&](int kt) {
+            long t = 0;
+            for (int l = 2; l <= T.nlev; l++)
+                for (int o = 0; o < 8; o++) t += div_up(T.group_start[l * 8 + o + 1] - T.group_start[l * 8 + o], kt);
+            return t;
+        };
+        while (m2l_kt > 16 && ntiles(m2l_kt) * rows < want) m2l_kt /= 2;
+        if (!S.tcm2l && m2l_kt < kDenseTileTargets) m2l_kt = 16;   // FP64 dense kernel: 64 or 16
+    }
+    S.m2l_kt = m2l_kt;
     S.m2l_a = (int)htiles.size();
     for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
     S.m2l_n = (int)htiles.size() - S.m2l_a;
@@ -480,7 +502,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
                            plan->T32.p, tv, p, S.mpole.p, S.local.p, prune, s, st);
     else if (S.dense)
         launch_m2l_dense(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p,
-                         tv, p, S.mpole.p, S.local.p, prune, s, st);
+                         tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, s, st);
     else
         launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
                          plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt, s, st);
@@ -641,6 +663,36 @@ int fmm3d_lfmm3d_plan_create(int iprec, int nsource, const double *d_source, int
     Timer tm(s, false);
     int ier = lap_setup(E->S, iprec, nsource, d_source, ifcharge, ifdipole, ifpot, iffld, ntarget, d_target,
                         ifpottarg, iffldtarg, s, tm);
+    Status st;
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!ier && !st.ok()) { g_ti.err = cudaGetErrorString(st.err); ier = 16; }
+    if (ier) {
+        delete E;
+        return ier;
+    }
+    E->made_on = s;
+    E->used.push_back(s);
+    *plan = E;
+    return 0;
+}
+
+int fmm3d_lfmm3d_plan_create_batched(int iprec, int ninst, const int *src_offsets, const double *d_source,
+                                     int ifcharge, int ifdipole, int ifpot, int iffld, const int *trg_offsets,
+                                     const double *d_target, int ifpottarg, int iffldtarg, void *stream, void **plan)
+{
+    if (!plan) return 1;
+    *plan = nullptr;
+    if (ninst < 1 || !src_offsets || src_offsets[0] != 0) return 4;
+    std::vector<int> so(src_offsets, src_offsets + ninst + 1), to(ninst + 1, 0);
+    if (trg_offsets) to.assign(trg_offsets, trg_offsets + ninst + 1);
+    for (int i = 0; i < ninst; i++)
+        if (so[i + 1] < so[i] || to[i + 1] < to[i] || to[0] != 0) return 4;
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    g_launch_count = 0;
+    auto *E = new LapPlanExec;
+    Timer tm(s, false);
+    int ier = lap_setup(E->S, iprec, so[ninst], d_source, ifcharge, ifdipole, ifpot, iffld, to[ninst], d_target,
+                        ifpottarg, iffldtarg, s, tm, &so, &to);
     Status st;
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!ier && !st.ok()) { g_ti.err = cudaGetErrorString(st.err); ier = 16; }

@@ -59,13 +59,19 @@ __global__ void k_build_m2l_ops(int p, const M2LOp *ops, const double *rot, cons
 }
 
 // ---------------------------------------------------------------- the GEMM
-constexpr int kTM = 64, kTN = 64, kTK = 16, kDenseThreads = 256;
+// kTN targets per tile: 64, or 16 when the problem is too small to fill the
+// GPU with 64-target tiles (every target's sums are formed in the same order
+// either way).
+constexpr int kTM = 64, kTK = 16, kDenseThreads = 256;
 
+template <int kTN>
 __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tiles, const int *grouped,
                                                              const Slot *slots, const long long *slot_toff,
                                                              const double2 *T, TreeView tv, int p,
                                                              const double2 *in, double2 *out, int prune)
 {
+    constexpr int NY = kTN / 16;            // targets per thread
+    constexpr int BPT = kTN * kTK / kDenseThreads;   // B entries staged per thread
     __shared__ double2 As[kTK][kTM];   // As[k][row]
     __shared__ double2 Bs[kTK][kTN];   // Bs[k][target]
     __shared__ int tg[kTN], sv[kTN];
@@ -75,11 +81,11 @@ __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tile
     const int NC = (p + 1) * (p + 1);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads; rows ty+16x, targets tx+16y
     if (threadIdx.x < kTN) tg[threadIdx.x] = threadIdx.x < tile.count ? grouped[tile.first + threadIdx.x] : -1;
-    double2 acc[4][4];
+    double2 acc[4][NY];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = cmk(0, 0);
+        for (int b = 0; b < NY; b++) acc[a][b] = cmk(0, 0);
     for (int si = 0; si < tile.nslot; si++) {
         const Slot sl = slots[tile.slot0 + si];
         const int R = (sl.pt + 1) * (sl.pt + 1);
@@ -115,10 +121,10 @@ __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tile
             }
             // B tile: targets j, coefficients k0..; gathered source multipoles
             {
-                int j = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
+                int j = threadIdx.x % kTN, c = (threadIdx.x / kTN) * BPT;
                 int sb = sv[j];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int q = 0; q < BPT; q++) {
                     int gc = k0 + c + q;
                     Bs[c + q][j] = (sb >= 0 && gc < R) ? in[(size_t)sb * NC + gc] : cmk(0, 0);
                 }
@@ -126,20 +132,22 @@ __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tile
             __syncthreads();
 #pragma unroll 4
             for (int k = 0; k < kTK; k++) {
-                double2 a[4], b[4];
+                double2 a[4], b[NY];
 #pragma unroll
-                for (int q = 0; q < 4; q++) { a[q] = As[k][ty + 16 * q]; b[q] = Bs[k][tx + 16 * q]; }
+                for (int q = 0; q < 4; q++) a[q] = As[k][ty + 16 * q];
+#pragma unroll
+                for (int q = 0; q < NY; q++) b[q] = Bs[k][tx + 16 * q];
 #pragma unroll
                 for (int x = 0; x < 4; x++)
 #pragma unroll
-                    for (int y = 0; y < 4; y++) cfma(acc[x][y], a[x], b[y]);
+                    for (int y = 0; y < NY; y++) cfma(acc[x][y], a[x], b[y]);
             }
             __syncthreads();
         }
     }
     // epilogue: this CTA owns rows row0..row0+63 of its targets
 #pragma unroll
-    for (int y = 0; y < 4; y++) {
+    for (int y = 0; y < NY; y++) {
         int t = tg[tx + 16 * y];
         if (t < 0) continue;
 #pragma unroll
@@ -164,11 +172,15 @@ void build_m2l_ops(int p, int nops, const M2LOp *d_ops, const double *rot, const
 
 void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                       const long long *slot_toff, const double2 *T, const TreeView &tv, int p, const double2 *in,
-                      double2 *out, int prune, cudaStream_t s, Status &st)
+                      double2 *out, int prune, int kt, cudaStream_t s, Status &st)
 {
     if (!st.ok() || ntiles == 0) return;
     dim3 g(ntiles, div_up((p + 1) * (p + 1), kTM));
-    k_m2l_dense<<<g, kDenseThreads, 0, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
+    if (kt <= 16) {
+        k_m2l_dense<16><<<g, kDenseThreads, 0, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
+    } else {
+        k_m2l_dense<64><<<g, kDenseThreads, 0, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
+    }
     FMM_LAUNCH_CHECK(st);
 }
 

@@ -18,9 +18,10 @@ struct M2LOp {
 void build_m2l_ops(int p, int nops, const M2LOp *d_ops, const double *rot, const double *dc, int lddc,
                    double2 *T, cudaStream_t s, Status &st);
 
+// kt: targets per tile (64, or 16 for problems too small to fill the GPU)
 void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                       const long long *slot_toff, const double2 *T, const TreeView &tv, int p, const double2 *in,
-                      double2 *out, int prune, cudaStream_t s, Status &st);
+                      double2 *out, int prune, int kt, cudaStream_t s, Status &st);
 
 }  // namespace fmm
 

@@ -217,6 +217,11 @@ int fmm3d_last_stats(long long *out, int n);
 int fmm3d_lfmm3d_plan_create(int iprec, int nsource, const double *d_source, int ifcharge, int ifdipole, int ifpot,
                              int iffld, int ntarget, const double *d_target, int ifpottarg, int iffldtarg,
                              void *stream, void **plan);
+/* The same for a batch of independent instances (offsets as in
+ * fmm3d_lfmm3dparttarg_batched_device; trg_offsets may be NULL). */
+int fmm3d_lfmm3d_plan_create_batched(int iprec, int ninst, const int *src_offsets, const double *d_source,
+                                     int ifcharge, int ifdipole, int ifpot, int iffld, const int *trg_offsets,
+                                     const double *d_target, int ifpottarg, int iffldtarg, void *stream, void **plan);
 int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *d_dipstr, const double *d_dipvec,
                               double *d_pot, double *d_fld, double *d_pottarg, double *d_fldtarg, int use_graph,
                               void *stream);

@@ -134,3 +134,28 @@ def test_plan_tree_queries_match_oracle(F):
     assert plan.getb(0)[0] == 2 and plan.getb(info["nboxes"] + 1)[0] == 2
     assert plan.getl(1, 6)[0] == 2
     plan.close()
+
+
+def test_batched_plan_equals_batched_call(F):
+    import torch
+    rng = np.random.default_rng(31)
+    srcs = [geometry(("cube", "plummer", "ellipsoid")[i % 3], int(rng.integers(500, 8000)), rng) for i in range(20)]
+    off = np.concatenate([[0], np.cumsum([len(x) for x in srcs])]).astype(np.int32)
+    src = torch.from_numpy(np.concatenate(srcs)).cuda()
+    n = int(off[-1])
+    q = torch.from_numpy(rng.uniform(-1, 1, (n, 2))).cuda()
+    F.set_precision(1)
+    try:
+        pot, fld = torch.zeros((n, 2), dtype=torch.float64, device="cuda"), torch.zeros((n, 6), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert F.lfmm3dparttarg_batched_device(1, off, src, q, None, None, pot, fld) == 0
+        plan = F.LaplacePlan(1, src, 1, 0, 1, 1, src_offsets=off)
+        p2, f2 = torch.zeros_like(pot), torch.zeros_like(fld)
+        torch.cuda.synchronize()
+        assert plan.execute(q, None, None, p2, f2) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(p2, pot) and torch.equal(f2, fld)
+        assert plan.info()["nboxes"] >= 20
+        plan.close()
+    finally:
+        F.set_precision(0)
