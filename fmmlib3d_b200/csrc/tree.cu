@@ -43,16 +43,32 @@ __global__ void k_bbox_partial(const double *src, int n, const double *trg, int 
     }
 }
 
+// Reduces the per-block partials with one CTA (min / max are exact in any order).
 __global__ void k_bbox_final(const double *part, int nb, double *geom /* c0x c0y c0z size */)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double mn[3], mx[3];
-    for (int d = 0; d < 3; d++) { mn[d] = part[d]; mx[d] = part[3 + d]; }
-    for (int b = 1; b < nb; b++)
+    double mn[3] = {1e308, 1e308, 1e308}, mx[3] = {-1e308, -1e308, -1e308};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
         for (int d = 0; d < 3; d++) {
             mn[d] = fmin(mn[d], part[6 * b + d]);
             mx[d] = fmax(mx[d], part[6 * b + 3 + d]);
         }
+    for (int d = 0; d < 3; d++)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    __shared__ double sh[32][6];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int d = 0; d < 3; d++) { sh[w][d] = mn[d]; sh[w][3 + d] = mx[d]; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ww++)
+        for (int d = 0; d < 3; d++) {
+            sh[0][d] = fmin(sh[0][d], sh[ww][d]);
+            sh[0][3 + d] = fmax(sh[0][3 + d], sh[ww][3 + d]);
+        }
+    for (int d = 0; d < 3; d++) { mn[d] = sh[0][d]; mx[d] = sh[0][3 + d]; }
     double size = __dsub_rn(mx[0], mn[0]);
     double sy = __dsub_rn(mx[1], mn[1]), sz = __dsub_rn(mx[2], mn[2]);
     if (sy > size) size = sy;
@@ -123,8 +139,9 @@ __global__ void k_keys(const double *pts, int n, const double *geom_all, const i
     int c[3] = {0, 0, 0};
     uint64_t key = 0;
     for (int l = 0; l < kMaxLevel; l++) {
-        double side = size / (double)(1 << l);
-        double side2 = side / 2;
+        // size / 2^l and side / 2 by exact power-of-two scaling (bitwise the same values)
+        double side = ldexp(size, -l);
+        double side2 = ldexp(side, -1);
         int oct = 0;
         for (int d = 0; d < 3; d++) {
             double ce = __dadd_rn(__dadd_rn(x0[d], __dmul_rn((double)c[d], side)), side2);
@@ -155,24 +172,39 @@ __device__ int lower_digit(const uint64_t *keys, int lo, int hi, int child_level
 }
 
 // Split decision and child ranges for the boxes of one level
-// (d3tallbem, src/d3tstrcr.f:1458-1578).
+// (d3tallbem, src/d3tstrcr.f:1458-1578).  Sixteen threads per box: the
+// fourteen digit boundaries (7 source, 7 target) are independent binary
+// searches over the box's sorted range, done in parallel.
+constexpr int kSplitLanes = 16;
+
 __global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, const int *nsrc, const int *trg0,
                         const int *ntrg, const uint64_t *ksrc, const uint64_t *ktrg, int *nkids, int *cs0,
                         int *cns, int *ct0, int *cnt)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nb) return;
-    int b = b0 + t;
-    int s0 = src0[b], ns = nsrc[b], q0 = trg0[b], nq = ntrg[b];
+    __shared__ int bound[128 / kSplitLanes][16];
+    const int g = threadIdx.x / kSplitLanes, j = threadIdx.x % kSplitLanes;
+    const int t = blockIdx.x * (blockDim.x / kSplitLanes) + g;
+    const bool live = t < nb;
+    int s0 = 0, ns = 0, q0 = 0, nq = 0;
+    bool split = false;
+    if (live) {
+        const int b = b0 + t;
+        s0 = src0[b]; ns = nsrc[b]; q0 = trg0[b]; nq = ntrg[b];
+        split = level < kMaxLevel && (ns > nbox || nq > nbox);
+        const int cl = level + 1;
+        if (split && j >= 1 && j <= 7) bound[g][j] = lower_digit(ksrc, s0, s0 + ns, cl, j);
+        if (split && j >= 9 && j <= 15) bound[g][j] = lower_digit(ktrg, q0, q0 + nq, cl, j - 8);
+    }
+    __syncthreads();
+    if (!live || j != 0) return;
     int k = 0;
-    if (level < kMaxLevel && (ns > nbox || nq > nbox)) {
-        int cl = level + 1;
+    if (split) {
         int sb[9], tb[9];
         sb[0] = s0; sb[8] = s0 + ns;
         tb[0] = q0; tb[8] = q0 + nq;
         for (int d = 1; d < 8; d++) {
-            sb[d] = lower_digit(ksrc, sb[d - 1], s0 + ns, cl, d);
-            tb[d] = lower_digit(ktrg, tb[d - 1], q0 + nq, cl, d);
+            sb[d] = bound[g][d];
+            tb[d] = bound[g][8 + d];
         }
         for (int d = 0; d < 8; d++) {
             cs0[8 * t + d] = sb[d];
@@ -472,7 +504,7 @@ void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, cons
         part.alloc(6 * nbb, s, st);
         if (!st.ok()) return;
         k_bbox_partial<<<nbb, 256, 0, s>>>(d_src, n, d_trg, m, part.p); FMM_COUNT_LAUNCH();
-        k_bbox_final<<<1, 32, 0, s>>>(part.p, nbb, geom.p); FMM_COUNT_LAUNCH();
+        k_bbox_final<<<1, 256, 0, s>>>(part.p, nbb, geom.p); FMM_COUNT_LAUNCH();
     } else {
         if (!dso.alloc(ninst + 1, s, st) || !dto.alloc(ninst + 1, s, st) || !pis.alloc(std::max(n, 1), s, st) ||
             !pit.alloc(std::max(m, 1), s, st))
@@ -545,8 +577,9 @@ void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, cons
         if (!nk.alloc(nb, s, st) || !kb.alloc(nb, s, st) || !cs0.alloc(8L * nb, s, st) ||
             !cns.alloc(8L * nb, s, st) || !ct0.alloc(8L * nb, s, st) || !cnt.alloc(8L * nb, s, st))
             return;
-        k_split<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nbox, T.src0.p, T.nsrc.p, T.trg0.p, T.ntrg.p,
-                                                 ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p, cnt.p); FMM_COUNT_LAUNCH();
+        k_split<<<div_up(nb, 128 / kSplitLanes), 128, 0, s>>>(b0, nb, level, nbox, T.src0.p, T.nsrc.p, T.trg0.p,
+                                                               T.ntrg.p, ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p,
+                                                               cnt.p); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         int total = 0;
         scan_exclusive_int(nk.p, kb.p, nb, s, st, &total);
