@@ -60,22 +60,26 @@ __global__ void k_build_m2l_ops(int p, const M2LOp *ops, const double *rot, cons
 
 // ---------------------------------------------------------------- the GEMM
 // kTN targets per tile: 64, or 16 when the problem is too small to fill the
-// GPU with 64-target tiles (every target's sums are formed in the same order
-// either way).
-constexpr int kTM = 64, kTK = 16, kDenseThreads = 256;
+// GPU with 64-target tiles; the small tiles take the operator in K blocks of
+// 64 instead of 16 (fewer round trips to L2 per slot, which is what bounds a
+// CTA that walks all 189 slots on a small problem).  The source boxes of the
+// next slot are looked up while the current slot is multiplied.  Every
+// target's sums are formed in the same order in all variants.
+constexpr int kTM = 64, kDenseThreads = 256;
 
-template <int kTN>
+template <int kTN, int kTK>
 __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tiles, const int *grouped,
                                                              const Slot *slots, const long long *slot_toff,
                                                              const double2 *T, TreeView tv, int p,
                                                              const double2 *in, double2 *out, int prune)
 {
-    constexpr int NY = kTN / 16;            // targets per thread
-    constexpr int BPT = kTN * kTK / kDenseThreads;   // B entries staged per thread
-    __shared__ double2 As[kTK][kTM];   // As[k][row]
-    __shared__ double2 Bs[kTK][kTN];   // Bs[k][target]
+    constexpr int NY = kTN / 16;                       // targets per thread
+    constexpr int APT = kTM * kTK / kDenseThreads;     // A entries staged per thread
+    constexpr int BPT = kTN * kTK / kDenseThreads;     // B entries staged per thread
+    extern __shared__ double2 dsm[];
+    double2(*As)[kTM] = reinterpret_cast<double2(*)[kTM]>(dsm);               // As[k][row]
+    double2(*Bs)[kTN] = reinterpret_cast<double2(*)[kTN]>(dsm + kTK * kTM);   // Bs[k][target]
     __shared__ int tg[kTN], sv[kTN];
-    __shared__ int anyv;
     const Tile tile = tiles[blockIdx.x];
     const int row0 = blockIdx.y * kTM;
     const int NC = (p + 1) * (p + 1);
@@ -86,35 +90,39 @@ __global__ void __launch_bounds__(kDenseThreads, 2) k_m2l_dense(const Tile *tile
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < NY; b++) acc[a][b] = cmk(0, 0);
+    __syncthreads();
+    // source box of target threadIdx.x (< kTN) for slot si, -1 if none
+    auto source_box = [&](int si) {
+        const int t = tg[threadIdx.x];
+        int sb = -1;
+        if (t >= 0 && !(prune && tv.ntrg[t] == 0)) {
+            const Slot sl = slots[tile.slot0 + si];
+            const int P = tv.parent[t];
+            const int C = P >= 0 ? tv.coll[27L * P + sl.coll] : -1;
+            sb = C >= 0 ? tv.child[8L * C + sl.oct] : -1;
+            if (sb >= 0 && tv.nsrc[sb] == 0) sb = -1;
+        }
+        return sb;
+    };
+    int next_sb = (threadIdx.x < kTN && tile.nslot > 0) ? source_box(0) : -1;
     for (int si = 0; si < tile.nslot; si++) {
+        const int cur_sb = next_sb;
+        if (threadIdx.x < kTN && si + 1 < tile.nslot) next_sb = source_box(si + 1);
         const Slot sl = slots[tile.slot0 + si];
         const int R = (sl.pt + 1) * (sl.pt + 1);
         if (row0 >= R) continue;  // uniform over the CTA
         __syncthreads();
-        if (threadIdx.x == 0) anyv = 0;
-        __syncthreads();
-        if (threadIdx.x < kTN) {
-            int t = tg[threadIdx.x], sb = -1;
-            if (t >= 0 && !(prune && tv.ntrg[t] == 0)) {
-                int P = tv.parent[t];
-                int C = P >= 0 ? tv.coll[27L * P + sl.coll] : -1;
-                sb = C >= 0 ? tv.child[8L * C + sl.oct] : -1;
-                if (sb >= 0 && tv.nsrc[sb] == 0) sb = -1;
-            }
-            sv[threadIdx.x] = sb;
-            if (sb >= 0) atomicOr(&anyv, 1);
-        }
-        __syncthreads();
-        if (!anyv) continue;
+        if (threadIdx.x < kTN) sv[threadIdx.x] = cur_sb;
+        if (!__syncthreads_or(threadIdx.x < kTN && cur_sb >= 0)) continue;
         const double2 *Tu = T + slot_toff[tile.slot0 + si];
         for (int k0 = 0; k0 < R; k0 += kTK) {
             // A tile: rows row0.., cols k0..; consecutive threads take consecutive
             // rows of a column (the operators are column-major)
             {
-                int r = threadIdx.x & 63, c = (threadIdx.x >> 6) * 4;
+                int r = threadIdx.x & 63, c = (threadIdx.x >> 6) * APT;
                 int gr = row0 + r;
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int q = 0; q < APT; q++) {
                     int gc = k0 + c + q;
                     As[c + q][r] = (gr < R && gc < R) ? Tu[(size_t)gc * R + gr] : cmk(0, 0);
                 }
@@ -177,9 +185,12 @@ void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const S
     if (!st.ok() || ntiles == 0) return;
     dim3 g(ntiles, div_up((p + 1) * (p + 1), kTM));
     if (kt <= 16) {
-        k_m2l_dense<16><<<g, kDenseThreads, 0, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
+        constexpr size_t sm = sizeof(double2) * 64 * (kTM + 16);
+        FMM_TRY(st, cudaFuncSetAttribute(k_m2l_dense<16, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_m2l_dense<16, 64><<<g, kDenseThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
     } else {
-        k_m2l_dense<64><<<g, kDenseThreads, 0, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
+        constexpr size_t sm = sizeof(double2) * 16 * (kTM + 64);
+        k_m2l_dense<64, 16><<<g, kDenseThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
     }
     FMM_LAUNCH_CHECK(st);
 }
