@@ -20,6 +20,22 @@ cudaStream_t thread_stream()
     return s;
 }
 
+SideStreams &side_streams()
+{
+    static thread_local SideStreams ss;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!ss.far || ss.dev != dev) {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        cudaStreamCreateWithPriority(&ss.far, cudaStreamNonBlocking, greatest);
+        cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming);
+        ss.dev = dev;
+    }
+    return ss;
+}
+
 // Keep freed workspace in the device's default memory pool across calls
 // instead of returning it to the driver at every synchronisation.
 void keep_pool_memory()

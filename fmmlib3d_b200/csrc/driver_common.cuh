@@ -4,6 +4,7 @@
 // caller's AoS arrays and the tree-ordered SoA arrays, and the host-array
 // wrapper of the Fortran-named entry points.
 #pragma once
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -29,13 +30,15 @@ struct Timer {
     cudaStream_t s;
     bool on;
     std::vector<cudaEvent_t> ev;
+    std::function<void(std::vector<double> &)> fix;   // optional rewrite of the intervals
     Timer(cudaStream_t s_, bool on_) : s(s_), on(on_) {}
-    void mark()
+    void mark() { mark_on(s); }
+    void mark_on(cudaStream_t st)
     {
         if (!on) return;
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, s);
+        cudaEventRecord(e, st);
         ev.push_back(e);
     }
     void finish(std::vector<double> &ms)
@@ -51,10 +54,20 @@ struct Timer {
         float t = 0;
         cudaEventElapsedTime(&t, ev.front(), ev.back());
         ms.push_back(t);
+        if (fix) fix(ms);
         for (auto e : ev) cudaEventDestroy(e);
         ev.clear();
     }
 };
+
+// Per-thread high-priority stream for the far-field passes of a call, and the
+// fork / join events between it and the call's stream (made once per thread).
+struct SideStreams {
+    cudaStream_t far = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    int dev = -1;
+};
+SideStreams &side_streams();
 
 // tree order <-> caller order (l3dreorder / l3dpsort / l3dfsort, src/lfmm3drouts.f:583-708)
 __global__ void k_gather_src(int n, const int *perm, const double *src, const double *q, const double *dq,

@@ -478,44 +478,25 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     }
     FMM_TRY(st, cudaMemsetAsync(S.mpole.p, 0, sizeof(double2) * S.mpole.n, s));
     FMM_TRY(st, cudaMemsetAsync(S.local.p, 0, sizeof(double2) * S.local.n, s));
+    // the outputs collect the near field and then the far field
+    for (auto *o : {&S.opot, &S.ofx, &S.ofy, &S.ofz, &S.tpot, &S.tfx, &S.tfy, &S.tfz})
+        if (o->n) FMM_TRY(st, cudaMemsetAsync(o->p, 0, sizeof(double2) * o->n, s));
     FMM_LAUNCH_CHECK(st);
     tm.mark();
-    // STEP 1: P2M at every childless box
-    launch_p2m(T.leaves.p, T.nleaves, tv, P, S.ifcharge, S.ifdipole, p, S.mpole.p, s, st);
-    tm.mark();
-    // STEP 3: M2M, levels nlev-1 .. 2
-    for (auto &r : S.m2m_rng)
-        launch_translate(0, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, plan->kt, s, st);
-    tm.mark();
-    // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
-    launch_p2l(T.grouped.p, T.nboxes, tv, P, S.ifcharge, S.ifdipole, p, S.local.p, s, st);
-    tm.mark();
-    // STEP 4: M2L over list 2, all levels >= 2
-    if (S.tcm2l) {
-        FMM_TRY(st, cudaMemsetAsync(S.tcerr.p, 0, sizeof(int), s));
-        convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, s, st);
-        launch_m2l_tc(g_tc_m2l - 1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
-                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, s, st);
-    } else if (S.mixed)
-        launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
-                           plan->T32.p, tv, p, S.mpole.p, S.local.p, prune, s, st);
-    else if (S.dense)
-        launch_m2l_dense(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p,
-                         tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, s, st);
-    else
-        launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt, s, st);
-    tm.mark();
-    // STEP 5: L2L, levels 2 .. nlev-1
-    for (auto &r : S.l2l_rng)
-        launch_translate(2, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, plan->kt, s, st);
-    tm.mark();
-    // STEPS 6, 7: M2P from list 3 and L2P (writes the outputs)
-    launch_eval(T.leaves.p, T.nleaves, tv, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
-                S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
-    tm.mark();
+    // The near field (STEP 8) runs on the call's stream while the far-field
+    // passes (STEPS 1-5) run on a high-priority side stream; they meet before
+    // STEPS 6-7, which add the far field to the outputs.  In the mixed form the
+    // two use different units (FP32 CUDA cores, tensor cores).
+    SideStreams &ss = side_streams();
+    const cudaStream_t f = ss.far;
+    FMM_TRY(st, cudaEventRecord(ss.fork, s));
+    FMM_TRY(st, cudaStreamWaitEvent(f, ss.fork, 0));
+    cudaEvent_t p2p0 = nullptr, p2p1 = nullptr;
+    if (tm.on) {
+        cudaEventCreate(&p2p0);
+        cudaEventCreate(&p2p1);
+        cudaEventRecord(p2p0, s);
+    }
     // STEP 8: P2P over self and list 1 (adds to the outputs)
     const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
     if (S.mixed)
@@ -524,7 +505,57 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     else
         launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
                    S.ifpot, S.iffld, ppt, pft, s, st);
+    if (tm.on) cudaEventRecord(p2p1, s);
+    // STEP 1: P2M at every childless box
+    launch_p2m(T.leaves.p, T.nleaves, tv, P, S.ifcharge, S.ifdipole, p, S.mpole.p, f, st);
+    tm.mark_on(f);
+    // STEP 3: M2M, levels nlev-1 .. 2
+    for (auto &r : S.m2m_rng)
+        launch_translate(0, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, plan->kt, f, st);
+    tm.mark_on(f);
+    // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
+    launch_p2l(T.grouped.p, T.nboxes, tv, P, S.ifcharge, S.ifdipole, p, S.local.p, f, st);
+    tm.mark_on(f);
+    // STEP 4: M2L over list 2, all levels >= 2
+    if (S.tcm2l) {
+        FMM_TRY(st, cudaMemsetAsync(S.tcerr.p, 0, sizeof(int), f));
+        convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, f, st);
+        launch_m2l_tc(g_tc_m2l - 1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, f, st);
+    } else if (S.mixed)
+        launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+                           plan->T32.p, tv, p, S.mpole.p, S.local.p, prune, f, st);
+    else if (S.dense)
+        launch_m2l_dense(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p,
+                         tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);
+    else
+        launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt, f, st);
+    tm.mark_on(f);
+    // STEP 5: L2L, levels 2 .. nlev-1
+    for (auto &r : S.l2l_rng)
+        launch_translate(2, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                         plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, plan->kt, f, st);
+    tm.mark_on(f);
+    FMM_TRY(st, cudaEventRecord(ss.join, f));
+    FMM_TRY(st, cudaStreamWaitEvent(s, ss.join, 0));
     tm.mark();
+    // STEPS 6, 7: M2P from list 3 and L2P (add the far field to the outputs)
+    launch_eval(T.leaves.p, T.nleaves, tv, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
+                S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
+    tm.mark();
+    if (tm.on) {
+        // intervals: ..., l2l, [wait for the near field], eval, scatter, total ->
+        // ..., l2l, eval, p2p (its own events), scatter, total
+        tm.fix = [p2p0, p2p1](std::vector<double> &ms) {
+            float t = 0;
+            cudaEventElapsedTime(&t, p2p0, p2p1);
+            cudaEventDestroy(p2p0);
+            cudaEventDestroy(p2p1);
+            if (ms.size() == 11) ms = {ms[0], ms[1], ms[2], ms[3], ms[4], ms[5], ms[6], ms[8], (double)t, ms[9], ms[10]};
+        };
+    }
     // unsort into the caller's order
     if (S.do_src) {
         k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, S.os, S.ifpot == 1 ? d_pot : nullptr,
