@@ -29,8 +29,10 @@ SideStreams &side_streams()
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
         cudaStreamCreateWithPriority(&ss.far, cudaStreamNonBlocking, greatest);
+        cudaStreamCreateWithFlags(&ss.copy, cudaStreamNonBlocking);
         cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
         cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ss.copied, cudaEventDisableTiming);
         ss.dev = dev;
     }
     return ss;

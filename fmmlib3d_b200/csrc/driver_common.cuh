@@ -16,6 +16,9 @@ namespace fmm {
 struct ThreadInfo {
     bool timing = false;
     bool want_stats = false;
+    // set by the host-array entry points while charges are still being copied:
+    // the charge-dependent passes wait for it
+    cudaEvent_t inputs_ready = nullptr;
     std::vector<double> ms;
     std::vector<long long> stats;
     std::string err;
@@ -63,8 +66,8 @@ struct Timer {
 // Per-thread high-priority stream for the far-field passes of a call, and the
 // fork / join events between it and the call's stream (made once per thread).
 struct SideStreams {
-    cudaStream_t far = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t far = nullptr, copy = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, copied = nullptr;
     int dev = -1;
 };
 SideStreams &side_streams();
@@ -94,12 +97,17 @@ inline TreeView make_treeview(const Tree &T)
 
 // ---------------------------------------------------------------- host-array entry points
 // Copies host inputs to the device, runs the device routine and copies the
-// requested outputs back; unrequested outputs are left untouched.
+// requested outputs back; unrequested outputs are left untouched.  The
+// positions go first on the call's stream; the charges and dipoles follow on
+// a copy stream, so that (from pinned host memory) they travel while the tree
+// is built.  With overlap_charges the device routine waits for them itself
+// (g_ti.inputs_ready) before its charge-dependent passes; otherwise the call's
+// stream waits before the routine starts.
 template <typename F>
 inline int with_device_arrays(int ns, const double *source, int ifcharge, const double *charge, int ifdipole,
                               const double *dipstr, const double *dipvec, int ifpot, double *pot, int iffld,
                               double *fld, int nt, const double *target, int ifpottarg, double *pottarg,
-                              int iffldtarg, double *fldtarg, F run)
+                              int iffldtarg, double *fldtarg, F run, bool overlap_charges = false)
 {
     cudaStream_t s = thread_stream();
     Status st;
@@ -116,15 +124,31 @@ inline int with_device_arrays(int ns, const double *source, int ifcharge, const 
     if (nt && iffldtarg == 1) ok = ok && dft.alloc(6L * nt, s, st);
     if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
     FMM_TRY(st, cudaMemcpyAsync(dsrc.p, source, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
-    if (ifcharge == 1) FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
-    if (ifdipole == 1) {
-        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, s));
-        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
-    }
     if (nt) FMM_TRY(st, cudaMemcpyAsync(dtrg.p, target, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+    SideStreams &ss = side_streams();
+    // the charge buffers were allocated on s: the copy stream starts after that
+    FMM_TRY(st, cudaEventRecord(ss.fork, s));
+    FMM_TRY(st, cudaStreamWaitEvent(ss.copy, ss.fork, 0));
+    if (ifcharge == 1)
+        FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, ss.copy));
+    if (ifdipole == 1) {
+        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, ss.copy));
+        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, ss.copy));
+    }
+    FMM_TRY(st, cudaEventRecord(ss.copied, ss.copy));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    if (overlap_charges) g_ti.inputs_ready = ss.copied;
+    else FMM_TRY(st, cudaStreamWaitEvent(s, ss.copied, 0));
     int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
-    if (ier) return ier;
+    if (g_ti.inputs_ready) {
+        // not consumed (an early error): order the stream after the copies anyway
+        cudaStreamWaitEvent(s, g_ti.inputs_ready, 0);
+        g_ti.inputs_ready = nullptr;
+    }
+    if (ier) {
+        cudaStreamSynchronize(s);
+        return ier;
+    }
     if (ifpot == 1) FMM_TRY(st, cudaMemcpyAsync(pot, dpot.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
     if (iffld == 1) FMM_TRY(st, cudaMemcpyAsync(fld, dfld.p, sizeof(double) * 6 * ns, cudaMemcpyDeviceToHost, s));
     if (nt && ifpottarg == 1) FMM_TRY(st, cudaMemcpyAsync(pottarg, dpt.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));

@@ -472,6 +472,10 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     const TreeView &tv = S.tv;
     const PointsSoA &P = S.P;
     const int prune = S.prune;
+    if (g_ti.inputs_ready) {   // charges still in flight from the host
+        FMM_TRY(st, cudaStreamWaitEvent(s, g_ti.inputs_ready, 0));
+        g_ti.inputs_ready = nullptr;
+    }
     if (S.ifcharge == 1 || S.ifdipole == 1) {
         k_gather_q<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_q, d_dq, d_dv, S.ifcharge == 1,
                                                    S.ifdipole == 1, P); FMM_COUNT_LAUNCH();
@@ -1035,7 +1039,8 @@ void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const doubl
             const double *t_, double *pt, double *ft, cudaStream_t s) {
             return lap_fmm_device(ip, ns, s_, *ifcharge, q, *ifdipole, dq, dv, *ifpot, po, *iffld, fo, nt, t_,
                                   *ifpottarg, pt, *iffldtarg, ft, s);
-        });
+        },
+        true);
 }
 
 void lfmm3dpartself_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
