@@ -60,6 +60,7 @@ _lib.fmm3d_set_m2l_mode.argtypes = [_I]
 _lib.fmm3d_set_precision.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l.restype = _I
+_lib.fmm3d_set_overlap.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l_group.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l_group.restype = _I
 _lib.fmm3d_tc_selftest.argtypes = [_I, _I, _P, _P, _P, _I]
@@ -399,6 +400,11 @@ def set_tensor_m2l(mode):
     """Mixed-form M2L: 0 FP32 CUDA cores, 1 (default) / 2 tensor cores (tcgen05, split TF32; staging variants)."""
     if _lib.fmm3d_set_tensor_m2l(int(mode)) != 0:
         raise ValueError("unknown tensor M2L mode %r" % (mode,))
+
+
+def set_overlap(on=True):
+    """Laplace: near field concurrent with the far field (default) or all passes serial (same results)."""
+    _lib.fmm3d_set_overlap(1 if on else 0)
 
 
 def set_tensor_m2l_group(slots):

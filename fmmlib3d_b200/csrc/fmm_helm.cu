@@ -299,6 +299,10 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     }
     PointsSoA P;
     P.x = sx.p; P.y = sy.p; P.z = sz.p; P.q = sq.p; P.dq = sdq.p; P.vx = svx.p; P.vy = svy.p; P.vz = svz.p;
+    if (g_ti.inputs_ready) {   // charges still in flight from the host
+        FMM_TRY(st, cudaStreamWaitEvent(s, g_ti.inputs_ready, 0));
+        g_ti.inputs_ready = nullptr;
+    }
     k_gather_src<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, d_q, d_dq, d_dv, ifcharge == 1,
                                                  ifdipole == 1, P); FMM_COUNT_LAUNCH();
     if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }
@@ -644,7 +648,8 @@ void hfmm3dparttarg_(int *ier, const int *iprec, const double *zk, const int *ns
             const double *t_, double *pt, double *ft, cudaStream_t s) {
             return helm_fmm_device(ip, k, ns, s_, *ifcharge, q, *ifdipole, dq, dv, *ifpot, po, *iffld, fo, nt, t_,
                                    *ifpottarg, pt, *iffldtarg, ft, s);
-        });
+        },
+        true);
 }
 
 void hfmm3dpartself_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *source,

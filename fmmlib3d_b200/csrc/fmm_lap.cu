@@ -105,6 +105,7 @@ static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense opera
 static int g_precision = 0; // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
 static int g_tc_m2l = 1;    // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
 static int g_tc_group = 1;  // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
+static int g_overlap = 1;   // near field concurrent with the far-field passes
 constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
 
 static std::mutex g_plan_mu;
@@ -490,26 +491,34 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // The near field (STEP 8) runs on the call's stream while the far-field
     // passes (STEPS 1-5) run on a high-priority side stream; they meet before
     // STEPS 6-7, which add the far field to the outputs.  In the mixed form the
-    // two use different units (FP32 CUDA cores, tensor cores).
+    // two use different units (FP32 CUDA cores, tensor cores).  With the
+    // overlap switched off (fmm3d_set_overlap(0)) everything runs on the call's
+    // stream, far field first, with the same arithmetic.
     SideStreams &ss = side_streams();
-    const cudaStream_t f = ss.far;
-    FMM_TRY(st, cudaEventRecord(ss.fork, s));
-    FMM_TRY(st, cudaStreamWaitEvent(f, ss.fork, 0));
+    const bool overlap = g_overlap != 0;
+    const cudaStream_t f = overlap ? ss.far : s;
+    if (overlap) {
+        FMM_TRY(st, cudaEventRecord(ss.fork, s));
+        FMM_TRY(st, cudaStreamWaitEvent(f, ss.fork, 0));
+    }
     cudaEvent_t p2p0 = nullptr, p2p1 = nullptr;
     if (tm.on) {
         cudaEventCreate(&p2p0);
         cudaEventCreate(&p2p1);
-        cudaEventRecord(p2p0, s);
     }
-    // STEP 8: P2P over self and list 1 (adds to the outputs)
-    const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
-    if (S.mixed)
-        launch_p2p32(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
-                     S.ifpot, S.iffld, ppt, pft, s, st);
-    else
-        launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
-                   S.ifpot, S.iffld, ppt, pft, s, st);
-    if (tm.on) cudaEventRecord(p2p1, s);
+    auto near_field = [&]() {
+        if (tm.on) cudaEventRecord(p2p0, s);
+        // STEP 8: P2P over self and list 1 (adds to the outputs)
+        const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
+        if (S.mixed)
+            launch_p2p32(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
+                         S.ifpot, S.iffld, ppt, pft, s, st);
+        else
+            launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
+                       S.ifpot, S.iffld, ppt, pft, s, st);
+        if (tm.on) cudaEventRecord(p2p1, s);
+    };
+    if (overlap) near_field();
     // STEP 1: P2M at every childless box
     launch_p2m(T.leaves.p, T.nleaves, tv, P, S.ifcharge, S.ifdipole, p, S.mpole.p, f, st);
     tm.mark_on(f);
@@ -542,8 +551,12 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         launch_translate(2, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
                          plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, plan->kt, f, st);
     tm.mark_on(f);
-    FMM_TRY(st, cudaEventRecord(ss.join, f));
-    FMM_TRY(st, cudaStreamWaitEvent(s, ss.join, 0));
+    if (overlap) {
+        FMM_TRY(st, cudaEventRecord(ss.join, f));
+        FMM_TRY(st, cudaStreamWaitEvent(s, ss.join, 0));
+    } else {
+        near_field();
+    }
     tm.mark();
     // STEPS 6, 7: M2P from list 3 and L2P (add the far field to the outputs)
     launch_eval(T.leaves.p, T.nleaves, tv, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
@@ -642,6 +655,7 @@ struct LapPlanExec {
     cudaStream_t made_on = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void *key[8] = {};
+    int key_overlap = -1;      // the overlap switch when the graph was captured
     int graph_launches = 0;
     std::vector<cudaStream_t> used;
     // host copy of the tree for the queries (filled on first use)
@@ -758,7 +772,7 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
     g_launch_count = 0;
     if (use_graph) {
         const void *key[8] = {d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, (const void *)s};
-        if (!E->exec || memcmp(key, E->key, sizeof key) != 0) {
+        if (!E->exec || memcmp(key, E->key, sizeof key) != 0 || E->key_overlap != g_overlap) {
             if (E->exec) cudaGraphExecDestroy(E->exec);
             E->exec = nullptr;
             cudaGraph_t g = nullptr;
@@ -775,6 +789,7 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
                 return 16;
             }
             memcpy(E->key, key, sizeof key);
+            E->key_overlap = g_overlap;
             E->graph_launches = g_launch_count;
         }
         FMM_TRY(st, cudaGraphLaunch(E->exec, s));
@@ -1090,6 +1105,12 @@ int fmm3d_set_tensor_m2l(int mode)
 {
     if (mode < 0 || mode > 2) return 1;
     g_tc_m2l = mode;
+    return 0;
+}
+
+int fmm3d_set_overlap(int on)
+{
+    g_overlap = on ? 1 : 0;
     return 0;
 }
 

@@ -186,6 +186,12 @@ int fmm3d_set_precision(int mode);
  * unknown mode. */
 int fmm3d_set_tensor_m2l(int mode);
 
+/* Laplace passes: 1 (default) runs the near field (P2P) concurrently with the
+ * far-field passes on a second stream; 0 runs all passes one after the other on
+ * the call's stream (same results bitwise; per-pass timings then show each
+ * kernel alone).  No counterpart in the reference. */
+int fmm3d_set_overlap(int on);
+
 /* Tensor-core M2L: number of list-2 slots summed in the tensor-core (TMEM)
  * accumulator before the sum is added, with round-to-nearest FP32 additions,
  * into the tile's running sum (default 1; 0 = one tensor-core sum per tile).

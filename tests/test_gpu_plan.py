@@ -159,3 +159,23 @@ def test_batched_plan_equals_batched_call(F):
         plan.close()
     finally:
         F.set_precision(0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_overlapped_and_serial_passes_agree_bitwise(F, precision):
+    """The near field concurrent with the far field (default) or all passes in order: same bits."""
+    import torch
+    n, m = 25000, 8000
+    src, trg, qs, ds, dv = _inputs(n, m, 40 + precision, "cube")
+    F.set_precision(precision)
+    try:
+        a, b = _outs(n, m), _outs(n, m)
+        assert F.lfmm3dparttarg_device(1, src, qs[0], ds[0], dv, a[0], a[1], trg, a[2], a[3]) == 0
+        F.set_overlap(False)
+        assert F.lfmm3dparttarg_device(1, src, qs[0], ds[0], dv, b[0], b[1], trg, b[2], b[3]) == 0
+        torch.cuda.synchronize()
+    finally:
+        F.set_overlap(True)
+        F.set_precision(0)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
