@@ -417,8 +417,10 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
         FMM_TRY(st, cudaMemcpyAsync(dxw.p, xw.data(), sizeof(double) * xw.size(), cudaMemcpyHostToDevice, s));
         build_hz((int)hb.size(), dblk.p, hb.data(), dxw.p, zk, pmax, rad.p, Z.p, s, st);
         // translation tiles per (level, octant) group
+        // targets per translation tile: buffers of at most ~50 KB, so that several
+        // CTAs share an SM (the passes are bound by L2 latency, not by reuse)
         kt = 8;
-        while (kt > 1 && (size_t)3 * kt * NC * 16 > 200 * 1024) kt /= 2;
+        while (kt > 1 && (size_t)3 * kt * NC * 16 > 50 * 1024) kt /= 2;
         auto make_tiles = [&](int lev, int base, int per_oct, int nslot) {
             for (int o = 0; o < 8; o++) {
                 int g = lev * 8 + o;
