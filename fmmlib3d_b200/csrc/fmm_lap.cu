@@ -93,7 +93,8 @@ struct LapPlan {
     DBuf<double> rot, dc;
     DBuf<Slot> slots;        // [0, 1512): M2L 8 octants x 189; [1512,1520): M2M; [1520,1528): L2L
     std::vector<Slot> hslots;
-    int kt = 8;
+    int kt = 8;       // targets per tile of M2M / L2L
+    int kt_m2l = 8;   // targets per tile of the rotate-shift-rotate M2L
     // dense M2L operators (p <= kDenseMaxP): one per list-2 offset, and the
     // operator offset of every M2L slot
     bool dense = false;
@@ -204,10 +205,15 @@ static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Stat
     build_rotations(p, P->ncls, dcs.p, P->rot.p, s, st);
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) return nullptr;
-    // tile size: three KT x (p+1)^2 complex buffers within ~200 KB of shared memory
+    // tile sizes: three KT x (p+1)^2 complex buffers.  M2M / L2L (8 slots per
+    // tile) within ~50 KB of shared memory, so that several CTAs share an SM;
+    // the rotate-shift-rotate M2L (189 slots, two rotation matrices read per
+    // slot and tile) within ~200 KB, so that the matrices serve more targets.
     int NC = (p + 1) * (p + 1);
     P->kt = 8;
-    while (P->kt > 1 && (size_t)3 * P->kt * NC * 16 > 200 * 1024) P->kt /= 2;
+    while (P->kt > 1 && (size_t)3 * P->kt * NC * 16 > 50 * 1024) P->kt /= 2;
+    P->kt_m2l = 8;
+    while (P->kt_m2l > 1 && (size_t)3 * P->kt_m2l * NC * 16 > 200 * 1024) P->kt_m2l /= 2;
     if (p <= kDenseMaxP) {
         // unique list-2 offsets and their operators
         std::map<int, int> uidx;
@@ -426,7 +432,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.tcm2l = S.mixed && g_tc_m2l > 0;
     // M2L tile size: the largest whose tile count fills the GPU (two CTAs per SM per
     // 64-row block); smaller tiles only add CTAs, every target's sums are unchanged
-    int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt;
+    int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt_m2l;
     if (S.dense && !(S.mixed && !S.tcm2l)) {
         const int rows = div_up(K, 64), want = 2 * device_sms();
         auto ntiles = [&](int kt) {
@@ -544,7 +550,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
                          tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);
     else
         launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt, f, st);
+                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt_m2l, f, st);
     tm.mark_on(f);
     // STEP 5: L2L, levels 2 .. nlev-1
     for (auto &r : S.l2l_rng)
