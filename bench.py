@@ -6,20 +6,21 @@ M = 2,000,000 separate targets, both uniform in the unit cube; complex charges
 and dipole strengths with parts uniform in [-1, 1]; dipole directions uniform on
 the unit sphere; iprec = 1; potential and field at sources and targets.
 Inputs are seeded synthetic data (no dataset is involved).  The step runs in
-two arithmetic forms: "mixed" (FP32 compensated P2P and FP32 M2L operators,
-FP64 elsewhere; the headline) and "fp64" (the reference's arithmetic
-throughout), both reported.
+two arithmetic forms: "mixed" (FP32 compensated P2P and M2L on the tensor
+cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
+"fp64" (the reference's arithmetic throughout), both reported.
 
   value     points/s = (N + M) * steps / device time of the mixed form, inputs
             resident in HBM (fmm3d_lfmm3dparttarg_device), max over ranks.
   e2e       the same metric through the Fortran C ABI (lfmm3dparttarg_) with
             pinned host arrays: H2D of inputs and D2H of outputs inside the
             timed region.
-  roofline  the dominant pass of the step, from the library's per-pass CUDA
-            events, against the FP32 (mixed) or FP64 (fp64 form) GEMM rate
-            measured in the same run (cuBLAS 8192^3) -- MEASURED_PEAKS.json
-            holds only HBM and bf16 figures, and the dominant passes are
-            CUDA-core arithmetic.
+  roofline  the dominant pass of the step and (roofline.passes) P2P and M2L,
+            from the library's per-pass CUDA events of one extra step with the
+            passes serialised, against GEMM rates measured in the same run
+            (cuBLAS 8192^3: FP32 CUDA cores for the mixed P2P, TF32 tensor cores
+            for the mixed M2L, FP64 for the fp64 form) -- MEASURED_PEAKS.json
+            holds only HBM and bf16 figures.
   errors    relative L2 error vs the FP64 direct sum at 1,000 seeded sources
             (self excluded) and 1,000 seeded targets, per output.
   cpu_baseline  the C restatement of the reference (oracle/, OpenMP, all host
@@ -30,6 +31,7 @@ throughout), both reported.
             lfmm3dpartself on 100,000 sources on the unit sphere (seed 1),
             charges only, iprec = 1, FP64, with the CPU restatement timed on
             the same input.
+  laplace_iprec2  the same N = M = 2M workload at iprec 2 (nterms 26), FP64.
   plans     repeated solves on a fixed geometry: single calls vs plan executes (tree built
             once) vs plan executes replaying a CUDA graph of the passes (sphere 100k and
             10k, FP64; the batched workload as a plan, mixed form).
@@ -561,6 +563,46 @@ def run_b200(args):
                 dist=dist if ws > 1 else None, arrays=(src, q, dq, dv, trg))
 
 
+def run_iprec2(args, R, steps=2):
+    """The same N = M workload at iprec 2 (nterms 26), FP64 form (the mixed form covers iprec <= 1)."""
+    torch, F = R["torch"], R["F"]
+    src, q, dq, dv, trg = R["arrays"]
+    n, m = R["n"], R["m"]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = lambda a: torch.from_numpy(a).to(dev)
+    d_src, d_q, d_dq, d_dv, d_trg = g(src), g(q), g(dq), g(dv), g(trg)
+    pot, fld = torch.empty((n, 2), dtype=torch.float64, device=dev), torch.empty((n, 6), dtype=torch.float64, device=dev)
+    pt, ft = torch.empty((m, 2), dtype=torch.float64, device=dev), torch.empty((m, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    F.set_precision(0)
+    F.set_timing(True)
+    step = lambda: F.lfmm3dparttarg_device(2, d_src, d_q, d_dq, d_dv, pot, fld, d_trg, pt, ft, stream=stream)
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    passes = []
+    for _ in range(steps):
+        if step() != 0:
+            raise RuntimeError("iprec 2 FMM failed: %s" % F.last_error())
+        passes.append(F.last_timing())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    rng = np.random.default_rng(98)
+    k = 500
+    si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
+    it = torch.from_numpy(si).to(dev)
+    dp, df = torch.empty((k, 2), dtype=torch.float64, device=dev), torch.empty((k, 6), dtype=torch.float64, device=dev)
+    F.direct_points_device(d_src, d_q, d_dq, d_dv, d_src[it.long()].contiguous(), it, dp, df, stream=stream)
+    torch.cuda.synchronize()
+    err = lambda a, b: float("%.3e" % float(torch.linalg.norm(a - b) / torch.linalg.norm(b)))
+    return {"workload": "laplace_lfmm3dparttarg_cube_2M_src_2M_targ_iprec2", "dtype": "f64",
+            "value": (n + m) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "errors": {"pot": err(pot[it.long()], dp), "fld": err(fld[it.long()], df)},
+            "pass_ms_mean": {kk: round(float(np.mean([p[kk] for p in passes])), 3) for kk in passes[0]}}
+
+
 def run_e2e(args, R):
     """Same workload through the Fortran C ABI with pinned host arrays (H2D + D2H timed)."""
     torch, F = R["torch"], R["F"]
@@ -813,6 +855,8 @@ def main(argv=None):
                                 "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
                                     args.cpu_sample, args.iprec, dt)}
     line["laplace_sphere"] = run_laplace_sphere(args, R)
+    if args.n == 2_000_000 and args.iprec == 1:
+        line["laplace_iprec2"] = run_iprec2(args, R)
     if args.batch_instances > 0:
         line["batched"] = run_batched(args, R)
     line["plans"] = run_plans(args, R, R.pop("batch_arrays", None))
