@@ -9,9 +9,11 @@
 // chunks.  The pair formulas are those of lpotfld3d /
 // lpotfld3d_dp (src/laprouts3d.f:1308-1368, 1962-2035).
 //
-// M2L in FP32: the dense per-offset operators (m2l_dense.cu) rounded to FP32,
-// box-scaled multipoles (all O(1)) rounded to FP32 on load, FP32
-// accumulation, and the tile added to the FP64 local expansion.
+// M2L in FP32 on the CUDA cores (k_m2l_dense32, used when the tensor-core
+// M2L of tc_m2l.cu is switched off): the dense per-offset operators
+// (m2l_dense.cu) rounded to FP32, box-scaled multipoles (all O(1)) rounded to
+// FP32 on load, FP32 accumulation, and the tile added to the FP64 local
+// expansion.
 #include "lap_kernels.cuh"
 #include "m2l_dense.cuh"
 
