@@ -212,8 +212,10 @@ static std::shared_ptr<LapPlan> get_plan(int p, double eps, cudaStream_t s, Stat
     int NC = (p + 1) * (p + 1);
     P->kt = 8;
     while (P->kt > 1 && (size_t)3 * P->kt * NC * 16 > 50 * 1024) P->kt /= 2;
+    // (up to order 26 the M2L kernel keeps its running sums in registers: two buffers)
+    const int m2l_nbuf = NC <= 3 * 256 ? 2 : 3;
     P->kt_m2l = 8;
-    while (P->kt_m2l > 1 && (size_t)3 * P->kt_m2l * NC * 16 > 200 * 1024) P->kt_m2l /= 2;
+    while (P->kt_m2l > 1 && (size_t)m2l_nbuf * P->kt_m2l * NC * 16 > 200 * 1024) P->kt_m2l /= 2;
     if (p <= kDenseMaxP) {
         // unique list-2 offsets and their operators
         std::map<int, int> uidx;
