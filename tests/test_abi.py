@@ -32,3 +32,16 @@ def test_library_exports_all_declared_symbols():
 def test_package_has_no_cpu_fallback():
     src = open(os.path.join(ROOT, "fmmlib3d_b200", "__init__.py")).read()
     assert "import oracle" not in src and "from oracle" not in src
+
+
+def test_fortran_module_binds_exported_symbols():
+    """include/fmm3d_b200.f90 (iso_c_binding interfaces) names only symbols the library exports,
+    and covers every reference entry point (no Fortran compiler here to build the module)."""
+    import fmmlib3d_b200 as F
+    src = open(os.path.join(ROOT, "include", "fmm3d_b200.f90")).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(\w+)"\)', src))
+    lib = ctypes.CDLL(F.LIBPATH)
+    assert bound and not [s for s in bound if not hasattr(lib, s)]
+    for s in ("lfmm3dpart_", "lfmm3dpartself_", "lfmm3dparttarg_", "l3dpartdirect_",
+              "hfmm3dpart_", "hfmm3dpartself_", "hfmm3dparttarg_", "h3dpartdirect_"):
+        assert s in bound

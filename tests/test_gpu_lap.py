@@ -285,3 +285,26 @@ def test_mixed_form_within_twice_reference_error(F, geom, iprec):
         eg, eo = rel(a, d), rel(o, d)
         assert eg < EPS[iprec]
         assert eg <= 2 * eo, (eg, eo)
+
+
+def test_target_only_mode_prunes_list2(F):
+    """ifpot = iffld = 0 with targets (lfmm3dpart's ifprune_list2 case): M2L into boxes without
+    targets is skipped; the target outputs still equal the oracle's, with fewer M2L pairs."""
+    rng = np.random.default_rng(77)
+    n, m = 30000, 4000
+    src = rng.random((n, 3))
+    trg = 0.3 * rng.random((m, 3)) + 0.05          # targets in one corner of the cube
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    F.set_stats(True)
+    try:
+        ier, _, _, pt, ft = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1, trg, 1, 1)
+        full_pairs = F.last_stats()["m2l_pairs"]
+        ier2, _, _, pt2, ft2 = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 0, 0, trg, 1, 1)
+        pruned_pairs = F.last_stats()["m2l_pairs"]
+    finally:
+        F.set_stats(False)
+    assert ier == 0 and ier2 == 0
+    assert pruned_pairs < full_pairs
+    _, _, _, opt, oft = O.lfmm3dparttarg(1, src, q, None, None, trg, ifpot=0, iffld=0)
+    assert rel(pt2, opt) < TOL_ORACLE and rel(ft2, oft) < TOL_ORACLE
+    assert rel(pt2, pt) < TOL_ORACLE and rel(ft2, ft) < TOL_ORACLE
