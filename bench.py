@@ -84,7 +84,7 @@ P2P_DRAM_BYTES_PER_POINT = 208.6   # 834.6 MB per launch at N = M = 2,000,000 (4
 def parse_args(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n", type=int, default=2_000_000, help="sources (= targets)")
@@ -101,6 +101,8 @@ def parse_args(argv=None):
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests per serving rate (0: skip)")
     ap.add_argument("--serve-rates", default="10,40,inf", help="Poisson arrival rates (requests/s)")
+    ap.add_argument("--autotune", metavar="PATH", default=None,
+                    help="tune the Laplace workloads' launch shapes into the JSON cache PATH and exit")
     ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched"], default="all",
                     help="all: the Laplace headline line with the other workloads' objects (default); "
                          "laplace / helmholtz / batched: one workload only (profiling runs)")
@@ -305,6 +307,7 @@ def run_batched(args, R):
     ev[1].record()
     torch.cuda.synchronize()
     ms = ev[0].elapsed_time(ev[1]) / steps
+    knobs, _ = F.last_tuning()
     # errors: 50 points of each of 20 seeded instances against the FP64 direct sum
     rng = np.random.default_rng(96)
     num = {"pot": 0.0, "fld": 0.0}
@@ -328,7 +331,8 @@ def run_batched(args, R):
     return {"workload": "laplace_batched_%d_instances_logN_1e3_2e5_iprec1_mixed" % args.batch_instances,
             "instances": args.batch_instances, "n_total": n, "value": n / (ms * 1e-3), "unit": UNIT,
             "ms_per_step": ms, "steps": steps, "gpu_launches_per_step": int(np.mean(launches)),
-            "errors": {kk: float("%.3e" % np.sqrt(num[kk] / den[kk])) for kk in num}, "pass_ms_mean": mean}
+            "errors": {kk: float("%.3e" % np.sqrt(num[kk] / den[kk])) for kk in num}, "pass_ms_mean": mean,
+            "tuning": knobs}
 
 
 def run_serving(args):
@@ -380,15 +384,20 @@ def reduce_max(dist, value, device):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clock and throttle reasons.  The sampler starts before the
+    warm-up (nvidia-smi needs a few hundred ms to produce its first line), every sample
+    carries nvidia-smi's timestamp, and only the samples inside the timed window
+    (`begin()` .. `stop()`, host wall clock) are summarised."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=25):
         self.gpu = gpu_index
         self.proc = None
+        self.interval_ms = interval_ms
+        self.t0 = None
         self.path = os.path.join(HERE, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
 
     def start(self):
@@ -396,39 +405,49 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, ValueError):
             self.proc = None
 
+    def begin(self):
+        """Start of the timed window."""
+        import datetime
+        self.t0 = datetime.datetime.now()
+
     def stop(self):
         if self.proc is None:
             return None
+        import datetime
+        t1 = datetime.datetime.now()
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.fh.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        if not rows:
             return None
+        inside = [r for r in rows if self.t0 is None or self.t0 <= r[0] <= t1]
+        window = bool(inside)
+        use = inside or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {nm for r in use for nm, v in zip(names, r[3]) if v.lower() == "active"}
+        mx = use[-1][2]
+        sm = [r[1] for r in use]
         loaded = [v for v in sm if mx and v > 0.5 * mx] or sm
         return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "in_timed_window": window, "interval_ms": self.interval_ms}
 
 
 def measured_peak(torch, dev, dtype, tf32=False):
@@ -522,16 +541,17 @@ def run_b200(args):
     def measure(form):
         F.set_precision(form)
         F.set_timing(True)
+        clk = ClockSampler(local)
+        clk.start()
         for w in range(args.warmup):
             F.set_stats(w == args.warmup - 1)   # tree statistics from the last warm-up call only
             step()
         F.set_stats(False)
         torch.cuda.synchronize()
-        clk = ClockSampler(local)
-        clk.start()
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        clk.begin()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         passes, launches = [], []
         ev[0].record()
@@ -544,6 +564,7 @@ def run_b200(args):
         if ws > 1:
             dist.barrier()
         clocks = clk.stop()
+        knobs, _ = F.last_tuning()
         # one more step with the passes serialised, after the timed region: per-kernel
         # times for the roofline (with the default overlap the near-field kernel shares the GPU)
         F.set_overlap(False)
@@ -554,7 +575,7 @@ def run_b200(args):
         total_ms = ev[0].elapsed_time(ev[args.steps])
         total_ms = reduce_max(dist if ws > 1 else None, total_ms, dev)
         return dict(total_ms=total_ms, step_ms=step_ms, passes=passes, launches=launches, stats=F.last_stats(),
-                    clocks=clocks, errs=errors(), points=n + m, serial=serial)
+                    clocks=clocks, errs=errors(), points=n + m, serial=serial, tuning=knobs)
 
     forms = {"mixed": measure(1), "fp64": measure(0)}
     peaks = {"fp64": measured_peak(torch, dev, torch.float64), "fp32": measured_peak(torch, dev, torch.float32),
@@ -790,9 +811,59 @@ def config_of(args, ws):
             "l2_policy": "inputs larger than L2 (%.0f MB per step of inputs vs 126 MB L2)" % (args.n * 104 / 1e6)}
 
 
+def run_autotune(args):
+    """Tune every Laplace workload of this bench (as plans on the same geometry and flags, so the
+    signatures equal those of the measured calls) and write the knobs to the JSON cache."""
+    import torch
+    import fmmlib3d_b200 as F
+    from fmmlib3d_b200 import autotune as A
+    torch.cuda.set_device(dist_env()[2])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    e = lambda k, c: torch.empty((k, c), dtype=torch.float64, device=dev)
+    path = os.path.abspath(args.autotune)
+    F.set_tuning_cache(path)
+    F.set_tensor_m2l(args.tensor_m2l)
+    out = {}
+
+    def one(name, precision, iprec, src, ins, outs, **kw):
+        F.set_precision(precision)
+        plan = F.LaplacePlan(iprec, src, **kw)
+        r = A.tune(plan, *ins, *outs, cache_path=path, log=lambda s: print(name, s, file=sys.stderr, flush=True))
+        out[name] = {"form": r["form"], "knobs": r["knobs"], "ms": round(r["ms"], 3),
+                     "start_ms": round(r["auto_ms"], 3), "trials": len(r["trials"]), "signature": r["signature"]}
+        plan.close()
+        F.set_precision(0)
+
+    n = m = args.n
+    src, q, dq, dv, trg = make_inputs(n, m, 2)
+    d = [g(a) for a in (src, q, dq, dv, trg)]
+    outs = (e(n, 2), e(n, 6), e(m, 2), e(m, 6))
+    flags = dict(ifcharge=1, ifdipole=1, ifpot=1, iffld=1, target=d[4], ifpottarg=1, iffldtarg=1)
+    one("cube_mixed", 1, 1, d[0], d[1:4], outs, **flags)
+    one("cube_fp64", 0, 1, d[0], d[1:4], outs, **flags)
+    if args.n == 2_000_000:
+        one("cube_iprec2_fp64", 0, 2, d[0], d[1:4], outs, **flags)
+    del d, outs
+    for ns in (100_000, 10_000):
+        s_src, s_q = sphere_inputs(ns)
+        one("sphere_%dk_fp64" % (ns // 1000), 0, 1, g(s_src), (g(s_q), None, None), (e(ns, 2), e(ns, 6)),
+            ifcharge=1, ifdipole=0, ifpot=1, iffld=1)
+    if args.batch_instances > 0:
+        b_src, b_q, off = batched_inputs(args.batch_instances)
+        nb = int(off[-1])
+        one("batched_mixed", 1, 1, g(b_src), (g(b_q), None, None), (e(nb, 2), e(nb, 6)),
+            ifcharge=1, ifdipole=0, ifpot=1, iffld=1, src_offsets=off)
+    return {"autotune": path, "device": torch.cuda.get_device_name(), "workloads": out}
+
+
 def main(argv=None):
     args = parse_args(argv)
     ws, rank, _ = dist_env()
+    if args.autotune:
+        if rank == 0:
+            print(json.dumps(run_autotune(args)), flush=True)
+        return 0
     if args.impl == "reference":
         line = run_reference(args)
         if line is not None:
@@ -831,7 +902,7 @@ def main(argv=None):
     def summary(M):
         return {"value": ws * (n + m) * args.steps / (M["total_ms"] * 1e-3), "ms_per_step": M["total_ms"] / args.steps,
                 "p50_ms": float(np.percentile(M["step_ms"], 50)), "p99_ms": float(np.percentile(M["step_ms"], 99)),
-                "errors": {k: float("%.3e" % v) for k, v in M["errs"].items()}}
+                "errors": {k: float("%.3e" % v) for k, v in M["errs"].items()}, "tuning": M["tuning"]}
 
     H = R["forms"]["mixed"]
     head = summary(H)

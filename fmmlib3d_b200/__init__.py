@@ -85,6 +85,19 @@ _lib.fmm3d_last_timing.restype = _I
 _lib.fmm3d_last_stats.argtypes = [_P, _I]
 _lib.fmm3d_last_stats.restype = _I
 _lib.fmm3d_last_error.restype = ctypes.c_char_p
+_lib.fmm3d_set_tuning_cache.argtypes = [ctypes.c_char_p]
+_lib.fmm3d_set_tuning_cache.restype = _I
+_lib.fmm3d_tuning_reload.restype = _I
+_lib.fmm3d_tuning_cache_path.argtypes = [ctypes.c_char_p, _I]
+_lib.fmm3d_tuning_cache_path.restype = _I
+_lib.fmm3d_lfmm3d_plan_set_tuning.argtypes = [_P, _P, _I]
+_lib.fmm3d_lfmm3d_plan_set_tuning.restype = _I
+_lib.fmm3d_lfmm3d_plan_get_tuning.argtypes = [_P, _P, _I]
+_lib.fmm3d_lfmm3d_plan_get_tuning.restype = _I
+_lib.fmm3d_lfmm3d_plan_signature.argtypes = [_P, ctypes.c_char_p, _I]
+_lib.fmm3d_lfmm3d_plan_signature.restype = _I
+_lib.fmm3d_last_tuning.argtypes = [_P, _I, ctypes.c_char_p, _I]
+_lib.fmm3d_last_tuning.restype = _I
 
 PASSES = ["tree", "sort", "p2m", "m2m", "p2l", "m2l", "l2l", "eval", "p2p", "scatter", "total"]
 
@@ -218,6 +231,55 @@ def lfmm3dparttarg_batched_device(iprec, src_offsets, source, charge, dipstr, di
         int(fldtarg is not None), ptr(fldtarg), _P(stream))
 
 
+TUNING_KNOBS = ("m2l_kt", "trans_kt", "tc_variant", "overlap", "p2p_ept")
+TUNING_FORMS = ("fp64-rotation", "fp64-dense", "mixed-cuda", "mixed-tc")
+
+
+def _knob_array(knobs):
+    if isinstance(knobs, dict):
+        unknown = set(knobs) - set(TUNING_KNOBS)
+        if unknown:
+            raise ValueError("unknown tuning knobs: %s" % sorted(unknown))
+        return [int(knobs.get(k, 0)) for k in TUNING_KNOBS]
+    a = [int(v) for v in knobs]
+    if len(a) != len(TUNING_KNOBS):
+        raise ValueError("expected %d knobs" % len(TUNING_KNOBS))
+    return a
+
+
+def _tuning_dict(out):
+    d = {k: int(out[i]) for i, k in enumerate(TUNING_KNOBS)}
+    d["form"] = TUNING_FORMS[int(out[len(TUNING_KNOBS)])]
+    d["from_cache"] = bool(out[len(TUNING_KNOBS) + 1])
+    return d
+
+
+def set_tuning_cache(path):
+    """Tuning cache file for later calls: a path, None (the default: $FMM3D_TUNING_CACHE,
+    else tuning_cache.json beside the library) or "" (no cache)."""
+    _lib.fmm3d_set_tuning_cache(None if path is None else str(path).encode())
+
+
+def tuning_reload():
+    """Re-read the tuning cache; returns the number of entries."""
+    return _lib.fmm3d_tuning_reload()
+
+
+def tuning_cache_path():
+    n = _lib.fmm3d_tuning_cache_path(None, 0)
+    buf = ctypes.create_string_buffer(max(n, 1))
+    _lib.fmm3d_tuning_cache_path(buf, len(buf))
+    return buf.value.decode()
+
+
+def last_tuning():
+    """(knobs dict, signature) of this thread's last single Laplace call."""
+    out = np.zeros(len(TUNING_KNOBS) + 2, np.int32)
+    buf = ctypes.create_string_buffer(1024)
+    _lib.fmm3d_last_tuning(_ptr(out), len(out), buf, len(buf))
+    return _tuning_dict(out), buf.value.decode()
+
+
 class LaplacePlan:
     """A Laplace FMM geometry kept on the device: build once for fixed sources and
     targets (device tensors, layouts as lfmm3dparttarg_device), then ``execute`` for
@@ -272,6 +334,27 @@ class LaplacePlan:
         lst = np.zeros(max(n.value, 1), np.int32)
         ier = _lib.fmm3d_lfmm3d_plan_getl(self._h, int(ibox), int(itype), _ptr(lst), ctypes.byref(n))
         return ier, lst[:n.value]
+
+    def set_tuning(self, knobs):
+        """Launch-shape knobs (dict with keys of ``TUNING_KNOBS`` or a sequence of five;
+        0 = automatic).  Returns 0, or 2 if this problem cannot take a value (the
+        plan keeps its previous knobs)."""
+        a = np.asarray(_knob_array(knobs), np.int32)
+        return _lib.fmm3d_lfmm3d_plan_set_tuning(self._h, _ptr(a), len(a))
+
+    def get_tuning(self):
+        """The knobs in use (0 where the form has none), the form and whether they came
+        from the tuning cache."""
+        out = np.zeros(len(TUNING_KNOBS) + 2, np.int32)
+        _lib.fmm3d_lfmm3d_plan_get_tuning(self._h, _ptr(out), len(out))
+        return _tuning_dict(out)
+
+    def signature(self):
+        """The plan's problem signature (the tuning cache key)."""
+        n = _lib.fmm3d_lfmm3d_plan_signature(self._h, None, 0)
+        buf = ctypes.create_string_buffer(max(n, 1))
+        _lib.fmm3d_lfmm3d_plan_signature(self._h, buf, len(buf))
+        return buf.value.decode()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -35,13 +35,17 @@ extern thread_local int g_launch_count;
 __host__ __device__ __forceinline__ double2 cmk(double a, double b) { return make_double2(a, b); }
 __host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// Products with the fused multiply-add written out: left to the compiler's
+// contraction, a.x*b.x - a.y*b.y may fuse either product, and the choice can
+// differ between instantiations of one kernel template (tile sizes), which
+// would make results depend on launch shapes.
 __host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_double2(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
 }
 __host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b)  // a * conj(b)
 {
-    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+    return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -(a.x * b.y)));
 }
 __host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __host__ __device__ __forceinline__ double2 cscal(double s, double2 a) { return make_double2(s * a.x, s * a.y); }

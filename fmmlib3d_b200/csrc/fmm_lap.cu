@@ -20,6 +20,7 @@
 #include "m2l_dense.cuh"
 #include "tree.cuh"
 #include "driver_common.cuh"
+#include "tuning.cuh"
 
 namespace fmm {
 
@@ -331,10 +332,123 @@ struct LapSetup {
     DBuf<int> tcerr;
     DBuf<Tile> dtiles;
     std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
-    int m2l_a = 0, m2l_n = 0, m2l_kt = 0;
+    int m2l_a = 0, m2l_n = 0, m2l_kt = 0, trans_kt = 0;
+    TuneKnobs knobs;          // as requested (0 = automatic); m2l_kt / trans_kt hold the values in use
+    bool knobs_from_cache = false;
+    std::string signature;
     PointsSoA P;
     OutSoA os, ot;
 };
+
+// Problem signature of the tuning cache: the form, the flags that select
+// kernel variants, and the sizes that set the launch shapes (log2 buckets).
+static std::string lap_signature(const LapSetup &S)
+{
+    const char *form = S.tcm2l ? "mixed-tc" : S.mixed ? "mixed-cuda" : S.dense ? "fp64-dense" : "fp64-rotation";
+    char b[512];
+    snprintf(b, sizeof b,
+             "laplace iprec=%d form=%s charge=%d dipole=%d out=%d%d%d%d inst=2^%d ns=2^%d nt=2^%d nlev=%d "
+             "nboxes=2^%d dev=%s",
+             S.iprec, form, S.ifcharge == 1, S.ifdipole == 1, S.ifpot == 1, S.iffld == 1,
+             S.do_trg && S.ifpottarg == 1, S.do_trg && S.iffldtarg == 1, log2_bucket(S.T.ninst),
+             log2_bucket(S.ns), log2_bucket(S.do_trg ? S.nt : 0), S.T.nlev, log2_bucket(S.T.nboxes),
+             device_tag().c_str());
+    return b;
+}
+
+// form code reported with the knobs: 0 FP64 rotations, 1 FP64 dense, 2 mixed CUDA-core M2L, 3 mixed tensor-core M2L
+static int lap_form(const LapSetup &S) { return S.tcm2l ? 3 : S.mixed ? 2 : S.dense ? 1 : 0; }
+
+// Translation tiles for the given knobs (0 = automatic): M2M / L2L tiles of
+// trans_kt targets per (level, octant) group, M2L tiles of m2l_kt.  Returns 2
+// for a knob this problem cannot take (tile size outside the kernel's range or
+// its shared memory), with S unchanged.
+static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st)
+{
+    Tree &T = S.T;
+    auto &plan = S.plan;
+    const int NC = S.K, p = S.p;
+    const size_t smax = 226 * 1024;   // opt-in limit less room for the kernel's static shared memory
+    auto trans_sm = [&](int nbuf, int kt) {
+        return (size_t)nbuf * kt * NC * sizeof(double2) + (p + 1) * sizeof(double2) + (2 * p + 4) * sizeof(double);
+    };
+    auto pow2_le8 = [](int v) { return v == 1 || v == 2 || v == 4 || v == 8; };
+    if (k.trans_kt && !(pow2_le8(k.trans_kt) && trans_sm(3, k.trans_kt) <= smax)) return 2;
+    if (k.m2l_kt) {
+        if (S.tcm2l) {
+            if (k.m2l_kt % 16 || k.m2l_kt < 16 || k.m2l_kt > kTcTileTargets) return 2;
+        } else if (S.mixed) {
+            if (k.m2l_kt != kDenseTileTargets) return 2;
+        } else if (S.dense) {
+            if (k.m2l_kt != 16 && k.m2l_kt != kDenseTileTargets) return 2;
+        } else {
+            const int nbuf = (k.m2l_kt == 8 && NC <= 3 * 256) ? 2 : 3;
+            if (!pow2_le8(k.m2l_kt) || trans_sm(nbuf, k.m2l_kt) > smax) return 2;
+        }
+    }
+    if (k.tc_variant < 0 || k.tc_variant > 2 || k.overlap < 0 || k.overlap > 2) return 2;
+    if (!(k.p2p_ept == 0 || k.p2p_ept == 1 || k.p2p_ept == 2 || k.p2p_ept == 4)) return 2;
+
+    auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot, std::vector<Tile> &out) {
+        for (int o = 0; o < 8; o++) {
+            int g = lev * 8 + o;
+            int a = T.group_start[g], bnd = T.group_start[g + 1];
+            for (int i = a; i < bnd; i += kt) {
+                Tile t;
+                t.first = i;
+                t.count = std::min(kt, bnd - i);
+                t.slot0 = slot0_base + o * per_oct_stride;
+                t.nslot = nslot;
+                out.push_back(t);
+            }
+        }
+    };
+    const int tkt = k.trans_kt ? k.trans_kt : plan->kt;
+    std::vector<Tile> htiles;
+    std::vector<std::pair<int, int>> m2m, l2l;
+    for (int l = T.nlev - 1; l >= 2; l--) {
+        int a = (int)htiles.size();
+        make_tiles(l, tkt, kSlotM2M, 0, 8, htiles);
+        m2m.push_back({a, (int)htiles.size() - a});
+    }
+    // M2L tile size (automatic): the largest whose tile count fills the GPU (two
+    // CTAs per SM per 64-row block); smaller tiles only add CTAs, every target's
+    // sums are unchanged
+    int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt_m2l;
+    if (k.m2l_kt) {
+        m2l_kt = k.m2l_kt;
+    } else if (S.dense && !(S.mixed && !S.tcm2l)) {
+        const int rows = div_up(S.K, 64), want = 2 * device_sms();
+        auto ntiles = [&](int kt) {
+            long t = 0;
+            for (int l = 2; l <= T.nlev; l++)
+                for (int o = 0; o < 8; o++) t += div_up(T.group_start[l * 8 + o + 1] - T.group_start[l * 8 + o], kt);
+            return t;
+        };
+        while (m2l_kt > 16 && ntiles(m2l_kt) * rows < want) m2l_kt /= 2;
+        if (!S.tcm2l && m2l_kt < kDenseTileTargets) m2l_kt = 16;   // FP64 dense kernel: 64 or 16
+    }
+    const int m2l_a = (int)htiles.size();
+    for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
+    const int m2l_n = (int)htiles.size() - m2l_a;
+    for (int l = 2; l <= T.nlev - 1; l++) {
+        int a = (int)htiles.size();
+        make_tiles(l + 1, tkt, kSlotL2L, 1, 1, htiles);
+        l2l.push_back({a, (int)htiles.size() - a});
+    }
+    if (htiles.size() != S.dtiles.n && !S.dtiles.alloc(htiles.size(), s, st)) return 16;
+    if (!htiles.empty())
+        FMM_TRY(st, cudaMemcpyAsync(S.dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
+    if (!st.ok()) return 16;
+    S.m2m_rng = m2m;
+    S.l2l_rng = l2l;
+    S.m2l_a = m2l_a;
+    S.m2l_n = m2l_n;
+    S.m2l_kt = m2l_kt;
+    S.trans_kt = tkt;
+    S.knobs = k;
+    return 0;
+}
 
 // charges and dipoles into tree order (l3dreorder, src/lfmm3drouts.f:667-691)
 __global__ void k_gather_q(int n, const int *perm, const double *q, const double *dq, const double *dv, int ifc,
@@ -408,57 +522,19 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.os.pot = S.opot.p; S.os.fx = S.ofx.p; S.os.fy = S.ofy.p; S.os.fz = S.ofz.p;
     S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
-    // tiles per (level, octant) group
-    auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot, std::vector<Tile> &out) {
-        for (int o = 0; o < 8; o++) {
-            int g = lev * 8 + o;
-            int a = T.group_start[g], bnd = T.group_start[g + 1];
-            for (int i = a; i < bnd; i += kt) {
-                Tile t;
-                t.first = i;
-                t.count = std::min(kt, bnd - i);
-                t.slot0 = slot0_base + o * per_oct_stride;
-                t.nslot = nslot;
-                out.push_back(t);
-            }
-        }
-    };
-    std::vector<Tile> htiles;
-    for (int l = T.nlev - 1; l >= 2; l--) {
-        int a = (int)htiles.size();
-        make_tiles(l, plan->kt, kSlotM2M, 0, 8, htiles);
-        S.m2m_rng.push_back({a, (int)htiles.size() - a});
-    }
     S.mixed = g_precision == 1 && iprec <= 1 && plan->dense;
     S.dense = (plan->dense && g_m2l_mode != 1) || S.mixed;
     S.tcm2l = S.mixed && g_tc_m2l > 0;
-    // M2L tile size: the largest whose tile count fills the GPU (two CTAs per SM per
-    // 64-row block); smaller tiles only add CTAs, every target's sums are unchanged
-    int m2l_kt = S.tcm2l ? kTcTileTargets : S.dense ? kDenseTileTargets : plan->kt_m2l;
-    if (S.dense && !(S.mixed && !S.tcm2l)) {
-        const int rows = div_up(K, 64), want = 2 * device_sms();
-        auto ntiles = [&](int kt) {
-            long t = 0;
-            for (int l = 2; l <= T.nlev; l++)
-                for (int o = 0; o < 8; o++) t += div_up(T.group_start[l * 8 + o + 1] - T.group_start[l * 8 + o], kt);
-            return t;
-        };
-        while (m2l_kt > 16 && ntiles(m2l_kt) * rows < want) m2l_kt /= 2;
-        if (!S.tcm2l && m2l_kt < kDenseTileTargets) m2l_kt = 16;   // FP64 dense kernel: 64 or 16
+    // launch shapes: the autotuner's cached setting for this problem, else automatic
+    S.signature = lap_signature(S);
+    TuneKnobs kn;
+    S.knobs_from_cache = tuning_lookup(S.signature, kn);
+    int tier = S.knobs_from_cache ? lap_tiles(S, kn, s, st) : 2;
+    if (tier == 2) {
+        S.knobs_from_cache = false;
+        tier = lap_tiles(S, TuneKnobs(), s, st);
     }
-    S.m2l_kt = m2l_kt;
-    S.m2l_a = (int)htiles.size();
-    for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
-    S.m2l_n = (int)htiles.size() - S.m2l_a;
-    for (int l = 2; l <= T.nlev - 1; l++) {
-        int a = (int)htiles.size();
-        make_tiles(l + 1, plan->kt, kSlotL2L, 1, 1, htiles);
-        S.l2l_rng.push_back({a, (int)htiles.size() - a});
-    }
-    if (!htiles.empty()) {
-        S.dtiles.alloc(htiles.size(), s, st);
-        FMM_TRY(st, cudaMemcpyAsync(S.dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
-    }
+    if (tier) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     S.ldm = K + (K & 1);
     if (S.tcm2l && (!S.mp32.alloc((size_t)T.nboxes * S.ldm, s, st) || !S.tcerr.alloc(1, s, st))) {
         g_ti.err = cudaGetErrorString(st.err);
@@ -503,7 +579,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // overlap switched off (fmm3d_set_overlap(0)) everything runs on the call's
     // stream, far field first, with the same arithmetic.
     SideStreams &ss = side_streams();
-    const bool overlap = g_overlap != 0;
+    const bool overlap = S.knobs.overlap ? S.knobs.overlap == 1 : g_overlap != 0;
     const cudaStream_t f = overlap ? ss.far : s;
     if (overlap) {
         FMM_TRY(st, cudaEventRecord(ss.fork, s));
@@ -520,7 +596,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
         if (S.mixed)
             launch_p2p32(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
-                         S.ifpot, S.iffld, ppt, pft, s, st);
+                         S.ifpot, S.iffld, ppt, pft, S.knobs.p2p_ept, s, st);
         else
             launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
                        S.ifpot, S.iffld, ppt, pft, s, st);
@@ -533,7 +609,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // STEP 3: M2M, levels nlev-1 .. 2
     for (auto &r : S.m2m_rng)
         launch_translate(0, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, plan->kt, f, st);
+                         plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, S.trans_kt, f, st);
     tm.mark_on(f);
     // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
     launch_p2l(T.grouped.p, T.nboxes, tv, P, S.ifcharge, S.ifdipole, p, S.local.p, f, st);
@@ -542,7 +618,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     if (S.tcm2l) {
         FMM_TRY(st, cudaMemsetAsync(S.tcerr.p, 0, sizeof(int), f));
         convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, f, st);
-        launch_m2l_tc(g_tc_m2l - 1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
+        const int tcv = S.knobs.tc_variant ? S.knobs.tc_variant - 1 : std::max(g_tc_m2l - 1, 0);
+        launch_m2l_tc(tcv, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
                       plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, f, st);
     } else if (S.mixed)
         launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
@@ -552,12 +629,12 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
                          tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);
     else
         launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, plan->kt_m2l, f, st);
+                         plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);
     tm.mark_on(f);
     // STEP 5: L2L, levels 2 .. nlev-1
     for (auto &r : S.l2l_rng)
         launch_translate(2, S.dtiles.p + r.first, r.second, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
-                         plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, plan->kt, f, st);
+                         plan->dc.p, plan->lddc, S.local.p, S.local.p, prune, S.trans_kt, f, st);
     tm.mark_on(f);
     if (overlap) {
         FMM_TRY(st, cudaEventRecord(ss.join, f));
@@ -632,6 +709,21 @@ static int lap_finish(LapSetup &S, cudaStream_t s, Status &st)
 }
 
 // ---------------------------------------------------------------- the FMM, one call
+// knobs of the last single call on this thread (fmm3d_last_tuning)
+thread_local std::string g_last_signature;
+thread_local int g_last_knobs[kNumKnobs + 2] = {};
+
+static void lap_effective_knobs(const LapSetup &S, int *out)
+{
+    out[0] = S.m2l_kt;
+    out[1] = S.trans_kt;
+    out[2] = S.tcm2l ? (S.knobs.tc_variant ? S.knobs.tc_variant : std::max(g_tc_m2l, 1)) : 0;
+    out[3] = S.knobs.overlap ? S.knobs.overlap : (g_overlap ? 1 : 2);
+    out[4] = S.mixed ? (S.knobs.p2p_ept ? S.knobs.p2p_ept : 4) : 0;
+    out[5] = lap_form(S);
+    out[6] = S.knobs_from_cache ? 1 : 0;
+}
+
 static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, const double *d_q, int ifdipole,
                           const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
                           double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
@@ -644,6 +736,8 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     int ier = lap_setup(S, iprec, ns, d_src, ifcharge, ifdipole, ifpot, iffld, nt, d_trg, ifpottarg, iffldtarg, s, tm,
                         so, to);
     if (ier) return ier;
+    g_last_signature = S.signature;
+    lap_effective_knobs(S, g_last_knobs);
     Status st;
     lap_passes(S, d_q, d_dq, d_dv, d_pot, d_fld, d_pottarg, d_fldtarg, s, tm, st);
     tm.finish(g_ti.ms);
@@ -663,7 +757,7 @@ struct LapPlanExec {
     cudaStream_t made_on = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void *key[8] = {};
-    int key_overlap = -1;      // the overlap switch when the graph was captured
+    int key_cfg = -1;          // the overlap and tensor-core switches when the graph was captured
     int graph_launches = 0;
     std::vector<cudaStream_t> used;
     // host copy of the tree for the queries (filled on first use)
@@ -780,7 +874,8 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
     g_launch_count = 0;
     if (use_graph) {
         const void *key[8] = {d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, (const void *)s};
-        if (!E->exec || memcmp(key, E->key, sizeof key) != 0 || E->key_overlap != g_overlap) {
+        const int cfg = g_overlap * 16 + g_tc_m2l;
+        if (!E->exec || memcmp(key, E->key, sizeof key) != 0 || E->key_cfg != cfg) {
             if (E->exec) cudaGraphExecDestroy(E->exec);
             E->exec = nullptr;
             cudaGraph_t g = nullptr;
@@ -797,7 +892,7 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
                 return 16;
             }
             memcpy(E->key, key, sizeof key);
-            E->key_overlap = g_overlap;
+            E->key_cfg = cfg;
             E->graph_launches = g_launch_count;
         }
         FMM_TRY(st, cudaGraphLaunch(E->exec, s));
@@ -825,6 +920,57 @@ int fmm3d_lfmm3d_plan_destroy(void *plan)
     }
     delete E;
     return 0;
+}
+
+int fmm3d_lfmm3d_plan_set_tuning(void *plan, const int *knobs, int n)
+{
+    if (!plan || !knobs || n < kNumKnobs) return 1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    for (int i = 0; i < kNumKnobs; i++)
+        if (knobs[i] < 0) return 2;
+    // the tiles may be in use by work in flight, and a captured graph holds them
+    for (auto s : E->used) cudaStreamSynchronize(s);
+    if (E->exec) cudaGraphExecDestroy(E->exec);
+    E->exec = nullptr;
+    Status st;
+    const TuneKnobs old = E->S.knobs;
+    int ier = lap_tiles(E->S, knobs_from_array(knobs), E->made_on, st);
+    if (ier == 0) E->S.knobs_from_cache = false;
+    else if (ier == 2) lap_tiles(E->S, old, E->made_on, st);
+    FMM_TRY(st, cudaStreamSynchronize(E->made_on));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return ier;
+}
+
+// out[0..4] = knobs in use (m2l_kt, trans_kt, tc_variant, overlap, p2p_ept; 0 = not
+// applicable to this form), out[5] = form, out[6] = 1 if they came from the cache
+int fmm3d_lfmm3d_plan_get_tuning(void *plan, int *out, int n)
+{
+    if (!plan || !out || n < kNumKnobs + 2) return 1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    lap_effective_knobs(E->S, out);
+    return 0;
+}
+
+int fmm3d_lfmm3d_plan_signature(void *plan, char *buf, int n)
+{
+    if (!plan) return -1;
+    auto *E = (LapPlanExec *)plan;
+    std::lock_guard<std::mutex> lk(E->mu);
+    const std::string &sg = E->S.signature;
+    if (!buf || n <= 0) return (int)sg.size() + 1;
+    snprintf(buf, (size_t)n, "%s", sg.c_str());
+    return (int)sg.size() + 1 <= n ? 0 : (int)sg.size() + 1;
+}
+
+// the knobs (as fmm3d_lfmm3d_plan_get_tuning) and signature of this thread's last single Laplace call
+int fmm3d_last_tuning(int *out, int n, char *sig, int nsig)
+{
+    if (out && n >= kNumKnobs + 2) memcpy(out, g_last_knobs, sizeof(int) * (kNumKnobs + 2));
+    if (sig && nsig > 0) snprintf(sig, (size_t)nsig, "%s", g_last_signature.c_str());
+    return (int)g_last_signature.size() + 1;
 }
 
 // out[0..9] = nboxes, nlev, nleaves, nterms, nsource, ntarget, centre x, y, z, side of the root cube

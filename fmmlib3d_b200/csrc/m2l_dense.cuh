@@ -28,10 +28,10 @@ void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const S
 namespace fmm {
 
 // Mixed-precision form (mixed.cu): FP32 P2P with compensated accumulation
-// and FP32 dense M2L.
+// (max_ept: at most 1, 2 or 4 evaluation points per lane) and FP32 dense M2L.
 void launch_p2p32(const int *leaves, int nleaves, const TreeView &tv, const PointsSoA &src, const double *tx,
                   const double *ty, const double *tz, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
-                  int ifpot, int iffld, int ifpottarg, int iffldtarg, cudaStream_t s, Status &st);
+                  int ifpot, int iffld, int ifpottarg, int iffldtarg, int max_ept, cudaStream_t s, Status &st);
 void convert_f32(long long n, const double2 *in, float2 *out, cudaStream_t s, Status &st);
 // Tensor-core (tcgen05, split TF32) form of the FP32 dense M2L (tc_m2l.cu):
 // tiles of up to 128 targets, FP32 multipoles with an even row stride ldm;

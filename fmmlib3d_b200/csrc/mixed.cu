@@ -83,7 +83,8 @@ template <bool CHG, bool DIP>
 __device__ __forceinline__ void pair64(double dx, double dy, double dz, double2 q, double2 d, double vx, double vy,
                                        double vz, double *a)
 {
-    double r2 = dx * dx + dy * dy + dz * dz;
+    // fused multiply-adds written out, so that every instantiation (points per lane) rounds alike
+    double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
     double ri = rsqrt(r2);
     double ri2 = ri * ri, ri3 = ri * ri2;
     if (CHG) {
@@ -95,12 +96,12 @@ __device__ __forceinline__ void pair64(double dx, double dy, double dz, double2 
         a[6] = fma(qx, dz, a[6]); a[7] = fma(qy, dz, a[7]);
     }
     if (DIP) {
-        double dot = dx * vx + dy * vy + dz * vz;
+        double dot = fma(dx, vx, fma(dy, vy, dz * vz));
         double t = dot * ri3;
         a[0] = fma(d.x, t, a[0]);
         a[1] = fma(d.y, t, a[1]);
         double rt = 3.0 * t * ri2;
-        double gx = rt * dx - ri3 * vx, gy = rt * dy - ri3 * vy, gz = rt * dz - ri3 * vz;
+        double gx = fma(rt, dx, -(ri3 * vx)), gy = fma(rt, dy, -(ri3 * vy)), gz = fma(rt, dz, -(ri3 * vz));
         a[2] = fma(d.x, gx, a[2]); a[3] = fma(d.y, gx, a[3]);
         a[4] = fma(d.x, gy, a[4]); a[5] = fma(d.y, gy, a[5]);
         a[6] = fma(d.x, gz, a[6]); a[7] = fma(d.y, gz, a[7]);
@@ -290,7 +291,8 @@ template <bool CHG, bool DIP>
 __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, TreeView tv, PointsSoA src,
                                                           const double *tx, const double *ty, const double *tz,
                                                           OutSoA outs, OutSoA outt, int do_src, int do_trg,
-                                                          int want_fs, int want_ft, int want_ps, int want_pt)
+                                                          int want_fs, int want_ft, int want_ps, int want_pt,
+                                                          int max_ept)
 {
     // per source: A = (x hi, y hi, z hi, charge re | vx), B = (x lo, y lo, z lo, charge im | vy),
     // C = (charge re, charge im, dipstr re, dipstr im), D = vz   (C, D with dipoles only)
@@ -299,14 +301,15 @@ __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, 
     __shared__ float whi[kEPT * 8][32], wlo[kEPT * 8][32];   // TwoSum pairs, [component][lane]
     const int b = leaves[blockIdx.x];
     const int ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
-    // passes of 32, 64 or 128 evaluation points (one, two or four per lane)
+    // passes of 32, 64 or 128 evaluation points (one, two or four per lane, at most
+    // max_ept); every point's sums run over the same sources in the same order
     for (int e0 = 0; e0 < ne;) {
         const int left = ne - e0;
-        if (left <= 32) {
+        if (left <= 32 || max_ept == 1) {
             p2p32_pass<CHG, DIP, 1>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
                                     want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
             e0 += 32;
-        } else if (left <= 64) {
+        } else if (left <= 64 || max_ept == 2) {
             p2p32_pass<CHG, DIP, 2>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
                                     want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
             e0 += 64;
@@ -320,23 +323,24 @@ __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, 
 
 void launch_p2p32(const int *leaves, int nleaves, const TreeView &tv, const PointsSoA &src, const double *tx,
                   const double *ty, const double *tz, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
-                  int ifpot, int iffld, int ifpottarg, int iffldtarg, cudaStream_t s, Status &st)
+                  int ifpot, int iffld, int ifpottarg, int iffldtarg, int max_ept, cudaStream_t s, Status &st)
 {
     if (nleaves == 0 || !st.ok()) return;
     int do_src = (ifpot == 1 || iffld == 1), do_trg = (ifpottarg == 1 || iffldtarg == 1);
     bool c = ifcharge == 1, d = ifdipole == 1;
+    if (max_ept != 1 && max_ept != 2) max_ept = 4;
     if (c && d) {
         k_p2p32<true, true><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                              do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
-                                                             ifpottarg == 1); FMM_COUNT_LAUNCH();
+                                                             ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     } else if (c) {
         k_p2p32<true, false><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                               do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
-                                                              ifpottarg == 1); FMM_COUNT_LAUNCH();
+                                                              ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     } else if (d) {
         k_p2p32<false, true><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                               do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
-                                                              ifpottarg == 1); FMM_COUNT_LAUNCH();
+                                                              ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     }
     FMM_LAUNCH_CHECK(st);
 }

@@ -243,6 +243,38 @@ int fmm3d_lfmm3d_plan_getb(void *plan, int ibox, int *box, double *center, doubl
  * 2 for a bad ibox or itype; list = NULL returns only the length in *nlist. */
 int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlist);
 
+/* ---- Launch-shape tuning (no counterpart in the reference, whose only
+ * tuning input is iprec).  Five knobs, 0 = automatic:
+ *   [0] M2L targets per tile (tensor-core form 16..128 in steps of 16; FP64
+ *       dense operators 16 or 64; FP32 CUDA-core form 64; rotations 1, 2, 4, 8),
+ *   [1] M2M / L2L targets per tile (1, 2, 4, 8),
+ *   [2] tensor-core M2L staging variant (1 or 2, as fmm3d_set_tensor_m2l),
+ *   [3] 1 = near field concurrent with the far field, 2 = passes in order,
+ *   [4] mixed-form P2P: at most 1, 2 or 4 evaluation points per lane.
+ * No knob changes the arithmetic: every setting gives the same outputs bitwise.
+ * Single calls and new plans take their knobs from the autotuner's JSON cache
+ * (fmmlib3d_b200/autotune.py) when it holds the problem's signature, else
+ * automatic values.  Cache file: the path set here (NULL: back to the default;
+ * "" or "none": no cache), else $FMM3D_TUNING_CACHE, else tuning_cache.json
+ * beside libfmm3d_b200.so. */
+int fmm3d_set_tuning_cache(const char *path);
+/* Re-read the cache file; returns the number of entries. */
+int fmm3d_tuning_reload(void);
+/* The cache path in use (returns 0, or the buffer size needed). */
+int fmm3d_tuning_cache_path(char *buf, int n);
+/* Set a plan's knobs (n >= 5).  Returns 0, 2 for a value this problem cannot
+ * take (the plan keeps its previous knobs), 16 on a CUDA error. */
+int fmm3d_lfmm3d_plan_set_tuning(void *plan, const int *knobs, int n);
+/* out (n >= 7): the five knobs in use (0 where the form has no such knob), the
+ * form (0 FP64 rotations, 1 FP64 dense operators, 2 mixed with CUDA-core M2L,
+ * 3 mixed with tensor-core M2L) and 1 if the knobs came from the cache. */
+int fmm3d_lfmm3d_plan_get_tuning(void *plan, int *out, int n);
+/* The plan's problem signature (the cache key); returns 0 or the buffer size needed. */
+int fmm3d_lfmm3d_plan_signature(void *plan, char *buf, int n);
+/* Knobs (as fmm3d_lfmm3d_plan_get_tuning) and signature of this thread's last
+ * single Laplace call; returns the signature's buffer size. */
+int fmm3d_last_tuning(int *out, int n, char *sig, int nsig);
+
 /* Human-readable description of the last CUDA error on this thread. */
 const char *fmm3d_last_error(void);
 
