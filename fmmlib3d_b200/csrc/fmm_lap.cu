@@ -579,7 +579,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // overlap switched off (fmm3d_set_overlap(0)) everything runs on the call's
     // stream, far field first, with the same arithmetic.
     SideStreams &ss = side_streams();
-    const bool overlap = S.knobs.overlap ? S.knobs.overlap == 1 : g_overlap != 0;
+    // fmm3d_set_overlap(0) forces the passes in order (per-pass timing); else the knob decides
+    const bool overlap = g_overlap != 0 && S.knobs.overlap != 2;
     const cudaStream_t f = overlap ? ss.far : s;
     if (overlap) {
         FMM_TRY(st, cudaEventRecord(ss.fork, s));
@@ -718,7 +719,7 @@ static void lap_effective_knobs(const LapSetup &S, int *out)
     out[0] = S.m2l_kt;
     out[1] = S.trans_kt;
     out[2] = S.tcm2l ? (S.knobs.tc_variant ? S.knobs.tc_variant : std::max(g_tc_m2l, 1)) : 0;
-    out[3] = S.knobs.overlap ? S.knobs.overlap : (g_overlap ? 1 : 2);
+    out[3] = (g_overlap != 0 && S.knobs.overlap != 2) ? 1 : 2;
     out[4] = S.mixed ? (S.knobs.p2p_ept ? S.knobs.p2p_ept : 4) : 0;
     out[5] = lap_form(S);
     out[6] = S.knobs_from_cache ? 1 : 0;

@@ -139,43 +139,60 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
         fresh = true;
         have_acc = true;
     };
+    // Source boxes of the staged targets for a slot: colleague of the target's
+    // parent, then that colleague's child.  Empty source boxes are not skipped:
+    // their multipoles are zero and add exact zeros.  The chain of the next slot
+    // is loaded while the current slot's stages run (colleagues with the first
+    // stage, children after it), so its dependent loads stay off the critical path.
+    int par[NPASS], cnx[NPASS], sbn[NPASS];
+#pragma unroll
+    for (int j = 0; j < NPASS; j++) {
+        const int n = tid / KB + TPP * j;
+        const int t = n < tile.count ? tg[n] : -1;
+        par[j] = (t >= 0 && !(prune && tv.ntrg[t] == 0)) ? tv.parent[t] : -1;
+    }
+    auto chain_coll = [&](const Slot &x) {
+#pragma unroll
+        for (int j = 0; j < NPASS; j++) cnx[j] = par[j] >= 0 ? tv.coll[27L * par[j] + x.coll] : -1;
+    };
+    auto chain_child = [&](const Slot &x) {
+#pragma unroll
+        for (int j = 0; j < NPASS; j++) sbn[j] = cnx[j] >= 0 ? tv.child[8L * cnx[j] + x.oct] : -1;
+    };
+    Slot sl_next = slots[tile.slot0];
+    chain_coll(sl_next);
+    chain_child(sl_next);
     for (int si = 0; si < tile.nslot && !aborted; si++) {
+        const Slot sl = sl_next;
+        int sbr[NPASS];
+#pragma unroll
+        for (int j = 0; j < NPASS; j++) sbr[j] = sbn[j];
+        const bool has_next = si + 1 < tile.nslot;
+        int chain = 0;   // next slot's chain: 0 not started, 1 colleagues loaded, 2 source boxes loaded
+        if (has_next) sl_next = slots[tile.slot0 + si + 1];
         do {  // one slot; break = nothing to add for it
-            const Slot sl = slots[tile.slot0 + si];
             const int R = (sl.pt + 1) * (sl.pt + 1);
             if (row0 >= R) break;
-            int sbr[NPASS];
             int have = 0;
 #pragma unroll
-            for (int j = 0; j < NPASS; j++) {
-                const int n = tid / KB + TPP * j;
-                const int t = n < tile.count ? tg[n] : -1;
-                int sb = -1;
-                if (t >= 0 && !(prune && tv.ntrg[t] == 0)) {
-                    const int P = tv.parent[t];
-                    const int C = P >= 0 ? tv.coll[27L * P + sl.coll] : -1;
-                    sb = C >= 0 ? tv.child[8L * C + sl.oct] : -1;
-                    if (sb >= 0 && tv.nsrc[sb] == 0) sb = -1;
-                }
-                sbr[j] = sb;
-                have |= sb >= 0;
-            }
+            for (int j = 0; j < NPASS; j++) have |= sbr[j] >= 0;
             if (!__syncthreads_or(have)) break;
+            if (has_next) { chain_coll(sl_next); chain = 1; }
             const float2 *Tu = T + slot_toff[tile.slot0 + si];
             const int nk = (2 * R + KC - 1) / KC;
-            // registers of one stage: operator pairs (A) and multipole pairs (B)
-            float2 ra0[NA], ra1[NA];
-            float4 rb[NPASS];
+            // registers of two stages in flight: operator pairs (A) and multipole pairs (B)
+            float2 ra0[2][NA], ra1[2][NA];
+            float4 rb[2][NPASS];
             // A: operator rows row0 .. row0 + 63, columns jb .. jb + KC/2 - 1 (column-major T);
             // B: the gathered source multipoles, coefficients jb .. jb + KC/2 - 1
-            auto load = [&](int kc) {
+            auto load = [&](int kc, int set) {
                 const int jb = kc * (KC / 2);
 #pragma unroll
                 for (int a = 0; a < NA; a++) {
                     const int task = tid + a * kTcThreads, i = task & 63, kb = task >> 6;
                     const int row = row0 + i, j0 = jb + 2 * kb;
-                    ra0[a] = (row < R && j0 < R) ? Tu[(size_t)j0 * R + row] : make_float2(0.f, 0.f);
-                    ra1[a] = (row < R && j0 + 1 < R) ? Tu[(size_t)(j0 + 1) * R + row] : make_float2(0.f, 0.f);
+                    ra0[set][a] = (row < R && j0 < R) ? Tu[(size_t)j0 * R + row] : make_float2(0.f, 0.f);
+                    ra1[set][a] = (row < R && j0 + 1 < R) ? Tu[(size_t)(j0 + 1) * R + row] : make_float2(0.f, 0.f);
                 }
 #pragma unroll
                 for (int j = 0; j < NPASS; j++) {
@@ -185,14 +202,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
                         v = *(const float4 *)(mp + (size_t)sbr[j] * ldm + j0);
                         if (j0 + 1 >= R) { v.z = 0.f; v.w = 0.f; }
                     }
-                    rb[j] = v;
+                    rb[set][j] = v;
                 }
             };
-            auto store = [&](unsigned char *base) {
+            auto store = [&](unsigned char *base, int set) {
 #pragma unroll
                 for (int a = 0; a < NA; a++) {
                     const int task = tid + a * kTcThreads, i = task & 63, kb = task >> 6;
-                    const float2 v0 = ra0[a], v1 = ra1[a];
+                    const float2 v0 = ra0[set][a], v1 = ra1[set][a];
                     float4 h, l;
                     unsigned char *ah = base + kb * kTcLBO, *al = base + OPB + kb * kTcLBO;
                     split4(make_float4(v0.x, -v0.y, v1.x, -v1.y), h, l);
@@ -207,28 +224,42 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
                     const int n = tid / KB + TPP * j, kb = tid % KB;
                     if (n >= N) continue;
                     float4 h, l;
-                    split4(rb[j], h, l);
+                    split4(rb[set][j], h, l);
                     *(float4 *)(base + 2 * OPB + kb * kTcLBO + n * 16) = h;
                     *(float4 *)(base + 3 * OPB + kb * kTcLBO + n * 16) = l;
                 }
             };
-            load(0);
-            for (int kc = 0; kc < nk; kc++, it++) {
+            // one stage: wait for its ring slot, stage it, start the loads two stages
+            // ahead, then one thread issues its MMAs
+            auto stage = [&](int kc, int set) {
                 const int st = it % S;
                 int late = 0;
                 if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
-                store(sm + st * STB);
-                if (kc + 1 < nk) load(kc + 1);     // next stage's loads in flight during this one's MMAs
+                store(sm + st * STB, set);
+                if (kc + 2 < nk) load(kc + 2, set);
                 fence_async_smem();
-                if (__syncthreads_or(late)) { aborted = true; break; }
+                if (__syncthreads_or(late)) { aborted = true; return false; }
                 if (tid == 0) {
                     tc_fence_after();
                     issue_stage<KC>(sbase + st * STB, tm, idesc, fresh && kc == 0, nprod);
                     tc_commit(&mbar[st]);
                 }
                 fresh = false;
+                it++;
+                if (chain == 1) { chain_child(sl_next); chain = 2; }
+                return true;
+            };
+            load(0, 0);
+            if (nk > 1) load(1, 1);
+            for (int kc = 0; kc < nk; kc += 2) {
+                if (!stage(kc, 0)) break;
+                if (kc + 1 < nk && !stage(kc + 1, 1)) break;
             }
         } while (0);
+        if (has_next && !aborted) {
+            if (chain == 0) chain_coll(sl_next);
+            if (chain <= 1) chain_child(sl_next);
+        }
         // group boundaries at fixed slot indices, so a target's sums do not
         // depend on which other targets share its tile
         if (!aborted && group > 0 && (si + 1) % group == 0 && !fresh) flush();

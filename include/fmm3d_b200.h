@@ -249,7 +249,8 @@ int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlis
  *       dense operators 16 or 64; FP32 CUDA-core form 64; rotations 1, 2, 4, 8),
  *   [1] M2M / L2L targets per tile (1, 2, 4, 8),
  *   [2] tensor-core M2L staging variant (1 or 2, as fmm3d_set_tensor_m2l),
- *   [3] 1 = near field concurrent with the far field, 2 = passes in order,
+ *   [3] 1 = near field concurrent with the far field, 2 = passes in order
+ *       (fmm3d_set_overlap(0) forces the passes in order whatever the knob),
  *   [4] mixed-form P2P: at most 1, 2 or 4 evaluation points per lane.
  * No knob changes the arithmetic: every setting gives the same outputs bitwise.
  * Single calls and new plans take their knobs from the autotuner's JSON cache
