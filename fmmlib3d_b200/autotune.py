@@ -1,7 +1,7 @@
 """Autotuner of the Laplace passes' launch shapes, with a JSON cache.
 
 Knobs (``TUNING_KNOBS``, 0 = automatic):
-  m2l_kt      M2L targets per tile (tensor-core form 16..128; FP64 dense operators 16 or 64;
+  m2l_kt      M2L targets per tile (tensor-core form 16..256; FP64 dense operators 16 or 64;
               rotations 1, 2, 4, 8)
   trans_kt    M2M / L2L targets per tile (1, 2, 4, 8)
   tc_variant  tensor-core M2L shared-memory staging (1: K chunks of 16, three stages;
@@ -37,7 +37,7 @@ def candidates(form):
     """(knob, values) in search order for a form (as ``LaplacePlan.get_tuning()["form"]``)."""
     c = []
     if form == "mixed-tc":
-        c.append(("m2l_kt", [16, 32, 64, 128]))
+        c.append(("m2l_kt", [16, 32, 64, 128, 256]))
     elif form == "fp64-dense":
         c.append(("m2l_kt", [16, 64]))
     elif form == "fp64-rotation":

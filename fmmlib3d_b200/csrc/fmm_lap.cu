@@ -376,7 +376,7 @@ static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st
     if (k.trans_kt && !(pow2_le8(k.trans_kt) && trans_sm(3, k.trans_kt) <= smax)) return 2;
     if (k.m2l_kt) {
         if (S.tcm2l) {
-            if (k.m2l_kt % 16 || k.m2l_kt < 16 || k.m2l_kt > kTcTileTargets) return 2;
+            if (k.m2l_kt % 16 || k.m2l_kt < 16 || k.m2l_kt > kTcTileTargetsMax) return 2;
         } else if (S.mixed) {
             if (k.m2l_kt != kDenseTileTargets) return 2;
         } else if (S.dense) {
@@ -425,6 +425,8 @@ static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st
                 for (int o = 0; o < 8; o++) t += div_up(T.group_start[l * 8 + o + 1] - T.group_start[l * 8 + o], kt);
             return t;
         };
+        // (256-target tensor-core tiles run one CTA per SM and measured slower on every
+        // workload tried; they are reached through the tuning knob only)
         while (m2l_kt > 16 && ntiles(m2l_kt) * rows < want) m2l_kt /= 2;
         if (!S.tcm2l && m2l_kt < kDenseTileTargets) m2l_kt = 16;   // FP64 dense kernel: 64 or 16
     }
@@ -621,7 +623,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, f, st);
         const int tcv = S.knobs.tc_variant ? S.knobs.tc_variant - 1 : std::max(g_tc_m2l - 1, 0);
         launch_m2l_tc(tcv, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
-                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, f, st);
+                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, S.m2l_kt, f,
+                      st);
     } else if (S.mixed)
         launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
                            plan->T32.p, tv, p, S.mpole.p, S.local.p, prune, f, st);

@@ -55,15 +55,18 @@ __device__ __forceinline__ void split4(float4 v, float4 &h, float4 &l)
 // the high parts and, for nprod >= 3, the two cross products, for nprod >= 4
 // also the product of the low parts (then the sum is the exact product of
 // hi + lo, i.e. of the operands to within about 2^-24 each).
-template <int KC>
+// Stage layout: A_hi, A_lo (128 rows, K-block stride kTcLBO), then B_hi, B_lo
+// (NMAX rows, K-block stride NMAX * 16 + 16).
+template <int KC, int NMAX = 128>
 __device__ __forceinline__ void issue_stage(uint32_t base, uint32_t tm, uint32_t idesc, bool first, int nprod)
 {
-    constexpr uint32_t OPB = (KC / 4) * kTcLBO;
+    constexpr uint32_t LBOB = NMAX * 16 + 16;
+    constexpr uint32_t OPA = (KC / 4) * kTcLBO, OPBB = (KC / 4) * LBOB;
 #pragma unroll
     for (int s = 0; s < KC / 8; s++) {
-        const uint32_t o = 2 * s * kTcLBO;
-        const uint64_t ah = tc_desc(base + o, kTcLBO, 128), al = tc_desc(base + OPB + o, kTcLBO, 128);
-        const uint64_t bh = tc_desc(base + 2 * OPB + o, kTcLBO, 128), bl = tc_desc(base + 3 * OPB + o, kTcLBO, 128);
+        const uint32_t oa = 2 * s * kTcLBO, ob = 2 * s * LBOB;
+        const uint64_t ah = tc_desc(base + oa, kTcLBO, 128), al = tc_desc(base + OPA + oa, kTcLBO, 128);
+        const uint64_t bh = tc_desc(base + 2 * OPA + ob, LBOB, 128), bl = tc_desc(base + 2 * OPA + OPBB + ob, LBOB, 128);
         tc_mma_tf32(tm, ah, bh, idesc, (first && s == 0) ? 0u : 1u);
         if (nprod >= 3) {
             tc_mma_tf32(tm, ah, bl, idesc, 1u);
@@ -73,36 +76,42 @@ __device__ __forceinline__ void issue_stage(uint32_t base, uint32_t tm, uint32_t
     }
 }
 
-template <int KC, int S>
-__global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, const int *grouped, const Slot *slots,
-                                                        const long long *slot_toff, const float2 *T, TreeView tv,
-                                                        int p, const float2 *mp, int ldm, double2 *out, int prune,
-                                                        int nprod, int group, int *err)
+// NMAX: targets per tile at most (128: two CTAs per SM, 256 TMEM columns;
+// 256: one CTA per SM, 512 TMEM columns, each staged operator serves twice
+// the targets).
+template <int KC, int S, int NMAX>
+__global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
+    k_m2l_tc(const Tile *tiles, const int *grouped, const Slot *slots, const long long *slot_toff, const float2 *T,
+             TreeView tv, int p, const float2 *mp, int ldm, double2 *out, int prune, int nprod, int group, int *err)
 {
     constexpr int KB = KC / 4;                 // 16-byte K blocks per stage
-    constexpr uint32_t OPB = KB * kTcLBO;      // one operand buffer
-    constexpr uint32_t STB = 4 * OPB;          // A_hi, A_lo, B_hi, B_lo
+    constexpr uint32_t OPB = KB * kTcLBO;      // one A buffer
+    constexpr uint32_t LBOB = NMAX * 16 + 16;  // K-block stride of B
+    constexpr uint32_t OPBB = KB * LBOB;       // one B buffer
+    constexpr uint32_t STB = 2 * OPB + 2 * OPBB;   // A_hi, A_lo, B_hi, B_lo
     constexpr int TPP = kTcThreads / KB;       // targets staged per pass
-    constexpr int NPASS = 128 / TPP;
+    constexpr int NPASS = NMAX / TPP;
+    constexpr int TCOLS = 2 * NMAX;            // TMEM columns: tensor-core sum, running sum
+    constexpr int HC = NMAX / 2;               // columns per warp (two warps per lane quarter)
     constexpr int NA = 64 * KB / kTcThreads;   // operator pairs staged per thread
     static_assert(64 * KB % kTcThreads == 0, "stage tasks must divide evenly");
     extern __shared__ unsigned char tc_smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smraw + 127) & ~(uintptr_t)127);
     __shared__ uint64_t mbar[S];
     __shared__ uint32_t tbase;
-    __shared__ int tg[128];
+    __shared__ int tg[NMAX];
     const Tile tile = tiles[blockIdx.x];
     const int row0 = 64 * blockIdx.y;          // first complex row of this CTA
     const int NC = (p + 1) * (p + 1);
     const int N = max(16, (tile.count + 15) & ~15);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid < 128) tg[tid] = tid < tile.count ? grouped[tile.first + tid] : -1;
+    for (int n = tid; n < NMAX; n += kTcThreads) tg[n] = n < tile.count ? grouped[tile.first + n] : -1;
     if (tid == 0) {
         for (int s = 0; s < S; s++) mbar_init(&mbar[s], 1);
         mbar_fence_init();
     }
     __syncwarp();
-    if (warp == 0) tmem_alloc(&tbase, 256);
+    if (warp == 0) tmem_alloc(&tbase, TCOLS);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -110,8 +119,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
     const uint32_t idesc = tc_idesc_tf32(128, N);
     const uint32_t sbase = smem_u32(sm);
     const int q = warp & 3, h = warp >> 2;     // TMEM lane quarter and column half of this warp
-    const uint32_t tD = tm + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * h);   // tensor-core sum (columns 0..127)
-    const uint32_t tA = tD + 128;                                                // FP32 running sum (128..255)
+    const uint32_t tD = tm + ((uint32_t)(32 * q) << 16) + (uint32_t)(HC * h);   // tensor-core sum (0 .. NMAX-1)
+    const uint32_t tA = tD + NMAX;                                              // FP32 running sum (NMAX .. 2 NMAX-1)
     int it = 0;
     bool aborted = false, fresh = true;        // fresh: the next MMA starts a new TMEM sum
     bool have_acc = false;                     // the running sum holds flushed groups
@@ -122,8 +131,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
         if (__syncthreads_or(!done)) { aborted = true; return; }
         tc_fence_after();
 #pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-            if (64 * h + c0 < N) {
+        for (int c0 = 0; c0 < HC; c0 += 16) {
+            if (HC * h + c0 < N) {
                 float v[16], a[16];
                 tmem_ld16(tD + c0, v);
                 if (have_acc) {
@@ -225,8 +234,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
                     if (n >= N) continue;
                     float4 h, l;
                     split4(rb[set][j], h, l);
-                    *(float4 *)(base + 2 * OPB + kb * kTcLBO + n * 16) = h;
-                    *(float4 *)(base + 3 * OPB + kb * kTcLBO + n * 16) = l;
+                    *(float4 *)(base + 2 * OPB + kb * LBOB + n * 16) = h;
+                    *(float4 *)(base + 2 * OPB + OPBB + kb * LBOB + n * 16) = l;
                 }
             };
             // one stage: wait for its ring slot, stage it, start the loads two stages
@@ -241,7 +250,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
                 if (__syncthreads_or(late)) { aborted = true; return false; }
                 if (tid == 0) {
                     tc_fence_after();
-                    issue_stage<KC>(sbase + st * STB, tm, idesc, fresh && kc == 0, nprod);
+                    issue_stage<KC, NMAX>(sbase + st * STB, tm, idesc, fresh && kc == 0, nprod);
                     tc_commit(&mbar[st]);
                 }
                 fresh = false;
@@ -270,14 +279,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
         tc_fence_after();
         const int L = 32 * q + lane, ci = L & 63, part = L >> 6, row = row0 + ci;
 #pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
-            if (64 * h + c0 < N) {
+        for (int c0 = 0; c0 < HC; c0 += 16) {
+            if (HC * h + c0 < N) {
                 float v[16];
                 tmem_ld16(tA + c0, v);
                 if (row < NC) {
 #pragma unroll
                     for (int u = 0; u < 16; u++) {
-                        const int n = 64 * h + c0 + u;
+                        const int n = HC * h + c0 + u;
                         const int t = n < tile.count ? tg[n] : -1;
                         if (t >= 0) {
                             double *o = (double *)(out + (size_t)t * NC + row) + part;
@@ -296,32 +305,35 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_m2l_tc(const Tile *tiles, con
     if (bad && tid == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tm, 256);
+    if (warp == 0) tmem_dealloc(tm, TCOLS);
 }
 
-template <int KC, int S>
+template <int KC, int S, int NMAX>
 static void launch_tc_t(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                         const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
                         int ldm, double2 *out, int prune, int nprod, int group, int *err, cudaStream_t s,
                         Status &st)
 {
-    const size_t sm = (size_t)S * 4 * (KC / 4) * kTcLBO + 128;
-    FMM_TRY(st, cudaFuncSetAttribute(k_m2l_tc<KC, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const size_t sm = (size_t)S * 2 * (KC / 4) * (kTcLBO + NMAX * 16 + 16) + 128;
+    FMM_TRY(st, cudaFuncSetAttribute(k_m2l_tc<KC, S, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 g(ntiles, div_up((p + 1) * (p + 1), 64));
-    k_m2l_tc<KC, S><<<g, kTcThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod,
+    k_m2l_tc<KC, S, NMAX><<<g, kTcThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod,
                                               group, err); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
 
 void launch_m2l_tc(int variant, const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                    const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
-                   int ldm, double2 *out, int prune, int nprod, int group, int *err, cudaStream_t s, Status &st)
+                   int ldm, double2 *out, int prune, int nprod, int group, int *err, int max_tile, cudaStream_t s,
+                   Status &st)
 {
     if (!st.ok() || ntiles == 0) return;
-    if (variant == 1)
-        launch_tc_t<32, 2>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
+    if (max_tile > 128)
+        launch_tc_t<16, 3, 256>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
+    else if (variant == 1)
+        launch_tc_t<32, 2, 128>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
     else
-        launch_tc_t<16, 3>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
+        launch_tc_t<16, 3, 128>(tiles, ntiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod, group, err, s, st);
 }
 
 // FP32 copy of the multipoles with an even row stride (16-byte aligned pairs).

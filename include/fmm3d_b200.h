@@ -245,7 +245,7 @@ int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlis
 
 /* ---- Launch-shape tuning (no counterpart in the reference, whose only
  * tuning input is iprec).  Five knobs, 0 = automatic:
- *   [0] M2L targets per tile (tensor-core form 16..128 in steps of 16; FP64
+ *   [0] M2L targets per tile (tensor-core form 16..256 in steps of 16; FP64
  *       dense operators 16 or 64; FP32 CUDA-core form 64; rotations 1, 2, 4, 8),
  *   [1] M2M / L2L targets per tile (1, 2, 4, 8),
  *   [2] tensor-core M2L staging variant (1 or 2, as fmm3d_set_tensor_m2l),

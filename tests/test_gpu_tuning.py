@@ -85,7 +85,7 @@ def test_bad_values_are_refused_and_the_plan_keeps_its_knobs(F):
     plan = F.LaplacePlan(1, src, 1, 0, 1, 1)
     assert plan.set_tuning({"m2l_kt": 32, "trans_kt": 4}) == 0
     before = plan.get_tuning()
-    for bad in ({"m2l_kt": 24}, {"m2l_kt": 256}, {"trans_kt": 3}, {"trans_kt": 16}, {"overlap": 3},
+    for bad in ({"m2l_kt": 24}, {"m2l_kt": 272}, {"trans_kt": 3}, {"trans_kt": 16}, {"overlap": 3},
                 {"tc_variant": 5}, {"p2p_ept": 3}):
         assert plan.set_tuning(bad) == 2, bad
         assert plan.get_tuning() == before
