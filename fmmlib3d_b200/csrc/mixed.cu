@@ -71,6 +71,30 @@ __device__ __forceinline__ void pair32(float exh, float eyh, float ezh, float ex
     }
 }
 
+// The same pair term with dipoles, the field factored as r^-3 [(q + 3 d t) dx - d v]
+// and the products -d v of the source (nv: re x, y, z, then im x, y, z) computed
+// once when the source is staged: 38 operations per pair instead of 42.
+template <bool CHG>
+__device__ __forceinline__ void pair32_dip(float exh, float eyh, float ezh, float exl, float eyl, float ezl,
+                                           float sxh, float syh, float szh, float sxl, float syl, float szl,
+                                           float2 q, float2 d, float vx, float vy, float vz, const float *nv,
+                                           float *a)
+{
+    float dx = (exh - sxh) + (exl - sxl), dy = (eyh - syh) + (eyl - syl), dz = (ezh - szh) + (ezl - szl);
+    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float ri = rsqrt_approx(r2);
+    float ri2 = ri * ri, ri3 = ri * ri2;
+    float t = fmaf(dx, vx, fmaf(dy, vy, dz * vz)) * ri2;
+    float ax = CHG ? fmaf(d.x, t, q.x) : d.x * t, ay = CHG ? fmaf(d.y, t, q.y) : d.y * t;
+    a[0] = fmaf(ax, ri, a[0]);
+    a[1] = fmaf(ay, ri, a[1]);
+    float t3 = 3.0f * t;
+    float bx = CHG ? fmaf(d.x, t3, q.x) : d.x * t3, by = CHG ? fmaf(d.y, t3, q.y) : d.y * t3;
+    a[2] = fmaf(ri3, fmaf(bx, dx, nv[0]), a[2]); a[3] = fmaf(ri3, fmaf(by, dx, nv[3]), a[3]);
+    a[4] = fmaf(ri3, fmaf(bx, dy, nv[1]), a[4]); a[5] = fmaf(ri3, fmaf(by, dy, nv[4]), a[5]);
+    a[6] = fmaf(ri3, fmaf(bx, dz, nv[2]), a[6]); a[7] = fmaf(ri3, fmaf(by, dz, nv[5]), a[7]);
+}
+
 __device__ __forceinline__ void split_df(double v, float &hi, float &lo)
 {
     hi = (float)v;
@@ -127,7 +151,7 @@ __device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, co
                                            const double *tx, const double *ty, const double *tz, OutSoA &outs,
                                            OutSoA &outt, int do_src, int do_trg, int want_fs, int want_ft,
                                            int want_ps, int want_pt, float4 *wA, float4 *wB, float4 *wC,
-                                           float *wD, float (*whi)[32], float (*wlo)[32])
+                                           float4 *wD, float4 *wE, float (*whi)[32], float (*wlo)[32])
 {
     const int lane = threadIdx.x;
     const double cx = tv.center[3L * b], cy = tv.center[3L * b + 1], cz = tv.center[3L * b + 2];
@@ -206,8 +230,7 @@ __device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, co
             }
         };
         advance();
-        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pc = pa;
-        float pdz = 0.f;
+        float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pc = pa, pd = pa, pe = pa;
         auto fetch = [&]() {
             int i = c0 + lane;
             if (j < nl && i < jn) {
@@ -218,10 +241,13 @@ __device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, co
                 if (DIP) {
                     pa.w = (float)src.vx[i];
                     pb.w = (float)src.vy[i];
-                    pdz = (float)src.vz[i];
+                    const float vz = (float)src.vz[i];
                     const double2 d = src.dq[i];
                     const double2 q = CHG ? src.q[i] : cmk(0, 0);
                     pc = make_float4((float)q.x, (float)q.y, (float)d.x, (float)d.y);
+                    // -d v (FP32 products of the FP32 operands), re then im
+                    pd = make_float4(vz, -pc.z * pa.w, -pc.z * pb.w, -pc.z * vz);
+                    pe = make_float4(-pc.w * pa.w, -pc.w * pb.w, -pc.w * vz, 0.f);
                 } else {
                     const double2 q = src.q[i];
                     pa.w = (float)q.x;
@@ -236,7 +262,7 @@ __device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, co
             if (lane < cn) {
                 wA[lane] = pa;
                 wB[lane] = pb;
-                if (DIP) { wC[lane] = pc; wD[lane] = pdz; }
+                if (DIP) { wC[lane] = pc; wD[lane] = pd; wE[lane] = pe; }
             }
             __syncwarp();
             c0 += 32;
@@ -250,21 +276,21 @@ __device__ __forceinline__ void p2p32_pass(int e0, int b, const TreeView &tv, co
 #pragma unroll 2
             for (int k = 0; k < cn; k++) {
                 const float4 A = wA[k], B = wB[k];
-                float2 q, d;
-                float vx = 0.f, vy = 0.f, vz = 0.f;
                 if (DIP) {
-                    const float4 C = wC[k];
-                    q = make_float2(C.x, C.y);
-                    d = make_float2(C.z, C.w);
-                    vx = A.w; vy = B.w; vz = wD[k];
-                } else {
-                    q = make_float2(A.w, B.w);
-                    d = make_float2(0.f, 0.f);
-                }
+                    const float4 C = wC[k], D = wD[k], E = wE[k];
+                    const float nv[6] = {D.y, D.z, D.w, E.x, E.y, E.z};
 #pragma unroll
-                for (int u = 0; u < kEPT; u++)
-                    pair32<CHG, DIP>(eh[u][0], eh[u][1], eh[u][2], el[u][0], el[u][1], el[u][2], A.x, A.y, A.z,
-                                     B.x, B.y, B.z, q, d, vx, vy, vz, a[u]);
+                    for (int u = 0; u < kEPT; u++)
+                        pair32_dip<CHG>(eh[u][0], eh[u][1], eh[u][2], el[u][0], el[u][1], el[u][2], A.x, A.y, A.z,
+                                        B.x, B.y, B.z, make_float2(C.x, C.y), make_float2(C.z, C.w), A.w, B.w, D.x,
+                                        nv, a[u]);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < kEPT; u++)
+                        pair32<CHG, false>(eh[u][0], eh[u][1], eh[u][2], el[u][0], el[u][1], el[u][2], A.x, A.y,
+                                           A.z, B.x, B.y, B.z, make_float2(A.w, B.w), make_float2(0.f, 0.f), 0.f,
+                                           0.f, 0.f, a[u]);
+                }
             }
 #pragma unroll
             for (int u = 0; u < kEPT; u++)
@@ -295,9 +321,9 @@ __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, 
                                                           int max_ept)
 {
     // per source: A = (x hi, y hi, z hi, charge re | vx), B = (x lo, y lo, z lo, charge im | vy),
-    // C = (charge re, charge im, dipstr re, dipstr im), D = vz   (C, D with dipoles only)
-    __shared__ float4 wA[32], wB[32], wC[32];
-    __shared__ float wD[32];
+    // C = (charge re, charge im, dipstr re, dipstr im), D = (vz, -d v re x, y, z),
+    // E = (-d v im x, y, z, 0)   (C, D, E with dipoles only)
+    __shared__ float4 wA[32], wB[32], wC[32], wD[32], wE[32];
     __shared__ float whi[kEPT * 8][32], wlo[kEPT * 8][32];   // TwoSum pairs, [component][lane]
     const int b = leaves[blockIdx.x];
     const int ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
@@ -307,15 +333,15 @@ __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, 
         const int left = ne - e0;
         if (left <= 32 || max_ept == 1) {
             p2p32_pass<CHG, DIP, 1>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 32;
         } else if (left <= 64 || max_ept == 2) {
             p2p32_pass<CHG, DIP, 2>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 64;
         } else {
             p2p32_pass<CHG, DIP, 4>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, whi, wlo);
+                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 128;
         }
     }
