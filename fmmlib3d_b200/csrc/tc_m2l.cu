@@ -130,19 +130,21 @@ __global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
         const bool done = mbar_wait_bounded(&mbar[last % S], (last / S) & 1);
         if (__syncthreads_or(!done)) { aborted = true; return; }
         tc_fence_after();
+        // 32 columns at a time, both loads under one wait, the stores completed once
+        // (columns past N within a 32-column block hold unused values)
 #pragma unroll
-        for (int c0 = 0; c0 < HC; c0 += 16) {
+        for (int c0 = 0; c0 < HC; c0 += 32) {
             if (HC * h + c0 < N) {
-                float v[16], a[16];
-                tmem_ld16(tD + c0, v);
+                float v[32], a[32];
+                tmem_ld32x2(tD + c0, tA + c0, v, a);
                 if (have_acc) {
-                    tmem_ld16(tA + c0, a);
 #pragma unroll
-                    for (int u = 0; u < 16; u++) v[u] += a[u];
+                    for (int u = 0; u < 32; u++) v[u] += a[u];
                 }
-                tmem_st16(tA + c0, v);
+                tmem_st32(tA + c0, v);
             }
         }
+        tmem_wait_st();
         tc_fence_before();
         __syncthreads();
         fresh = true;
