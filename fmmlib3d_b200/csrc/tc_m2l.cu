@@ -223,12 +223,13 @@ __global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
                     const float2 v0 = ra0[set][a], v1 = ra1[set][a];
                     float4 h, l;
                     unsigned char *ah = base + kb * kTcLBO, *al = base + OPB + kb * kTcLBO;
-                    split4(make_float4(v0.x, -v0.y, v1.x, -v1.y), h, l);
-                    *(float4 *)(ah + i * 16) = h;
-                    *(float4 *)(al + i * 16) = l;
-                    split4(make_float4(v0.y, v0.x, v1.y, v1.x), h, l);
-                    *(float4 *)(ah + (64 + i) * 16) = h;
-                    *(float4 *)(al + (64 + i) * 16) = l;
+                    // one split serves both rows: rounding to nearest is odd, so the
+                    // parts of -x are those of x negated
+                    split4(make_float4(v0.x, v0.y, v1.x, v1.y), h, l);
+                    *(float4 *)(ah + i * 16) = make_float4(h.x, -h.y, h.z, -h.w);
+                    *(float4 *)(al + i * 16) = make_float4(l.x, -l.y, l.z, -l.w);
+                    *(float4 *)(ah + (64 + i) * 16) = make_float4(h.y, h.x, h.w, h.z);
+                    *(float4 *)(al + (64 + i) * 16) = make_float4(l.y, l.x, l.w, l.z);
                 }
 #pragma unroll
                 for (int j = 0; j < NPASS; j++) {
