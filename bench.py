@@ -78,7 +78,7 @@ P2P_FLOPS_PER_PAIR = 62
 P2P_FLOPS_CHARGE = 31
 # DRAM bytes per evaluation point of one mixed-form P2P launch (k_p2p32), from the
 # committed ncu capture (profiles/); traffic scales with the points, not the pairs.
-P2P_DRAM_BYTES_PER_POINT = 208.6   # 834.6 MB per launch at N = M = 2,000,000 (4M evaluation points)
+P2P_DRAM_BYTES_PER_POINT = 235.2   # 941.0 MB per launch at N = M = 2,000,000 (4M evaluation points)
 
 
 def parse_args(argv=None):
