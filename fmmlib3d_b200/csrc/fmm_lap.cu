@@ -359,6 +359,26 @@ static std::string lap_signature(const LapSetup &S)
 // form code reported with the knobs: 0 FP64 rotations, 1 FP64 dense, 2 mixed CUDA-core M2L, 3 mixed tensor-core M2L
 static int lap_form(const LapSetup &S) { return S.tcm2l ? 3 : S.mixed ? 2 : S.dense ? 1 : 0; }
 
+// Tiles of one (level, octant) group and translation kind: boxes [a, bnd) of
+// the grouped box array in runs of kt, written from tile tile0 on.
+struct TileSeg {
+    int tile0, a, bnd, kt, slot0, nslot;
+};
+
+__global__ void k_make_tiles(const TileSeg *segs, Tile *tiles)
+{
+    const TileSeg g = segs[blockIdx.x];
+    const int n = (g.bnd - g.a + g.kt - 1) / g.kt;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        Tile t;
+        t.first = g.a + j * g.kt;
+        t.count = min(g.kt, g.bnd - t.first);
+        t.slot0 = g.slot0;
+        t.nslot = g.nslot;
+        tiles[g.tile0 + j] = t;
+    }
+}
+
 // Translation tiles for the given knobs (0 = automatic): M2M / L2L tiles of
 // trans_kt targets per (level, octant) group, M2L tiles of m2l_kt.  Returns 2
 // for a knob this problem cannot take (tile size outside the kernel's range or
@@ -389,27 +409,24 @@ static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st
     if (k.tc_variant < 0 || k.tc_variant > 2 || k.overlap < 0 || k.overlap > 2) return 2;
     if (!(k.p2p_ept == 0 || k.p2p_ept == 1 || k.p2p_ept == 2 || k.p2p_ept == 4)) return 2;
 
-    auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot, std::vector<Tile> &out) {
+    // tile segments on the host (a few per level), the tiles themselves on the device
+    std::vector<TileSeg> segs;
+    int ntile = 0;
+    auto make_tiles = [&](int lev, int kt, int slot0_base, int per_oct_stride, int nslot) {
         for (int o = 0; o < 8; o++) {
             int g = lev * 8 + o;
             int a = T.group_start[g], bnd = T.group_start[g + 1];
-            for (int i = a; i < bnd; i += kt) {
-                Tile t;
-                t.first = i;
-                t.count = std::min(kt, bnd - i);
-                t.slot0 = slot0_base + o * per_oct_stride;
-                t.nslot = nslot;
-                out.push_back(t);
-            }
+            if (bnd <= a) continue;
+            segs.push_back({ntile, a, bnd, kt, slot0_base + o * per_oct_stride, nslot});
+            ntile += div_up(bnd - a, kt);
         }
     };
     const int tkt = k.trans_kt ? k.trans_kt : plan->kt;
-    std::vector<Tile> htiles;
     std::vector<std::pair<int, int>> m2m, l2l;
     for (int l = T.nlev - 1; l >= 2; l--) {
-        int a = (int)htiles.size();
-        make_tiles(l, tkt, kSlotM2M, 0, 8, htiles);
-        m2m.push_back({a, (int)htiles.size() - a});
+        int a = ntile;
+        make_tiles(l, tkt, kSlotM2M, 0, 8);
+        m2m.push_back({a, ntile - a});
     }
     // M2L tile size (automatic): the largest whose tile count fills the GPU (two
     // CTAs per SM per 64-row block); smaller tiles only add CTAs, every target's
@@ -430,17 +447,22 @@ static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st
         while (m2l_kt > 16 && ntiles(m2l_kt) * rows < want) m2l_kt /= 2;
         if (!S.tcm2l && m2l_kt < kDenseTileTargets) m2l_kt = 16;   // FP64 dense kernel: 64 or 16
     }
-    const int m2l_a = (int)htiles.size();
-    for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189, htiles);
-    const int m2l_n = (int)htiles.size() - m2l_a;
+    const int m2l_a = ntile;
+    for (int l = 2; l <= T.nlev; l++) make_tiles(l, m2l_kt, 0, 189, 189);
+    const int m2l_n = ntile - m2l_a;
     for (int l = 2; l <= T.nlev - 1; l++) {
-        int a = (int)htiles.size();
-        make_tiles(l + 1, tkt, kSlotL2L, 1, 1, htiles);
-        l2l.push_back({a, (int)htiles.size() - a});
+        int a = ntile;
+        make_tiles(l + 1, tkt, kSlotL2L, 1, 1);
+        l2l.push_back({a, ntile - a});
     }
-    if (htiles.size() != S.dtiles.n && !S.dtiles.alloc(htiles.size(), s, st)) return 16;
-    if (!htiles.empty())
-        FMM_TRY(st, cudaMemcpyAsync(S.dtiles.p, htiles.data(), sizeof(Tile) * htiles.size(), cudaMemcpyHostToDevice, s));
+    if ((size_t)ntile != S.dtiles.n && !S.dtiles.alloc(ntile, s, st)) return 16;
+    if (!segs.empty()) {
+        DBuf<TileSeg> dsegs;
+        if (!dsegs.alloc(segs.size(), s, st)) return 16;
+        FMM_TRY(st, cudaMemcpyAsync(dsegs.p, segs.data(), sizeof(TileSeg) * segs.size(), cudaMemcpyHostToDevice, s));
+        k_make_tiles<<<(unsigned)segs.size(), 256, 0, s>>>(dsegs.p, S.dtiles.p); FMM_COUNT_LAUNCH();
+        FMM_LAUNCH_CHECK(st);
+    }
     if (!st.ok()) return 16;
     S.m2m_rng = m2m;
     S.l2l_rng = l2l;
