@@ -333,6 +333,12 @@ struct LapSetup {
     DBuf<Tile> dtiles;
     std::vector<std::pair<int, int>> m2m_rng, l2l_rng;  // per level: [first tile, count)
     int m2l_a = 0, m2l_n = 0, m2l_kt = 0, trans_kt = 0;
+    // mixed form: list-3 boxes with few sources and the list-4 boxes of boxes with
+    // few points are summed with the near field; tv_near is tv with list 1
+    // replaced by the widened near list, tv_far with lists 3 and 4 by the rest
+    DBuf<int> nl_start, nl_idx, fl_start, fl_idx, f4_start, f4_idx;
+    TreeView tv_near, tv_far;
+    int l3_direct = 0;        // source / point count up to which lists 3 / 4 go to the near field (0: none)
     TuneKnobs knobs;          // as requested (0 = automatic); m2l_kt / trans_kt hold the values in use
     bool knobs_from_cache = false;
     std::string signature;
@@ -474,6 +480,103 @@ static int lap_tiles(LapSetup &S, const TuneKnobs &k, cudaStream_t s, Status &st
     return 0;
 }
 
+// Mixed form, near field widened by source or point count.  A list-3 box c of
+// leaf b is a separated box whose multipole the reference evaluates at b's
+// points (l3dmpeval_trunc0); a list-4 box c of box a is a separated leaf whose
+// sources the reference expands about a (l3dformta_trunc0), the expansion
+// then reaching every point below a.  When c holds at most `thr` sources
+// (list 3), or a holds at most `thr` evaluation points (list 4), summing c's
+// sources directly at the points is cheaper than the (p+2)^2 harmonics per
+// point or per source, and exact.  Every box owns a contiguous range of the
+// tree-ordered sources, so the near-field kernel takes such boxes as they are.
+// Near list of leaf b: list 1, the small list-3 boxes, then the list-4 boxes of
+// b and of each ancestor with few points; far lists 3 and 4: the others.
+__device__ __forceinline__ bool l4_direct(const TreeView &tv, int a, int thr, int do_src, int do_trg)
+{
+    return (do_src ? tv.nsrc[a] : 0) + (do_trg ? tv.ntrg[a] : 0) <= thr;
+}
+
+__global__ void k_near_count(int nb, TreeView tv, int thr, int do_src, int do_trg, int *cn, int *c3, int *c4)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    int near = 0, far3 = 0;
+    for (int k = tv.l3_start[b]; k < tv.l3_start[b + 1]; k++) {
+        if (tv.nsrc[tv.l3_idx[k]] <= thr) near++;
+        else far3++;
+    }
+    if (tv.nchild[b] == 0) {
+        near += tv.l1_start[b + 1] - tv.l1_start[b];
+        for (int a = b; a >= 0; a = tv.parent[a])
+            if (l4_direct(tv, a, thr, do_src, do_trg)) near += tv.l4_start[a + 1] - tv.l4_start[a];
+    } else {
+        near = 0;
+    }
+    cn[b] = near;
+    c3[b] = far3;
+    c4[b] = l4_direct(tv, b, thr, do_src, do_trg) ? 0 : tv.l4_start[b + 1] - tv.l4_start[b];
+}
+
+__global__ void k_near_fill(int nb, TreeView tv, int thr, int do_src, int do_trg, const int *n0, const int *f30,
+                            const int *f40, int *nidx, int *f3idx, int *f4idx)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const bool leaf = tv.nchild[b] == 0;
+    int o = n0[b], f = f30[b];
+    if (leaf)
+        for (int k = tv.l1_start[b]; k < tv.l1_start[b + 1]; k++) nidx[o++] = tv.l1_idx[k];
+    for (int k = tv.l3_start[b]; k < tv.l3_start[b + 1]; k++) {
+        const int c = tv.l3_idx[k];
+        if (tv.nsrc[c] <= thr) { if (leaf) nidx[o++] = c; }
+        else f3idx[f++] = c;
+    }
+    if (leaf)
+        for (int a = b; a >= 0; a = tv.parent[a])
+            if (l4_direct(tv, a, thr, do_src, do_trg))
+                for (int k = tv.l4_start[a]; k < tv.l4_start[a + 1]; k++) nidx[o++] = tv.l4_idx[k];
+    if (!l4_direct(tv, b, thr, do_src, do_trg)) {
+        int g = f40[b];
+        for (int k = tv.l4_start[b]; k < tv.l4_start[b + 1]; k++) f4idx[g++] = tv.l4_idx[k];
+    }
+}
+
+static void lap_widen_near(LapSetup &S, int thr, cudaStream_t s, Status &st)
+{
+    Tree &T = S.T;
+    const int nb = T.nboxes;
+    S.tv_near = S.tv_far = S.tv;
+    S.l3_direct = 0;
+    if (thr <= 0 || nb == 0) return;
+    DBuf<int> cn, c3, c4;
+    if (!cn.alloc(nb + 1, s, st) || !c3.alloc(nb + 1, s, st) || !c4.alloc(nb + 1, s, st) ||
+        !S.nl_start.alloc(nb + 1, s, st) || !S.fl_start.alloc(nb + 1, s, st) || !S.f4_start.alloc(nb + 1, s, st))
+        return;
+    cn.zero(st);
+    c3.zero(st);
+    c4.zero(st);
+    k_near_count<<<div_up(nb, 256), 256, 0, s>>>(nb, S.tv, thr, S.do_src, S.do_trg, cn.p, c3.p, c4.p); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    int tn = 0, t3 = 0, t4 = 0;
+    scan_exclusive_int(cn.p, S.nl_start.p, nb + 1, s, st, &tn);
+    scan_exclusive_int(c3.p, S.fl_start.p, nb + 1, s, st, &t3);
+    scan_exclusive_int(c4.p, S.f4_start.p, nb + 1, s, st, &t4);
+    if (!st.ok() || !S.nl_idx.alloc(std::max(tn, 1), s, st) || !S.fl_idx.alloc(std::max(t3, 1), s, st) ||
+        !S.f4_idx.alloc(std::max(t4, 1), s, st))
+        return;
+    k_near_fill<<<div_up(nb, 256), 256, 0, s>>>(nb, S.tv, thr, S.do_src, S.do_trg, S.nl_start.p, S.fl_start.p,
+                                               S.f4_start.p, S.nl_idx.p, S.fl_idx.p, S.f4_idx.p); FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    if (!st.ok()) return;
+    S.tv_near.l1_start = S.nl_start.p;
+    S.tv_near.l1_idx = S.nl_idx.p;
+    S.tv_far.l3_start = S.fl_start.p;
+    S.tv_far.l3_idx = S.fl_idx.p;
+    S.tv_far.l4_start = S.f4_start.p;
+    S.tv_far.l4_idx = S.f4_idx.p;
+    S.l3_direct = thr;
+}
+
 // charges and dipoles into tree order (l3dreorder, src/lfmm3drouts.f:667-691)
 __global__ void k_gather_q(int n, const int *perm, const double *q, const double *dq, const double *dv, int ifc,
                            int ifd, PointsSoA o)
@@ -559,6 +662,9 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
         tier = lap_tiles(S, TuneKnobs(), s, st);
     }
     if (tier) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    // mixed form: small list-3 / list-4 interactions join the near field (FP64 keeps the reference's lists)
+    lap_widen_near(S, S.mixed ? (p + 2) * (p + 2) / 2 : 0, s, st);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     S.ldm = K + (K & 1);
     if (S.tcm2l && (!S.mp32.alloc((size_t)T.nboxes * S.ldm, s, st) || !S.tcerr.alloc(1, s, st))) {
         g_ti.err = cudaGetErrorString(st.err);
@@ -620,8 +726,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         // STEP 8: P2P over self and list 1 (adds to the outputs)
         const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
         if (S.mixed)
-            launch_p2p32(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
-                         S.ifpot, S.iffld, ppt, pft, S.knobs.p2p_ept, s, st);
+            launch_p2p32(T.leaves.p, T.nleaves, S.tv_near, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge,
+                         S.ifdipole, S.ifpot, S.iffld, ppt, pft, S.knobs.p2p_ept, s, st);
         else
             launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
                        S.ifpot, S.iffld, ppt, pft, s, st);
@@ -637,7 +743,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
                          plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, S.trans_kt, f, st);
     tm.mark_on(f);
     // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
-    launch_p2l(T.grouped.p, T.nboxes, tv, P, S.ifcharge, S.ifdipole, p, S.local.p, f, st);
+    launch_p2l(T.grouped.p, T.nboxes, S.tv_far, P, S.ifcharge, S.ifdipole, p, S.local.p, f, st);
     tm.mark_on(f);
     // STEP 4: M2L over list 2, all levels >= 2
     if (S.tcm2l) {
@@ -670,7 +776,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     }
     tm.mark();
     // STEPS 6, 7: M2P from list 3 and L2P (add the far field to the outputs)
-    launch_eval(T.leaves.p, T.nleaves, tv, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
+    launch_eval(T.leaves.p, T.nleaves, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
                 S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
     tm.mark();
     if (tm.on) {
@@ -705,8 +811,8 @@ static void lap_stats(LapSetup &S, cudaStream_t s, Status &st)
     acc.alloc(1 + 128, s, st);
     acc.zero(st);
     if (!st.ok()) return;
-    k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, S.tv, S.do_src, S.do_trg,
-                                                                acc.p); FMM_COUNT_LAUNCH();
+    k_stats<<<div_up(std::max(T.nleaves, 1), 256), 256, 0, s>>>(T.nleaves, T.leaves.p, S.tv_near, S.do_src,
+                                                                S.do_trg, acc.p); FMM_COUNT_LAUNCH();
     for (int l = 2; l <= T.nlev; l++) {
         k_m2l_count<<<div_up(T.lev_count[l], 128), 128, 0, s>>>(T.lev_start[l], T.lev_count[l], S.tv,
                                                                S.plan->slots.p, S.prune, acc.p + 1); FMM_COUNT_LAUNCH();
