@@ -57,6 +57,8 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
 Multi-GPU: an FMM call does not shard; `--gpus N` runs N independent replicas
 (one per rank, scaling "weak"), timed as the max over ranks.
 `--impl reference` times the CPU restatement on the host cores (rank 0 only).
+`--autotune PATH` tunes the Laplace workloads' launch shapes (fmmlib3d_b200.autotune) into the
+JSON cache PATH and exits; every measured workload reports the knobs it ran with ("tuning").
 """
 import argparse
 import json
