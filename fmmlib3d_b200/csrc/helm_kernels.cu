@@ -508,9 +508,10 @@ void launch_htranslate(int kind, const Tile *tiles, int ntiles, const int *group
 // ================================================================ point operators
 // Legendre recurrence coefficients for the column recurrences in registers:
 // g_ha[n][m] = sqrt((n+m-1)(n-m-1)), g_hb[n][m] = 1/sqrt((n-m)(n+m)),
-// g_hs[n] = sqrt(2n+1), g_hc[m] = sqrt((2m-1)/(2m)).
+// g_hs[n] = sqrt(2n+1), g_hc[m] = sqrt((2m-1)/(2m)); the weights of the radial
+// derivative of j_n, g_hq[n] = n/(2n+1), and g_hr[n] = 1/(2n+1).
 constexpr int kHTab = kHelmMaxP + 3;
-__device__ double g_ha[kHTab * kHTab], g_hb[kHTab * kHTab], g_hs[kHTab], g_hc[kHTab];
+__device__ double g_ha[kHTab * kHTab], g_hb[kHTab * kHTab], g_hs[kHTab], g_hc[kHTab], g_hq[kHTab], g_hr[kHTab];
 
 __global__ void k_htab_init()
 {
@@ -518,6 +519,8 @@ __global__ void k_htab_init()
     if (i < kHTab) {
         g_hs[i] = sqrt(2 * i + 1.0);
         g_hc[i] = i > 0 ? sqrt((2 * i - 1.0) / (2 * i)) : 0.0;
+        g_hq[i] = i / (2 * i + 1.0);
+        g_hr[i] = 1.0 / (2 * i + 1.0);
     }
     if (i >= kHTab * kHTab) return;
     int n = i / kHTab, m = i % kHTab;
@@ -872,6 +875,7 @@ __global__ void __launch_bounds__(kHEvalThreads) k_heval(const int *leaves, Tree
                 hank_dev(p > 1 ? p : 1, z, sc, f, nullptr, T);
             }
             const double r = g.r, ct = g.ct, st = g.st, u = -st;
+            const double isc = 1.0 / sc, ir = 1.0 / r;
             const double2 zi = cdiv(cmk(1, 0), z), e1 = cmk(g.cp, g.sp);
             double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
             double2 em = cmk(1, 0);
@@ -897,14 +901,15 @@ __global__ void __launch_bounds__(kHEvalThreads) k_heval(const int *leaves, Tree
                     if (isloc) {
                         if (n == 0) { fd = cscal(-sc, f[T]); fu = cmk(0, 0); }
                         else {
+                            // j_n' = [n j_{n-1} - (n+1) j_{n+1}] / (2n+1) in the scaled functions
                             const double2 fm = f[(n - 1) * T], fp = f[(n + 1) * T];
-                            const double d1 = n / (2 * n + 1.0), d2 = 1.0 - d1;
-                            fd = csub(cscal(d1 / sc, fm), cscal(d2 * sc, fp));
-                            fu = cscal(1.0 / (2 * n + 1.0), cmul(zk, cadd(cscal(sc, fp), cscal(1.0 / sc, fm))));
+                            const double d1 = __ldg(&g_hq[n]), d2 = 1.0 - d1;
+                            fd = csub(cscal(d1 * isc, fm), cscal(d2 * sc, fp));
+                            fu = cscal(__ldg(&g_hr[n]), cmul(zk, cadd(cscal(sc, fp), cscal(isc, fm))));
                         }
                     } else {
-                        fd = n == 0 ? cscal(-1.0 / sc, f[T]) : csub(cscal(sc, f[(n - 1) * T]), cmul(cscal(n + 1.0, zi), fn));
-                        fu = cscal(1.0 / r, fn);
+                        fd = n == 0 ? cscal(-isc, f[T]) : csub(cscal(sc, f[(n - 1) * T]), cmul(cscal(n + 1.0, zi), fn));
+                        fu = cscal(ir, fn);
                     }
                     fd = cmul(fd, zk);
                     if (m == 0) {
