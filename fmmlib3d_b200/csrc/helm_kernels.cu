@@ -971,7 +971,8 @@ __device__ __forceinline__ void hpair(double dx, double dy, double dz, double2 z
                                       double2 &fz)
 {
     double r2 = dx * dx + dy * dy + dz * dz;
-    double r = sqrt(r2), ri = 1.0 / r, ri2 = ri * ri;
+    // 1/r from one reciprocal square root (within an ulp of 1/sqrt), r = r^2 / r
+    double ri = rsqrt(r2), r = r2 * ri, ri2 = ri * ri;
     double s, c;
     sincos(zk.x * r, &s, &c);
     double ee = zk.y == 0.0 ? ri : exp(-zk.y * r) * ri;
