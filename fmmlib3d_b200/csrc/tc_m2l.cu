@@ -2,8 +2,8 @@
 //
 // The dense per-offset operators T_D (m2l_dense.cu) applied to gathered source
 // multipoles are products of complex matrices.  Here each CTA owns 64 complex
-// rows of the local expansions of a tile of up to 128 target boxes and
-// streams the tile's 189 list-2 slots:
+// rows of the local expansions of a tile of up to NMAX (128, or 256 as a
+// tuning option) target boxes and streams the tile's 189 list-2 slots:
 //   D[r, t] += sum_k A[r, k] B[t, k]
 // with the complex product embedded in real arithmetic:
 //   A rows 0..63   (real parts):      [Re T, -Im T] interleaved per column,
@@ -11,16 +11,19 @@
 //   B (per target): [Re M, Im M] interleaved per coefficient.
 // A and B are rounded to FP32, split into TF32 pairs x = hi + lo (both
 // rounded to nearest, so hi + lo is x to about 2^-24), and
-// D += A_hi B_hi + A_hi B_lo + A_lo B_hi + A_lo B_lo is issued as
-// tcgen05.mma kind::tf32 (M = 128, N = targets, K = 8) by one thread, with D
+// D += A_hi B_hi + A_hi B_lo + A_lo B_hi (+ A_lo B_lo with nprod 4) is issued
+// as tcgen05.mma kind::tf32 (M = 128, N = targets, K = 8) by one thread, with D
 // in TMEM (FP32).
 // Operands are staged in shared memory by all threads (gather of the source
 // multipoles, split, K-major no-swizzle layout) in a ring of S stages; each
-// stage is released by a tcgen05.commit on its mbarrier.  The tensor cores
-// accumulate a group of slots (TMEM columns 0..127); the group's sum is then
-// added by the CUDA cores, with round-to-nearest FP32 additions, into a
-// running sum held in TMEM columns 128..255: long tensor-core accumulations
-// lose accuracy, groups of a few slots keep the FP32 CUDA-core form's error.
+// stage is released by a tcgen05.commit on its mbarrier.  The global loads of
+// a stage are issued two stages ahead (a register ring), and the gather chain
+// of the next slot (colleague, then child box) is loaded while the current
+// slot's stages run.  The tensor cores accumulate a group of slots (TMEM
+// columns 0..NMAX-1); the group's sum is then added by the CUDA cores, with
+// round-to-nearest FP32 additions, into a running sum held in TMEM columns
+// NMAX..2 NMAX-1: long tensor-core accumulations lose accuracy, groups of a
+// few slots keep the FP32 CUDA-core form's error.
 // At the end every warp reads its TMEM lane quarter of the running sum and
 // adds the tile into the FP64 locals.
 // Every wait is bounded: on expiry the kernel records an error, waits (again
