@@ -47,7 +47,9 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
             Laplace, 30% Helmholtz with zk uniform in [1, 20], N log-uniform in
             [1e3, 1e6], iprec in {0, 1, 2}, cube / Plummer / ellipsoid
             geometries), Poisson arrivals at swept rates: p50/p99 latency and
-            points/s per rate (host arrays in and out, copies included).
+            points/s per rate (host arrays in and out, copies included);
+            serving_mixed: the same stream with the Laplace requests of iprec <= 1
+            in the mixed form.
   helmholtz the Helmholtz workload measured in the same run (not the
             headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
             unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
@@ -337,13 +339,15 @@ def run_batched(args, R):
             "tuning": knobs}
 
 
-def run_serving(args):
-    """Swept-rate serving measurement (one warm-up pass over the same requests first)."""
+def run_serving(args, precision=None):
+    """Swept-rate serving measurement (one warm-up pass over the same requests first); precision 1
+    serves the Laplace requests with iprec <= 1 in the mixed form."""
     from fmmlib3d_b200.serving import FMMServer, make_request_stream, run_stream
     reqs = make_request_stream(args.serve_requests, seed=7)
-    srv = FMMServer(slots=4)
+    srv = FMMServer(slots=4, precision=precision)
     out = {"slots": 4, "requests_per_rate": len(reqs), "mean_n": float(np.mean([len(r.source) for r in reqs])),
-           "laplace_fraction": float(np.mean([r.kernel == "laplace" for r in reqs])), "rates": []}
+           "laplace_fraction": float(np.mean([r.kernel == "laplace" for r in reqs])),
+           "precision": "mixed for Laplace iprec <= 1" if precision == 1 else "fp64", "rates": []}
     try:
         run_stream(srv, reqs, float("inf"))  # warm-up: plans, pools
         for rate in [float(x) for x in args.serve_rates.split(",")]:
@@ -935,6 +939,7 @@ def main(argv=None):
     line["plans"] = run_plans(args, R, R.pop("batch_arrays", None))
     if args.serve_requests > 0 and ws == 1:
         line["serving"] = run_serving(args)
+        line["serving_mixed"] = run_serving(args, precision=1)
     if args.helm_n > 0:
         H2 = run_helm(args, R)
         if rank == 0 and ws == 1 and not args.no_cpu and args.helm_cpu_sample > 0:

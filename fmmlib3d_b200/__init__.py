@@ -58,6 +58,8 @@ _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
 _lib.fmm3d_set_m2l_mode.argtypes = [_I]
 _lib.fmm3d_set_precision.argtypes = [_I]
+_lib.fmm3d_set_precision_thread.argtypes = [_I]
+_lib.fmm3d_set_precision_thread.restype = _I
 _lib.fmm3d_set_tensor_m2l.argtypes = [_I]
 _lib.fmm3d_set_tensor_m2l.restype = _I
 _lib.fmm3d_set_overlap.argtypes = [_I]
@@ -477,6 +479,13 @@ def set_m2l_mode(mode):
 def set_precision(mode):
     """0 FP64 throughout (default), 1 mixed FP32 P2P/M2L for iprec <= 1."""
     _lib.fmm3d_set_precision(int(mode))
+
+
+def set_precision_thread(mode):
+    """Arithmetic form for later calls on this host thread only: 0 FP64, 1 mixed (iprec <= 1),
+    -1 follow the process-wide ``set_precision``."""
+    if _lib.fmm3d_set_precision_thread(int(mode)) != 0:
+        raise ValueError("unknown precision mode %r" % (mode,))
 
 
 def set_tensor_m2l(mode):

@@ -105,6 +105,7 @@ struct LapPlan {
 };
 static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
 static int g_precision = 0; // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
+thread_local int g_precision_thread = -1;   // this thread's form (-1: the process-wide one)
 static int g_tc_m2l = 1;    // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
 static int g_tc_group = 1;  // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
 static int g_overlap = 1;   // near field concurrent with the far-field passes
@@ -649,7 +650,8 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.os.pot = S.opot.p; S.os.fx = S.ofx.p; S.os.fy = S.ofy.p; S.os.fz = S.ofz.p;
     S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
-    S.mixed = g_precision == 1 && iprec <= 1 && plan->dense;
+    const int form = g_precision_thread >= 0 ? g_precision_thread : g_precision;
+    S.mixed = form == 1 && iprec <= 1 && plan->dense;
     S.dense = (plan->dense && g_m2l_mode != 1) || S.mixed;
     S.tcm2l = S.mixed && g_tc_m2l > 0;
     // launch shapes: the autotuner's cached setting for this problem, else automatic
@@ -1384,6 +1386,13 @@ int fmm3d_set_timing(int on)
 int fmm3d_set_precision(int mode)
 {
     g_precision = mode;
+    return 0;
+}
+
+int fmm3d_set_precision_thread(int mode)
+{
+    if (mode < -1 || mode > 1) return 1;
+    g_precision_thread = mode;
     return 0;
 }
 

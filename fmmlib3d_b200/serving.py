@@ -10,7 +10,7 @@ thread its own stream), so the admitted requests' kernels, copies and
 workspace allocations overlap on the device.  Every call is independent and
 deterministic, so a request's result is the same alone and in the mix.
 
-    server = FMMServer(slots=4)
+    server = FMMServer(slots=4)       # precision=1: mixed form for Laplace requests with iprec <= 1
     fut = server.submit(Request("helmholtz", source, charge, iprec=1, zk=5.0))
     pot, fld = fut.result().pot, fut.result().fld
     server.close()
@@ -36,6 +36,7 @@ class Request:
     iprec: int = 1
     zk: complex = 0.0
     tag: object = None
+    precision: int = None           # 0 FP64, 1 mixed (Laplace, iprec <= 1); None: the server's
     submitted: float = field(default=0.0, repr=False)
 
 
@@ -70,11 +71,14 @@ def projected_bytes(req):
 
 
 class FMMServer:
-    def __init__(self, slots=4, hbm_budget_bytes=None, device=0):
+    def __init__(self, slots=4, hbm_budget_bytes=None, device=0, precision=None):
+        """precision: arithmetic form of Laplace requests that do not name one (0 FP64, 1 mixed
+        for iprec <= 1; None: the process-wide setting)."""
         import torch
         import fmmlib3d_b200 as F
         self._torch, self._F = torch, F
         self.device = device
+        self.precision = precision
         if hbm_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(device)
             hbm_budget_bytes = int(0.8 * free)
@@ -157,7 +161,13 @@ class FMMServer:
                 ier = F.hfmm3dparttarg_device(req.iprec, req.zk, src, chg, None, None, pot, fld,
                                               stream=stream.cuda_stream)
             else:
-                ier = F.lfmm3dparttarg_device(req.iprec, src, chg, None, None, pot, fld, stream=stream.cuda_stream)
+                form = req.precision if req.precision is not None else self.precision
+                F.set_precision_thread(-1 if form is None else form)
+                try:
+                    ier = F.lfmm3dparttarg_device(req.iprec, src, chg, None, None, pot, fld,
+                                                  stream=stream.cuda_stream)
+                finally:
+                    F.set_precision_thread(-1)
             hp = torch.empty((n, 2), dtype=torch.float64, pin_memory=True)
             hf = torch.empty((n, 6), dtype=torch.float64, pin_memory=True)
             hp.copy_(pot, non_blocking=True)

@@ -177,6 +177,11 @@ int fmm3d_set_m2l_mode(int mode);
  * operators, FP64 for the tree, geometry, recurrences, rotations and the
  * other passes.  iprec >= 2 always runs FP64. */
 int fmm3d_set_precision(int mode);
+/* The same for the calling host thread only: 0 or 1 override the process-wide
+ * setting for later calls made on this thread, -1 (the default) follows it.
+ * Lets a multi-threaded caller (a serving loop) choose the form per request.
+ * Returns 1 for an unknown mode. */
+int fmm3d_set_precision_thread(int mode);
 
 /* M2L of the mixed form (iprec <= 1, nterms <= 16) on the tensor cores:
  * 0 = FP32 CUDA cores, 1 or 2 = tcgen05 kind::tf32 with operands split into

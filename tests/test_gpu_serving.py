@@ -60,3 +60,33 @@ def test_budget_limits_concurrency():
     finally:
         srv.close()
     assert stats["max_ier"] == 0 and srv.max_running == 1
+
+
+def test_precision_per_request():
+    """A server in the mixed form (and requests that override it) gives every request the bits of a
+    single call in that request's form; the process-wide setting is left as it was."""
+    from fmmlib3d_b200.serving import FMMServer, run_stream
+    import fmmlib3d_b200 as F
+    reqs = _requests(10, 5)
+    for i, r in enumerate(reqs):
+        if r.kernel == "laplace" and i % 4 == 1:
+            r.precision = 0
+    srv = FMMServer(slots=4, precision=1)
+    try:
+        stats, res = run_stream(srv, reqs, float("inf"))
+    finally:
+        srv.close()
+    assert stats["max_ier"] == 0
+    for r, a in zip(reqs, res):
+        form = 1 if r.precision is None else r.precision
+        if r.kernel == "laplace":
+            F.set_precision(form)
+            try:
+                ier, pot, fld, _, _ = F.lfmm3dparttarg(r.iprec, r.source, 1, r.charge, 0, None, None, 1, 1)
+            finally:
+                F.set_precision(0)
+        else:
+            ier, pot, fld, _, _ = F.hfmm3dparttarg(r.iprec, r.zk, r.source, 1, r.charge, 0, None, None, 1, 1)
+        assert ier == 0 and np.array_equal(a.pot, pot) and np.array_equal(a.fld, fld), (r.tag, r.kernel, r.iprec)
+    with pytest.raises(ValueError):
+        F.set_precision_thread(2)
