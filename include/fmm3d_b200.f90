@@ -95,5 +95,11 @@ module fmm3d_b200
       integer(c_int), value :: mode
     end function
 
+    ! The same for the calling thread only (-1: follow fmm3d_set_precision).
+    integer(c_int) function fmm3d_set_precision_thread(mode) bind(C, name="fmm3d_set_precision_thread")
+      import :: c_int
+      integer(c_int), value :: mode
+    end function
+
   end interface
 end module fmm3d_b200
