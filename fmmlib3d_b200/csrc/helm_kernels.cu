@@ -800,15 +800,23 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
         k_hform<IR, C, D, CHV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);           \
         FMM_COUNT_LAUNCH();                                                                                   \
     } while (0)
+    // chunks of 8 or 16 sources; 4 at orders whose staging would not fit
+    // (above ~54).  The chunk size does not change the order of any sum.
+#define FMM_HF_FIT(IR, C, D, CHV)                                                                             \
+    do {                                                                                                      \
+        if (sizeof(double) * HFormSmem<CHV, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, CHV);           \
+        else FMM_HF(IR, C, D, 4);                                                                             \
+    } while (0)
     if (irreg) {
-        if (c && d) FMM_HF(true, true, true, 8);
-        else if (c) FMM_HF(true, true, false, 16);
-        else FMM_HF(true, false, true, 8);
+        if (c && d) FMM_HF_FIT(true, true, true, 8);
+        else if (c) FMM_HF_FIT(true, true, false, 16);
+        else FMM_HF_FIT(true, false, true, 8);
     } else {
-        if (c && d) FMM_HF(false, true, true, 8);
-        else if (c) FMM_HF(false, true, false, 16);
-        else FMM_HF(false, false, true, 8);
+        if (c && d) FMM_HF_FIT(false, true, true, 8);
+        else if (c) FMM_HF_FIT(false, true, false, 16);
+        else FMM_HF_FIT(false, false, true, 8);
     }
+#undef FMM_HF_FIT
 #undef FMM_HF
     FMM_LAUNCH_CHECK(st);
 }

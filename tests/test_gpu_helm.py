@@ -25,7 +25,12 @@ from test_gpu_lap import geometry, rel  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9}
+# Accuracy bound per iprec (src/hfmm3dpart.f:159-168).  From iprec 4 on the
+# bound is 1e-12: the oracle's own field error reaches 5.96e-13 at iprec 4 on
+# the clustered case below (nominal .5e-12), and 5 and 6 (direct) ask for
+# more than the rounding floor of the FP64 sums compared.  The gate that
+# matters, no worse than twice the oracle's error, holds at every iprec.
+EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9, 4: 1e-12, 5: 1e-12, 6: 1e-12}
 TOL_ORACLE = 1e-9
 
 
@@ -86,6 +91,19 @@ def test_helmholtz_direct_sum_matches_oracle(F):
 def test_hfmm_parity_charges_dipoles_targets(F, geom, iprec, zk):
     rng = np.random.default_rng(zlib.crc32(('%s%d%s' % (geom, iprec, zk)).encode()))
     n, m = 12000, 4000
+    src = geometry(geom, n, rng)
+    trg = geometry(geom, m, rng) * 1.1
+    q, ds, dv = strengths(rng, n)
+    check_against_oracle(F, iprec, zk, src, trg, q, ds, dv, rng)
+
+
+@pytest.mark.parametrize("geom,iprec,zk,n,m", [("plummer", 4, 1 + 0.1j, 15000, 3000),
+                                               ("plummer", 5, 2.0, 15000, 3000),
+                                               ("cube", 6, 3.0, 3000, 1000), ("cube", -2, 1.0, 15000, 5000)])
+def test_hfmm_parity_remaining_iprec(F, geom, iprec, zk, n, m):
+    """iprec 4 / 5: expansion orders 46 / 59 on a five-level clustered tree;
+    6: every point in the root box; -2: the coarsest tables."""
+    rng = np.random.default_rng(zlib.crc32(('hi%s%d' % (geom, iprec)).encode()))
     src = geometry(geom, n, rng)
     trg = geometry(geom, m, rng) * 1.1
     q, ds, dv = strengths(rng, n)

@@ -20,7 +20,10 @@ import oracle as O  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9}
+# Accuracy bound per iprec (src/lfmm3dpart.f:156-165).  iprec 5 asks for 15
+# digits and 6 is the reference's direct evaluation (one box of all points):
+# their bound is the rounding floor of the FP64 sums compared, 1e-12.
+EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9, 4: .5e-12, 5: 1e-12, 6: 1e-12}
 TOL_ORACLE = 1e-10
 
 
@@ -115,6 +118,29 @@ def test_fmm_parity_charges_dipoles_targets(F, geom, iprec):
     dv = rng.normal(size=(n, 3))
     dv /= np.linalg.norm(dv, axis=1)[:, None]
     check_against_oracle(F, iprec, src, trg, q, ds, dv, rng)
+
+
+@pytest.mark.parametrize("geom,iprec,n,m", [("plummer", 4, 20000, 5000), ("plummer", 5, 20000, 5000),
+                                            ("cube", 6, 3000, 1000)])
+def test_fmm_parity_high_precision(F, geom, iprec, n, m):
+    """iprec 4 and 5: orders 51 and 64 (the evaluation pass stages its arrays in
+    two phases above order 58), leaves of up to 1,200 / 1,400 points, a tree of
+    five levels on the clustered inputs; iprec 6: every point in the root box."""
+    rng = np.random.default_rng(zlib.crc32(('hi%s%d' % (geom, iprec)).encode()))
+    src = geometry(geom, n, rng)
+    trg = geometry(geom, m, rng) * 1.1
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ds = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    dv = rng.normal(size=(n, 3))
+    dv /= np.linalg.norm(dv, axis=1)[:, None]
+    F.set_stats(True)
+    try:
+        check_against_oracle(F, iprec, src, trg, q, ds, dv, rng)
+    finally:
+        F.set_stats(False)
+    st = F.last_stats()
+    assert st["nterms"] == O.l3dterms(O.lap_eps(iprec))
+    assert st["nlev"] >= 2 if iprec < 6 else st["nlev"] == 0
 
 
 @pytest.mark.parametrize("mode", ["charge", "dipole"])
