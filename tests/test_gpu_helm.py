@@ -110,6 +110,38 @@ def test_hfmm_parity_remaining_iprec(F, geom, iprec, zk, n, m):
     check_against_oracle(F, iprec, zk, src, trg, q, ds, dv, rng)
 
 
+def test_hfmm_flags_and_coincident_points(F):
+    """As for Laplace: flags other than 1 are off (src/hfmm3dpart.f:601-617), and a
+    target on top of a source gets a non-finite value (no guard), nothing else."""
+    rng = np.random.default_rng(18)
+    n, m, zk = 3000, 800, 2.0 + 0.1j
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    sentinel = 7.25 + 3.5j
+    pot, pt = np.full(n, sentinel), np.full(m, sentinel)
+    fld, ft = np.zeros((n, 3), complex), np.zeros((m, 3), complex)
+    lib = F.lib()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ier = ctypes.c_int(-1)
+    zkc = np.array([zk], complex)
+    dummy = np.zeros(2, complex)
+    lib.hfmm3dparttarg_(ctypes.byref(ier), I(1), P(zkc), I(n), P(src), I(1), P(q), I(3), P(dummy), P(src), I(0),
+                        P(pot), I(1), P(fld), I(m), P(trg), I(-4), P(pt), I(1), P(ft))
+    assert ier.value == 0
+    assert np.all(pot == sentinel) and np.all(pt == sentinel)
+    _, _, ofld, _, oft = O.hfmm3dparttarg(1, zk, src, q, None, None, trg)
+    assert rel(fld, ofld) < TOL_ORACLE and rel(ft, oft) < TOL_ORACLE
+    trg[5] = src[123]
+    ier, pot, fld, pt, ft = F.hfmm3dparttarg(1, zk, src, 1, q, 0, None, None, 1, 1, trg, 1, 1)
+    _, opot, ofld, opt, oft = O.hfmm3dparttarg(1, zk, src, q, None, None, trg)
+    assert ier == 0 and not np.isfinite(opt[5]) and not np.isfinite(pt[5]) and not np.all(np.isfinite(ft[5]))
+    keep = np.arange(m) != 5
+    assert np.all(np.isfinite(pot)) and np.all(np.isfinite(pt[keep])) and np.all(np.isfinite(ft[keep]))
+    assert rel(pot, opot) < TOL_ORACLE and rel(fld, ofld) < TOL_ORACLE
+    assert rel(pt[keep], opt[keep]) < TOL_ORACLE and rel(ft[keep], oft[keep]) < TOL_ORACLE
+
+
 @pytest.mark.parametrize("mode", ["charge", "dipole"])
 def test_hfmm_parity_source_kinds(F, mode):
     rng = np.random.default_rng(7)

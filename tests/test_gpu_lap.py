@@ -233,6 +233,38 @@ def test_unrequested_outputs_untouched(F):
     assert rel(ft, oft) < TOL_ORACLE
 
 
+def test_flags_other_than_one_are_off_and_coincident_points_are_not_guarded(F):
+    """A flag is on only when it equals 1 (`if (ifpot .eq. 1)`, src/lfmm3dpart.f:
+    634-650); a target on top of a source gets a non-finite value, as in the
+    reference (no guard, src/laprouts3d.f:1270-1272), and no other output moves."""
+    rng = np.random.default_rng(17)
+    n, m = 3000, 800
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    sentinel = 7.25 + 3.5j
+    pot, pt = np.full(n, sentinel), np.full(m, sentinel)
+    fld, ft = np.zeros((n, 3), complex), np.zeros((m, 3), complex)
+    lib = F.lib()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ier = ctypes.c_int(-1)
+    dummy = np.zeros(2, complex)
+    lib.lfmm3dparttarg_(ctypes.byref(ier), I(1), I(n), P(src), I(1), P(q), I(2), P(dummy), P(src), I(-1), P(pot),
+                        I(1), P(fld), I(m), P(trg), I(7), P(pt), I(1), P(ft))
+    assert ier.value == 0
+    assert np.all(pot == sentinel) and np.all(pt == sentinel)
+    _, _, ofld, _, oft = O.lfmm3dparttarg(1, src, q, None, None, trg)
+    assert rel(fld, ofld) < TOL_ORACLE and rel(ft, oft) < TOL_ORACLE
+    trg[5] = src[123]
+    ier, pot, fld, pt, ft = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1, trg, 1, 1)
+    _, opot, ofld, opt, oft = O.lfmm3dparttarg(1, src, q, None, None, trg)
+    assert ier == 0 and not np.isfinite(opt[5]) and not np.isfinite(pt[5]) and not np.all(np.isfinite(ft[5]))
+    keep = np.arange(m) != 5
+    assert np.all(np.isfinite(pot)) and np.all(np.isfinite(pt[keep])) and np.all(np.isfinite(ft[keep]))
+    assert rel(pot, opot) < TOL_ORACLE and rel(fld, ofld) < TOL_ORACLE
+    assert rel(pt[keep], opt[keep]) < TOL_ORACLE and rel(ft[keep], oft[keep]) < TOL_ORACLE
+
+
 def test_repeat_calls_bitwise_identical(F):
     rng = np.random.default_rng(15)
     n = 20000
