@@ -79,6 +79,8 @@ _lib.fmm3d_lfmm3d_plan_destroy.restype = _I
 _lib.fmm3d_lfmm3d_plan_info.argtypes = [_P, _P, _I]
 _lib.fmm3d_lfmm3d_plan_info.restype = _I
 _lib.fmm3d_lfmm3d_plan_getb.argtypes = [_P, _I, _P, _P, _P]
+_lib.fmm3d_d3tstrcrem.argtypes = [_I, _P, _I, _I, _P, _I, _I, _I, _P, ctypes.POINTER(_P)]
+_lib.fmm3d_d3tstrcrem.restype = _I
 _lib.fmm3d_lfmm3d_plan_getb.restype = _I
 _lib.fmm3d_lfmm3d_plan_getl.argtypes = [_P, _I, _I, _P, ctypes.POINTER(_I)]
 _lib.fmm3d_lfmm3d_plan_getl.restype = _I
@@ -368,6 +370,24 @@ class LaplacePlan:
             self.close()
         except Exception:  # noqa: BLE001 -- interpreter shutdown
             pass
+
+
+class OctTree(LaplacePlan):
+    """d3tstrcrem (src/d3tstrcr.f:264-460): the adaptive octree of device tensors
+    ``source`` (N, 3) and ``target`` (M, 3) alone, with the reference's options
+    (``ifempty`` = 1 keeps empty boxes; every box above ``minlevel`` is split;
+    none at ``maxlevel`` or deeper, capped at 21 levels).  Answers ``info``,
+    ``getb`` and ``getl`` like a plan; it has no charges to execute."""
+
+    def __init__(self, source, nbox, target=None, ifempty=0, minlevel=0, maxlevel=100, stream=0):
+        h = _P()
+        m = 0 if target is None else target.shape[0]
+        tp = None if target is None else _P(target.data_ptr())
+        ier = _lib.fmm3d_d3tstrcrem(source.shape[0], _P(source.data_ptr()), int(nbox), m, tp, int(ifempty),
+                                    int(minlevel), int(maxlevel), _P(stream), ctypes.byref(h))
+        if ier != 0:
+            raise RuntimeError("d3tstrcrem failed, ier=%d: %s" % (ier, last_error()))
+        self._h = h
 
 
 def _zk(zk):

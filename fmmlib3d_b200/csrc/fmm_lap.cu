@@ -961,6 +961,47 @@ int fmm3d_lfmm3d_plan_create(int iprec, int nsource, const double *d_source, int
     return 0;
 }
 
+// d3tstrcrem (src/d3tstrcr.f:264-460): the tree alone, for the tree queries
+// (fmm3d_lfmm3d_plan_getb / _getl / _info; _destroy frees it).  Device arrays
+// as for fmm3d_lfmm3d_plan_create.  ier 128 when nsource < 1 (as the
+// reference); levels are capped at 21.  ier 4 for nbox < 1, and for box counts
+// beyond 32-bit indexing: empty boxes kept above minlevel make 8^minlevel
+// boxes (minlevel <= 7 then), and every level down to minlevel holds up to
+// one box per point.
+int fmm3d_d3tstrcrem(int nsource, const double *d_source, int nbox, int ntarget, const double *d_target,
+                     int ifempty, int minlevel, int maxlevel, void *stream, void **tree)
+{
+    if (!tree) return 1;
+    *tree = nullptr;
+    if (nsource < 1) return 128;
+    const int lmin = std::max(0, std::min(minlevel, maxlevel));
+    if (nbox < 1 || ntarget < 0) return 4;
+    if (ifempty == 1 && lmin > 7) return 4;
+    if (((long)nsource + ntarget) * (std::min(lmin, kMaxLevel) + 1) > (1L << 30)) return 4;
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    g_launch_count = 0;
+    keep_pool_memory();
+    auto *E = new LapPlanExec;
+    E->S.ns = nsource;
+    E->S.nt = ntarget;
+    TreeOptions opt;
+    opt.ifempty = ifempty;
+    opt.minlevel = minlevel;
+    opt.maxlevel = maxlevel;
+    Status st;
+    build_tree(E->S.T, d_source, nsource, d_target, ntarget, nbox, s, st, opt);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) {
+        g_ti.err = cudaGetErrorString(st.err);
+        delete E;
+        return 16;
+    }
+    E->made_on = s;
+    E->used.push_back(s);
+    *tree = E;
+    return 0;
+}
+
 int fmm3d_lfmm3d_plan_create_batched(int iprec, int ninst, const int *src_offsets, const double *d_source,
                                      int ifcharge, int ifdipole, int ifpot, int iffld, const int *trg_offsets,
                                      const double *d_target, int ifpottarg, int iffldtarg, void *stream, void **plan)
@@ -997,6 +1038,7 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
 {
     if (!plan) return 1;
     auto *E = (LapPlanExec *)plan;
+    if (!E->S.plan) return 4;   // a tree from fmm3d_d3tstrcrem: no FMM on it
     std::lock_guard<std::mutex> lk(E->mu);
     cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
     if (std::find(E->used.begin(), E->used.end(), s) == E->used.end()) {
@@ -1060,6 +1102,7 @@ int fmm3d_lfmm3d_plan_set_tuning(void *plan, const int *knobs, int n)
 {
     if (!plan || !knobs || n < kNumKnobs) return 1;
     auto *E = (LapPlanExec *)plan;
+    if (!E->S.plan) return 4;   // a tree from fmm3d_d3tstrcrem: no FMM on it
     std::lock_guard<std::mutex> lk(E->mu);
     for (int i = 0; i < kNumKnobs; i++)
         if (knobs[i] < 0) return 2;
@@ -1083,6 +1126,7 @@ int fmm3d_lfmm3d_plan_get_tuning(void *plan, int *out, int n)
 {
     if (!plan || !out || n < kNumKnobs + 2) return 1;
     auto *E = (LapPlanExec *)plan;
+    if (!E->S.plan) return 4;   // a tree from fmm3d_d3tstrcrem: no FMM on it
     std::lock_guard<std::mutex> lk(E->mu);
     lap_effective_knobs(E->S, out);
     return 0;
@@ -1092,6 +1136,7 @@ int fmm3d_lfmm3d_plan_signature(void *plan, char *buf, int n)
 {
     if (!plan) return -1;
     auto *E = (LapPlanExec *)plan;
+    if (!E->S.plan) return 4;   // a tree from fmm3d_d3tstrcrem: no FMM on it
     std::lock_guard<std::mutex> lk(E->mu);
     const std::string &sg = E->S.signature;
     if (!buf || n <= 0) return (int)sg.size() + 1;
@@ -1144,8 +1189,11 @@ int fmm3d_lfmm3d_plan_getb(void *plan, int ibox, int *box, double *center, doubl
         box[14] = E->nsrc[b];
         box[15] = E->trg0[b] + 1;
         box[16] = E->ntrg[b];
-        box[17] = E->nsrc[b] == 0 ? 0 : (nk == 0 ? 1 : 2);
-        box[18] = E->ntrg[b] == 0 ? 0 : (nk == 0 ? 1 : 2);
+        // type 2 only for a box split because it held more than nbox points
+        // (a box split to reach minlevel stays 1, src/d3tstrcr.f:1490-1498)
+        const bool over = nk > 0 && (E->nsrc[b] > E->S.T.nbox || E->ntrg[b] > E->S.T.nbox);
+        box[17] = E->nsrc[b] == 0 ? 0 : (over ? 2 : 1);
+        box[18] = E->ntrg[b] == 0 ? 0 : (over ? 2 : 1);
         box[19] = 0;
     }
     const double side = (E->binst.empty() ? E->S.T.size : E->geom[4L * E->binst[b] + 3]) / (double)(1L << E->level[b]);

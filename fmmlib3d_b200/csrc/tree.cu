@@ -177,9 +177,9 @@ __device__ int lower_digit(const uint64_t *keys, int lo, int hi, int child_level
 // searches over the box's sorted range, done in parallel.
 constexpr int kSplitLanes = 16;
 
-__global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, const int *nsrc, const int *trg0,
-                        const int *ntrg, const uint64_t *ksrc, const uint64_t *ktrg, int *nkids, int *cs0,
-                        int *cns, int *ct0, int *cnt)
+__global__ void k_split(int b0, int nb, int level, int nbox, TreeOptions opt, const int *src0, const int *nsrc,
+                        const int *trg0, const int *ntrg, const uint64_t *ksrc, const uint64_t *ktrg, int *nkids,
+                        int *cs0, int *cns, int *ct0, int *cnt)
 {
     __shared__ int bound[128 / kSplitLanes][16];
     const int g = threadIdx.x / kSplitLanes, j = threadIdx.x % kSplitLanes;
@@ -190,7 +190,7 @@ __global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, co
     if (live) {
         const int b = b0 + t;
         s0 = src0[b]; ns = nsrc[b]; q0 = trg0[b]; nq = ntrg[b];
-        split = level < kMaxLevel && (ns > nbox || nq > nbox);
+        split = level < opt.maxlevel && (ns > nbox || nq > nbox || level < opt.minlevel);
         const int cl = level + 1;
         if (split && j >= 1 && j <= 7) bound[g][j] = lower_digit(ksrc, s0, s0 + ns, cl, j);
         if (split && j >= 9 && j <= 15) bound[g][j] = lower_digit(ktrg, q0, q0 + nq, cl, j - 8);
@@ -211,14 +211,14 @@ __global__ void k_split(int b0, int nb, int level, int nbox, const int *src0, co
             cns[8 * t + d] = sb[d + 1] - sb[d];
             ct0[8 * t + d] = tb[d];
             cnt[8 * t + d] = tb[d + 1] - tb[d];
-            k += (sb[d + 1] > sb[d]) || (tb[d + 1] > tb[d]);
+            k += opt.ifempty == 1 || (sb[d + 1] > sb[d]) || (tb[d + 1] > tb[d]);
         }
     }
     nkids[t] = k;
 }
 
-__global__ void k_make_children(int b0, int nb, int level, int next0, const int *kbase, const int *nkids,
-                                const int *cs0, const int *cns, const int *ct0, const int *cnt,
+__global__ void k_make_children(int b0, int nb, int level, int next0, int keep_empty, const int *kbase,
+                                const int *nkids, const int *cs0, const int *cns, const int *ct0, const int *cnt,
                                 const double *geom_all, int *ijk, int *lev, int *par, int *oct, int *nch,
                                 int *child, int *src0, int *nsrc, int *trg0, int *ntrg, double *center, int *binst)
 {
@@ -234,7 +234,7 @@ __global__ void k_make_children(int b0, int nb, int level, int next0, const int 
     double side = size / (double)(1 << (level + 1)), side2 = side / 2;
     for (int d = 0; d < 8; d++) {
         int ns = cns[8 * t + d], nq = cnt[8 * t + d];
-        if (ns == 0 && nq == 0) continue;
+        if (ns == 0 && nq == 0 && !keep_empty) continue;
         int c[3] = {2 * ijk[3 * b] + (d & 1), 2 * ijk[3 * b + 1] + ((d >> 1) & 1), 2 * ijk[3 * b + 2] + ((d >> 2) & 1)};
         for (int e = 0; e < 3; e++) {
             ijk[3L * id + e] = c[e];
@@ -480,15 +480,20 @@ void instance_major(DBuf<uint64_t> &keys, DBuf<int> &perm, const DBuf<int> &pins
 }  // namespace
 
 void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
-                Status &st)
+                Status &st, const TreeOptions &opt)
 {
     std::vector<int> so = {0, n}, to = {0, m};
-    build_forest(T, d_src, so, d_trg, to, nbox, s, st);
+    build_forest(T, d_src, so, d_trg, to, nbox, s, st, opt);
 }
 
 void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, const double *d_trg,
-                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st)
+                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st, const TreeOptions &opt_in)
 {
+    TreeOptions opt = opt_in;
+    opt.ifempty = opt.ifempty == 1;
+    opt.minlevel = std::max(0, std::min(opt.minlevel, kMaxLevel));
+    opt.maxlevel = std::max(0, std::min(opt.maxlevel, kMaxLevel));
+    T.nbox = nbox;
     const int ninst = (int)so.size() - 1;
     const int n = so[ninst], m = to[ninst];
     T.n = n;
@@ -577,15 +582,15 @@ void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, cons
         if (!nk.alloc(nb, s, st) || !kb.alloc(nb, s, st) || !cs0.alloc(8L * nb, s, st) ||
             !cns.alloc(8L * nb, s, st) || !ct0.alloc(8L * nb, s, st) || !cnt.alloc(8L * nb, s, st))
             return;
-        k_split<<<div_up(nb, 128 / kSplitLanes), 128, 0, s>>>(b0, nb, level, nbox, T.src0.p, T.nsrc.p, T.trg0.p,
-                                                               T.ntrg.p, ks.p, kt.p, nk.p, cs0.p, cns.p, ct0.p,
-                                                               cnt.p); FMM_COUNT_LAUNCH();
+        k_split<<<div_up(nb, 128 / kSplitLanes), 128, 0, s>>>(b0, nb, level, nbox, opt, T.src0.p, T.nsrc.p,
+                                                               T.trg0.p, T.ntrg.p, ks.p, kt.p, nk.p, cs0.p, cns.p,
+                                                               ct0.p, cnt.p); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         int total = 0;
         scan_exclusive_int(nk.p, kb.p, nb, s, st, &total);
         if (!st.ok()) return;
         if (total > 0 && !ensure(nboxes + total, nboxes)) return;
-        k_make_children<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nboxes, kb.p, nk.p, cs0.p, cns.p, ct0.p,
+        k_make_children<<<div_up(nb, 128), 128, 0, s>>>(b0, nb, level, nboxes, opt.ifempty, kb.p, nk.p, cs0.p, cns.p, ct0.p,
                                                          cnt.p, geom.p, T.ijk.p, T.level.p, T.parent.p,
                                                          T.octant.p, T.nchild.p, T.child.p, T.src0.p, T.nsrc.p,
                                                          T.trg0.p, T.ntrg.p, T.center.p, T.binst.p); FMM_COUNT_LAUNCH();

@@ -35,11 +35,21 @@ struct Tree {
     DBuf<int> grouped;                       // box ids
     std::vector<int> group_start;            // host, (nlev+1)*8 + 1 entries
     int cap = 0;
+    int nbox = 0;                            // refinement threshold the tree was built with
+};
+
+// Refinement options of d3tstrcrem (src/d3tstrcr.f:264-460; applied in
+// d3tallbem, :1450-1451, 1490-1498, 1529-1530): a box splits while it holds more than nbox sources
+// or targets or lies above minlevel, never at or below maxlevel (capped at
+// kMaxLevel here), and with ifempty = 1 its empty children are kept.  The
+// defaults are those d3tstrcr uses.
+struct TreeOptions {
+    int ifempty = 0, minlevel = 0, maxlevel = kMaxLevel;
 };
 
 // Builds the tree for device arrays src (n x 3, AoS) and trg (m x 3).
 void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m, int nbox, cudaStream_t s,
-                Status &st);
+                Status &st, const TreeOptions &opt = TreeOptions());
 
 // A forest of independent trees, one per instance: instance i owns sources
 // so[i]..so[i+1]-1 and targets to[i]..to[i+1]-1 of the concatenated arrays
@@ -47,7 +57,8 @@ void build_tree(Tree &T, const double *d_src, int n, const double *d_trg, int m,
 // refinement rule; points are sorted instance-major, boxes of one level of all
 // instances are contiguous, and lists never cross instances.
 void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, const double *d_trg,
-                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st);
+                  const std::vector<int> &to, int nbox, cudaStream_t s, Status &st,
+                  const TreeOptions &opt = TreeOptions());
 
 __host__ __device__ __forceinline__ int coll_slot(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
 

@@ -241,12 +241,24 @@ int fmm3d_lfmm3d_plan_destroy(void *plan);
 int fmm3d_lfmm3d_plan_info(void *plan, double *out, int n);
 /* d3tgetb: box(20) (level; i, j, k; parent; children; first source (1-based in tree
  * order), count; first target, count; source and target type 0 empty / 1 leaf /
- * 2 subdivided; 0), centre(3) and corners(3,8) of box ibox (1-based); ier 2 for a
- * bad ibox. */
+ * 2 subdivided for holding more than nbox points; 0), centre(3) and corners(3,8)
+ * of box ibox (1-based); ier 2 for a bad ibox. */
 int fmm3d_lfmm3d_plan_getb(void *plan, int ibox, int *box, double *center, double *corners);
 /* d3tgetl: list itype (1..5) of box ibox as 1-based box numbers; ier 4 when empty,
  * 2 for a bad ibox or itype; list = NULL returns only the length in *nlist. */
 int fmm3d_lfmm3d_plan_getl(void *plan, int ibox, int itype, int *list, int *nlist);
+/* d3tstrcrem (src/d3tstrcr.f:264-460): the adaptive octree of device arrays
+ * d_source (nsource x 3) and d_target (ntarget x 3) alone, with the reference's
+ * refinement options: a box splits while it holds more than nbox sources or
+ * targets or its level is below minlevel, never at maxlevel or deeper (capped at
+ * 21 levels), and ifempty = 1 keeps empty children.  The handle answers
+ * fmm3d_lfmm3d_plan_info / _getb / _getl (box types: 2 only for a box split for
+ * its point count) and is freed by fmm3d_lfmm3d_plan_destroy; _execute and the
+ * tuning calls return 4 on it.  ier 128 when nsource < 1 (as the reference); 4
+ * for nbox < 1, for ifempty = 1 with minlevel above 7 (8^minlevel boxes), and
+ * when (nsource + ntarget) x (minlevel + 1) exceeds 2^30. */
+int fmm3d_d3tstrcrem(int nsource, const double *d_source, int nbox, int ntarget, const double *d_target,
+                     int ifempty, int minlevel, int maxlevel, void *stream, void **tree);
 
 /* ---- Launch-shape tuning (no counterpart in the reference, whose only
  * tuning input is iprec).  Five knobs, 0 = automatic:

@@ -233,9 +233,14 @@ static void tree_grow(otree *t, int need)
     t->cap = nc;
 }
 
-/* d3tallbem (src/d3tstrcr.f:1242-1583) with ifempty=0, minlevel=0,
- * maxlevel=100 as set by d3tstrcr (src/d3tstrcr.f:181-182).              */
-static void build_boxes(otree *t, const double *z, int n, const double *zt, int nt, int nbox)
+/* d3tallbem (src/d3tstrcr.f:1242-1583): a box splits unless it holds at most
+ * nbox sources and nbox targets and lies at minlevel or below (:1490-1491);
+ * only a box over nbox is marked subdivided (:1495-1498); levels stop at
+ * min(198, maxlevel) (:1450-1451); empty children are kept when ifempty = 1
+ * (:1529-1530).  d3tstrcr uses ifempty=0, minlevel=0, maxlevel=100
+ * (src/d3tstrcr.f:181-182).                                               */
+static void build_boxes_em(otree *t, const double *z, int n, const double *zt, int nt, int nbox, int ifempty,
+                           int minlevel, int maxlevel)
 {
     double xmin = z[0], xmax = z[0], ymin = z[1], ymax = z[1], zmin = z[2], zmax = z[2];
     for (int i = 0; i < n; i++) {
@@ -279,7 +284,7 @@ static void build_boxes(otree *t, const double *z, int n, const double *zt, int 
     int *work = malloc(sizeof(int) * (size_t)((n > nt ? n : nt) + 1));
     t->laddr[0] = 0; t->laddr[1] = 1;
     int nboxes = 1, nlev = 0;
-    int maxlev = 100;
+    int maxlev = maxlevel < 198 ? maxlevel : 198;
     for (int level = 0; level < maxlev; level++) {
         int d0 = t->laddr[2 * level], d1 = d0 + t->laddr[2 * level + 1];
         t->laddr[2 * (level + 1)] = nboxes;
@@ -287,9 +292,11 @@ static void build_boxes(otree *t, const double *z, int n, const double *zt, int 
         for (int dad = d0; dad < d1; dad++) {
             int *bd = t->box + 20 * (size_t)dad;
             int np = bd[B_NSRC], ntp = bd[B_NTRG];
-            if (np <= nbox && ntp <= nbox) continue;
-            if (bd[B_STYPE] == 1) bd[B_STYPE] = 2;
-            if (bd[B_TTYPE] == 1) bd[B_TTYPE] = 2;
+            if (np <= nbox && ntp <= nbox && level >= minlevel) continue;
+            if (np > nbox || ntp > nbox) {
+                if (bd[B_STYPE] == 1) bd[B_STYPE] = 2;
+                if (bd[B_TTYPE] == 1) bd[B_TTYPE] = 2;
+            }
             double c[3];
             d3tcentf(t->center0, t->size, level, bd[B_I], bd[B_J], bd[B_K], c);
             int is[8], ns[8], ist[8], nst[8];
@@ -299,7 +306,7 @@ static void build_boxes(otree *t, const double *z, int n, const double *zt, int 
             int ii = bd[B_I], jj = bd[B_J], kk = bd[B_K];
             int slot = 0;
             for (int d = 0; d < 8; d++) {
-                if (ns[d] == 0 && nst[d] == 0) continue;
+                if (ns[d] == 0 && nst[d] == 0 && ifempty != 1) continue;
                 tree_grow(t, nboxes + 1);
                 bd = t->box + 20 * (size_t)dad;
                 int *bs = t->box + 20 * (size_t)nboxes;
@@ -335,6 +342,11 @@ static void build_boxes(otree *t, const double *z, int n, const double *zt, int 
         t->center[3 * i + 1] = y00 + (bi[B_J] - 1) * side + side2;
         t->center[3 * i + 2] = z00 + (bi[B_K] - 1) * side + side2;
     }
+}
+
+static void build_boxes(otree *t, const double *z, int n, const double *zt, int nt, int nbox)
+{
+    build_boxes_em(t, z, n, zt, nt, nbox, 0, 0, 100);
 }
 
 /* d3tifint (src/d3tstrcr.f:1075-1172): do two boxes intersect or touch,
@@ -460,6 +472,16 @@ void *oracle_tree_build(int n, const double *z, int nt, const double *zt, int nb
 {
     otree *t = calloc(1, sizeof(otree));
     build_boxes(t, z, n, zt, nt, nbox);
+    build_lists(t);
+    return t;
+}
+
+/* d3tstrcrem (src/d3tstrcr.f:264-460): the same tree with its refinement options. */
+void *oracle_tree_build_em(int n, const double *z, int nt, const double *zt, int nbox, int ifempty, int minlevel,
+                           int maxlevel)
+{
+    otree *t = calloc(1, sizeof(otree));
+    build_boxes_em(t, z, n, zt, nt, nbox, ifempty, minlevel, maxlevel);
     build_lists(t);
     return t;
 }

@@ -40,6 +40,8 @@ def lib():
         _lib.oracle_lap_nbox.argtypes = [c_int, c_int, c_int]
         _lib.oracle_tree_build.restype = P
         _lib.oracle_tree_build.argtypes = [c_int, P, c_int, P, c_int]
+        _lib.oracle_tree_build_em.restype = P
+        _lib.oracle_tree_build_em.argtypes = [c_int, P, c_int, P, c_int, c_int, c_int, c_int]
         for f in ("oracle_tree_nboxes", "oracle_tree_nlev"):
             getattr(_lib, f).restype = c_int
             getattr(_lib, f).argtypes = [P]
@@ -156,12 +158,14 @@ def lfmm3dparttarg(iprec, source, charge=None, dipstr=None, dipvec=None, target=
 class Tree:
     """The oracle's octree (d3tstrcr semantics) exported as numpy arrays."""
 
-    def __init__(self, source, target, nbox):
+    def __init__(self, source, target, nbox, ifempty=0, minlevel=0, maxlevel=100):
+        """ifempty / minlevel / maxlevel: the options of d3tstrcrem (the defaults are d3tstrcr's)."""
         L = lib()
         src = _f64(source, (0, 3))
         trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
         n, m = src.shape[0], trg.shape[0]
-        h = L.oracle_tree_build(c_int(n), _p(src), c_int(m), _p(trg if m else np.zeros((1, 3))), c_int(nbox))
+        h = L.oracle_tree_build_em(c_int(n), _p(src), c_int(m), _p(trg if m else np.zeros((1, 3))), c_int(nbox),
+                                   c_int(ifempty), c_int(minlevel), c_int(maxlevel))
         try:
             nb = L.oracle_tree_nboxes(h)
             self.nboxes = nb

@@ -94,16 +94,10 @@ def test_plan_graph_follows_new_pointers_and_charges(F):
     plan.close()
 
 
-def test_plan_tree_queries_match_oracle(F):
-    import torch
-    n, m = 6000, 2000
-    rng = np.random.default_rng(21)
-    src = geometry("plummer", n, rng)
-    trg = geometry("plummer", m, rng) * 0.9
-    dev = torch.device("cuda", 0)
-    plan = F.LaplacePlan(1, torch.from_numpy(src).to(dev), 1, 0, 1, 1, torch.from_numpy(trg).to(dev), 1, 1)
+def compare_tree(plan, T):
+    """The plan's tree (getb / getl) equals the oracle tree T: the same boxes by
+    (level, i, j, k), counts, types, parents, children and lists 1-5 as sets."""
     info = plan.info()
-    T = O.Tree(src, trg, O.lap_nbox(1, n, m))
     assert info["nboxes"] == T.nboxes and info["nlev"] == T.nlev
     key = lambda lev, i, j, k: (int(lev), int(i), int(j), int(k))
     okey = {key(*T.box[b, 0:4]): b for b in range(T.nboxes)}
@@ -133,6 +127,17 @@ def test_plan_tree_queries_match_oracle(F):
             assert {to_o[c] for c in lst} == set(T.list_of(ty, to_o[ib]).tolist()), (ib, ty)
     assert plan.getb(0)[0] == 2 and plan.getb(info["nboxes"] + 1)[0] == 2
     assert plan.getl(1, 6)[0] == 2
+
+
+def test_plan_tree_queries_match_oracle(F):
+    import torch
+    n, m = 6000, 2000
+    rng = np.random.default_rng(21)
+    src = geometry("plummer", n, rng)
+    trg = geometry("plummer", m, rng) * 0.9
+    dev = torch.device("cuda", 0)
+    plan = F.LaplacePlan(1, torch.from_numpy(src).to(dev), 1, 0, 1, 1, torch.from_numpy(trg).to(dev), 1, 1)
+    compare_tree(plan, O.Tree(src, trg, O.lap_nbox(1, n, m)))
     plan.close()
 
 
@@ -179,3 +184,22 @@ def test_overlapped_and_serial_passes_agree_bitwise(F, precision):
         F.set_precision(0)
     for x, y in zip(a, b):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("ifempty,minlevel,maxlevel", [(0, 0, 100), (1, 0, 100), (0, 3, 100), (1, 2, 4),
+                                                       (0, 0, 2)])
+def test_d3tstrcrem_matches_oracle(F, ifempty, minlevel, maxlevel):
+    """d3tstrcrem (src/d3tstrcr.f:264): empty boxes kept or dropped, a minimum
+    and a maximum level, on clustered sources and targets."""
+    import torch
+    rng = np.random.default_rng(3)
+    src = geometry("plummer", 3000, rng)
+    trg = geometry("plummer", 1000, rng) * 0.9
+    dev = torch.device("cuda", 0)
+    tree = F.OctTree(torch.from_numpy(src).to(dev), 40, torch.from_numpy(trg).to(dev), ifempty, minlevel,
+                     maxlevel)
+    compare_tree(tree, O.Tree(src, trg, 40, ifempty, minlevel, maxlevel))
+    assert tree.execute() == 4
+    tree.close()
+    with pytest.raises(RuntimeError):
+        F.OctTree(torch.from_numpy(src).to(dev)[:0], 40)
