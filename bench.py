@@ -13,8 +13,9 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
   value     points/s = (N + M) * steps / device time of the mixed form, inputs
             resident in HBM (fmm3d_lfmm3dparttarg_device), max over ranks.
   e2e       the same metric through the Fortran C ABI (lfmm3dparttarg_) with
-            pinned host arrays: H2D of inputs and D2H of outputs inside the
-            timed region.
+            host arrays: H2D of inputs and D2H of outputs inside the timed
+            region; pageable numpy arrays (what a Fortran caller passes) as
+            the value, pinned arrays beside it.
   roofline  the dominant pass of the step and (roofline.passes) P2P and M2L,
             from the library's per-pass CUDA events of one extra step with the
             passes serialised, against GEMM rates measured in the same run
@@ -24,9 +25,15 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
   errors    relative L2 error vs the FP64 direct sum at 1,000 seeded sources
             (self excluded) and 1,000 seeded targets, per output.
   cpu_baseline  the C restatement of the reference (oracle/, OpenMP, all host
-            cores) on a bounded sample (N = M = 500,000 of the same
-            distribution); the Fortran reference cannot be compiled (no
-            Fortran compiler on either machine).
+            cores): one call on the whole workload, with the same inputs; the
+            Fortran reference cannot be compiled (no Fortran compiler on
+            either machine).
+  parity    the oracle's FMM on each workload's own inputs (the headline
+            cube, the 100k sphere, the Helmholtz sphere) at the same seeded
+            evaluation points as the errors: per output the GPU's FP64 form
+            against the oracle's FMM, the oracle's error against its own FP64
+            direct sum, the GPU forms' errors, and their ratio to the
+            oracle's (the acceptance gate: at most 2).
   laplace_sphere  the CPU-runnable Laplace workload measured in the same run:
             lfmm3dpartself on 100,000 sources on the unit sphere (seed 1),
             charges only, iprec = 1, FP64, with the CPU restatement timed on
@@ -53,12 +60,13 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
   helmholtz the Helmholtz workload measured in the same run (not the
             headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
             unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
-            FP64, with its errors, per-pass times and a CPU sample of the
-            restatement (100,000 sources).
+            FP64, with its errors, per-pass times and the restatement's time
+            on the same inputs.
 
 Multi-GPU: an FMM call does not shard; `--gpus N` runs N independent replicas
 (one per rank, scaling "weak"), timed as the max over ranks.
-`--impl reference` times the CPU restatement on the host cores (rank 0 only).
+`--impl reference` times the CPU restatement on the host cores (rank 0 only), one call on the
+whole headline workload per step.
 `--autotune PATH` tunes the Laplace workloads' launch shapes (fmmlib3d_b200.autotune) into the
 JSON cache PATH and exits; every measured workload reports the knobs it ran with ("tuning").
 """
@@ -93,7 +101,8 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n", type=int, default=2_000_000, help="sources (= targets)")
     ap.add_argument("--iprec", type=int, default=1)
-    ap.add_argument("--cpu-sample", type=int, default=500_000, help="sources (= targets) of the CPU sample")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="sources (= targets) of the reference arm's steps (0: the workload's own --n)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-samples", type=int, default=1000)
@@ -101,7 +110,8 @@ def parse_args(argv=None):
     ap.add_argument("--tensor-m2l", type=int, default=1,
                     help="mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (tcgen05 split TF32)")
     ap.add_argument("--helm-n", type=int, default=1_000_000, help="sources of the Helmholtz workload (0: skip)")
-    ap.add_argument("--helm-cpu-sample", type=int, default=100_000)
+    ap.add_argument("--helm-cpu-sample", type=int, default=1_000_000,
+                    help="sources of the Helmholtz oracle call (parity and CPU baseline; capped at --helm-n)")
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched workload (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests per serving rate (0: skip)")
     ap.add_argument("--serve-rates", default="10,40,inf", help="Poisson arrival rates (requests/s)")
@@ -186,12 +196,18 @@ def run_laplace_sphere(args, R, n=100_000):
            "errors": {"pot": float("%.3e" % float(torch.linalg.norm(d_pot[it.long()] - dp) / torch.linalg.norm(dp))),
                       "fld": float("%.3e" % float(torch.linalg.norm(d_fld[it.long()] - df) / torch.linalg.norm(df)))}}
     if R["rank"] == 0 and not args.no_cpu:
-        import oracle
-        t0 = time.perf_counter()
-        oracle.lfmm3dparttarg(1, src, q[:, 0] + 1j * q[:, 1])
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
-                               "kind": "port", "sample": "the whole workload, one call (%.2f s)" % dt}
+        gv = {"pot": d_pot[it.long()].cpu().numpy(), "fld": d_fld[it.long()].cpu().numpy()}
+        gd = {"pot": dp.cpu().numpy(), "fld": df.cpu().numpy()}
+
+        def cpu_job(line):
+            dt, rep = oracle_laplace_parity(1, src, q, None, None, None, si, None, {"fp64": gv}, gd)
+            rep.update(points="%d seeded sources (self excluded)" % k, inputs="the sphere workload's own inputs",
+                       oracle_call_s=round(dt, 3))
+            line.setdefault("parity", {})["laplace_sphere"] = rep
+            out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
+                                   "kind": "port", "sample": "the whole workload, one call (%.2f s)" % dt}
+
+        R.setdefault("cpu_jobs", []).append(cpu_job)
     return out
 
 
@@ -363,7 +379,7 @@ def run_serving(args, precision=None):
 def cpu_helm_sample(n):
     """One hfmm3dpartself restatement call on the sphere workload with n sources; returns seconds."""
     import oracle
-    src, q = helm_inputs(n, seed=5)
+    src, q = helm_inputs(n, seed=3)
     t0 = time.perf_counter()
     ier = oracle.hfmm3dparttarg(HELM_IPREC, HELM_ZK, src, q[:, 0] + 1j * q[:, 1])[0]
     t1 = time.perf_counter()
@@ -404,12 +420,13 @@ class ClockSampler:
         self.proc = None
         self.interval_ms = interval_ms
         self.t0 = None
-        self.path = os.path.join(HERE, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="fmm3d_clocks_gpu%d_" % self.gpu, suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
@@ -442,6 +459,10 @@ class ClockSampler:
                 rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not rows:
             return None
         inside = [r for r in rows if self.t0 is None or self.t0 <= r[0] <= t1]
@@ -477,7 +498,7 @@ def measured_peak(torch, dev, dtype, tf32=False):
     return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def cpu_fmm_sample(n, iprec, seed=11):
+def cpu_fmm_sample(n, iprec, seed=2):
     """One run of the CPU restatement (oracle/) on n sources + n targets; returns (seconds, points)."""
     import oracle
     src, q, dq, dv, trg = make_inputs(n, n, seed)
@@ -494,6 +515,88 @@ def cpu_threads():
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def sample_indices(n, m, k, seed=99):
+    """The seeded evaluation points of the error and parity checks: k sources and k targets."""
+    rng = np.random.default_rng(seed)
+    si = np.sort(rng.choice(n, min(k, n), replace=False)).astype(np.int32)
+    ti = np.sort(rng.choice(m, min(k, m), replace=False)).astype(np.int32) if m else np.zeros(0, np.int32)
+    return si, ti
+
+
+def _as_pairs(z, width):
+    """complex (k,) or (k,3) -> float64 (k, width) in the library's interleaved layout."""
+    return np.ascontiguousarray(z).view(np.float64).reshape(len(z), width)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(float(np.linalg.norm(b)), 1e-300))
+
+
+def parity_report(oracle_vals, direct_vals, gpu_forms, gpu_direct=None, gate=2.0):
+    """Per output: the GPU's FP64 form against the oracle's FMM on the same points, each error
+    against the oracle's FP64 direct sum, and the GPU errors divided by the oracle's (the
+    acceptance criterion: at most `gate`).  gpu_forms maps a form name to its sampled outputs."""
+    out = {}
+    ok = True
+    for key in oracle_vals:
+        o, d = oracle_vals[key], direct_vals[key]
+        e_or = _rel(o, d)
+        row = {"oracle_err": float("%.3e" % e_or)}
+        for form, vals in gpu_forms.items():
+            e = _rel(vals[key], d)
+            row["gpu_%s_err" % form] = float("%.3e" % e)
+            row["%s_over_oracle" % form] = round(e / max(e_or, 1e-300), 3)
+            ok = ok and e <= gate * e_or
+            if form == "fp64":
+                row["gpu_fp64_vs_oracle"] = float("%.3e" % _rel(vals[key], o))
+        if gpu_direct is not None:
+            row["gpu_direct_vs_oracle_direct"] = float("%.3e" % _rel(gpu_direct[key], d))
+        out[key] = row
+    out["gate"] = "GPU error <= %g x the oracle's, per output" % gate
+    out["pass"] = bool(ok)
+    return out
+
+
+def oracle_laplace_parity(iprec, src, q, dq, dv, trg, si, ti, gpu_forms, gpu_direct=None):
+    """The oracle's FMM (the C restatement of lfmm3dparttarg, OpenMP over all host cores) on the
+    whole workload, timed, and its FP64 direct sum at the sampled points; returns (seconds, report)."""
+    import oracle
+    c = lambda a: None if a is None else a[:, 0] + 1j * a[:, 1]
+    t0 = time.perf_counter()
+    ier, pot, fld, pt, ft = oracle.lfmm3dparttarg(iprec, src, c(q), c(dq), dv, trg)
+    dt = time.perf_counter() - t0
+    if ier != 0:
+        raise RuntimeError("oracle ier=%d" % ier)
+    ov = {"pot": _as_pairs(pot[si], 2), "fld": _as_pairs(fld[si], 6)}
+    dp, df = oracle.direct_at(src, src[si], si, c(q), c(dq), dv)
+    dv_ = {"pot": _as_pairs(dp, 2), "fld": _as_pairs(df, 6)}
+    if trg is not None and len(ti):
+        ov.update(pottarg=_as_pairs(pt[ti], 2), fldtarg=_as_pairs(ft[ti], 6))
+        tp, tf = oracle.direct_at(src, trg[ti], None, c(q), c(dq), dv)
+        dv_.update(pottarg=_as_pairs(tp, 2), fldtarg=_as_pairs(tf, 6))
+    return dt, parity_report(ov, dv_, gpu_forms, gpu_direct)
+
+
+def oracle_helm_parity(S):
+    """The oracle's hfmm3dpartself (C restatement, OpenMP) on the Helmholtz workload's own inputs,
+    timed, against the GPU's FP64 outputs at the sampled sources; returns (seconds, report)."""
+    import oracle
+    src, q, si = S["src"], S["q"][:, 0] + 1j * S["q"][:, 1], S["si"]
+    t0 = time.perf_counter()
+    ier, pot, fld, _, _ = oracle.hfmm3dparttarg(HELM_IPREC, HELM_ZK, src, q)
+    dt = time.perf_counter() - t0
+    if ier != 0:
+        raise RuntimeError("oracle ier=%d" % ier)
+    dp, df = oracle.hdirect_at(HELM_ZK, src, src[si], si, q)
+    rep = parity_report({"pot": _as_pairs(pot[si], 2), "fld": _as_pairs(fld[si], 6)},
+                        {"pot": _as_pairs(dp, 2), "fld": _as_pairs(df, 6)},
+                        {"fp64": {"pot": S["pot"], "fld": S["fld"]}},
+                        {"pot": S["direct_pot"], "fld": S["direct_fld"]})
+    rep.update(points="%d seeded sources (self excluded)" % len(si), inputs="the Helmholtz workload's own inputs",
+               oracle_call_s=round(dt, 2))
+    return dt, rep
 
 
 def run_b200(args):
@@ -526,11 +629,11 @@ def run_b200(args):
             raise RuntimeError("FMM ier=%d: %s" % (ier, F.last_error()))
 
     def errors():
-        rng = np.random.default_rng(99)
-        k = min(args.err_samples, n)
-        si = np.sort(rng.choice(n, k, replace=False)).astype(np.int32)
-        ti = np.sort(rng.choice(m, k, replace=False)).astype(np.int32)
-        out = {}
+        """Relative L2 errors vs the GPU's FP64 direct sum at the sampled points, and the sampled
+        values themselves (FMM outputs and direct sums, for the parity check against the oracle)."""
+        si, ti = sample_indices(n, m, args.err_samples)
+        k = len(si)
+        out, vals = {}, {"si": si, "ti": ti}
         dp = torch.empty((k, 2), dtype=torch.float64, device=dev)
         df = torch.empty((k, 6), dtype=torch.float64, device=dev)
         for name, idx, pts, skip, P, Fd in (("src", si, d_src[si], torch.from_numpy(si).to(dev), d_pot, d_fld),
@@ -540,9 +643,12 @@ def run_b200(args):
             if ier != 0:
                 raise RuntimeError("direct ier=%d" % ier)
             it = torch.from_numpy(idx).to(dev).long()
-            out["pot" if name == "src" else "pottarg"] = float(torch.linalg.norm(P[it] - dp) / torch.linalg.norm(dp))
-            out["fld" if name == "src" else "fldtarg"] = float(torch.linalg.norm(Fd[it] - df) / torch.linalg.norm(df))
-        return out
+            kp, kf = ("pot", "fld") if name == "src" else ("pottarg", "fldtarg")
+            out[kp] = float(torch.linalg.norm(P[it] - dp) / torch.linalg.norm(dp))
+            out[kf] = float(torch.linalg.norm(Fd[it] - df) / torch.linalg.norm(df))
+            vals[kp], vals[kf] = P[it].cpu().numpy(), Fd[it].cpu().numpy()
+            vals["direct_" + kp], vals["direct_" + kf] = dp.cpu().numpy(), df.cpu().numpy()
+        return out, vals
 
     def measure(form):
         F.set_precision(form)
@@ -580,8 +686,9 @@ def run_b200(args):
         step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
         total_ms = ev[0].elapsed_time(ev[args.steps])
         total_ms = reduce_max(dist if ws > 1 else None, total_ms, dev)
+        errs, vals = errors()
         return dict(total_ms=total_ms, step_ms=step_ms, passes=passes, launches=launches, stats=F.last_stats(),
-                    clocks=clocks, errs=errors(), points=n + m, serial=serial, tuning=knobs)
+                    clocks=clocks, errs=errs, samples=vals, points=n + m, serial=serial, tuning=knobs)
 
     forms = {"mixed": measure(1), "fp64": measure(0)}
     peaks = {"fp64": measured_peak(torch, dev, torch.float64), "fp32": measured_peak(torch, dev, torch.float32),
@@ -631,45 +738,59 @@ def run_iprec2(args, R, steps=2):
 
 
 def run_e2e(args, R):
-    """Same workload through the Fortran C ABI with pinned host arrays (H2D + D2H timed)."""
+    """Same workload through the Fortran C ABI (lfmm3dparttarg_) with host arrays, H2D of the inputs
+    and D2H of the outputs inside the timed region: pageable arrays (what a Fortran or numpy caller
+    passes; the headline) and pinned arrays."""
     torch, F = R["torch"], R["F"]
     src, q, dq, dv, trg = R["arrays"]
     n, m = R["n"], R["m"]
+    import ctypes
+    lib = F.lib()
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    ier = ctypes.c_int(0)
+
+    def measure(ins, outs, ptr):
+        P = lambda a: ctypes.c_void_p(ptr(a))
+
+        def call():
+            lib.lfmm3dparttarg_(ctypes.byref(ier), I(args.iprec), I(n), P(ins[0]), I(1), P(ins[1]), I(1), P(ins[2]),
+                                P(ins[3]), I(1), P(outs[0]), I(1), P(outs[1]), I(m), P(ins[4]), I(1), P(outs[2]), I(1),
+                                P(outs[3]))
+            if ier.value != 0:
+                raise RuntimeError("e2e ier=%d" % ier.value)
+
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        if R["dist"] is not None:
+            R["dist"].barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            call()  # synchronous: returns after the outputs are in host memory
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        return reduce_max(R["dist"], dt, "cuda")
+
+    shapes = ((n, 2), (n, 6), (m, 2), (m, 6))
+    # pageable: plain numpy arrays (outputs freshly allocated, as a caller's own arrays)
+    ins = [np.ascontiguousarray(a) for a in (src, q, dq, dv, trg)]
+    outs = [np.empty(sh) for sh in shapes]
+    dt_page = measure(ins, outs, lambda a: a.ctypes.data)
 
     def pinned(a):
         t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = a
         return t
 
-    h = [pinned(a) for a in (src, q, dq, dv, trg)]
-    outs = [torch.empty(s, dtype=torch.float64, pin_memory=True) for s in ((n, 2), (n, 6), (m, 2), (m, 6))]
-    import ctypes
-    lib = F.lib()
-    P = lambda t: ctypes.c_void_p(t.data_ptr())
-    I = lambda v: ctypes.byref(ctypes.c_int(v))
-    ier = ctypes.c_int(0)
-
-    def call():
-        lib.lfmm3dparttarg_(ctypes.byref(ier), I(args.iprec), I(n), P(h[0]), I(1), P(h[1]), I(1), P(h[2]), P(h[3]),
-                            I(1), P(outs[0]), I(1), P(outs[1]), I(m), P(h[4]), I(1), P(outs[2]), I(1), P(outs[3]))
-        if ier.value != 0:
-            raise RuntimeError("e2e ier=%d" % ier.value)
-
-    for _ in range(args.warmup):
-        call()
-    torch.cuda.synchronize()
-    if R["dist"] is not None:
-        R["dist"].barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        call()  # synchronous: returns after the outputs are in host memory
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    dt = reduce_max(R["dist"], dt, "cuda")
+    h = [pinned(a) for a in ins]
+    houts = [torch.empty(sh, dtype=torch.float64, pin_memory=True) for sh in shapes]
+    dt_pin = measure(h, houts, lambda t: t.data_ptr())
     h2d = n * (24 + 16 + 16 + 24) + m * 24
     d2h = n * (16 + 48) + m * (16 + 48)
-    return {"value": R["ws"] * (n + m) * args.steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * dt / args.steps, "host_memory": "pinned"}
+    rate = lambda dt: R["ws"] * (n + m) * args.steps / dt
+    return {"value": rate(dt_page), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": 1e3 * dt_page / args.steps, "host_memory": "pageable (numpy arrays)",
+            "pinned": {"value": rate(dt_pin), "ms_per_step": 1e3 * dt_pin / args.steps}}
 
 
 def run_helm(args, R):
@@ -722,6 +843,9 @@ def run_helm(args, R):
         raise RuntimeError("Helmholtz direct ier=%d" % ier)
     errs = {"pot": float(torch.linalg.norm(d_pot[it.long()] - dp) / torch.linalg.norm(dp)),
             "fld": float(torch.linalg.norm(d_fld[it.long()] - df) / torch.linalg.norm(df))}
+    R["helm_samples"] = dict(src=src, q=q, si=si, pot=d_pot[it.long()].cpu().numpy(),
+                             fld=d_fld[it.long()].cpu().numpy(), direct_pot=dp.cpu().numpy(),
+                             direct_fld=df.cpu().numpy())
     mean = {kk: round(float(np.mean([p[kk] for p in passes])), 3) for kk in passes[0]}
     out = {"workload": "helmholtz_hfmm3dpartself_sphere_%dk_zk_8pi_iprec2" % (n // 1000), "n_sources": n,
            "zk": "8*pi", "iprec": HELM_IPREC, "dtype": "f64",
@@ -778,12 +902,13 @@ def m2l_flops(pt):
 
 
 def run_reference(args):
-    """CPU restatement of the reference (oracle/, OpenMP over all host cores) on a bounded sample."""
+    """CPU restatement of the reference (oracle/, OpenMP over all host cores): every step is one
+    lfmm3dparttarg call on the whole workload (the same N, M, distribution and seed as the GPU
+    arm's), so both arms report the same config."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return None
-    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
-    n = args.cpu_sample
+    n = args.cpu_sample or args.n
     for _ in range(args.warmup):
         cpu_fmm_sample(n, args.iprec)
     times = []
@@ -799,11 +924,14 @@ def run_reference(args):
                 "unit": UNIT, "sample": "%d sources, one call (%.1f s)" % (args.helm_cpu_sample, dt)}
     sample = "N=M=%d uniform cube, charges+dipoles, iprec=%d, one lfmm3dparttarg restatement call per step" % (
         n, args.iprec)
+    config = config_of(args, ws)
+    if n != args.n:
+        config["cpu_steps_n"] = n
     return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "p50_ms": 1e3 * float(np.percentile(times, 50)), "p99_ms": 1e3 * float(np.percentile(times, 99)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(args, ws), "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores,
+            "config": config, "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores,
                                                              "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "helmholtz": helm}
@@ -866,6 +994,7 @@ def run_autotune(args):
 def main(argv=None):
     args = parse_args(argv)
     ws, rank, _ = dist_env()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
     if args.autotune:
         if rank == 0:
             print(json.dumps(run_autotune(args)), flush=True)
@@ -881,9 +1010,11 @@ def main(argv=None):
         torch.cuda.set_device(dist_env()[2])
         R = dict(torch=torch, F=F, rank=rank, ws=1, dist=None)
         out = run_helm(args, R)
-        print(json.dumps({"metric": "Helmholtz FMM pts/s (sphere, zk=8pi, iprec=2)", "value": out["value"],
-                          "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-                          "helmholtz": out}), flush=True)
+        line = {"metric": "Helmholtz FMM pts/s (sphere, zk=8pi, iprec=2)", "value": out["value"], "unit": UNIT,
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "helmholtz": out}
+        if not args.no_cpu and args.helm_cpu_sample >= args.helm_n:
+            dt, line["parity"] = oracle_helm_parity(R.pop("helm_samples"))
+        print(json.dumps(line), flush=True)
         return 0
     if args.workload == "batched":
         import torch
@@ -924,13 +1055,28 @@ def main(argv=None):
                                                   gpu_launches=int(sum(R["forms"]["fp64"]["launches"])))},
             "stats": {k: v for k, v in H["stats"].items() if k != "m2l_pt_hist"}}
     line["forms"]["mixed_over_fp64"] = round(head["value"] / line["forms"]["fp64"]["value"], 3)
-    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+    # CPU work (the oracle on each workload's own inputs: parity at the sampled points, and its
+    # time as the CPU baseline) runs after every GPU workload, so that it does not share the host
+    # with them
+    cpu_jobs = R.setdefault("cpu_jobs", [])
     if rank == 0 and ws == 1 and not args.no_cpu:
-        dt, pts = cpu_fmm_sample(args.cpu_sample, args.iprec)
-        line["cpu_baseline"] = {"value": pts / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
-                                "kind": "port",
-                                "sample": "N=M=%d uniform cube, charges+dipoles, iprec=%d, one call (%.1f s)" % (
-                                    args.cpu_sample, args.iprec, dt)}
+        def cube_job(line):
+            src, q, dq, dv, trg = R["arrays"]
+            Sm, Sf = R["forms"]["mixed"]["samples"], R["forms"]["fp64"]["samples"]
+            keys = ("pot", "fld", "pottarg", "fldtarg")
+            gpu_forms = {"fp64": {k: Sf[k] for k in keys}, "mixed": {k: Sm[k] for k in keys}}
+            dt, rep = oracle_laplace_parity(args.iprec, src, q, dq, dv, trg, Sf["si"], Sf["ti"], gpu_forms,
+                                            {k: Sf["direct_" + k] for k in keys})
+            rep.update(points="%d seeded sources (self excluded) and %d seeded targets" % (len(Sf["si"]),
+                                                                                           len(Sf["ti"])),
+                       inputs="the headline workload's own inputs", oracle_call_s=round(dt, 2))
+            line.setdefault("parity", {})["laplace_cube"] = rep
+            line["cpu_baseline"] = {"value": (n + m) / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                    "kind": "port",
+                                    "sample": "the whole workload (N=M=%d uniform cube, charges+dipoles, iprec=%d), "
+                                              "one lfmm3dparttarg restatement call (%.1f s)" % (n, args.iprec, dt)}
+
+        cpu_jobs.append(cube_job)
     line["laplace_sphere"] = run_laplace_sphere(args, R)
     if args.n == 2_000_000 and args.iprec == 1:
         line["laplace_iprec2"] = run_iprec2(args, R)
@@ -943,12 +1089,25 @@ def main(argv=None):
     if args.helm_n > 0:
         H2 = run_helm(args, R)
         if rank == 0 and ws == 1 and not args.no_cpu and args.helm_cpu_sample > 0:
-            dt = cpu_helm_sample(args.helm_cpu_sample)
-            H2["cpu_baseline"] = {"value": args.helm_cpu_sample / dt, "unit": UNIT,
-                                  "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                                  "sample": "%d sources, same distribution, one call (%.1f s)" % (
-                                      args.helm_cpu_sample, dt)}
+            HS = R.pop("helm_samples")
+
+            def helm_job(line):
+                if args.helm_cpu_sample >= args.helm_n:
+                    dt, rep = oracle_helm_parity(HS)
+                    line.setdefault("parity", {})["helmholtz_sphere"] = rep
+                    what = "the whole workload (the same inputs), one call (%.1f s)" % dt
+                    nc = args.helm_n
+                else:
+                    dt = cpu_helm_sample(args.helm_cpu_sample)
+                    what = "%d sources, same distribution, one call (%.1f s)" % (args.helm_cpu_sample, dt)
+                    nc = args.helm_cpu_sample
+                H2["cpu_baseline"] = {"value": nc / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                      "kind": "port", "sample": what}
+
+            cpu_jobs.append(helm_job)
         line["helmholtz"] = H2
+    for job in cpu_jobs:
+        job(line)
     if R["dist"] is not None:
         R["dist"].barrier()
         R["dist"].destroy_process_group()

@@ -6,6 +6,7 @@
 #pragma once
 #include <functional>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lap_kernels.cuh"
@@ -19,6 +20,9 @@ struct ThreadInfo {
     // set by the host-array entry points while charges are still being copied:
     // the charge-dependent passes wait for it
     cudaEvent_t inputs_ready = nullptr;
+    // set with inputs_ready when a helper thread is still staging the charges
+    // from pageable host memory: joined before the event is waited on
+    std::function<void()> inputs_join;
     std::vector<double> ms;
     std::vector<long long> stats;
     std::string err;
@@ -28,6 +32,51 @@ extern thread_local ThreadInfo g_ti;
 
 cudaStream_t thread_stream();
 void keep_pool_memory();
+
+// The device routine's wait for charges still being copied from the host:
+// joins the staging helper thread (if any), then orders `s` after the copies.
+inline void wait_host_inputs(cudaStream_t s, Status &st)
+{
+    if (g_ti.inputs_join) {
+        std::function<void()> f = std::move(g_ti.inputs_join);
+        g_ti.inputs_join = nullptr;
+        f();
+    }
+    if (g_ti.inputs_ready) {
+        FMM_TRY(st, cudaStreamWaitEvent(s, g_ti.inputs_ready, 0));
+        g_ti.inputs_ready = nullptr;
+    }
+}
+
+// ---------------------------------------------------------------- pageable host memory
+// A Fortran (or numpy) caller passes pageable arrays; cudaMemcpyAsync from
+// pageable memory is staged by the driver through its own small pinned
+// buffer by one host thread.  Large pageable transfers here go instead
+// through a pinned ring of the calling host thread (kStageSlots chunks of
+// kStageChunk bytes, allocated on first use and kept), the host-side copies
+// split over the library's copy threads and each chunk's DMA overlapping the
+// host copy of the next.
+constexpr size_t kStageChunk = 16u << 20;
+constexpr int kStageSlots = 6;
+constexpr size_t kStageMin = 4u << 20;   // smaller transfers keep cudaMemcpyAsync
+
+struct StageRing {
+    char *buf = nullptr;
+    cudaEvent_t ev[kStageSlots] = {};
+    int next = 0;
+    int dev = -1;
+};
+// The ring of the calling host thread on the current device (nullptr if
+// pinned memory cannot be had: the caller then falls back to cudaMemcpyAsync).
+StageRing *stage_ring();
+// True for host memory that is neither pinned nor registered with CUDA.
+bool host_pageable(const void *p);
+// Stream-ordered copies between pageable host memory and the device through
+// `ring`.  The host side is synchronous: staged_h2d returns once every chunk
+// is in the ring and its DMA is enqueued on s (the source may then be
+// reused); staged_d2h returns once dst holds the data.
+void staged_h2d(StageRing &ring, void *dst, const void *src, size_t bytes, cudaStream_t s, Status &st);
+void staged_d2h(StageRing &ring, void *dst, const void *src, size_t bytes, cudaStream_t s, Status &st);
 
 struct Timer {
     cudaStream_t s;
@@ -99,10 +148,11 @@ inline TreeView make_treeview(const Tree &T)
 // Copies host inputs to the device, runs the device routine and copies the
 // requested outputs back; unrequested outputs are left untouched.  The
 // positions go first on the call's stream; the charges and dipoles follow on
-// a copy stream, so that (from pinned host memory) they travel while the tree
-// is built.  With overlap_charges the device routine waits for them itself
-// (g_ti.inputs_ready) before its charge-dependent passes; otherwise the call's
-// stream waits before the routine starts.
+// a copy stream, so that they travel while the tree is built: from pinned
+// memory as DMA, from pageable memory (large arrays) staged by a helper host
+// thread through the pinned ring.  With overlap_charges the device routine
+// waits for them itself (wait_host_inputs) before its charge-dependent
+// passes; otherwise the call's stream waits before the routine starts.
 template <typename F>
 inline int with_device_arrays(int ns, const double *source, int ifcharge, const double *charge, int ifdipole,
                               const double *dipstr, const double *dipvec, int ifpot, double *pot, int iffld,
@@ -114,6 +164,7 @@ inline int with_device_arrays(int ns, const double *source, int ifcharge, const 
     if (ns < 0) ns = 0;
     if (nt < 0) nt = 0;
     DBuf<double> dsrc, dq, ddq, ddv, dtrg, dpot, dfld, dpt, dft;
+    alloc_fail_point(1);
     bool ok = dsrc.alloc(3L * std::max(ns, 1), s, st);
     if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
     if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st) && ddv.alloc(3L * ns, s, st);
@@ -123,36 +174,70 @@ inline int with_device_arrays(int ns, const double *source, int ifcharge, const 
     if (nt && ifpottarg == 1) ok = ok && dpt.alloc(2L * nt, s, st);
     if (nt && iffldtarg == 1) ok = ok && dft.alloc(6L * nt, s, st);
     if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    FMM_TRY(st, cudaMemcpyAsync(dsrc.p, source, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, s));
-    if (nt) FMM_TRY(st, cudaMemcpyAsync(dtrg.p, target, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, s));
+    // large transfers from / to pageable memory go through the pinned ring
+    const size_t in_bytes = sizeof(double) * ((size_t)3 * ns + (ifcharge == 1 ? 2 * ns : 0) +
+                                              (ifdipole == 1 ? 5 * ns : 0) + 3 * (size_t)nt);
+    StageRing *ring = (in_bytes >= kStageMin && host_pageable(source)) ? stage_ring() : nullptr;
+    auto h2d = [&](void *d, const void *h, size_t bytes, cudaStream_t stream) {
+        if (ring && bytes >= kStageMin) staged_h2d(*ring, d, h, bytes, stream, st);
+        else FMM_TRY(st, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
+    };
+    h2d(dsrc.p, source, sizeof(double) * 3 * ns, s);
+    if (nt) h2d(dtrg.p, target, sizeof(double) * 3 * nt, s);
     SideStreams &ss = side_streams();
     // the charge buffers were allocated on s: the copy stream starts after that
     FMM_TRY(st, cudaEventRecord(ss.fork, s));
     FMM_TRY(st, cudaStreamWaitEvent(ss.copy, ss.fork, 0));
-    if (ifcharge == 1)
-        FMM_TRY(st, cudaMemcpyAsync(dq.p, charge, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, ss.copy));
-    if (ifdipole == 1) {
-        FMM_TRY(st, cudaMemcpyAsync(ddq.p, dipstr, sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, ss.copy));
-        FMM_TRY(st, cudaMemcpyAsync(ddv.p, dipvec, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, ss.copy));
-    }
-    FMM_TRY(st, cudaEventRecord(ss.copied, ss.copy));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    if (overlap_charges) g_ti.inputs_ready = ss.copied;
-    else FMM_TRY(st, cudaStreamWaitEvent(s, ss.copied, 0));
-    int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
-    if (g_ti.inputs_ready) {
-        // not consumed (an early error): order the stream after the copies anyway
-        cudaStreamWaitEvent(s, g_ti.inputs_ready, 0);
-        g_ti.inputs_ready = nullptr;
+    Status cst;   // status of the charge copies (written by the helper thread when there is one)
+    auto copy_charges = [&, ring]() {
+        auto hc = [&](void *d, const void *h, size_t bytes) {
+            if (ring && bytes >= kStageMin) staged_h2d(*ring, d, h, bytes, ss.copy, cst);
+            else FMM_TRY(cst, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ss.copy));
+        };
+        if (ifcharge == 1) hc(dq.p, charge, sizeof(double) * 2 * ns);
+        if (ifdipole == 1) {
+            hc(ddq.p, dipstr, sizeof(double) * 2 * ns);
+            hc(ddv.p, dipvec, sizeof(double) * 3 * ns);
+        }
+        FMM_TRY(cst, cudaEventRecord(ss.copied, ss.copy));
+    };
+    std::thread helper;
+    if (ring && overlap_charges) {
+        // pageable charges: a helper thread stages them while this thread builds the tree
+        int dev = 0;
+        cudaGetDevice(&dev);
+        helper = std::thread([&, dev]() {
+            cudaSetDevice(dev);
+            copy_charges();
+        });
+        g_ti.inputs_join = [&helper]() { if (helper.joinable()) helper.join(); };
+        g_ti.inputs_ready = ss.copied;
+    } else {
+        copy_charges();
+        if (!cst.ok()) { g_ti.err = cudaGetErrorString(cst.err); return 8; }
+        if (overlap_charges) g_ti.inputs_ready = ss.copied;
+        else FMM_TRY(st, cudaStreamWaitEvent(s, ss.copied, 0));
     }
+    int ier = run(dsrc.p, dq.p, ddq.p, ddv.p, dpot.p, dfld.p, dtrg.p, dpt.p, dft.p, s);
+    if (g_ti.inputs_join || g_ti.inputs_ready) {
+        // not consumed (an early error): order the stream after the copies anyway
+        wait_host_inputs(s, st);
+    }
+    if (helper.joinable()) helper.join();
+    if (!ier && !cst.ok()) { g_ti.err = cudaGetErrorString(cst.err); ier = 8; }
     if (ier) {
         cudaStreamSynchronize(s);
         return ier;
     }
-    if (ifpot == 1) FMM_TRY(st, cudaMemcpyAsync(pot, dpot.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
-    if (iffld == 1) FMM_TRY(st, cudaMemcpyAsync(fld, dfld.p, sizeof(double) * 6 * ns, cudaMemcpyDeviceToHost, s));
-    if (nt && ifpottarg == 1) FMM_TRY(st, cudaMemcpyAsync(pottarg, dpt.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));
-    if (nt && iffldtarg == 1) FMM_TRY(st, cudaMemcpyAsync(fldtarg, dft.p, sizeof(double) * 6 * nt, cudaMemcpyDeviceToHost, s));
+    auto d2h = [&](void *h, const void *d, size_t bytes) {
+        if (ring && bytes >= kStageMin && host_pageable(h)) staged_d2h(*ring, h, d, bytes, s, st);
+        else FMM_TRY(st, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    if (ifpot == 1) d2h(pot, dpot.p, sizeof(double) * 2 * ns);
+    if (iffld == 1) d2h(fld, dfld.p, sizeof(double) * 6 * ns);
+    if (nt && ifpottarg == 1) d2h(pottarg, dpt.p, sizeof(double) * 2 * nt);
+    if (nt && iffldtarg == 1) d2h(fldtarg, dft.p, sizeof(double) * 6 * nt);
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     return 0;

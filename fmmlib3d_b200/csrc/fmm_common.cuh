@@ -71,6 +71,22 @@ constexpr int kMaxLevel = 21;  // 3 key bits per level in a 64-bit key
 constexpr int kMaxP = 80;
 
 // ---------------------------------------------------------------- device buffers
+// Test hook (fmm3d_inject_alloc_failure): when positive, counts this host
+// thread's workspace allocations down and fails the one that reaches zero as
+// if the device were out of memory.  Armed at the start of one allocation
+// phase of a call by alloc_fail_point (the phases of the reference's error
+// codes: 1 the host-array entry points' device copies, 2 the octree, 3 the
+// per-point workspace, 4 the expansions).
+extern thread_local int g_alloc_fail_countdown;
+extern thread_local int g_alloc_fail_phase;
+inline void alloc_fail_point(int phase)
+{
+    if (g_alloc_fail_phase == phase) {
+        g_alloc_fail_phase = 0;
+        g_alloc_fail_countdown = 1;
+    }
+}
+
 // Stream-ordered allocations from the device's default memory pool, so that
 // repeated calls reuse HBM without synchronising the device.
 template <typename T>
@@ -94,6 +110,10 @@ struct DBuf {
         s = stream;
         n = count;
         if (count == 0) return true;
+        if (g_alloc_fail_countdown > 0 && st.ok() && --g_alloc_fail_countdown == 0) {
+            st.err = cudaErrorMemoryAllocation;
+            st.where = "injected allocation failure";
+        }
         FMM_TRY(st, cudaMallocAsync((void **)&p, sizeof(T) * count, stream));
         if (!st.ok()) { p = nullptr; n = 0; return false; }
         return true;

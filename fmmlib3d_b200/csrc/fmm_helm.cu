@@ -248,10 +248,15 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     Timer tm(s, g_ti.timing);
     tm.mark();
     Tree T;
+    alloc_fail_point(2);
     build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
     tm.mark();
-    // per-level orders and scales (src/hfmm3dpart.f:336-340, 398-405)
+    // per-level orders and scales (src/hfmm3dpart.f:336-340, 398-405).  In
+    // hfmm3dparttarg zk is not declared complex, so under its implicit real*8
+    // typing the scale rule sees only the real part (the first of zk's two
+    // doubles): scale = min(1, |Re(zk)| * size / 2^l).  The orders (h3dterms)
+    // and every operator receive the complex zk.
     const cplx zkc(zk.x, zk.y);
     const int nlev = T.nlev;
     HLevels lv;
@@ -260,7 +265,7 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     int pmax = 1;
     for (int l = 0; l <= nlev; l++) {
         bsize[l] = T.size / pow(2.0, l);
-        double bs = std::abs(bsize[l] * zkc);
+        double bs = std::abs(bsize[l] * zk.x);
         lv.sc[l] = bs < 1 ? bs : 1.0;
         if (l >= 2) {
             int e;
@@ -276,6 +281,7 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     const int NC = (pmax + 1) * (pmax + 1);
     DBuf<double> sx, sy, sz, svx, svy, svz, tx, ty, tz;
     DBuf<double2> sq, sdq, opot, ofx, ofy, ofz, tpot, tfx, tfy, tfz, mpole, local;
+    alloc_fail_point(3);
     bool ok = sx.alloc(ns, s, st) && sy.alloc(ns, s, st) && sz.alloc(ns, s, st);
     if (ifcharge == 1) ok = ok && sq.alloc(ns, s, st);
     if (ifdipole == 1) ok = ok && sdq.alloc(ns, s, st) && svx.alloc(ns, s, st) && svy.alloc(ns, s, st) && svz.alloc(ns, s, st);
@@ -290,6 +296,7 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
     const bool far = nlev >= 2;
     if (far) {
+        alloc_fail_point(4);
         if (!mpole.alloc((size_t)T.nboxes * NC, s, st) || !local.alloc((size_t)T.nboxes * NC, s, st)) {
             g_ti.err = cudaGetErrorString(st.err);
             return 16;
@@ -299,10 +306,7 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     }
     PointsSoA P;
     P.x = sx.p; P.y = sy.p; P.z = sz.p; P.q = sq.p; P.dq = sdq.p; P.vx = svx.p; P.vy = svy.p; P.vz = svz.p;
-    if (g_ti.inputs_ready) {   // charges still in flight from the host
-        FMM_TRY(st, cudaStreamWaitEvent(s, g_ti.inputs_ready, 0));
-        g_ti.inputs_ready = nullptr;
-    }
+    wait_host_inputs(s, st);   // charges still in flight from the host
     k_gather_src<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_src, d_q, d_dq, d_dv, ifcharge == 1,
                                                  ifdipole == 1, P); FMM_COUNT_LAUNCH();
     if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }

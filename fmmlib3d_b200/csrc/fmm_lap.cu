@@ -9,6 +9,7 @@
 
 #include <map>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -103,12 +104,34 @@ struct LapPlan {
     DBuf<float2> T32;        // the same operators rounded to FP32 (mixed form)
     DBuf<long long> slot_toff;
 };
-static int g_m2l_mode = 0;  // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
-static int g_precision = 0; // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
-thread_local int g_precision_thread = -1;   // this thread's form (-1: the process-wide one)
-static int g_tc_m2l = 1;    // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
-static int g_tc_group = 1;  // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
-static int g_overlap = 1;   // near field concurrent with the far-field passes
+// Switches of the Laplace calls: a process-wide value (fmm3d_set_m2l_mode,
+// _precision, _tensor_m2l, _tensor_m2l_group, _overlap) and a per-host-thread
+// override (fmm3d_set_switch_thread; -1 follows the process-wide value), read
+// on the calling thread when a call or a plan execution starts, so that a
+// thread (a serving worker) can set its own without touching other threads'
+// calls.
+enum Switch {
+    kSwM2LMode = 0,    // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
+    kSwPrecision = 1,  // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
+    kSwTensorM2L = 2,  // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
+    kSwTcGroup = 3,    // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
+    kSwOverlap = 4,    // near field concurrent with the far-field passes
+    kNumSw = 5
+};
+static std::atomic<int> g_sw[kNumSw] = {{0}, {0}, {1}, {1}, {1}};
+static thread_local int g_sw_thread[kNumSw] = {-1, -1, -1, -1, -1};
+static inline int sw(int k) { return g_sw_thread[k] >= 0 ? g_sw_thread[k] : g_sw[k].load(std::memory_order_relaxed); }
+static bool sw_valid(int k, int v)
+{
+    switch (k) {
+    case kSwM2LMode: return v >= 0 && v <= 2;
+    case kSwPrecision: return v == 0 || v == 1;
+    case kSwTensorM2L: return v >= 0 && v <= 2;
+    case kSwTcGroup: return v >= 0;
+    case kSwOverlap: return v == 0 || v == 1;
+    }
+    return false;
+}
 constexpr int kSlotM2M = 8 * 189, kSlotL2L = 8 * 189 + 8;
 
 static std::mutex g_plan_mu;
@@ -618,11 +641,13 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.ifpottarg = ifpottarg; S.iffldtarg = iffldtarg;
     tm.mark();
     Tree &T = S.T;
+    alloc_fail_point(2);
     if (so) build_forest(T, d_src, *so, d_trg, *to, nbox, s, st);
     else build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
     tm.mark();
     const int K = S.K;
+    alloc_fail_point(3);
     bool ok = S.sx.alloc(ns, s, st) && S.sy.alloc(ns, s, st) && S.sz.alloc(ns, s, st);
     if (ifcharge == 1) ok = ok && S.sq.alloc(ns, s, st);
     if (ifdipole == 1)
@@ -635,6 +660,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     if (S.do_trg && ifpottarg == 1) ok = ok && S.tpot.alloc(nt, s, st);
     if (S.do_trg && iffldtarg == 1) ok = ok && S.tfx.alloc(nt, s, st) && S.tfy.alloc(nt, s, st) && S.tfz.alloc(nt, s, st);
     if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    alloc_fail_point(4);
     if (!S.mpole.alloc((size_t)T.nboxes * K, s, st) || !S.local.alloc((size_t)T.nboxes * K, s, st)) {
         g_ti.err = cudaGetErrorString(st.err);
         return 16;
@@ -650,10 +676,10 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.os.pot = S.opot.p; S.os.fx = S.ofx.p; S.os.fy = S.ofy.p; S.os.fz = S.ofz.p;
     S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
-    const int form = g_precision_thread >= 0 ? g_precision_thread : g_precision;
+    const int form = sw(kSwPrecision);
     S.mixed = form == 1 && iprec <= 1 && plan->dense;
-    S.dense = (plan->dense && g_m2l_mode != 1) || S.mixed;
-    S.tcm2l = S.mixed && g_tc_m2l > 0;
+    S.dense = (plan->dense && sw(kSwM2LMode) != 1) || S.mixed;
+    S.tcm2l = S.mixed && sw(kSwTensorM2L) > 0;
     // launch shapes: the autotuner's cached setting for this problem, else automatic
     S.signature = lap_signature(S);
     TuneKnobs kn;
@@ -689,10 +715,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     const TreeView &tv = S.tv;
     const PointsSoA &P = S.P;
     const int prune = S.prune;
-    if (g_ti.inputs_ready) {   // charges still in flight from the host
-        FMM_TRY(st, cudaStreamWaitEvent(s, g_ti.inputs_ready, 0));
-        g_ti.inputs_ready = nullptr;
-    }
+    wait_host_inputs(s, st);   // charges still in flight from the host
     if (S.ifcharge == 1 || S.ifdipole == 1) {
         k_gather_q<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_q, d_dq, d_dv, S.ifcharge == 1,
                                                    S.ifdipole == 1, P); FMM_COUNT_LAUNCH();
@@ -712,7 +735,7 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // stream, far field first, with the same arithmetic.
     SideStreams &ss = side_streams();
     // fmm3d_set_overlap(0) forces the passes in order (per-pass timing); else the knob decides
-    const bool overlap = g_overlap != 0 && S.knobs.overlap != 2;
+    const bool overlap = sw(kSwOverlap) != 0 && S.knobs.overlap != 2;
     const cudaStream_t f = overlap ? ss.far : s;
     if (overlap) {
         FMM_TRY(st, cudaEventRecord(ss.fork, s));
@@ -751,9 +774,9 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     if (S.tcm2l) {
         FMM_TRY(st, cudaMemsetAsync(S.tcerr.p, 0, sizeof(int), f));
         convert_mp_f32(T.nboxes, K, S.ldm, S.mpole.p, S.mp32.p, f, st);
-        const int tcv = S.knobs.tc_variant ? S.knobs.tc_variant - 1 : std::max(g_tc_m2l - 1, 0);
+        const int tcv = S.knobs.tc_variant ? S.knobs.tc_variant - 1 : std::max(sw(kSwTensorM2L) - 1, 0);
         launch_m2l_tc(tcv, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
-                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, g_tc_group, S.tcerr.p, S.m2l_kt, f,
+                      plan->T32.p, tv, p, S.mp32.p, S.ldm, S.local.p, prune, 3, sw(kSwTcGroup), S.tcerr.p, S.m2l_kt, f,
                       st);
     } else if (S.mixed)
         launch_m2l_dense32(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p,
@@ -851,8 +874,8 @@ static void lap_effective_knobs(const LapSetup &S, int *out)
 {
     out[0] = S.m2l_kt;
     out[1] = S.trans_kt;
-    out[2] = S.tcm2l ? (S.knobs.tc_variant ? S.knobs.tc_variant : std::max(g_tc_m2l, 1)) : 0;
-    out[3] = (g_overlap != 0 && S.knobs.overlap != 2) ? 1 : 2;
+    out[2] = S.tcm2l ? (S.knobs.tc_variant ? S.knobs.tc_variant : std::max(sw(kSwTensorM2L), 1)) : 0;
+    out[3] = (sw(kSwOverlap) != 0 && S.knobs.overlap != 2) ? 1 : 2;
     out[4] = S.mixed ? (S.knobs.p2p_ept ? S.knobs.p2p_ept : 4) : 0;
     out[5] = lap_form(S);
     out[6] = S.knobs_from_cache ? 1 : 0;
@@ -1050,7 +1073,7 @@ int fmm3d_lfmm3d_plan_execute(void *plan, const double *d_charge, const double *
     g_launch_count = 0;
     if (use_graph) {
         const void *key[8] = {d_charge, d_dipstr, d_dipvec, d_pot, d_fld, d_pottarg, d_fldtarg, (const void *)s};
-        const int cfg = g_overlap * 16 + g_tc_m2l;
+        const int cfg = sw(kSwOverlap) * 16 + sw(kSwTensorM2L);
         if (!E->exec || memcmp(key, E->key, sizeof key) != 0 || E->key_cfg != cfg) {
             if (E->exec) cudaGraphExecDestroy(E->exec);
             E->exec = nullptr;
@@ -1433,40 +1456,52 @@ int fmm3d_set_timing(int on)
 
 int fmm3d_set_precision(int mode)
 {
-    g_precision = mode;
+    g_sw[kSwPrecision] = mode;
     return 0;
 }
 
 int fmm3d_set_precision_thread(int mode)
 {
     if (mode < -1 || mode > 1) return 1;
-    g_precision_thread = mode;
+    g_sw_thread[kSwPrecision] = mode;
     return 0;
 }
 
 int fmm3d_set_tensor_m2l(int mode)
 {
     if (mode < 0 || mode > 2) return 1;
-    g_tc_m2l = mode;
+    g_sw[kSwTensorM2L] = mode;
     return 0;
 }
 
 int fmm3d_set_overlap(int on)
 {
-    g_overlap = on ? 1 : 0;
+    g_sw[kSwOverlap] = on ? 1 : 0;
     return 0;
 }
 
 int fmm3d_set_tensor_m2l_group(int slots)
 {
     if (slots < 0) return 1;
-    g_tc_group = slots;
+    g_sw[kSwTcGroup] = slots;
     return 0;
 }
 
 int fmm3d_set_m2l_mode(int mode)
 {
-    g_m2l_mode = mode;
+    g_sw[kSwM2LMode] = mode;
+    return 0;
+}
+
+int fmm3d_set_switch_thread(int which, int value)
+{
+    if (which < 0 || which >= kNumSw) return 1;
+    if (value == -1) {
+        g_sw_thread[which] = -1;
+        return 0;
+    }
+    if (!sw_valid(which, value)) return 1;
+    g_sw_thread[which] = value;
     return 0;
 }
 

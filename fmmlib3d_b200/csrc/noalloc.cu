@@ -6,8 +6,13 @@
 // after start-up because they synchronise the device.  For them the O(N^2)
 // sum of l3dpartdirect is offered with its scratch (the structure-of-arrays
 // copies of the inputs and of the outputs) in a fixed array declared at file
-// scope below.  Every GPU that loads the library holds that array (11 MB)
-// until the process exits.
+// scope below.  Every GPU that loads the library's device code holds that
+// array (11 MB) until the process exits.  Under CUDA's default lazy module
+// loading the array and the kernels used here are loaded on a device by the
+// first call made there (which may allocate device memory for them); later
+// calls allocate nothing.  The cached device address belongs to the device's
+// current primary context: after cudaDeviceReset on that device, calls here
+// are invalid until the process restarts.
 #include <mutex>
 
 #include "../../include/fmm3d_b200.h"
@@ -75,7 +80,9 @@ __global__ void k_na_out(int n, OutSoA o, double *pot, double *fld)
 
 }  // namespace
 
-static const char *g_noalloc_msg = "";
+// per host thread, as fmm3d_last_error: calls on different GPUs may run
+// concurrently from different threads
+static thread_local const char *g_noalloc_msg = "";
 
 static int noalloc_direct(int ns, const double *src, int ifc, const double *q, int ifd, const double *dq,
                           const double *dv, int ifpot, double *pot, int iffld, double *fld, int nt,

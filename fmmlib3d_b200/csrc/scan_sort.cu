@@ -206,6 +206,7 @@ void radix_sort_u64(uint64_t *d_keys, int *d_vals, int n, int bits, cudaStream_t
     for (int shift = 0; shift < bits; shift += kRadixBits) {
         k_radix_hist<<<ntiles, kSortThreads, 0, s>>>(ka, n, shift, hist.p, ntiles); FMM_COUNT_LAUNCH();
         scan_exclusive_int(hist.p, hist.p, kRadix * ntiles, s, st, nullptr);
+        if (!st.ok()) return;   // unscanned counts are not offsets: the scatter must not run
         k_radix_scatter<<<ntiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist.p, ntiles); FMM_COUNT_LAUNCH();
         FMM_LAUNCH_CHECK(st);
         std::swap(ka, kb);

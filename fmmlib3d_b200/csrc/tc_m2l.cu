@@ -85,7 +85,8 @@ __device__ __forceinline__ void issue_stage(uint32_t base, uint32_t tm, uint32_t
 template <int KC, int S, int NMAX>
 __global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
     k_m2l_tc(const Tile *tiles, const int *grouped, const Slot *slots, const long long *slot_toff, const float2 *T,
-             TreeView tv, int p, const float2 *mp, int ldm, double2 *out, int prune, int nprod, int group, int *err)
+             TreeView tv, int p, const float2 *mp, int ldm, double2 *out, int prune, int nprod, int group, int *err,
+             int expire_stage_waits)
 {
     constexpr int KB = KC / 4;                 // 16-byte K blocks per stage
     constexpr uint32_t OPB = KB * kTcLBO;      // one A buffer
@@ -249,7 +250,8 @@ __global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
             auto stage = [&](int kc, int set) {
                 const int st = it % S;
                 int late = 0;
-                if (it >= S && !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1)) late = 1;
+                // (expire_stage_waits: the error-path test, every stage wait counts as expired)
+                if (it >= S && (expire_stage_waits || !mbar_wait_bounded(&mbar[st], ((it - S) / S) & 1))) late = 1;
                 store(sm + st * STB, set);
                 if (kc + 2 < nk) load(kc + 2, set);
                 fence_async_smem();
@@ -314,6 +316,10 @@ __global__ void __launch_bounds__(kTcThreads, NMAX == 128 ? 2 : 1)
     if (warp == 0) tmem_dealloc(tm, TCOLS);
 }
 
+// Test hook (fmm3d_inject_tc_wait_expiry): the tensor-core M2L kernels this
+// host thread launches treat every stage wait as expired.
+static thread_local int g_tc_expire_waits = 0;
+
 template <int KC, int S, int NMAX>
 static void launch_tc_t(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots,
                         const long long *slot_toff, const float2 *T, const TreeView &tv, int p, const float2 *mp,
@@ -324,7 +330,7 @@ static void launch_tc_t(const Tile *tiles, int ntiles, const int *grouped, const
     FMM_TRY(st, cudaFuncSetAttribute(k_m2l_tc<KC, S, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 g(ntiles, div_up((p + 1) * (p + 1), 64));
     k_m2l_tc<KC, S, NMAX><<<g, kTcThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod,
-                                              group, err); FMM_COUNT_LAUNCH();
+                                              group, err, g_tc_expire_waits); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
 
@@ -441,6 +447,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_selftest(int N, int K, con
 }  // namespace fmm
 
 using namespace fmm;
+
+// Error-path test of the tensor-core M2L: with on = 1 the kernels launched by
+// later calls on this thread take their bounded-wait error path at the first
+// stage wait (the wait counts as expired): every CTA that gets there stops
+// issuing MMAs, waits (with the normal bound) for the MMAs it has issued,
+// frees its TMEM and records the error, so the call returns ier 16 and the
+// context stays usable.  0 turns it off.
+extern "C" int fmm3d_inject_tc_wait_expiry(int on)
+{
+    fmm::g_tc_expire_waits = on ? 1 : 0;
+    return 0;
+}
 
 // Runs the tensor-core self-test on the current device: D (128 x N) from
 // A (128 x K) and B (N x K), host arrays.  N in 16..128 (multiple of 16), K a

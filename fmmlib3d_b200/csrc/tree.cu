@@ -678,6 +678,7 @@ void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, cons
     int gbits = 8;
     while ((1 << gbits) < ngroups + 1) gbits += 8;
     radix_sort_u64(gk.p, T.grouped.p, nboxes, gbits, s, st);
+    if (!st.ok()) return;
     k_group_bounds<<<div_up(nboxes + 1, 256), 256, 0, s>>>(nboxes, gk.p, ngroups, gs.p); FMM_COUNT_LAUNCH();
     T.group_start.assign(ngroups + 1, 0);
     FMM_TRY(st, cudaMemcpyAsync(T.group_start.data(), gs.p, sizeof(int) * (ngroups + 1), cudaMemcpyDeviceToHost, s));

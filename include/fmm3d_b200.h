@@ -138,11 +138,17 @@ int fmm3d_h3ddirect_points_device(const double *zk, int nsource, const double *d
  * a fixed 11 MB array in the library's device image, present on every GPU
  * that loads the library until the process exits.  Limit: nsource and
  * ntarget each at most 65536 (larger sizes return 8 without touching the
- * GPU).  The first call on a device looks up the array's device address, so
- * make it before any stream capture.  Calls share the array: calls whose
- * GPU work overlaps (other streams, other host threads) race; serialise
- * them.  stream NULL = the legacy default stream.  Returns ier (0 ok, 8 size
- * limit, 16 CUDA error); fmm3d_noalloc_last_error() describes the failure. */
+ * GPU).  The first call on a device is the set-up: it looks up the array's
+ * device address and, under CUDA's default lazy module loading, loads the
+ * array and the kernels used here, which can allocate device memory once.
+ * Make that first call at start-up, before the caller's allocator takes the
+ * GPU's memory and before any stream capture (or run with
+ * CUDA_MODULE_LOADING=EAGER); later calls allocate nothing.  The address is
+ * cached per device: after cudaDeviceReset, calls are invalid.  Calls share
+ * the array: calls whose GPU work overlaps (other streams, other host
+ * threads) race; serialise them.  stream NULL = the legacy default stream.
+ * Returns ier (0 ok, 8 size limit, 16 CUDA error);
+ * fmm3d_noalloc_last_error() describes this thread's last failure. */
 int fmm3d_l3dpartdirect_noalloc(int nsource, const double *d_source, int ifcharge, const double *d_charge,
                                 int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
                                 double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
@@ -182,6 +188,31 @@ int fmm3d_set_precision(int mode);
  * Lets a multi-threaded caller (a serving loop) choose the form per request.
  * Returns 1 for an unknown mode. */
 int fmm3d_set_precision_thread(int mode);
+
+/* Per-host-thread override of one of the switches above (no counterpart in
+ * the reference): which = 0 M2L form (fmm3d_set_m2l_mode), 1 arithmetic form
+ * (fmm3d_set_precision), 2 tensor-core M2L (fmm3d_set_tensor_m2l), 3 slots per
+ * tensor-core sum (fmm3d_set_tensor_m2l_group), 4 near/far overlap
+ * (fmm3d_set_overlap); value -1 follows the process-wide setting again.  Later
+ * calls made on this thread use the override; other threads' calls are not
+ * affected.  Returns 1 for an unknown switch or value. */
+int fmm3d_set_switch_thread(int which, int value);
+
+/* Error-path tests (no counterpart in the reference, whose error codes come
+ * from failed allocations: ier 4 tree, 8 per-point workspace, 16 expansions,
+ * src/lfmm3dpart.f:309-330, 424-466).
+ * fmm3d_inject_alloc_failure(phase): the next FMM call made on this host
+ * thread that reaches the phase fails its first device allocation there as
+ * if the device were out of memory: phase 1 the host-array entry points'
+ * device copies of the caller's arrays (ier 8), 2 the octree (ier 4), 3 the
+ * per-point workspace (ier 8), 4 the expansions (ier 16); 0 cancels.  One
+ * call only; the caller's host outputs are left untouched.
+ * fmm3d_inject_tc_wait_expiry(on): the tensor-core M2L kernels launched by
+ * later calls on this thread treat their first stage wait as expired and
+ * take their error path (drain their issued MMAs, free TMEM, flag the error):
+ * the call returns 16.  Both return 1 for an unknown phase. */
+int fmm3d_inject_alloc_failure(int nth);
+int fmm3d_inject_tc_wait_expiry(int on);
 
 /* M2L of the mixed form (iprec <= 1, nterms <= 16) on the tensor cores:
  * 0 = FP32 CUDA cores, 1 or 2 = tcgen05 kind::tf32 with operands split into

@@ -961,9 +961,18 @@ static void translate(int kind, const double *c_from, const double *c_to, const 
     cart2polarl(rv, &d, &th, &ph);
     int K = (p + 1) * (p + 1);
     cplx *a = calloc(K, sizeof(cplx)), *b = calloc(K, sizeof(cplx)), *cz = calloc(K, sizeof(cplx));
-    cplx e1 = cexp(I * ph);
+    /* powers e^{i m phi} by repeated multiplication, as the reference's ephi
+     * arrays (src/l3dtrans.f:1329-1340) */
+    cplx ephi_store[2 * 202 + 3], *ephi = ephi_store + 202 + 1;
+    ephi[0] = 1.0;
+    ephi[1] = cexp(I * ph);
+    ephi[-1] = conj(ephi[1]);
+    for (int l = 1; l <= p; l++) {
+        ephi[l + 1] = ephi[l] * ephi[1];
+        ephi[-1 - l] = conj(ephi[l + 1]);
+    }
     for (int l = 0; l <= nt; l++)
-        for (int m = -l; m <= l; m++) a[EI(l, m)] = in[EI(l, m)] * cpow(e1, m);
+        for (int m = -l; m <= l; m++) a[EI(l, m)] = in[EI(l, m)] * ephi[m];
     double *rf = NULL, *rb = NULL;
     if (rotf) { rf = (double *)rotf; rb = (double *)rotb; }
     else {
@@ -1012,7 +1021,7 @@ static void translate(int kind, const double *c_from, const double *c_to, const 
     int nout = kind == 1 ? nt : p;
     rot_apply(rb, ldr, nout, cz, a);
     for (int l = 0; l <= nout; l++)
-        for (int m = -l; m <= l; m++) out[EI(l, m)] += cpow(e1, -m) * a[EI(l, m)];
+        for (int m = -l; m <= l; m++) out[EI(l, m)] += ephi[-m] * a[EI(l, m)];
     if (!rotf) { free(rf); free(rb); }
     free(a); free(b); free(cz);
 }

@@ -884,7 +884,9 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
     int nterms[202];
     for (int i = 0; i <= nlev; i++) {
         scale[i] = 1.0;
-        double bs = cabs((T.size / pow(2.0, i)) * zk);
+        /* zk is implicitly real*8 in hfmm3dparttarg (src/hfmm3dpart.f:145, no
+         * complex declaration), so this rule reads only Re(zk) (:337-341) */
+        double bs = fabs((T.size / pow(2.0, i)) * creal(zk));
         if (bs < 1) scale[i] = bs;
         bsize[i] = T.size / pow(2.0, i);
         int e;

@@ -87,7 +87,10 @@ def test_helmholtz_direct_sum_matches_oracle(F):
 @pytest.mark.parametrize("geom,iprec,zk", [("cube", 1, 1 + 0.1j), ("cube", 2, 10.0), ("sphere", 2, 8 * np.pi),
                                            ("cube", 0, 3.0), ("plummer", 1, 5.0), ("cube", 3, 20.0),
                                            ("sphere", -1, 2.0), ("ellipsoid", 2, 4 + 0.5j), ("cube", 1, 40.0),
-                                           ("cube", 2, 0.01), ("cube", 3, 60.0)])
+                                           ("cube", 2, 0.01), ("cube", 3, 60.0),
+                                           # Im(zk) far above Re(zk): the per-level scales follow the
+                                           # reference's Re(zk)-only rule (src/hfmm3dpart.f:337-341)
+                                           ("cube", 1, 1 + 10j), ("sphere", 2, 0.5 + 6j)])
 def test_hfmm_parity_charges_dipoles_targets(F, geom, iprec, zk):
     rng = np.random.default_rng(zlib.crc32(('%s%d%s' % (geom, iprec, zk)).encode()))
     n, m = 12000, 4000

@@ -298,6 +298,64 @@ def test_device_entry_point_matches_host_entry_point(F):
     assert np.array_equal(c(pt, 1), h[3]) and np.array_equal(c(ft, 3), h[4])
 
 
+@pytest.mark.parametrize("kernel", ["laplace", "helmholtz"])
+def test_pageable_host_arrays_equal_pinned_and_device(F, kernel):
+    """Arrays above the staging threshold (4 MB) from pageable memory go through the library's
+    pinned ring and copy threads; pinned arrays go straight to DMA.  Both must give the device
+    entry point's results bitwise, and the inputs must be left as they were."""
+    import torch
+    rng = np.random.default_rng(17)
+    n, m = 260000, 230000
+    src, trg = rng.random((n, 3)), rng.random((m, 3))
+    q = rng.uniform(-1, 1, (n, 2))
+    ds = rng.uniform(-1, 1, (n, 2))
+    dv = rng.normal(size=(n, 3))
+    ins = [src, q, ds, dv, trg]
+    keep = [a.copy() for a in ins]
+    lib = F.lib()
+    P = lambda a: ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+    I = lambda v: ctypes.byref(ctypes.c_int(v))
+    zk = np.array([2.0, 0.1])
+    iprec = 1 if kernel == "laplace" else 0
+
+    def host_call(arrs, outs):
+        ier = ctypes.c_int(-1)
+        head = [ctypes.byref(ier), I(iprec)] + ([P(zk)] if kernel == "helmholtz" else [])
+        fn = lib.lfmm3dparttarg_ if kernel == "laplace" else lib.hfmm3dparttarg_
+        fn(*head, I(n), P(arrs[0]), I(1), P(arrs[1]), I(1), P(arrs[2]), P(arrs[3]), I(1), P(outs[0]), I(1),
+           P(outs[1]), I(m), P(arrs[4]), I(1), P(outs[2]), I(1), P(outs[3]))
+        return ier.value
+
+    shapes = ((n, 2), (n, 6), (m, 2), (m, 6))
+    page_out = [np.full(sh, np.nan) for sh in shapes]
+    assert host_call(ins, page_out) == 0, F.last_error()
+    assert host_call(ins, page_out) == 0, F.last_error()   # again, into the same (now mapped) arrays
+    for a, b in zip(ins, keep):
+        assert np.array_equal(a, b)
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    pin_out = [torch.full(sh, np.nan, dtype=torch.float64, pin_memory=True) for sh in shapes]
+    assert host_call([pinned(a) for a in ins], pin_out) == 0, F.last_error()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dev_out = [torch.empty(sh, dtype=torch.float64, device="cuda") for sh in shapes]
+    stream = torch.cuda.current_stream().cuda_stream
+    if kernel == "laplace":
+        ier = F.lfmm3dparttarg_device(iprec, d(src), d(q), d(ds), d(dv), *dev_out[:2], d(trg), *dev_out[2:],
+                                      stream=stream)
+    else:
+        ier = F.hfmm3dparttarg_device(iprec, complex(*zk), d(src), d(q), d(ds), d(dv), *dev_out[:2], d(trg),
+                                      *dev_out[2:], stream=stream)
+    torch.cuda.synchronize()
+    assert ier == 0
+    for a, b, c in zip(page_out, pin_out, dev_out):
+        assert np.array_equal(a, b.numpy())
+        assert np.array_equal(a, c.cpu().numpy())
+
+
 @pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("geom,iprec", [("cube", 1), ("sphere", 0), ("plummer", -1)])
 def test_m2l_forms_agree_with_oracle(F, mode, geom, iprec):

@@ -136,7 +136,8 @@ def test_helmholtz_operators_compose():
 
 
 @pytest.mark.parametrize("iprec,zk,geom", [(0, 3.0, "cube"), (1, 1 + 0.1j, "cube"), (2, 10.0, "cube"),
-                                           (2, 8 * np.pi, "sphere"), (1, 30.0, "cube")])
+                                           (2, 8 * np.pi, "sphere"), (1, 30.0, "cube"),
+                                           (1, 1 + 10j, "cube"), (2, 0.5 + 6j, "sphere")])
 def test_helmholtz_fmm_within_bound(iprec, zk, geom):
     rng = np.random.default_rng(11 + iprec)
     n, m = 12000, 3000
