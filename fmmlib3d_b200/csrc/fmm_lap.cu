@@ -111,7 +111,8 @@ struct LapPlan {
 // thread (a serving worker) can set its own without touching other threads'
 // calls.
 enum Switch {
-    kSwM2LMode = 0,    // 0 automatic, 1 rotate-shift-rotate, 2 dense operators
+    kSwM2LMode = 0,    // 0 automatic, 1 rotate-shift-rotate, 2 dense operators, 3 rotate-shift-rotate
+                       // on the CUDA cores (1 and 0 use the FP64 tensor cores up to order 28)
     kSwPrecision = 1,  // 0 FP64 throughout, 1 mixed (FP32 P2P and M2L) for iprec <= 1
     kSwTensorM2L = 2,  // mixed-form M2L: 0 FP32 CUDA cores, 1/2 tensor cores (stage variants 0/1)
     kSwTcGroup = 3,    // tensor-core M2L: slots per TMEM sum (0: one sum per tile)
@@ -124,7 +125,7 @@ static inline int sw(int k) { return g_sw_thread[k] >= 0 ? g_sw_thread[k] : g_sw
 static bool sw_valid(int k, int v)
 {
     switch (k) {
-    case kSwM2LMode: return v >= 0 && v <= 2;
+    case kSwM2LMode: return v >= 0 && v <= 3;
     case kSwPrecision: return v == 0 || v == 1;
     case kSwTensorM2L: return v >= 0 && v <= 2;
     case kSwTcGroup: return v >= 0;
@@ -678,7 +679,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
 
     const int form = sw(kSwPrecision);
     S.mixed = form == 1 && iprec <= 1 && plan->dense;
-    S.dense = (plan->dense && sw(kSwM2LMode) != 1) || S.mixed;
+    S.dense = (plan->dense && sw(kSwM2LMode) != 1 && sw(kSwM2LMode) != 3) || S.mixed;
     S.tcm2l = S.mixed && sw(kSwTensorM2L) > 0;
     // launch shapes: the autotuner's cached setting for this problem, else automatic
     S.signature = lap_signature(S);
@@ -784,6 +785,9 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     else if (S.dense)
         launch_m2l_dense(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, plan->slot_toff.p, plan->T.p,
                          tv, p, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);
+    else if (sw(kSwM2LMode) != 3 && S.m2l_kt <= 8 && m2l_rot_dmma_supported(p))
+        launch_m2l_rot_dmma(S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
+                            plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, f, st);
     else
         launch_translate(1, S.dtiles.p + S.m2l_a, S.m2l_n, T.grouped.p, plan->slots.p, tv, p, plan->rot.p,
                          plan->dc.p, plan->lddc, S.mpole.p, S.local.p, prune, S.m2l_kt, f, st);

@@ -82,6 +82,13 @@ void build_rotations(int p, int ncls, const double *d_cs, double *d_rot, cudaStr
 
 __host__ __device__ inline size_t rot_class_size(int p) { return (size_t)(p + 1) * (2 * p + 1) * (2 * p + 3) / 3; }
 
+// FP64 rotate-shift-rotate M2L with its products on the FP64 tensor cores
+// (m2l_rot_dmma.cu), tiles of up to 8 targets, orders up to 28.
+bool m2l_rot_dmma_supported(int p);
+void launch_m2l_rot_dmma(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots, const TreeView &tv,
+                         int p, const double *rot, const double *dc, int lddc, const double2 *in, double2 *out,
+                         int prune, cudaStream_t s, Status &st);
+
 void launch_direct(int nsrc, const double *sx, const double *sy, const double *sz, const double2 *q,
                    const double2 *dq, const double *vx, const double *vy, const double *vz, int ifcharge,
                    int ifdipole, int neval, const double *ex, const double *ey, const double *ez, const int *skip, int self,

@@ -173,8 +173,10 @@ int fmm3d_set_stats(int on);
 
 /* M2L form: 0 automatic (dense per-offset operators for nterms <= 16,
  * rotate-shift-rotate otherwise), 1 always rotate-shift-rotate, 2 dense
- * where available.  Both give the same results to rounding; the switch
- * exists for testing and measurement. */
+ * where available, 3 rotate-shift-rotate on the CUDA cores (modes 0 and 1
+ * run the rotations and z-shifts as FP64 tensor-core products up to order
+ * 28).  All give the same results to rounding; the switch exists for testing
+ * and measurement. */
 int fmm3d_set_m2l_mode(int mode);
 
 /* Arithmetic form of later calls (process-wide): 0 = FP64 throughout (the

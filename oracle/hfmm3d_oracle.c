@@ -757,6 +757,211 @@ static void rotcache_free(rotcache *c)
     free(c->theta); free(c->mat);
 }
 
+/* ---- rotation by projection, rotviaprojf90 (src/rotproj.f:883-940), used
+ * by the reference's Helmholtz translations for orders >= 30
+ * (src/h3dtrans.f:318-345, 1335-1362, 2102-2131).                          */
+
+/* next235_cproj (src/rotproj.f:123-149): the smallest even 2^a 3^b 5^c >= base */
+static int next235(double base)
+{
+    int n = 2 * (int)(base / 2.0 + .9999);
+    if (n <= 0) n = 2;
+    for (;;) {
+        int d = n;
+        while (d % 2 == 0) d /= 2;
+        while (d % 3 == 0) d /= 3;
+        while (d % 5 == 0) d /= 5;
+        if (d == 1) return n;
+        n += 2;
+    }
+}
+
+/* ylgndrini (src/yrecursion.f:679-711) */
+static void ylgndrini_r(int nmax, double *rat1, double *rat2)
+{
+    int ld = nmax + 1;
+#define R1(n, m) rat1[(n) * ld + (m)]
+#define R2(n, m) rat2[(n) * ld + (m)]
+    R1(0, 0) = 1; R2(0, 0) = 1;
+    for (int m = 0; m <= nmax; m++) {
+        if (m > 0) { R1(m, m) = sqrt((2 * m - 1.0) / (2 * m)); R2(m, m) = 1; }
+        if (m < nmax) { R1(m + 1, m) = sqrt(2 * m + 1.0); R2(m + 1, m) = 1; }
+        for (int n = m + 2; n <= nmax; n++) {
+            R1(n, m) = (2 * n - 1) / sqrt((double)(n - m) * (n + m));
+            R2(n, m) = sqrt((n + m - 1.0) * (n - m - 1.0)) / sqrt((double)(n - m) * (n + m));
+        }
+    }
+}
+
+/* ylgndru2sf (src/yrecursion.f:909-980): y(n,m) = sqrt((n-m)!/(n+m)!) P_n^m(x),
+ * for m > 0 divided by sqrt(1-x^2); d = dy/dx, for m > 0 times sqrt(1-x^2) */
+static void ylgndru2sf_r(int nmax, double x, double *y, double *d, const double *rat1, const double *rat2)
+{
+    int ld = nmax + 1;
+#define Y_(n, m) y[(n) * ld + (m)]
+#define D_(n, m) d[(n) * ld + (m)]
+    double u = -sqrt((1 - x) * (1 + x)), u2 = (1 - x) * (1 + x);
+    Y_(0, 0) = 1; D_(0, 0) = 0;
+    if (0 < nmax) { Y_(1, 0) = x * Y_(0, 0) * R1(1, 0); D_(1, 0) = (x * D_(0, 0) + Y_(0, 0)) * R1(1, 0); }
+    for (int n = 2; n <= nmax; n++) {
+        Y_(n, 0) = R1(n, 0) * x * Y_(n - 1, 0) - R2(n, 0) * Y_(n - 2, 0);
+        D_(n, 0) = R1(n, 0) * (x * D_(n - 1, 0) + Y_(n - 1, 0)) - R2(n, 0) * D_(n - 2, 0);
+    }
+    for (int m = 1; m <= nmax; m++) {
+        if (m == 1) Y_(m, m) = Y_(m - 1, m - 1) * (-1) * R1(m, m);
+        else Y_(m, m) = Y_(m - 1, m - 1) * u * R1(m, m);
+        D_(m, m) = Y_(m, m) * (-m) * x;
+        if (m < nmax) {
+            Y_(m + 1, m) = x * Y_(m, m) * R1(m + 1, m);
+            D_(m + 1, m) = (x * D_(m, m) + u2 * Y_(m, m)) * R1(m + 1, m);
+        }
+        for (int n = m + 2; n <= nmax; n++) {
+            Y_(n, m) = R1(n, m) * x * Y_(n - 1, m) - R2(n, m) * Y_(n - 2, m);
+            D_(n, m) = R1(n, m) * (x * D_(n - 1, m) + u2 * Y_(n - 1, m)) - R2(n, m) * D_(n - 2, m);
+        }
+    }
+}
+
+/* ylgndr2pm_opt (src/yrecursion.f:1871-1903): the values of ylgndru2sf at -x */
+static void ylgndr2pm_r(int nterms, double *y, double *d)
+{
+    int ld = nterms + 1;
+    for (int n = 0; n <= nterms; n += 2) {
+        for (int m = 0; m <= n; m += 2) D_(n, m) = -D_(n, m);
+        for (int m = 1; m <= n; m += 2) Y_(n, m) = -Y_(n, m);
+    }
+    for (int n = 1; n <= nterms; n += 2) {
+        for (int m = 0; m <= n; m += 2) Y_(n, m) = -Y_(n, m);
+        for (int m = 1; m <= n; m += 2) D_(n, m) = -D_(n, m);
+    }
+}
+
+/* Forward DFT c_k = sum_j x_j e^{-2 pi i jk/n}, the transform of FFTPACK's
+ * zfftf (src/dfft.f:942; the reference computes it by a mixed-radix FFT). */
+static void dft_forward(int n, const cplx *x, cplx *c)
+{
+    for (int k = 0; k < n; k++) {
+        cplx s = 0;
+        for (int j = 0; j < n; j++) {
+            long jk = ((long)j * k) % n;
+            double a = -2 * M_PI * (double)jk / n;
+            s += x[j] * (cos(a) + I * sin(a));
+        }
+        c[k] = s;
+    }
+}
+
+/* rotviaproj0 (src/rotproj.f:152-219) with getmeridian (:222-283), evalall2
+ * (:507-705) and projectonynm2 (:798-875): rotation of the expansion `in`
+ * (degrees 0..nterms) by beta about the y axis into `out`.  The expansion and
+ * its derivative along the rotated meridians are evaluated at nquad
+ * equispaced nodes of the rotated equator (half of them by the reflection
+ * x -> -x), and projected onto the spherical harmonics by a transform along
+ * the equator.                                                             */
+static void rotviaproj(double beta, int nterms, const cplx *in, cplx *out)
+{
+    const int nquad = next235(2.0 * nterms + 2), ld = nterms + 1;
+    double *ct = malloc(sizeof(double) * 4 * nquad), *stt = ct + nquad, *cph = stt + nquad, *sph = cph + nquad;
+    /* getmeridian */
+    {
+        double ca = cos(beta), sa = sin(beta);
+        for (int i = 0; i < nquad; i++) {
+            double phi = 2 * M_PI * i / nquad, theta = M_PI / 2.0;
+            double xp = cos(phi) * sin(theta), yp = sin(phi) * sin(theta), zp = cos(theta);
+            double x = ca * xp + sa * zp, y = yp, z = -sa * xp + ca * zp;
+            double proj = sqrt(x * x + y * y);
+            if (proj <= 1.0e-16) { cph[i] = 1.0; sph[i] = 0.0; }
+            else { cph[i] = x / proj; sph[i] = y / proj; }
+            ct[i] = z;
+            stt[i] = proj;
+        }
+    }
+    double *rat1 = calloc((size_t)ld * ld, sizeof(double)), *rat2 = calloc((size_t)ld * ld, sizeof(double));
+    double *y = calloc((size_t)ld * ld, sizeof(double)), *d = calloc((size_t)ld * ld, sizeof(double));
+    cplx *uval = calloc((size_t)nquad * ld, sizeof(cplx)), *uder = calloc((size_t)nquad * ld, sizeof(cplx));
+    cplx *epm = malloc(sizeof(cplx) * (2 * nterms + 3)), *eph = epm + nterms + 1;
+    /* evalall2 */
+    {
+        double cbeta = cos(beta), sbeta = -sin(beta);
+        ylgndrini_r(nterms, rat1, rat2);
+        int nquad2 = nquad / 2, nquad4 = nquad2 / 2 + 1;
+        for (int jj = 1; jj <= nquad4; jj++) {
+            for (int pass = 0; pass < 2; pass++) {
+                int col;
+                double ctheta, stheta, cphi, sphi;
+                if (pass == 0) {
+                    col = jj;
+                    ctheta = ct[jj - 1]; stheta = stt[jj - 1]; cphi = cph[jj - 1]; sphi = sph[jj - 1];
+                    ylgndru2sf_r(nterms, ctheta, y, d, rat1, rat2);
+                } else {
+                    int reflect = !(jj == 1 || (jj == nquad4 && nquad2 % 2 == 0));
+                    if (!reflect) break;
+                    col = nquad2 - jj + 2;
+                    ylgndr2pm_r(nterms, y, d);
+                    ctheta = -ct[jj - 1]; stheta = stt[jj - 1]; cphi = -cph[jj - 1]; sphi = sph[jj - 1];
+                }
+                double dir1 = -sbeta, dir2 = 0, dir3 = cbeta;
+                double proj2 = (cphi * ctheta) * dir1 + (sphi * ctheta) * dir2 + (-stheta) * dir3;
+                double proj1 = (-sphi) * dir1 + cphi * dir2 + 0 * dir3;
+                cplx e1 = cphi + I * sphi;
+                eph[0] = 1;
+                eph[1] = e1; eph[-1] = conj(e1);
+                for (int i = 2; i <= nterms; i++) { eph[i] = eph[i - 1] * e1; eph[-i] = conj(eph[i]); }
+                for (int n = 0; n <= nterms; n++) {
+                    cplx uv = 0, ut = 0, up = 0;
+                    for (int m = 1; m <= n; m++) {
+                        cplx z1 = eph[m] * in[EI(n, m)], z2 = eph[-m] * in[EI(n, -m)];
+                        cplx zs = z1 + z2, zd = z1 - z2;
+                        uv += Y_(n, m) * zs;
+                        ut += D_(n, m) * zs;
+                        up -= Y_(n, m) * m * zd;
+                    }
+                    uv = stheta * uv + Y_(n, 0) * in[EI(n, 0)];
+                    ut = ut + D_(n, 0) * stheta * in[EI(n, 0)];
+                    cplx v = uv, dv = ut * proj2 + up * I * proj1;
+                    uval[(size_t)n * nquad + col - 1] = v;
+                    uder[(size_t)n * nquad + col - 1] = dv;
+                    uval[(size_t)n * nquad + col - 1 + nquad / 2] = (n % 2 == 0) ? v : -v;
+                    uder[(size_t)n * nquad + col - 1 + nquad / 2] = (n % 2 == 0) ? -dv : dv;
+                }
+            }
+        }
+    }
+    /* projectonynm2 */
+    {
+        double h = 1.0 / nquad;
+        ylgndru2sf_r(nterms, 0.0, y, d, rat1, rat2);
+        cplx *av = malloc(sizeof(cplx) * 2 * nquad), *cv = av + nquad;
+        for (int n = 0; n <= nterms; n++) {
+            double dn = sqrt(2 * n + 1.0);
+            for (int i = 0; i < nquad; i++) av[i] = uval[(size_t)n * nquad + i] * dn + uder[(size_t)n * nquad + i];
+            dft_forward(nquad, av, cv);
+            for (int m = -n; m <= n; m++) {
+                cplx alpha = (m >= 0 ? cv[m] : cv[nquad + m]) * h;
+                int am = m < 0 ? -m : m;
+                out[EI(n, m)] = alpha / (Y_(n, am) * dn - D_(n, am));
+            }
+        }
+        free(av);
+    }
+#undef R1
+#undef R2
+#undef Y_
+#undef D_
+    free(ct); free(rat1); free(rat2); free(y); free(d); free(uval); free(uder); free(epm);
+}
+
+void oracle_rotviaproj(double beta, int nterms, const cplx *in, cplx *out) { rotviaproj(beta, nterms, in, out); }
+
+void oracle_rotviarecur(double beta, int nterms, const cplx *in, cplx *out)
+{
+    size_t sz = (size_t)(nterms + 1) * (nterms + 1) * (2 * nterms + 1);
+    double *r = malloc(sz * sizeof(double));
+    rot_init(r, nterms, beta);
+    rot_apply(r, nterms, nterms, in, out);
+    free(r);
+}
+
 /* One translation: phases e^{i m phi}, rotation by theta, z-shift, rotation
  * by -theta, phases e^{-i m phi}, added into `out`: h3dmpmpquad0
  * (src/h3dtrans.f:211-363), h3dmplocquad_trunc0 (:1229-1376) and
@@ -774,11 +979,17 @@ static void htranslate(int kind, cplx zk, const double *c_from, const double *c_
     for (int l = 1; l <= pm; l++) { e[l + 1] = e[l] * e[1]; e[-1 - l] = conj(e[l + 1]); }
     cplx *a = calloc(K, sizeof(cplx)), *b = calloc(K, sizeof(cplx)), *cz = calloc(K, sizeof(cplx));
     for (int l = 0; l <= nin; l++) for (int m = -l; m <= l; m++) a[EI(l, m)] = in[EI(l, m)] * e[m];
-    rot_apply(rotcache_get(rc, th), rc->ldm, nin, a, b);
+    /* orders >= 30 rotate by projection (rotviaprojf90), lower ones by the
+     * recursion (rotviarecur3f90): forward on the source order for M2M and
+     * M2L, on the target order for L2L; backward on the target order
+     * (src/h3dtrans.f:318, 340, 1335, 1356, 2102, 2127)                   */
+    if ((kind == 2 ? nout : nin) >= 30) rotviaproj(th, nin, a, b);
+    else rot_apply(rotcache_get(rc, th), rc->ldm, nin, a, b);
     if (kind == 0) hzshift_m2m(zk, sc1, b, nin, sc2, cz, nout, radius, d, x, w, nq);
     else if (kind == 1) hzshift_m2l(zk, sc1, b, nin, sc2, cz, nout, radius, d, x, w, nq);
     else hzshift_l2l(zk, sc1, b, nin, sc2, cz, nout, radius, d, x, w, nq);
-    rot_apply(rotcache_get(rc, -th), rc->ldm, nout, cz, a);
+    if (nout >= 30) rotviaproj(-th, nout, cz, a);
+    else rot_apply(rotcache_get(rc, -th), rc->ldm, nout, cz, a);
     for (int l = 0; l <= nout; l++) for (int m = -l; m <= l; m++) out[EI(l, m)] += e[-m] * a[EI(l, m)];
     free(em); free(a); free(b); free(cz);
 }

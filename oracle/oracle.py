@@ -277,6 +277,22 @@ def h3dterms_list2(size, zk, eps):
     return t.reshape(7, 7, 7)
 
 
+def rotviaproj(beta, nterms, coef):
+    """Rotation about the y axis by projection (rotviaprojf90); coef: (nterms+1)^2 complex."""
+    a = np.ascontiguousarray(coef, dtype=np.complex128)
+    out = np.zeros((nterms + 1) ** 2, np.complex128)
+    lib().oracle_rotviaproj(c_dbl(beta), c_int(nterms), _p(a), _p(out))
+    return out
+
+
+def rotviarecur(beta, nterms, coef):
+    """The same rotation by the three-term recursion (rotviarecur3p_init / _apply)."""
+    a = np.ascontiguousarray(coef, dtype=np.complex128)
+    out = np.zeros((nterms + 1) ** 2, np.complex128)
+    lib().oracle_rotviarecur(c_dbl(beta), c_int(nterms), _p(a), _p(out))
+    return out
+
+
 def legewhts(n):
     x = np.zeros(n); w = np.zeros(n)
     lib().oracle_legewhts(c_int(n), _p(x), _p(w))

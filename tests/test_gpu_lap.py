@@ -356,10 +356,12 @@ def test_pageable_host_arrays_equal_pinned_and_device(F, kernel):
         assert np.array_equal(a, c.cpu().numpy())
 
 
-@pytest.mark.parametrize("mode", [1, 2])
-@pytest.mark.parametrize("geom,iprec", [("cube", 1), ("sphere", 0), ("plummer", -1)])
+@pytest.mark.parametrize("mode", [1, 2, 3])
+@pytest.mark.parametrize("geom,iprec", [("cube", 1), ("sphere", 0), ("plummer", -1), ("cube", 2), ("plummer", 2)])
 def test_m2l_forms_agree_with_oracle(F, mode, geom, iprec):
-    """Rotate-shift-rotate (mode 1) and dense per-offset operators (mode 2) both match the oracle."""
+    """Rotate-shift-rotate with its products on the FP64 tensor cores (mode 1), dense per-offset
+    operators (mode 2, orders <= 16, else the rotations) and rotate-shift-rotate on the CUDA cores
+    (mode 3) all match the oracle."""
     rng = np.random.default_rng(zlib.crc32(('m2l%s%d%d' % (geom, iprec, mode)).encode()))
     n, m = 20000, 5000
     src = geometry(geom, n, rng)

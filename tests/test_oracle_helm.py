@@ -169,3 +169,19 @@ def test_helmholtz_golden_fixture_reproduces():
     for a, b in ((pot, "pot"), (fld, "fld"), (pt, "pottarg"), (ft, "fldtarg")):
         assert rel(a[:100], d[b]) < 1e-12
         assert rel(a[:100], d["d" + b]) < EPS[1]
+
+
+@pytest.mark.parametrize("p", [12, 30, 31, 40, 67])
+def test_rotation_by_projection_matches_recursion_and_is_unitary(p):
+    """rotviaprojf90 (the reference's rotation for orders >= 30, src/rotproj.f:883) and the
+    recursion of rotviarecur3 give the same rotation where the recursion is stable; the
+    projection preserves the norm (the rotation is unitary) and -beta undoes +beta at every
+    order, including those where the recursion drifts."""
+    rng = np.random.default_rng(p)
+    a = rng.normal(size=(p + 1) ** 2) + 1j * rng.normal(size=(p + 1) ** 2)
+    for beta in (0.3, -1.1, 2.5):
+        x = O.rotviaproj(beta, p, a)
+        assert abs(np.linalg.norm(x) - np.linalg.norm(a)) < 1e-13 * np.linalg.norm(a)
+        assert rel(O.rotviaproj(-beta, p, x), a) < 1e-13
+        if p <= 40:
+            assert rel(x, O.rotviarecur(beta, p, a)) < 1e-12
