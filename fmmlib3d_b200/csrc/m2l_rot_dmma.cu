@@ -14,18 +14,21 @@
 //   back rotation, degree n:     E[r][n, m]   = sum_m' X0[r][n, m'] D_n[m][m']
 // (D, Z real: the real and imaginary rows share every B fragment.)  The work
 // of each product is cut into tasks of one degree (order) and 8 output
-// columns, dealt to the 8 warps round robin; the back rotation's tasks are
+// columns, dealt to the 16 warps round robin; the back rotation's tasks are
 // dealt the same way for every slot, so each warp keeps the running sums of
 // its tasks (8 targets x 8 coefficients) in registers across all slots and
-// adds them into the local expansions once at the end.  Each task loads its
-// rotation-matrix column block from L2 into registers before its MMAs.
-// Orders up to kRdMaxP (28): two 16-row expansion buffers in shared memory.
+// adds them into the local expansions once at the end.  A rotation task loads
+// its B fragments (a column block of D_n, from L2) into registers before its
+// MMAs; z-shift B fragments are formed from the binomial table (L1) and the
+// powers of rt.  Orders up to kRdMaxP (28): two 16-row expansion buffers in
+// shared memory, one CTA of 16 warps per SM.
 #include "lap_kernels.cuh"
 
 namespace fmm {
 
-constexpr int kRdThreads = 256;     // 8 warps
-constexpr int kRdMaxTasks = 16;     // back-rotation tasks per warp (orders <= 28: at most 16)
+constexpr int kRdWarps = 16;
+constexpr int kRdMaxP = 28;
+constexpr int kRdMaxTasks = 8;      // back-rotation tasks per warp (orders <= 28: at most 120 tasks)
 constexpr int kRdMaxKs = 15;        // K steps of one degree (2 * 28 + 1 = 57 columns: 15 steps of 4)
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
@@ -35,11 +38,14 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-// row stride of the expansion buffers: >= (p+1)^2 and = 4 (mod 16) doubles, so
-// that the 8 rows x 4 doubles of an A fragment fall into two bank wavefronts
+// Row stride of the expansion buffers: at least (p+1)^2 + 4 (the A fragments
+// of a degree's last K step read up to 3 entries past the degree; those meet
+// zero B entries and are finite, the buffers being cleared at the start) and
+// = 4 (mod 16) doubles, so that the 8 rows x 4 doubles of an A fragment fall
+// into two bank wavefronts.
 __host__ __device__ inline int rd_ld(int p)
 {
-    const int nc = (p + 1) * (p + 1);
+    const int nc = (p + 1) * (p + 1) + 4;
     return nc + ((4 - nc % 16) + 16) % 16;
 }
 
@@ -51,7 +57,53 @@ __host__ __device__ inline int rd_ntasks(int p)
     return t;
 }
 
-__global__ void __launch_bounds__(kRdThreads, 1)
+// z-shift tasks (order m, block of 8 target degrees) of truncation p
+__host__ __device__ inline int rd_nz(int p)
+{
+    int t = 0;
+    for (int m = -p; m <= p; m++) t += (p + 1 - (m < 0 ? -m : m) + 7) / 8;
+    return t;
+}
+
+// One rotation task: rows fr (real) and 8 + fr (imaginary) of X, degree n
+// (columns e0 .. e0 + w - 1), times the column block `col` of the (2n+1)^2
+// matrix Dn, read as Dn[k * w + col] (forward, TR = false) or Dn[col * w + k]
+// (transposed, TR = true).  KS: K steps held in registers (>= nks); the A
+// loads of the last step may run past the degree into finite entries that
+// meet zero B entries.
+template <int KS, bool TR>
+__device__ __forceinline__ void rd_rot_task(const double *X, int LD, int fr, int fq, int w, int e0, int col,
+                                            const double *Dn, double &c0r, double &c1r, double &c0i, double &c1i)
+{
+    const int nks = (w + 3) / 4;
+    double bf[KS];
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        const int kk = 4 * ks + fq;
+        bf[ks] = (ks < nks && kk < w && col < w) ? (TR ? Dn[col * w + kk] : Dn[kk * w + col]) : 0.0;
+    }
+    const double *xr = X + fr * LD + e0 + fq, *xi = X + (8 + fr) * LD + e0 + fq;
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        if (ks >= nks) break;
+        dmma(c0r, c1r, xr[4 * ks], bf[ks]);
+        dmma(c0i, c1i, xi[4 * ks], bf[ks]);
+    }
+}
+
+template <bool TR>
+__device__ __forceinline__ void rd_rot(const double *X, int LD, int fr, int fq, int n, int col, const double *Dn,
+                                       double &c0r, double &c1r, double &c0i, double &c1i)
+{
+    const int w = 2 * n + 1, e0 = n * n;
+    c0r = c1r = c0i = c1i = 0.0;
+    if (w <= 16) rd_rot_task<4, TR>(X, LD, fr, fq, w, e0, col, Dn, c0r, c1r, c0i, c1i);
+    else if (w <= 32) rd_rot_task<8, TR>(X, LD, fr, fq, w, e0, col, Dn, c0r, c1r, c0i, c1i);
+    else if (w <= 48) rd_rot_task<12, TR>(X, LD, fr, fq, w, e0, col, Dn, c0r, c1r, c0i, c1i);
+    else rd_rot_task<kRdMaxKs, TR>(X, LD, fr, fq, w, e0, col, Dn, c0r, c1r, c0i, c1i);
+}
+
+__global__ void __launch_bounds__(32 * kRdWarps, 1)
     k_m2l_rot_dmma(const Tile *tiles, const int *grouped, const Slot *slots, TreeView tv, int p, const double *rot,
                    const double *dc, int lddc, const double2 *in, double2 *out, int prune)
 {
@@ -62,15 +114,25 @@ __global__ void __launch_bounds__(kRdThreads, 1)
     double *pw = (double *)(eph + (p + 1));          // rt^-(l+1), l = 0..2p+2
     short *tn = (short *)(pw + 2 * p + 3);           // task -> degree
     short *tb = tn + NT;                             // task -> column block
+    short *em = tb + NT;                             // coefficient index -> m
+    short *zt = em + NC;                             // z-shift tasks of the slot's truncation: (m + p) << 8 | block
     __shared__ int tg[8], sv[8];
-    __shared__ int anyv;
+    __shared__ int anyv, zpt, nzs;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int fr = lane >> 2, fq = lane & 3;          // fragment row (target) and quad index
     const Tile tile = tiles[blockIdx.x];
     if (tid < 8) tg[tid] = tid < tile.count ? grouped[tile.first + tid] : -1;
     for (int t = 0, n = 0; n <= p; n++)
         for (int b = 0; b < (2 * n + 8) / 8; b++, t++)
-            if (t % kRdThreads == tid) { tn[t] = (short)n; tb[t] = (short)b; }
+            if (t % (32 * kRdWarps) == tid) { tn[t] = (short)n; tb[t] = (short)b; }
+    for (int e = tid; e < NC; e += 32 * kRdWarps) {
+        int n = (int)sqrtf((float)e);
+        while (n * n > e) n--;
+        while ((n + 1) * (n + 1) <= e) n++;
+        em[e] = (short)(e - n * n - n);
+    }
+    for (int i = tid; i < 32 * LD; i += 32 * kRdWarps) X0[i] = 0.0;   // X0 and X1
+    if (tid == 0) zpt = -1;
     const size_t csz = rot_class_size(p);
     double acc[kRdMaxTasks][4];   // back-rotation running sums: (re, im) of columns oc, oc + 1
 #pragma unroll
@@ -98,23 +160,31 @@ __global__ void __launch_bounds__(kRdThreads, 1)
         if (tid == 32) {
             double2 e1 = cmk(sl.ex, sl.ey), e = cmk(1, 0);
             for (int m = 0; m <= p; m++) { eph[m] = e; e = cmul(e, e1); }
+        }
+        if (tid == 64) {
             const double ir = 1.0 / sl.rt;
             double x = ir;
             for (int l = 0; l <= 2 * p + 2; l++) { pw[l] = x; x *= ir; }
+        }
+        if (tid == 96 && zpt != sl.pt) {
+            int t = 0;
+            for (int m = -sl.pt; m <= sl.pt; m++) {
+                const int L = sl.pt + 1 - (m < 0 ? -m : m);
+                for (int b = 0; b < (L + 7) / 8; b++) zt[t++] = (short)(((m + p) << 8) | b);
+            }
+            nzs = t;
+            zpt = sl.pt;
         }
         __syncthreads();
         if (!anyv) continue;
         const int pt = sl.pt, R = (pt + 1) * (pt + 1);
         // gather, times e^{i m phi}: real parts to rows 0..7, imaginary parts to rows 8..15
-        for (int i = tid; i < 8 * R; i += kRdThreads) {
+        for (int i = tid; i < 8 * R; i += 32 * kRdWarps) {
             const int k = i / R, e = i - k * R;
             const int sb = sv[k];
             double2 v = cmk(0, 0);
             if (sb >= 0) {
-                int n = (int)sqrtf((float)e);
-                while (n * n > e) n--;
-                while ((n + 1) * (n + 1) <= e) n++;
-                const int m = e - n * n - n;
+                const int m = em[e];
                 const double2 ph = m >= 0 ? eph[m] : cconj(eph[-m]);
                 v = cmul(in[(size_t)sb * NC + e], ph);
             }
@@ -123,28 +193,13 @@ __global__ void __launch_bounds__(kRdThreads, 1)
         }
         __syncthreads();
         const double *Rc = rot + csz * sl.cls;
-        const int NTs = rd_ntasks(pt);
+        const int NTs = rd_ntasks(pt), nz = nzs;
         // forward rotation
-        for (int t = warp; t < NTs; t += 8) {
-            const int n = tn[t], b = tb[t], w = 2 * n + 1, e0 = n * n, nks = (w + 3) / 4;
+        for (int t = warp; t < NTs; t += kRdWarps) {
+            const int n = tn[t], b = tb[t], w = 2 * n + 1, e0 = n * n;
             const double *Dn = Rc + (size_t)n * (4 * n * n - 1) / 3;
-            const int col = 8 * b + fr;
-            double bf[kRdMaxKs];
-#pragma unroll
-            for (int ks = 0; ks < kRdMaxKs; ks++) {
-                const int kk = 4 * ks + fq;
-                bf[ks] = (ks < nks && kk < w && col < w) ? Dn[kk * w + col] : 0.0;
-            }
-            double c0r = 0, c1r = 0, c0i = 0, c1i = 0;
-#pragma unroll
-            for (int ks = 0; ks < kRdMaxKs; ks++) {
-                if (ks >= nks) break;
-                const int kk = 4 * ks + fq;
-                const double ar = kk < w ? X0[fr * LD + e0 + kk] : 0.0;
-                const double ai = kk < w ? X0[(8 + fr) * LD + e0 + kk] : 0.0;
-                dmma(c0r, c1r, ar, bf[ks]);
-                dmma(c0i, c1i, ai, bf[ks]);
-            }
+            double c0r, c1r, c0i, c1i;
+            rd_rot<false>(X0, LD, fr, fq, n, 8 * b + fr, Dn, c0r, c1r, c0i, c1i);
             const int oc = 8 * b + 2 * fq;
             if (oc < w) { X1[fr * LD + e0 + oc] = c0r; X1[(8 + fr) * LD + e0 + oc] = c0i; }
             if (oc + 1 < w) { X1[fr * LD + e0 + oc + 1] = c1r; X1[(8 + fr) * LD + e0 + oc + 1] = c1i; }
@@ -152,42 +207,37 @@ __global__ void __launch_bounds__(kRdThreads, 1)
         __syncthreads();
         // z-shift, order by order: out (j, m) = sum_l c(j, l, m) in (l, m), j, l in |m| .. pt,
         // c = (-1)^(j+|m|) sqrt(C(l+j, l-m) C(l+j, l+m)) / rt^(l+j+1)
-        {
-            int t = 0;
-            for (int m = -pt; m <= pt; m++) {
-                const int am = m < 0 ? -m : m, L = pt + 1 - am, nb = (L + 7) / 8, nks = (L + 3) / 4;
-                for (int b = 0; b < nb; b++, t++) {
-                    if ((t & 7) != warp) continue;
-                    const int j = am + 8 * b + fr;   // this lane's B column (target degree)
-                    const double sg = ((j + am) & 1) ? -1.0 : 1.0;
-                    double c0r = 0, c1r = 0, c0i = 0, c1i = 0;
-                    for (int ks = 0; ks < nks; ks++) {
-                        const int l = am + 4 * ks + fq;   // this lane's K index (source degree)
-                        double bz = 0.0, ar = 0.0, ai = 0.0;
-                        if (l <= pt) {
-                            const int ei = l * l + l + m;
-                            ar = X1[fr * LD + ei];
-                            ai = X1[(8 + fr) * LD + ei];
-                            if (j <= pt) {
-                                const int lj = l + j;
-                                bz = sg * pw[lj] * dc[lj * lddc + (l - m)] * dc[lj * lddc + (l + m)];
-                            }
-                        }
-                        dmma(c0r, c1r, ar, bz);
-                        dmma(c0i, c1i, ai, bz);
-                    }
-                    const int j0 = am + 8 * b + 2 * fq;
-                    if (j0 <= pt) {
-                        const int eo = j0 * j0 + j0 + m;
-                        X0[fr * LD + eo] = c0r;
-                        X0[(8 + fr) * LD + eo] = c0i;
-                    }
-                    if (j0 + 1 <= pt) {
-                        const int eo = (j0 + 1) * (j0 + 1) + (j0 + 1) + m;
-                        X0[fr * LD + eo] = c1r;
-                        X0[(8 + fr) * LD + eo] = c1i;
+        for (int t = warp; t < nz; t += kRdWarps) {
+            const int m = (zt[t] >> 8) - p, b = zt[t] & 255;
+            const int am = m < 0 ? -m : m, L = pt + 1 - am, nks = (L + 3) / 4;
+            const int j = am + 8 * b + fr;   // this lane's B column (target degree)
+            const double sg = ((j + am) & 1) ? -1.0 : 1.0;
+            double c0r = 0, c1r = 0, c0i = 0, c1i = 0;
+            for (int ks = 0; ks < nks; ks++) {
+                const int l = am + 4 * ks + fq;   // this lane's K index (source degree)
+                double bz = 0.0, ar = 0.0, ai = 0.0;
+                if (l <= pt) {
+                    const int ei = l * l + l + m;
+                    ar = X1[fr * LD + ei];
+                    ai = X1[(8 + fr) * LD + ei];
+                    if (j <= pt) {
+                        const int lj = l + j;
+                        bz = sg * pw[lj] * dc[lj * lddc + (l - m)] * dc[lj * lddc + (l + m)];
                     }
                 }
+                dmma(c0r, c1r, ar, bz);
+                dmma(c0i, c1i, ai, bz);
+            }
+            const int j0 = am + 8 * b + 2 * fq;
+            if (j0 <= pt) {
+                const int eo = j0 * j0 + j0 + m;
+                X0[fr * LD + eo] = c0r;
+                X0[(8 + fr) * LD + eo] = c0i;
+            }
+            if (j0 + 1 <= pt) {
+                const int eo = (j0 + 1) * (j0 + 1) + (j0 + 1) + m;
+                X0[fr * LD + eo] = c1r;
+                X0[(8 + fr) * LD + eo] = c1i;
             }
         }
         __syncthreads();
@@ -195,27 +245,12 @@ __global__ void __launch_bounds__(kRdThreads, 1)
         const bool live = sv[fr] >= 0;
 #pragma unroll
         for (int lt = 0; lt < kRdMaxTasks; lt++) {
-            const int t = 8 * lt + warp;
+            const int t = kRdWarps * lt + warp;
             if (t >= NTs) break;
-            const int n = tn[t], b = tb[t], w = 2 * n + 1, e0 = n * n, nks = (w + 3) / 4;
+            const int n = tn[t], b = tb[t], w = 2 * n + 1;
             const double *Dn = Rc + (size_t)n * (4 * n * n - 1) / 3;
-            const int col = 8 * b + fr;
-            double bf[kRdMaxKs];
-#pragma unroll
-            for (int ks = 0; ks < kRdMaxKs; ks++) {
-                const int kk = 4 * ks + fq;
-                bf[ks] = (ks < nks && kk < w && col < w) ? Dn[col * w + kk] : 0.0;
-            }
-            double c0r = 0, c1r = 0, c0i = 0, c1i = 0;
-#pragma unroll
-            for (int ks = 0; ks < kRdMaxKs; ks++) {
-                if (ks >= nks) break;
-                const int kk = 4 * ks + fq;
-                const double ar = kk < w ? X0[fr * LD + e0 + kk] : 0.0;
-                const double ai = kk < w ? X0[(8 + fr) * LD + e0 + kk] : 0.0;
-                dmma(c0r, c1r, ar, bf[ks]);
-                dmma(c0i, c1i, ai, bf[ks]);
-            }
+            double c0r, c1r, c0i, c1i;
+            rd_rot<true>(X0, LD, fr, fq, n, 8 * b + fr, Dn, c0r, c1r, c0i, c1i);
             if (live) {
                 const int oc = 8 * b + 2 * fq;
                 const int m0 = oc - n, m1 = oc + 1 - n;
@@ -240,7 +275,7 @@ __global__ void __launch_bounds__(kRdThreads, 1)
     if (t < 0) return;
 #pragma unroll
     for (int lt = 0; lt < kRdMaxTasks; lt++) {
-        const int ti = 8 * lt + warp;
+        const int ti = kRdWarps * lt + warp;
         if (ti >= NT) break;
         const int n = tn[ti], b = tb[ti], w = 2 * n + 1, oc = 8 * b + 2 * fq;
         double2 *o = out + (size_t)t * NC + n * n;
@@ -249,7 +284,7 @@ __global__ void __launch_bounds__(kRdThreads, 1)
     }
 }
 
-bool m2l_rot_dmma_supported(int p) { return p >= 1 && p <= 28 && rd_ntasks(p) <= 8 * kRdMaxTasks; }
+bool m2l_rot_dmma_supported(int p) { return p >= 1 && p <= kRdMaxP && rd_ntasks(p) <= kRdWarps * kRdMaxTasks; }
 
 void launch_m2l_rot_dmma(const Tile *tiles, int ntiles, const int *grouped, const Slot *slots, const TreeView &tv,
                          int p, const double *rot, const double *dc, int lddc, const double2 *in, double2 *out,
@@ -257,10 +292,11 @@ void launch_m2l_rot_dmma(const Tile *tiles, int ntiles, const int *grouped, cons
 {
     if (ntiles == 0 || !st.ok()) return;
     const size_t sm = sizeof(double) * (32 * (size_t)rd_ld(p)) + sizeof(double2) * (p + 1) +
-                      sizeof(double) * (2 * p + 3) + sizeof(short) * 2 * rd_ntasks(p);
+                      sizeof(double) * (2 * p + 3) +
+                      sizeof(short) * (2 * rd_ntasks(p) + (p + 1) * (p + 1) + rd_nz(p));
     FMM_TRY(st, cudaFuncSetAttribute(k_m2l_rot_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     if (!st.ok()) return;
-    k_m2l_rot_dmma<<<ntiles, kRdThreads, sm, s>>>(tiles, grouped, slots, tv, p, rot, dc, lddc, in, out, prune);
+    k_m2l_rot_dmma<<<ntiles, 32 * kRdWarps, sm, s>>>(tiles, grouped, slots, tv, p, rot, dc, lddc, in, out, prune);
     FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
