@@ -89,7 +89,7 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
         }
     }
     if (ntop == 0) return 8;
-    unsigned long long fl[2] = {0ull, 0ull};  // rescale events at index i <= 127
+    unsigned long long fl[4] = {0ull, 0ull, 0ull, 0ull};  // rescale events at index i <= 255
     if (ntop <= nt + 1) f[ntop * fs] = cmk(0, 0);
     double2 a = cmk(0, 0), b = cmk(1, 0);    // f(i+1), f(i)
     for (int i = ntop - 1; i >= 1; i--) {
@@ -97,7 +97,7 @@ __device__ int bess_dev(int nt, double2 z, double scale, double2 *f, double2 *fd
         if (cabs2(c) > ub) {
             b = cscal(ubinv, b);
             c = cscal(ubinv, c);
-            if (i < 128) fl[i >> 6] |= 1ull << (i & 63);
+            if (i < 256) fl[i >> 6] |= 1ull << (i & 63);
         }
         if (i <= nt + 1) f[i * fs] = b;
         a = b;
@@ -332,6 +332,7 @@ void build_hz(int nblk, const HZBlock *d_blk, const HZBlock *h_blk, const double
 // z-shift operator of the slot (per |m| dense block), D(theta)^T and
 // e^{-i m phi}, and accumulates in shared memory.
 constexpr int kHTransThreads = 256;
+constexpr size_t kHTransSmemMax = 200 * 1024;   // larger buffers go to global scratch
 
 __device__ __forceinline__ int hsrc_of(int kind, const TreeView &tv, int t, const HSlot &sl)
 {
@@ -352,21 +353,27 @@ __device__ __forceinline__ int deg_of(int e)
     return n;
 }
 
-template <int KIND, int KT>
-__global__ void __launch_bounds__(kHTransThreads) k_htranslate(const Tile *tiles, const int *grouped,
+// gs: null, or global scratch of gridDim.x x 3 KT (pmax+1)^2 entries for the
+// three expansion buffers (orders whose buffers do not fit in shared memory);
+// the CTAs then walk the tiles with a grid stride.
+template <int KIND, int KT, bool GS>
+__global__ void __launch_bounds__(kHTransThreads) k_htranslate(const Tile *tiles, int ntiles, const int *grouped,
                                                                const HSlot *slots, TreeView tv, int pmax,
                                                                const double *rot, const double2 *Z,
-                                                               const double2 *in, double2 *out, int prune)
+                                                               const double2 *in, double2 *out, int prune,
+                                                               double2 *gs)
 {
     extern __shared__ double2 sm[];
     const int NC = (pmax + 1) * (pmax + 1);
-    double2 *acc = sm;
+    double2 *acc = GS ? gs + (size_t)blockIdx.x * 3 * KT * NC : sm;
     double2 *bA = acc + (size_t)KT * NC;
     double2 *bB = bA + (size_t)KT * NC;
-    double2 *eph = bB + (size_t)KT * NC;  // e^{i m phi}, m = 0..pmax
+    double2 *eph = GS ? sm : bB + (size_t)KT * NC;  // e^{i m phi}, m = 0..pmax
     __shared__ int tg[8], sv[8];
     __shared__ int anyv;
-    const Tile tile = tiles[blockIdx.x];
+    for (int tix = blockIdx.x; tix < (GS ? ntiles : blockIdx.x + 1); tix += gridDim.x) {
+    if (GS) __syncthreads();
+    const Tile tile = tiles[tix];
     if (threadIdx.x < 8) {
         int t = threadIdx.x < tile.count ? grouped[tile.first + threadIdx.x] : -1;
         if (t >= 0 && KIND == 0 && tv.nchild[t] == 0) t = -1;
@@ -469,20 +476,28 @@ __global__ void __launch_bounds__(kHTransThreads) k_htranslate(const Tile *tiles
         if (KIND == 0) *o = acc[i];
         else *o = cadd(*o, acc[i]);
     }
+    }
 }
 
 template <int KIND>
 static void launch_htranslate_kind(const Tile *tiles, int ntiles, const int *grouped, const HSlot *slots,
                                    const TreeView &tv, int pmax, const double *rot, const double2 *Z,
-                                   const double2 *in, double2 *out, int prune, int kt, size_t sm, cudaStream_t s,
-                                   Status &st)
+                                   const double2 *in, double2 *out, int prune, int kt, size_t sm, int grid,
+                                   double2 *gs, cudaStream_t s, Status &st)
 {
 #define FMM_HTR(KTV)                                                                                           \
     do {                                                                                                       \
-        FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)sm));                                                            \
-        k_htranslate<KIND, KTV><<<ntiles, kHTransThreads, sm, s>>>(tiles, grouped, slots, tv, pmax, rot, Z, in, \
-                                                                   out, prune);                                \
+        if (gs) {                                                                                              \
+            FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV, true>,                                    \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
+            k_htranslate<KIND, KTV, true><<<grid, kHTransThreads, sm, s>>>(tiles, ntiles, grouped, slots, tv,  \
+                                                                           pmax, rot, Z, in, out, prune, gs);  \
+        } else {                                                                                               \
+            FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV, false>,                                   \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
+            k_htranslate<KIND, KTV, false><<<grid, kHTransThreads, sm, s>>>(tiles, ntiles, grouped, slots, tv, \
+                                                                            pmax, rot, Z, in, out, prune, gs); \
+        }                                                                                                      \
         FMM_COUNT_LAUNCH();                                                                                    \
     } while (0)
     if (kt == 8) FMM_HTR(8);
@@ -499,9 +514,17 @@ void launch_htranslate(int kind, const Tile *tiles, int ntiles, const int *group
     if (ntiles == 0 || !st.ok()) return;
     int NC = (pmax + 1) * (pmax + 1);
     size_t sm = (size_t)3 * kt * NC * sizeof(double2) + (pmax + 1) * sizeof(double2);
-    if (kind == 0) launch_htranslate_kind<0>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
-    else if (kind == 1) launch_htranslate_kind<1>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
-    else launch_htranslate_kind<2>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, s, st);
+    int grid = ntiles;
+    DBuf<double2> gs;
+    if (sm > kHTransSmemMax) {
+        // high orders: the three buffers in global scratch, one slice per CTA of a grid-stride launch
+        grid = std::min(ntiles, 2 * 148);
+        if (!gs.alloc((size_t)grid * 3 * kt * NC, s, st)) return;
+        sm = (pmax + 1) * sizeof(double2);
+    }
+    if (kind == 0) launch_htranslate_kind<0>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, grid, gs.p, s, st);
+    else if (kind == 1) launch_htranslate_kind<1>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, grid, gs.p, s, st);
+    else launch_htranslate_kind<2>(tiles, ntiles, grouped, slots, tv, pmax, rot, Z, in, out, prune, kt, sm, grid, gs.p, s, st);
     FMM_LAUNCH_CHECK(st);
 }
 
@@ -800,12 +823,15 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
         k_hform<IR, C, D, CHV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);           \
         FMM_COUNT_LAUNCH();                                                                                   \
     } while (0)
-    // chunks of 8 or 16 sources; 4 at orders whose staging would not fit
-    // (above ~54).  The chunk size does not change the order of any sum.
+    // chunks of 8 or 16 sources; 4, 2 or 1 at orders whose staging would not
+    // fit (above ~54, ~80, ~110).  The chunk size does not change the order of
+    // any sum.
 #define FMM_HF_FIT(IR, C, D, CHV)                                                                             \
     do {                                                                                                      \
         if (sizeof(double) * HFormSmem<CHV, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, CHV);           \
-        else FMM_HF(IR, C, D, 4);                                                                             \
+        else if (sizeof(double) * HFormSmem<4, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, 4);          \
+        else if (sizeof(double) * HFormSmem<2, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, 2);          \
+        else FMM_HF(IR, C, D, 1);                                                                             \
     } while (0)
     if (irreg) {
         if (c && d) FMM_HF_FIT(true, true, true, 8);
@@ -831,14 +857,16 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
 // Legendre column recurrence in registers.
 constexpr int kHEvalThreads = 128;
 
-__global__ void __launch_bounds__(kHEvalThreads) k_heval(const int *leaves, TreeView tv, const double *sx,
+// T threads per CTA: 128, or 32 at orders whose radial columns of 128 points
+// would not fit in shared memory beside the coefficients.
+template <int T>
+__global__ void __launch_bounds__(T) k_heval(const int *leaves, TreeView tv, const double *sx,
                                                         const double *sy, const double *sz, const double *tx,
                                                         const double *ty, const double *tz, HLevels lv, int NC,
                                                         double2 zk, const double2 *mpole, const double2 *local,
                                                         OutSoA outs, OutSoA outt, int do_src, int do_trg)
 {
     extern __shared__ double2 hsm[];
-    constexpr int T = kHEvalThreads;
     const int b = leaves[blockIdx.x];
     const int blev = tv.level[b];
     const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
@@ -961,9 +989,17 @@ void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const doub
     htab_init(s, st);
     int pm = max_p(lv);
     size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * kHEvalThreads);
-    FMM_TRY(st, cudaFuncSetAttribute(k_heval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_heval<<<nleaves, kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
-                                               outt, do_src, do_trg); FMM_COUNT_LAUNCH();
+    if (sm <= 226 * 1024) {
+        FMM_TRY(st, cudaFuncSetAttribute(k_heval<kHEvalThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_heval<kHEvalThreads><<<nleaves, kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk,
+                                                                  mpole, local, outs, outt, do_src, do_trg);
+    } else {
+        sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * 32);
+        FMM_TRY(st, cudaFuncSetAttribute(k_heval<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_heval<32><<<nleaves, 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
+                                            outt, do_src, do_trg);
+    }
+    FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
 

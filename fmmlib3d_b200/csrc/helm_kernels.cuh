@@ -10,7 +10,10 @@
 
 namespace fmm {
 
-constexpr int kHelmMaxP = 60;
+// Largest Helmholtz expansion order: the evaluation kernel keeps a box's
+// (p+1)^2 coefficients and 32 points' radial columns in shared memory.
+constexpr int kHelmMaxP = 104;
+static_assert(kHelmMaxP <= kRotTabP, "rotation tables shorter than the Helmholtz orders");
 
 // Expansion order and scale of every level.
 struct HLevels {

@@ -80,6 +80,10 @@ void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w);
 // Rotation matrices about the y axis for each class (cos, sin of theta).
 void build_rotations(int p, int ncls, const double *d_cs, double *d_rot, cudaStream_t s, Status &st);
 
+// Largest order of the rotation matrices (build_rotations): the length of its
+// recurrence tables.
+constexpr int kRotTabP = 130;
+
 __host__ __device__ inline size_t rot_class_size(int p) { return (size_t)(p + 1) * (2 * p + 1) * (2 * p + 3) / 3; }
 
 // FP64 rotate-shift-rotate M2L with its products on the FP64 tensor cores

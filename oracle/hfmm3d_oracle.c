@@ -837,18 +837,36 @@ static void ylgndr2pm_r(int nterms, double *y, double *d)
 }
 
 /* Forward DFT c_k = sum_j x_j e^{-2 pi i jk/n}, the transform of FFTPACK's
- * zfftf (src/dfft.f:942; the reference computes it by a mixed-radix FFT). */
+ * zfftf (src/dfft.f:942; the reference computes it by a mixed-radix FFT):
+ * here a textbook recursive mixed-radix (2, 3, 5) decimation in time, n being
+ * 2^a 3^b 5^c (next235).  tw[j] = e^{-2 pi i j / N} for the full size N.    */
+static void fft235(int n, const cplx *x, int stride, cplx *out, const cplx *tw, int N)
+{
+    if (n == 1) { out[0] = x[0]; return; }
+    const int r = (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : 5, m = n / r, step = N / n;
+    cplx *sub = malloc(sizeof(cplx) * n);
+    for (int q = 0; q < r; q++) fft235(m, x + (size_t)q * stride, stride * r, sub + (size_t)q * m, tw, N);
+    for (int k = 0; k < m; k++)
+        for (int s2 = 0; s2 < r; s2++) {
+            cplx acc = 0;
+            for (int q = 0; q < r; q++) {
+                long e = ((long)q * (k + (long)m * s2)) % n;
+                acc += sub[(size_t)q * m + k] * tw[e * step];
+            }
+            out[k + (size_t)m * s2] = acc;
+        }
+    free(sub);
+}
+
 static void dft_forward(int n, const cplx *x, cplx *c)
 {
+    cplx *tw = malloc(sizeof(cplx) * n);
     for (int k = 0; k < n; k++) {
-        cplx s = 0;
-        for (int j = 0; j < n; j++) {
-            long jk = ((long)j * k) % n;
-            double a = -2 * M_PI * (double)jk / n;
-            s += x[j] * (cos(a) + I * sin(a));
-        }
-        c[k] = s;
+        double a = -2 * M_PI * (double)k / n;
+        tw[k] = cos(a) + I * sin(a);
     }
+    fft235(n, x, 1, c, tw, n);
+    free(tw);
 }
 
 /* rotviaproj0 (src/rotproj.f:152-219) with getmeridian (:222-283), evalall2

@@ -113,6 +113,31 @@ def test_hfmm_parity_remaining_iprec(F, geom, iprec, zk, n, m):
     check_against_oracle(F, iprec, zk, src, trg, q, ds, dv, rng)
 
 
+@pytest.mark.parametrize("zk,iprec,order", [(40 * np.pi, 2, 80), (48 * np.pi, 2, 92), (55 * np.pi, 1, 93)])
+def test_hfmm_high_orders(F, zk, iprec, order):
+    """Expansion orders above 60 (20 to 27 wavelengths across the sphere): the translation
+    buffers move to global scratch, the evaluation kernel runs 32 points per CTA and the
+    P2M/P2L staging takes smaller chunks; results still match the oracle and the direct sum."""
+    rng = np.random.default_rng(zlib.crc32(('high%d%d' % (iprec, order)).encode()))
+    n = 8000
+    src = geometry("sphere", n, rng)
+    q, ds, dv = strengths(rng, n)
+    oier, _, _, _, _, nts = O.hfmm3dparttarg(iprec, zk, src, q, nterms=True)
+    assert max(nts[2:]) == order
+    check_against_oracle(F, iprec, zk, src, None, q, None, None, rng)
+
+
+def test_hfmm_order_above_the_limit_is_refused(F):
+    """Orders above 104 return ier 16 with a message, outputs untouched (the reference runs to 1000)."""
+    rng = np.random.default_rng(77)
+    n = 6000
+    src = geometry("sphere", n, rng)
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ier, pot, fld, _, _ = F.hfmm3dparttarg(1, 70 * np.pi, src, 1, q, 0, None, None, 1, 1)
+    assert ier == 16
+    assert "expansion order" in F.last_error()
+
+
 def test_hfmm_flags_and_coincident_points(F):
     """As for Laplace: flags other than 1 are off (src/hfmm3dpart.f:601-617), and a
     target on top of a source gets a non-finite value (no guard), nothing else."""
