@@ -1070,10 +1070,25 @@ void oracle_translate(int kind, const double *c_from, const double *c_to, const 
 /* lfmm3dparttarg (src/lfmm3dpart.f:138-522) with lfmm3dparttargmain
  * (:528-1169) and lfmm3d_list2 (src/lfmm3drouts.f:148-566).  `tinfo`
  * (optional) receives the wall time of the tree and of steps 1..8.        */
-void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *source, int ifcharge,
-                           const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
-                           int ifpot, cplx *pot, int iffld, cplx *fld, int ntarget, const double *target,
-                           int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg, double *tinfo)
+static double *taevalhess_ini(int nterms);
+static double *mpevalhess_ini(int nterms);
+static void taevalhess(double rscale, const double *center, const cplx *loc, int nterms, const double *targ,
+                       cplx *pot, int iffld, cplx *fld, int ifhess, cplx *hess, const double *sc);
+static void mpevalhess(double rscale, const double *center, const cplx *mp, int nterms, const double *targ,
+                       cplx *pot, int iffld, cplx *fld, int ifhess, cplx *hess, const double *sc);
+static void direct_hess_one(int ns, const double *src, int ifcharge, const cplx *charge, int ifdipole,
+                            const cplx *dipstr, const double *dipvec, const double *t, long skip, cplx h[6]);
+
+/* lfmm3dparttarg with optional Hessian outputs (ifhess / ifhesstarg, 6 per
+ * point).  Potentials and fields are computed exactly as without them; the
+ * Hessians add, at each evaluation point, the list-3 multipoles
+ * (l3dmpevalhessd_trunc), the leaf's local (l3dtaevalhessd_trunc) and the
+ * near pairs (lpotfld3dhess, lpotfld3dhess_dp), all with rscale = 1.     */
+static void lfmm_core(int *ier, int iprec, int nsource, const double *source, int ifcharge,
+                      const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
+                      int ifpot, cplx *pot, int iffld, cplx *fld, int ifhess, cplx *hess, int ntarget,
+                      const double *target, int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg,
+                      int ifhesstarg, cplx *hesstarg, double *tinfo)
 {
     *ier = 0;
     double eps = oracle_lap_eps(iprec);
@@ -1105,6 +1120,10 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
     cplx *pt = calloc((size_t)(ntarget > 0 ? ntarget : 1), sizeof(cplx));
     cplx *ft = calloc(3 * (size_t)(ntarget > 0 ? ntarget : 1), sizeof(cplx));
     cplx *mpole = calloc((size_t)nb * K, sizeof(cplx)), *local = calloc((size_t)nb * K, sizeof(cplx));
+    cplx *hs = ifhess == 1 ? calloc(6 * (size_t)nsource, sizeof(cplx)) : NULL;
+    cplx *ht = ifhesstarg == 1 ? calloc(6 * (size_t)(ntarget > 0 ? ntarget : 1), sizeof(cplx)) : NULL;
+    double *scm = (ifhess == 1 || ifhesstarg == 1) ? mpevalhess_ini(p) : NULL;
+    double *sct = (ifhess == 1 || ifhesstarg == 1) ? taevalhess_ini(p) : NULL;
 #define BX(b, f) T.box[20 * (size_t)(b) + (f)]
 #define LS(ty, b) T.lstart[ty][b]
 #define LE(ty, b) T.lstart[ty][(b) + 1]
@@ -1156,7 +1175,7 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
     tm[3] = omp_get_wtime();
     int itable[343];
     oracle_l3dterms_list2(eps, itable);
-    int ifprune = !(ifpot == 1 || iffld == 1);
+    int ifprune = !(ifpot == 1 || iffld == 1 || ifhess == 1);
     size_t rsz = (size_t)(p + 1) * (p + 1) * (2 * p + 1);
     double *rotf = malloc(rsz * 343 * sizeof(double)), *rotb = malloc(rsz * 343 * sizeof(double));
 #pragma omp parallel for
@@ -1214,15 +1233,24 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
                 const double *cj = T.center + 3 * (size_t)jb;
                 const cplx *mj = mpole + (size_t)jb * K;
                 cplx pv, fv[3];
+                cplx hv[6], ph, fh[3];
                 for (int i = BX(ib, B_SRC0); i < BX(ib, B_SRC0) + BX(ib, B_NSRC); i++) {
                     mpeval(cj, mj, p, ss + 3 * (size_t)i, &pv, fv, pp, ppd);
                     if (ifpot == 1) ps[i] += pv;
                     if (iffld == 1) { fs[3 * (size_t)i] += fv[0]; fs[3 * (size_t)i + 1] += fv[1]; fs[3 * (size_t)i + 2] += fv[2]; }
+                    if (ifhess == 1) {
+                        mpevalhess(1.0, cj, mj, p, ss + 3 * (size_t)i, &ph, 0, fh, 1, hv, scm);
+                        for (int k = 0; k < 6; k++) hs[6 * (size_t)i + k] += hv[k];
+                    }
                 }
                 for (int i = BX(ib, B_TRG0); i < BX(ib, B_TRG0) + BX(ib, B_NTRG); i++) {
                     mpeval(cj, mj, p, ts + 3 * (size_t)i, &pv, fv, pp, ppd);
                     if (ifpottarg == 1) pt[i] += pv;
                     if (iffldtarg == 1) { ft[3 * (size_t)i] += fv[0]; ft[3 * (size_t)i + 1] += fv[1]; ft[3 * (size_t)i + 2] += fv[2]; }
+                    if (ifhesstarg == 1) {
+                        mpevalhess(1.0, cj, mj, p, ts + 3 * (size_t)i, &ph, 0, fh, 1, hv, scm);
+                        for (int k = 0; k < 6; k++) ht[6 * (size_t)i + k] += hv[k];
+                    }
                 }
             }
         }
@@ -1232,16 +1260,24 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
             if (nkids(&T, ib) != 0 || BX(ib, B_LEV) < 2) continue;
             const double *cb = T.center + 3 * (size_t)ib;
             const cplx *lb = local + (size_t)ib * K;
-            cplx pv, fv[3];
+            cplx pv, fv[3], hv[6], ph, fh[3];
             for (int i = BX(ib, B_SRC0); i < BX(ib, B_SRC0) + BX(ib, B_NSRC); i++) {
                 taeval(cb, lb, p, ss + 3 * (size_t)i, &pv, fv, pp, ppd);
                 if (ifpot == 1) ps[i] += pv;
                 if (iffld == 1) { fs[3 * (size_t)i] += fv[0]; fs[3 * (size_t)i + 1] += fv[1]; fs[3 * (size_t)i + 2] += fv[2]; }
+                if (ifhess == 1) {
+                    taevalhess(1.0, cb, lb, p, ss + 3 * (size_t)i, &ph, 0, fh, 1, hv, sct);
+                    for (int k = 0; k < 6; k++) hs[6 * (size_t)i + k] += hv[k];
+                }
             }
             for (int i = BX(ib, B_TRG0); i < BX(ib, B_TRG0) + BX(ib, B_NTRG); i++) {
                 taeval(cb, lb, p, ts + 3 * (size_t)i, &pv, fv, pp, ppd);
                 if (ifpottarg == 1) pt[i] += pv;
                 if (iffldtarg == 1) { ft[3 * (size_t)i] += fv[0]; ft[3 * (size_t)i + 1] += fv[1]; ft[3 * (size_t)i + 2] += fv[2]; }
+                if (ifhesstarg == 1) {
+                    taevalhess(1.0, cb, lb, p, ts + 3 * (size_t)i, &ph, 0, fh, 1, hv, sct);
+                    for (int k = 0; k < 6; k++) ht[6 * (size_t)i + k] += hv[k];
+                }
             }
         }
         free(pp); free(ppd);
@@ -1257,7 +1293,7 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
             int jb = li == 0 ? ib : LI(1, LS(1, ib) + li - 1);
             int js0 = BX(jb, B_SRC0), jn = BX(jb, B_NSRC);
             if (jn == 0) continue;
-            cplx pv, fv[3];
+            cplx pv, fv[3], hv[6];
             if (ifpot == 1 || iffld == 1)
                 for (int i = s0; i < s0 + ns; i++) {
                     direct_one(jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0, dvs + 3 * (size_t)js0,
@@ -1265,12 +1301,24 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
                     if (ifpot == 1) ps[i] += pv;
                     if (iffld == 1) { fs[3 * (size_t)i] += fv[0]; fs[3 * (size_t)i + 1] += fv[1]; fs[3 * (size_t)i + 2] += fv[2]; }
                 }
+            if (ifhess == 1)
+                for (int i = s0; i < s0 + ns; i++) {
+                    direct_hess_one(jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                    dvs + 3 * (size_t)js0, ss + 3 * (size_t)i, jb == ib ? i - s0 : -1, hv);
+                    for (int k = 0; k < 6; k++) hs[6 * (size_t)i + k] += hv[k];
+                }
             if (ifpottarg == 1 || iffldtarg == 1)
                 for (int i = t0; i < t0 + ntg; i++) {
                     direct_one(jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0, dvs + 3 * (size_t)js0,
                                ts + 3 * (size_t)i, -1, iffldtarg, &pv, fv);
                     if (ifpottarg == 1) pt[i] += pv;
                     if (iffldtarg == 1) { ft[3 * (size_t)i] += fv[0]; ft[3 * (size_t)i + 1] += fv[1]; ft[3 * (size_t)i + 2] += fv[2]; }
+                }
+            if (ifhesstarg == 1)
+                for (int i = t0; i < t0 + ntg; i++) {
+                    direct_hess_one(jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                    dvs + 3 * (size_t)js0, ts + 3 * (size_t)i, -1, hv);
+                    for (int k = 0; k < 6; k++) ht[6 * (size_t)i + k] += hv[k];
                 }
         }
     }
@@ -1281,20 +1329,44 @@ void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *sourc
         int j = T.iz[i];
         if (ifpot == 1) pot[j] = ps[i];
         if (iffld == 1) for (int d = 0; d < 3; d++) fld[3 * (size_t)j + d] = fs[3 * (size_t)i + d];
+        if (ifhess == 1) for (int d = 0; d < 6; d++) hess[6 * (size_t)j + d] = hs[6 * (size_t)i + d];
     }
     for (int i = 0; i < ntarget; i++) {
         int j = T.iztarg[i];
         if (ifpottarg == 1) pottarg[j] = pt[i];
         if (iffldtarg == 1) for (int d = 0; d < 3; d++) fldtarg[3 * (size_t)j + d] = ft[3 * (size_t)i + d];
+        if (ifhesstarg == 1) for (int d = 0; d < 6; d++) hesstarg[6 * (size_t)j + d] = ht[6 * (size_t)i + d];
     }
 #undef BX
 #undef LS
 #undef LE
 #undef LI
     free(ss); free(ts); free(qs); free(dss); free(dvs); free(ps); free(fs); free(pt); free(ft);
-    free(mpole); free(local);
+    free(mpole); free(local); free(hs); free(ht); free(scm); free(sct);
     tree_free(&T);
+}
+
+void oracle_lfmm3dparttarg(int *ier, int iprec, int nsource, const double *source, int ifcharge,
+                           const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
+                           int ifpot, cplx *pot, int iffld, cplx *fld, int ntarget, const double *target,
+                           int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg, double *tinfo)
+{
+    lfmm_core(ier, iprec, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, pot, iffld, fld, 0,
+              NULL, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg, 0, NULL, tinfo);
+}
+
+void oracle_lfmm3dparttarg_hess(int *ier, int iprec, int nsource, const double *source, int ifcharge,
+                                const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
+                                int ifpot, cplx *pot, int iffld, cplx *fld, int ifhess, cplx *hess, int ntarget,
+                                const double *target, int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg,
+                                int ifhesstarg, cplx *hesstarg)
+{
+    lfmm_core(ier, iprec, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, pot, iffld, fld, ifhess,
+              hess, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg, ifhesstarg, hesstarg, NULL);
 }
 
 /* The Helmholtz restatement shares the tree, lists and rotations above. */
 #include "hfmm3d_oracle.c"
+
+/* Laplace Hessians (pair, local and multipole evaluators, FMM driver). */
+#include "lhess_oracle.c"

@@ -155,6 +155,32 @@ def lfmm3dparttarg(iprec, source, charge=None, dipstr=None, dipvec=None, target=
     return out + (tinfo,) if timing else out
 
 
+def lfmm3dparttarg_hess(iprec, source, charge=None, dipstr=None, dipvec=None, target=None,
+                        ifpot=1, iffld=1, ifhess=1, ifpottarg=1, iffldtarg=1, ifhesstarg=1):
+    """lfmm3dparttarg with Hessians (dxx,dyy,dzz,dxy,dxz,dyz per point):
+    returns (ier, pot, fld, hess, pottarg, fldtarg, hesstarg)."""
+    src = _f64(source, (0, 3))
+    n = src.shape[0]
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _c128(charge, n)
+    ds = _c128(dipstr, n)
+    dv = _f64(dipvec, (max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    hs = np.zeros((max(n, 1), 6), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ht = np.zeros((max(m, 1), 6), np.complex128)
+    ier = c_int(0)
+    lib().oracle_lfmm3dparttarg_hess(
+        ctypes.byref(ier), c_int(iprec), c_int(n), _p(src), c_int(int(charge is not None)), _p(q),
+        c_int(int(dipstr is not None)), _p(ds), _p(dv), c_int(ifpot), _p(pot), c_int(iffld), _p(fld),
+        c_int(ifhess), _p(hs), c_int(m), _p(trg if m else np.zeros((1, 3))), c_int(ifpottarg if m else 0), _p(pt),
+        c_int(iffldtarg if m else 0), _p(ft), c_int(ifhesstarg if m else 0), _p(ht))
+    return ier.value, pot[:n], fld[:n], hs[:n], pt[:m], ft[:m], ht[:m]
+
+
 class Tree:
     """The oracle's octree (d3tstrcr semantics) exported as numpy arrays."""
 
@@ -232,6 +258,37 @@ def taeval(c, lo, p, pts):
     lib().oracle_taeval(_p(_f64(c, (3,))), _p(np.ascontiguousarray(lo, np.complex128)), c_int(p), c_int(k),
                         _p(pts), _p(pot), _p(fld))
     return pot, fld
+
+
+def taevalhess(c, lo, p, pts, rscale=1.0):
+    """l3dtaevalhessd_trunc at each point: (pot, fld, hess[dxx,dyy,dzz,dxy,dxz,dyz])."""
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128); hess = np.zeros((k, 6), np.complex128)
+    lib().oracle_taevalhess(c_dbl(rscale), _p(_f64(c, (3,))), _p(np.ascontiguousarray(lo, np.complex128)),
+                            c_int(p), c_int(k), _p(pts), _p(pot), _p(fld), _p(hess))
+    return pot, fld, hess
+
+
+def mpevalhess(c, mp, p, pts, rscale=1.0):
+    """l3dmpevalhessd_trunc at each point: (pot, fld, hess)."""
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    pot = _cdouble_arr(k); fld = np.zeros((k, 3), np.complex128); hess = np.zeros((k, 6), np.complex128)
+    lib().oracle_mpevalhess(c_dbl(rscale), _p(_f64(c, (3,))), _p(np.ascontiguousarray(mp, np.complex128)),
+                            c_int(p), c_int(k), _p(pts), _p(pot), _p(fld), _p(hess))
+    return pot, fld, hess
+
+
+def direct_hess_at(source, pts, skip=None, charge=None, dipstr=None, dipvec=None):
+    """Direct-sum Hessians (lpotfld3dhess, lpotfld3dhess_dp) at pts; skip[k] is excluded at point k."""
+    source = _f64(source, (0, 3)); n = source.shape[0]
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    hess = np.zeros((k, 6), np.complex128)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.int64)
+    lib().oracle_l3ddirect_points_hess(c_int(n), _p(source), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                                       c_int(int(dipstr is not None)), _p(_c128(dipstr, n)),
+                                       _p(_f64(dipvec, (max(n, 1), 3))), c_int(k), _p(pts),
+                                       None if sk is None else _p(sk), _p(hess))
+    return hess
 
 
 def translate(kind, c_from, c_to, coef, p, nt=None):
