@@ -861,7 +861,7 @@ PEAK_SOURCE = {"fp64": "cuBLAS DGEMM 8192^3", "fp32": "cuBLAS SGEMM 8192^3 (TF32
                "tf32": "cuBLAS SGEMM 8192^3 with TF32 (tensor cores)"}
 
 
-def roofline_of(M, peaks, form, tensor_m2l=False):
+def roofline_of(M, peaks, form, tensor_m2l=False, iprec=1):
     """Roofline of the dominant pass (and of P2P and M2L separately) of one form, from the per-pass
     CUDA events of its timed steps.  P2P and M2L are compute passes: P2P on the CUDA cores (FP32 in
     the mixed form, FP64 otherwise), M2L on the tensor cores (TF32) when the mixed form runs it there.
@@ -873,13 +873,20 @@ def roofline_of(M, peaks, form, tensor_m2l=False):
     alone = {k: float(M["serial"][k]) for k in keys} if M.get("serial") else mean
     top = max(alone, key=alone.get)
     st = M["stats"]
+    # the mixed form applies to iprec <= 1; above, both forms run FP64
+    if iprec > 1:
+        form, tensor_m2l = "fp64", False
     cuda = "fp32" if form == "mixed" else "fp64"
+    # the FP64 rotate-shift-rotate M2L (orders <= 28) runs its products on the FP64 tensor cores (DMMA)
+    dmma = cuda == "fp64" and M.get("tuning", {}).get("form") == "fp64-rotation" and st.get("nterms", 99) <= 28
     per = {}
     p2p_flops = st["p2p_pairs"] * P2P_FLOPS_PER_PAIR
     m2l_fl = sum(cnt * m2l_flops(pt) for pt, cnt in st["m2l_pt_hist"].items())
     for name, flops, bound in (("p2p", p2p_flops, cuda), ("m2l", m2l_fl, "tf32" if tensor_m2l else cuda)):
         ach = flops / (alone[name] * 1e-3) / 1e12
-        per[name] = {"bound": "tensor" if bound == "tf32" else bound + " CUDA cores", "achieved": round(ach, 3),
+        label = ("tensor" if bound == "tf32" else
+                 "fp64 tensor cores (DMMA)" if (name == "m2l" and dmma) else bound + " CUDA cores")
+        per[name] = {"bound": label, "achieved": round(ach, 3),
                      "peak": round(peaks[bound], 2), "unit": "TFLOP/s", "frac": round(ach / peaks[bound], 4),
                      "peak_source": PEAK_SOURCE[bound] + ", measured in this run", "flops_per_launch": float(flops),
                      "ms": round(alone[name], 3)}
@@ -1049,9 +1056,10 @@ def main(argv=None):
             "dtype": "f32/f64 mixed (P2P, M2L in f32; tree, recurrences, other passes f64)",
             "data": "synthetic (seeded uniform cube; charges, dipoles)", "config": config_of(args, ws),
             "errors": head["errors"], "gpu_launches": int(sum(H["launches"])), "clocks": H["clocks"], "e2e": e2e,
-            "roofline": roofline_of(H, R["peaks"], "mixed", tensor_m2l=args.tensor_m2l > 0),
+            "roofline": roofline_of(H, R["peaks"], "mixed", tensor_m2l=args.tensor_m2l > 0, iprec=args.iprec),
             "forms": {"mixed": head, "fp64": dict(summary(R["forms"]["fp64"]),
-                                                  roofline=roofline_of(R["forms"]["fp64"], R["peaks"], "fp64"),
+                                                  roofline=roofline_of(R["forms"]["fp64"], R["peaks"], "fp64",
+                                                                       iprec=args.iprec),
                                                   gpu_launches=int(sum(R["forms"]["fp64"]["launches"])))},
             "stats": {k: v for k, v in H["stats"].items() if k != "m2l_pt_hist"}}
     line["forms"]["mixed_over_fp64"] = round(head["value"] / line["forms"]["fp64"]["value"], 3)

@@ -54,6 +54,15 @@ _lib.fmm3d_lfmm3dparttarg_batched_device.restype = _I
 _lib.fmm3d_lfmm3dparttarg_batched_device.argtypes = [_I, _I, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _I,
                                                      _P, _I, _P, _P]
 _lib.fmm3d_last_launches.restype = _I
+_lib.lfmm3dparttarghess_.restype = None
+_lib.l3dtaevalhess_.restype = None
+_lib.l3dmpevalhess_.restype = None
+_lib.fmm3d_lfmm3dparttarg_hess_device.restype = _I
+_lib.fmm3d_lfmm3dparttarg_hess_device.argtypes = [_I, _I, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
+                                                  _I, _P, _I, _P, _I, _P, _P]
+for _name in ("fmm3d_l3dtaevalhess_device", "fmm3d_l3dmpevalhess_device"):
+    getattr(_lib, _name).restype = _I
+    getattr(_lib, _name).argtypes = [ctypes.c_double, _P, _P, _I, _I, _P, _P, _I, _P, _I, _P, _P]
 _lib.fmm3d_set_timing.argtypes = [_I]
 _lib.fmm3d_set_stats.argtypes = [_I]
 _lib.fmm3d_set_m2l_mode.argtypes = [_I]
@@ -155,6 +164,94 @@ def lfmm3dparttarg(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, if
                          _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg),
                          _ptr(ft))
     return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dparttarghess(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld, ifhess,
+                       target=None, ifpottarg=0, iffldtarg=0, ifhesstarg=0):
+    """lfmm3dparttarg with Hessians; returns (ier, pot, fld, hess, pottarg, fldtarg, hesstarg).
+
+    hess / hesstarg: (N, 6) complex, ordered dxx, dyy, dzz, dxy, dxz, dyz.
+    """
+    src = _pts(source)
+    n = src.shape[0]
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    m = trg.shape[0]
+    q = _cplx(charge, n)
+    ds = _cplx(dipstr, n)
+    dv = _pts(dipvec) if (ifdipole == 1 and dipvec is not None) else np.zeros((max(n, 1), 3))
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    hs = np.zeros((max(n, 1), 6), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ht = np.zeros((max(m, 1), 6), np.complex128)
+    ier = ctypes.c_int(0)
+    _lib.lfmm3dparttarghess_(ctypes.byref(ier), _iref(iprec), _iref(n), _ptr(src), _iref(ifcharge), _ptr(q),
+                             _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld),
+                             _iref(ifhess), _ptr(hs), _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt),
+                             _iref(iffldtarg), _ptr(ft), _iref(ifhesstarg), _ptr(ht))
+    return ier.value, pot[:n], fld[:n], hs[:n], pt[:m], ft[:m], ht[:m]
+
+
+def _expansion_layout(coef, nterms):
+    """Compact expansion (index n*n+n+m) -> the reference's (0:nterms, -nterms:nterms) column-major array."""
+    out = np.zeros((2 * nterms + 1, nterms + 1), np.complex128)
+    for n in range(nterms + 1):
+        for m in range(-n, n + 1):
+            out[m + nterms, n] = coef[n * n + n + m]
+    return out
+
+
+def _evalhess(fn, rscale, center, coef, nterms, ztarg, iffld=1, ifhess=1):
+    c = np.ascontiguousarray(coef, np.complex128)
+    if c.ndim == 1:
+        c = _expansion_layout(c, nterms)
+    ctr = np.ascontiguousarray(center, np.float64)
+    z = np.ascontiguousarray(ztarg, np.float64)
+    pot = np.zeros(1, np.complex128)
+    fld = np.zeros(3, np.complex128)
+    hess = np.zeros(6, np.complex128)
+    ier = ctypes.c_int(0)
+    fn(ctypes.byref(ctypes.c_double(rscale)), _ptr(ctr), _ptr(c), _iref(nterms), _ptr(z), _ptr(pot), _iref(iffld),
+       _ptr(fld), _iref(ifhess), _ptr(hess), ctypes.byref(ier))
+    return ier.value, pot[0], fld, hess
+
+
+def l3dtaevalhess(rscale, center, local, nterms, ztarg, iffld=1, ifhess=1):
+    """l3dtaevalhess at one point; ``local``: compact (index n*n+n+m) or (2p+1, p+1) reference layout.
+    Returns (ier, pot, fld(3), hess(6))."""
+    return _evalhess(_lib.l3dtaevalhess_, rscale, center, local, nterms, ztarg, iffld, ifhess)
+
+
+def l3dmpevalhess(rscale, center, mpole, nterms, ztarg, iffld=1, ifhess=1):
+    """l3dmpevalhess at one point (layouts as l3dtaevalhess)."""
+    return _evalhess(_lib.l3dmpevalhess_, rscale, center, mpole, nterms, ztarg, iffld, ifhess)
+
+
+def evalhess_device(kind, rscale, center, coef, nterms, targ, pot, fld=None, hess=None, stream=0):
+    """One expansion at many device points.  kind "local" or "mpole"; ``coef``: device float64 tensor in
+    the reference layout ((2p+1)*(p+1)*2 doubles); ``targ`` (M,3); outputs ``pot`` (M,2), ``fld`` (M,6),
+    ``hess`` (M,12) float64 or None.  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    fn = _lib.fmm3d_l3dtaevalhess_device if kind == "local" else _lib.fmm3d_l3dmpevalhess_device
+    ctr = np.ascontiguousarray(center, np.float64)
+    return fn(float(rscale), _ptr(ctr), ptr(coef), nterms, targ.shape[0], ptr(targ), ptr(pot), int(fld is not None),
+              ptr(fld), int(hess is not None), ptr(hess), _P(stream))
+
+
+def lfmm3dparttarg_hess_device(iprec, source, charge, dipstr, dipvec, pot, fld, hess, target=None, pottarg=None,
+                               fldtarg=None, hesstarg=None, stream=0):
+    """lfmm3dparttarg_device with Hessians: ``hess`` / ``hesstarg`` (N,12) float64 tensors or None."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = source.shape[0]
+    m = 0 if target is None else target.shape[0]
+    return _lib.fmm3d_lfmm3dparttarg_hess_device(
+        iprec, n, ptr(source), int(charge is not None), ptr(charge), int(dipstr is not None), ptr(dipstr),
+        ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), int(hess is not None),
+        ptr(hess), m, ptr(target), int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg),
+        int(hesstarg is not None), ptr(hesstarg), _P(stream))
 
 
 def lfmm3dpartself(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld):

@@ -18,6 +18,7 @@
 
 #include "../../include/fmm3d_b200.h"
 #include "lap_kernels.cuh"
+#include "hess.cuh"
 #include "m2l_dense.cuh"
 #include "tree.cuh"
 #include "driver_common.cuh"
@@ -369,6 +370,12 @@ struct LapSetup {
     std::string signature;
     PointsSoA P;
     OutSoA os, ot;
+    // Hessian outputs (dxx, dyy, dzz, dxy, dxz, dyz), set before lap_setup;
+    // computed in FP64 with the near / far split of the potentials
+    int ifhess = 0, ifhesstarg = 0;
+    DBuf<double2> shess[6], thess[6];
+    HessSoA hs, ht;
+    double *hess_out = nullptr, *hesstarg_out = nullptr;
 };
 
 // Problem signature of the tuning cache: the form, the flags that select
@@ -654,8 +661,12 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     if (ifdipole == 1)
         ok = ok && S.sdq.alloc(ns, s, st) && S.svx.alloc(ns, s, st) && S.svy.alloc(ns, s, st) && S.svz.alloc(ns, s, st);
     if (nt) ok = ok && S.tx.alloc(nt, s, st) && S.ty.alloc(nt, s, st) && S.tz.alloc(nt, s, st);
-    S.do_src = ifpot == 1 || iffld == 1;
-    S.do_trg = (ifpottarg == 1 || iffldtarg == 1) && nt > 0;
+    S.do_src = ifpot == 1 || iffld == 1 || S.ifhess == 1;
+    S.do_trg = (ifpottarg == 1 || iffldtarg == 1 || S.ifhesstarg == 1) && nt > 0;
+    if (S.ifhess == 1)
+        for (int c = 0; c < 6; c++) ok = ok && S.shess[c].alloc(ns, s, st);
+    if (S.do_trg && S.ifhesstarg == 1)
+        for (int c = 0; c < 6; c++) ok = ok && S.thess[c].alloc(nt, s, st);
     if (ifpot == 1) ok = ok && S.opot.alloc(ns, s, st);
     if (iffld == 1) ok = ok && S.ofx.alloc(ns, s, st) && S.ofy.alloc(ns, s, st) && S.ofz.alloc(ns, s, st);
     if (S.do_trg && ifpottarg == 1) ok = ok && S.tpot.alloc(nt, s, st);
@@ -673,7 +684,12 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, S.tx.p, S.ty.p, S.tz.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     S.tv = make_treeview(T);
-    S.prune = !(ifpot == 1 || iffld == 1);
+    S.prune = !(ifpot == 1 || iffld == 1 || S.ifhess == 1);
+    for (int c = 0; c < 6; c++) { S.hs.h[c] = S.shess[c].p; S.ht.h[c] = S.thess[c].p; }
+    if (S.ifhess == 1 || S.ifhesstarg == 1) {
+        hess_init_constants(st);
+        if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    }
     S.os.pot = S.opot.p; S.os.fx = S.ofx.p; S.os.fy = S.ofy.p; S.os.fz = S.ofz.p;
     S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
@@ -726,6 +742,11 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // the outputs collect the near field and then the far field
     for (auto *o : {&S.opot, &S.ofx, &S.ofy, &S.ofz, &S.tpot, &S.tfx, &S.tfy, &S.tfz})
         if (o->n) FMM_TRY(st, cudaMemsetAsync(o->p, 0, sizeof(double2) * o->n, s));
+    for (int c = 0; c < 6; c++) {
+        if (S.shess[c].n) FMM_TRY(st, cudaMemsetAsync(S.shess[c].p, 0, sizeof(double2) * S.shess[c].n, s));
+        if (S.thess[c].n) FMM_TRY(st, cudaMemsetAsync(S.thess[c].p, 0, sizeof(double2) * S.thess[c].n, s));
+    }
+    const int hsrc = S.ifhess == 1, htrg = S.do_trg && S.ifhesstarg == 1;
     FMM_LAUNCH_CHECK(st);
     tm.mark();
     // The near field (STEP 8) runs on the call's stream while the far-field
@@ -757,6 +778,9 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         else
             launch_p2p(T.leaves.p, T.nleaves, tv, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge, S.ifdipole,
                        S.ifpot, S.iffld, ppt, pft, s, st);
+        // Hessians of the same near pairs (FP64 in every form)
+        launch_p2p_hess(T.leaves.p, T.nleaves, S.mixed ? S.tv_near : tv, P, S.tx.p, S.ty.p, S.tz.p, S.hs, S.ht,
+                        S.ifcharge, S.ifdipole, hsrc, htrg, s, st);
         if (tm.on) cudaEventRecord(p2p1, s);
     };
     if (overlap) near_field();
@@ -807,6 +831,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     // STEPS 6, 7: M2P from list 3 and L2P (add the far field to the outputs)
     launch_eval(T.leaves.p, T.nleaves, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
                 S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
+    launch_eval_hess(T.leaves.p, T.nleaves, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
+                     S.local.p, S.hs, S.ht, hsrc, htrg, s, st);
     tm.mark();
     if (tm.on) {
         // intervals: ..., l2l, [wait for the near field], eval, scatter, total ->
@@ -828,6 +854,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         k_scatter_out<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, S.ot, S.ifpottarg == 1 ? d_pottarg : nullptr,
                                                       S.iffldtarg == 1 ? d_fldtarg : nullptr); FMM_COUNT_LAUNCH();
     }
+    if (hsrc) launch_scatter_hess(ns, T.perm_src.p, S.hs, S.hess_out, s, st);
+    if (htrg) launch_scatter_hess(nt, T.perm_trg.p, S.ht, S.hesstarg_out, s, st);
     FMM_LAUNCH_CHECK(st);
     tm.mark();
 }
@@ -889,11 +917,16 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
                           const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
                           double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
                           int iffldtarg, double *d_fldtarg, cudaStream_t s, const std::vector<int> *so = nullptr,
-                          const std::vector<int> *to = nullptr)
+                          const std::vector<int> *to = nullptr, int ifhess = 0, double *d_hess = nullptr,
+                          int ifhesstarg = 0, double *d_hesstarg = nullptr)
 {
     g_launch_count = 0;
     Timer tm(s, g_ti.timing);
     LapSetup S;
+    S.ifhess = ifhess == 1 ? 1 : 0;
+    S.ifhesstarg = ifhesstarg == 1 ? 1 : 0;
+    S.hess_out = d_hess;
+    S.hesstarg_out = d_hesstarg;
     int ier = lap_setup(S, iprec, ns, d_src, ifcharge, ifdipole, ifpot, iffld, nt, d_trg, ifpottarg, iffldtarg, s, tm,
                         so, to);
     if (ier) return ier;
@@ -1342,6 +1375,47 @@ int fmm3d_lfmm3dparttarg_device(int iprec, int nsource, const double *d_source, 
                           iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
 }
 
+int fmm3d_lfmm3dparttarg_hess_device(int iprec, int nsource, const double *d_source, int ifcharge,
+                                     const double *d_charge, int ifdipole, const double *d_dipstr,
+                                     const double *d_dipvec, int ifpot, double *d_pot, int iffld, double *d_fld,
+                                     int ifhess, double *d_hess, int ntarget, const double *d_target, int ifpottarg,
+                                     double *d_pottarg, int iffldtarg, double *d_fldtarg, int ifhesstarg,
+                                     double *d_hesstarg, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return lap_fmm_device(iprec, nsource, d_source, ifcharge, d_charge, ifdipole, d_dipstr, d_dipvec, ifpot, d_pot,
+                          iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s, nullptr,
+                          nullptr, ifhess, d_hess, ifhesstarg, d_hesstarg);
+}
+
+int fmm3d_l3dtaevalhess_device(double rscale, const double *center, const double *d_local, int nterms, int npts,
+                               const double *d_targ, double *d_pot, int iffld, double *d_fld, int ifhess,
+                               double *d_hess, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    Status st;
+    g_launch_count = 0;
+    launch_expeval_hess(true, rscale, center, d_local, nterms, npts, d_targ, d_pot, iffld, d_fld, ifhess, d_hess, s,
+                        st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+int fmm3d_l3dmpevalhess_device(double rscale, const double *center, const double *d_mpole, int nterms, int npts,
+                               const double *d_targ, double *d_pot, int iffld, double *d_fld, int ifhess,
+                               double *d_hess, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    Status st;
+    g_launch_count = 0;
+    launch_expeval_hess(false, rscale, center, d_mpole, nterms, npts, d_targ, d_pot, iffld, d_fld, ifhess, d_hess, s,
+                        st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
 int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
                                double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
@@ -1419,6 +1493,101 @@ void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const doubl
                                   *ifpottarg, pt, *iffldtarg, ft, s);
         },
         true);
+}
+
+// Host arrays in and out, as lfmm3dparttarg_, plus the Hessians.  The
+// outputs of a failed call are left untouched.
+void lfmm3dparttarghess_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                         const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                         const int *ifpot, double *pot, const int *iffld, double *fld, const int *ifhess,
+                         double *hess, const int *ntarget, const double *target, const int *ifpottarg,
+                         double *pottarg, const int *iffldtarg, double *fldtarg, const int *ifhesstarg,
+                         double *hesstarg)
+{
+    const int ns = std::max(*nsource, 0), nt = std::max(*ntarget, 0);
+    cudaStream_t s = thread_stream();
+    Status st;
+    DBuf<double> src, q, dq, dv, trg, po, fo, ho, pt, ft, ht;
+    alloc_fail_point(1);
+    bool ok = src.alloc(3L * std::max(ns, 1), s, st);
+    if (*ifcharge == 1) ok = ok && q.alloc(2L * ns, s, st);
+    if (*ifdipole == 1) ok = ok && dq.alloc(2L * ns, s, st) && dv.alloc(3L * ns, s, st);
+    if (nt) ok = ok && trg.alloc(3L * nt, s, st);
+    if (*ifpot == 1) ok = ok && po.alloc(2L * ns, s, st);
+    if (*iffld == 1) ok = ok && fo.alloc(6L * ns, s, st);
+    if (*ifhess == 1) ok = ok && ho.alloc(12L * ns, s, st);
+    if (nt && *ifpottarg == 1) ok = ok && pt.alloc(2L * nt, s, st);
+    if (nt && *iffldtarg == 1) ok = ok && ft.alloc(6L * nt, s, st);
+    if (nt && *ifhesstarg == 1) ok = ok && ht.alloc(12L * nt, s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); *ier = 8; return; }
+    auto h2d = [&](DBuf<double> &d, const double *h, size_t n) {
+        if (n) FMM_TRY(st, cudaMemcpyAsync(d.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    };
+    h2d(src, source, 3L * ns);
+    if (*ifcharge == 1) h2d(q, charge, 2L * ns);
+    if (*ifdipole == 1) { h2d(dq, dipstr, 2L * ns); h2d(dv, dipvec, 3L * ns); }
+    if (nt) h2d(trg, target, 3L * nt);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); *ier = 8; return; }
+    int e = lap_fmm_device(*iprec, ns, src.p, *ifcharge, q.p, *ifdipole, dq.p, dv.p, *ifpot, po.p, *iffld, fo.p, nt,
+                           trg.p, nt ? *ifpottarg : 0, pt.p, nt ? *iffldtarg : 0, ft.p, s, nullptr, nullptr, *ifhess,
+                           ho.p, nt ? *ifhesstarg : 0, ht.p);
+    if (e) { *ier = e; return; }
+    auto d2h = [&](double *h, DBuf<double> &d) {
+        if (d.n) FMM_TRY(st, cudaMemcpyAsync(h, d.p, sizeof(double) * d.n, cudaMemcpyDeviceToHost, s));
+    };
+    if (*ifpot == 1) d2h(pot, po);
+    if (*iffld == 1) d2h(fld, fo);
+    if (*ifhess == 1) d2h(hess, ho);
+    if (nt && *ifpottarg == 1) d2h(pottarg, pt);
+    if (nt && *iffldtarg == 1) d2h(fldtarg, ft);
+    if (nt && *ifhesstarg == 1) d2h(hesstarg, ht);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    *ier = st.ok() ? 0 : 16;
+    if (!st.ok()) g_ti.err = cudaGetErrorString(st.err);
+}
+
+// One expansion at one point, with the calling sequence of l3dtaevalhess /
+// l3dmpevalhess (src/laprouts3d.f:5297, 5229): rscale, center(3),
+// expansion(0:nterms, -nterms:nterms), nterms, ztarg(3), pot, iffld, fld(3),
+// ifhess, hess(6), ier.  For many points use fmm3d_l3dtaevalhess_device.
+static void expeval_hess_host(bool loc, const double *rscale, const double *center, const double *coef,
+                              const int *nterms, const double *ztarg, double *pot, const int *iffld, double *fld,
+                              const int *ifhess, double *hess, int *ier)
+{
+    const int p = *nterms;
+    cudaStream_t s = thread_stream();
+    Status st;
+    DBuf<double> c, t, out;
+    const size_t nc = 2L * (p + 1) * (2 * p + 1);
+    if (p < 0 || !c.alloc(nc, s, st) || !t.alloc(3, s, st) || !out.alloc(2 + 6 + 12, s, st)) {
+        *ier = p < 0 ? 16 : 8;
+        return;
+    }
+    FMM_TRY(st, cudaMemcpyAsync(c.p, coef, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    FMM_TRY(st, cudaMemcpyAsync(t.p, ztarg, sizeof(double) * 3, cudaMemcpyHostToDevice, s));
+    launch_expeval_hess(loc, *rscale, center, c.p, p, 1, t.p, out.p, *iffld, out.p + 2, *ifhess, out.p + 8, s, st);
+    double h[20];
+    FMM_TRY(st, cudaMemcpyAsync(h, out.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); *ier = 16; return; }
+    pot[0] = h[0]; pot[1] = h[1];
+    if (*iffld == 1) memcpy(fld, h + 2, 6 * sizeof(double));
+    if (*ifhess == 1) memcpy(hess, h + 8, 12 * sizeof(double));
+    *ier = 0;
+}
+
+void l3dtaevalhess_(const double *rscale, const double *center, const double *local, const int *nterms,
+                    const double *ztarg, double *pot, const int *iffld, double *fld, const int *ifhess, double *hess,
+                    int *ier)
+{
+    expeval_hess_host(true, rscale, center, local, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier);
+}
+
+void l3dmpevalhess_(const double *rscale, const double *center, const double *mpole, const int *nterms,
+                    const double *ztarg, double *pot, const int *iffld, double *fld, const int *ifhess, double *hess,
+                    int *ier)
+{
+    expeval_hess_host(false, rscale, center, mpole, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier);
 }
 
 void lfmm3dpartself_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,

@@ -71,7 +71,58 @@ void h3dpartdirect_(const double *zk, const int *nsource, const double *source, 
                     const double *target, const int *ifpottarg, double *pottarg, const int *iffldtarg,
                     double *fldtarg);
 
+/* Replaces l3dtaevalhess (src/laprouts3d.f:5297-5363; it calls
+ * l3dtaevalhessdini + l3dtaevalhessd, :7613, :7384) and l3dmpevalhess
+ * (:5229-5295; l3dmpevalhessdini + l3dmpevalhessd, :7129, :6945): potential,
+ * field = -gradient (iffld = 1) and Hessian hess(6) = dxx, dyy, dzz, dxy, dxz,
+ * dyz (ifhess = 1) of one local / multipole expansion
+ * expansion(0:nterms, -nterms:nterms) with scaling rscale about center, at
+ * ztarg.  ier = 0, or 8 / 16 (device memory, nterms outside 0..74).  One point
+ * per call; fmm3d_l3dtaevalhess_device evaluates many points in one call. */
+void l3dtaevalhess_(const double *rscale, const double *center, const double *local, const int *nterms,
+                    const double *ztarg, double *pot, const int *iffld, double *fld, const int *ifhess, double *hess,
+                    int *ier);
+void l3dmpevalhess_(const double *rscale, const double *center, const double *mpole, const int *nterms,
+                    const double *ztarg, double *pot, const int *iffld, double *fld, const int *ifhess, double *hess,
+                    int *ier);
+
 /* ---- extensions (no counterpart in the reference) ---------------------- */
+
+/* lfmm3dparttarg_ with Hessians: ifhess / ifhesstarg = 1 also return
+ * hess(6, nsource) / hesstarg(6, ntarget), complex*16, ordered dxx, dyy, dzz,
+ * dxy, dxz, dyz (the order of l3dmpevalhessd / l3dtaevalhessd and of the
+ * sort l3dhsort, src/lfmm3drouts.f:621).  The reference has the evaluators
+ * (l3dmpevalhessd_trunc :7194, l3dtaevalhessd_trunc :7682, lpotfld3dhess
+ * :5442, lpotfld3dhess_dp :5619) but no particle driver that calls them; this
+ * one runs the FMM of lfmm3dparttarg and adds, at every evaluation point, the
+ * Hessians of its near pairs, its list-3 multipoles and its leaf's local
+ * expansion.  Potentials and fields are those of lfmm3dparttarg_ bit for bit
+ * (same form, same kernels); the Hessians are computed in FP64 in every form. */
+void lfmm3dparttarghess_(int *ier, const int *iprec, const int *nsource, const double *source, const int *ifcharge,
+                         const double *charge, const int *ifdipole, const double *dipstr, const double *dipvec,
+                         const int *ifpot, double *pot, const int *iffld, double *fld, const int *ifhess,
+                         double *hess, const int *ntarget, const double *target, const int *ifpottarg,
+                         double *pottarg, const int *iffldtarg, double *fldtarg, const int *ifhesstarg,
+                         double *hesstarg);
+
+/* The same on device-resident arrays, enqueued on `stream`. */
+int fmm3d_lfmm3dparttarg_hess_device(int iprec, int nsource, const double *d_source, int ifcharge,
+                                     const double *d_charge, int ifdipole, const double *d_dipstr,
+                                     const double *d_dipvec, int ifpot, double *d_pot, int iffld, double *d_fld,
+                                     int ifhess, double *d_hess, int ntarget, const double *d_target, int ifpottarg,
+                                     double *d_pottarg, int iffldtarg, double *d_fldtarg, int ifhesstarg,
+                                     double *d_hesstarg, void *stream);
+
+/* l3dtaevalhess / l3dmpevalhess at npts device-resident points targ(3, npts):
+ * pot(npts), fld(3, npts) (iffld = 1), hess(6, npts) (ifhess = 1), complex*16,
+ * in device memory; the expansion (reference layout) in device memory, rscale
+ * and center(3) on the host.  Synchronous; returns ier. */
+int fmm3d_l3dtaevalhess_device(double rscale, const double *center, const double *d_local, int nterms, int npts,
+                               const double *d_targ, double *d_pot, int iffld, double *d_fld, int ifhess,
+                               double *d_hess, void *stream);
+int fmm3d_l3dmpevalhess_device(double rscale, const double *center, const double *d_mpole, int nterms, int npts,
+                               const double *d_targ, double *d_pot, int iffld, double *d_fld, int ifhess,
+                               double *d_hess, void *stream);
 
 /* lfmm3dparttarg on arrays already resident in device memory (same layouts),
  * enqueued on `stream` (a cudaStream_t, or NULL for the library's own
