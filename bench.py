@@ -56,7 +56,9 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
             geometries), Poisson arrivals at swept rates: p50/p99 latency and
             points/s per rate (host arrays in and out, copies included);
             serving_mixed: the same stream with the Laplace requests of iprec <= 1
-            in the mixed form.
+            in the mixed form; serving_repeated: the Laplace requests drawn from
+            8 repeated source sets with fresh charges, served by resident plans
+            (tree kept on the device, CUDA-graph replay).
   helmholtz the Helmholtz workload measured in the same run (not the
             headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
             unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
@@ -113,8 +115,8 @@ def parse_args(argv=None):
     ap.add_argument("--helm-cpu-sample", type=int, default=1_000_000,
                     help="sources of the Helmholtz oracle call (parity and CPU baseline; capped at --helm-n)")
     ap.add_argument("--batch-instances", type=int, default=4096, help="instances of the batched workload (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=40, help="requests per serving rate (0: skip)")
-    ap.add_argument("--serve-rates", default="10,40,inf", help="Poisson arrival rates (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=400, help="requests per serving rate (0: skip)")
+    ap.add_argument("--serve-rates", default="20,60,inf", help="Poisson arrival rates (requests/s)")
     ap.add_argument("--autotune", metavar="PATH", default=None,
                     help="tune the Laplace workloads' launch shapes into the JSON cache PATH and exit")
     ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched"], default="all",
@@ -355,24 +357,39 @@ def run_batched(args, R):
             "tuning": knobs}
 
 
-def run_serving(args, precision=None):
+def run_serving(args, precision=None, geometries=0, rates=None):
     """Swept-rate serving measurement (one warm-up pass over the same requests first); precision 1
-    serves the Laplace requests with iprec <= 1 in the mixed form."""
+    serves the Laplace requests with iprec <= 1 in the mixed form; geometries > 0 draws the Laplace
+    requests from that many repeated source sets, served by resident plans."""
     from fmmlib3d_b200.serving import FMMServer, make_request_stream, run_stream
-    reqs = make_request_stream(args.serve_requests, seed=7)
+    reqs = make_request_stream(args.serve_requests, seed=7, geometries=geometries)
     srv = FMMServer(slots=4, precision=precision)
     out = {"slots": 4, "requests_per_rate": len(reqs), "mean_n": float(np.mean([len(r.source) for r in reqs])),
            "laplace_fraction": float(np.mean([r.kernel == "laplace" for r in reqs])),
            "precision": "mixed for Laplace iprec <= 1" if precision == 1 else "fp64", "rates": []}
+    if geometries:
+        out["repeated_geometries"] = geometries
     try:
-        run_stream(srv, reqs, float("inf"))  # warm-up: plans, pools
-        for rate in [float(x) for x in args.serve_rates.split(",")]:
+        run_stream(srv, reqs, float("inf"))  # warm-up: memory pools, operator plans, resident geometry plans
+        for rate in [float(x) for x in (rates or args.serve_rates).split(",")]:
             st, _ = run_stream(srv, reqs, rate, seed=int(rate) if rate != float("inf") else 0)
             st["rate_hz"] = None if rate == float("inf") else rate
             out["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()})
         out["max_on_gpu"] = srv.max_running
+        if geometries:
+            out.update({k: v for k, v in srv.stats().items() if k.startswith("plan") or k.startswith("resident")})
     finally:
         srv.close()
+    if geometries:
+        # the same stream with plans switched off: every request rebuilds its tree
+        srv = FMMServer(slots=4, precision=precision, plan_bytes=0)
+        try:
+            run_stream(srv, reqs, float("inf"))
+            st, _ = run_stream(srv, reqs, float("inf"), seed=0)
+            out["saturated_without_plans"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()
+                                              if k in ("points_per_s", "p50_ms", "p99_ms", "max_ier")}
+        finally:
+            srv.close()
     return out
 
 
@@ -1094,6 +1111,7 @@ def main(argv=None):
     if args.serve_requests > 0 and ws == 1:
         line["serving"] = run_serving(args)
         line["serving_mixed"] = run_serving(args, precision=1)
+        line["serving_repeated"] = run_serving(args, geometries=8, rates="60,inf")
     if args.helm_n > 0:
         H2 = run_helm(args, R)
         if rank == 0 and ws == 1 and not args.no_cpu and args.helm_cpu_sample > 0:

@@ -3,6 +3,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <map>
 #include <atomic>
 #include <condition_variable>
 #include <deque>
@@ -283,6 +284,30 @@ __global__ void k_split_c(int n, const double *c, double2 *o)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) o[i] = make_double2(c[2L * i], c[2L * i + 1]);
+}
+
+cudaError_t smem_allow_fn(const void *func, size_t bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> cap_of;   // (function, device) -> limit set
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair(func, dev);
+    auto it = cap_of.find(key);
+    if (it == cap_of.end()) {
+        int optin = 0;
+        cudaFuncAttributes fa;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess ||
+            (e = cudaFuncGetAttributes(&fa, func)) != cudaSuccess)
+            return e;
+        const size_t cap = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+        if ((e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap)) != cudaSuccess)
+            return e;
+        it = cap_of.emplace(key, cap).first;
+    }
+    return bytes <= it->second ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 }  // namespace fmm

@@ -70,6 +70,22 @@ __host__ __device__ __forceinline__ int tidx(int n, int m) { return (n * (n + 1)
 constexpr int kMaxLevel = 21;  // 3 key bits per level in a 64-bit key
 constexpr int kMaxP = 80;
 
+// ---------------------------------------------------------------- dynamic shared memory
+// Lets `func` take `bytes` of dynamic shared memory per block.  The limit is
+// a process-wide attribute of the function: set per launch to that launch's
+// size, a host thread could lower it just before another thread (a serving
+// slot, a plan on its own stream) launches a larger problem, whose launch then
+// fails.  So it is raised once per device to the most the device gives one
+// block (less the function's static shared memory) and never lowered; the
+// launch's own size still sets its occupancy.  Returns cudaErrorInvalidValue
+// when `bytes` is beyond the device.
+cudaError_t smem_allow_fn(const void *func, size_t bytes);
+template <class T>
+inline cudaError_t smem_allow(T *func, size_t bytes)
+{
+    return smem_allow_fn((const void *)func, bytes);
+}
+
 // ---------------------------------------------------------------- device buffers
 // Test hook (fmm3d_inject_alloc_failure): when positive, counts this host
 // thread's workspace allocations down and fails the one that reaches zero as

@@ -318,7 +318,7 @@ void build_hz(int nblk, const HZBlock *d_blk, const HZBlock *h_blk, const double
     dim3 g1(nblk, div_up(maxq, 64));
     k_hz_radial<<<g1, 64, 0, s>>>(d_blk, d_xw, zk, pmax, rad); FMM_COUNT_LAUNCH();
     size_t sm = sizeof(double) * (3 * kHzNodes * (pmax + 1) + 3 * kHzNodes);
-    FMM_TRY(st, cudaFuncSetAttribute(k_hz_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FMM_TRY(st, smem_allow(k_hz_build, (int)sm));
     dim3 g2(nblk, pmax + 1);
     k_hz_build<<<g2, kHzThreads, sm, s>>>(d_blk, d_xw, pmax, rad, Z); FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
@@ -488,13 +488,13 @@ static void launch_htranslate_kind(const Tile *tiles, int ntiles, const int *gro
 #define FMM_HTR(KTV)                                                                                           \
     do {                                                                                                       \
         if (gs) {                                                                                              \
-            FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV, true>,                                    \
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
+            FMM_TRY(st, smem_allow(k_htranslate<KIND, KTV, true>,                                    \
+                                             (int)sm));           \
             k_htranslate<KIND, KTV, true><<<grid, kHTransThreads, sm, s>>>(tiles, ntiles, grouped, slots, tv,  \
                                                                            pmax, rot, Z, in, out, prune, gs);  \
         } else {                                                                                               \
-            FMM_TRY(st, cudaFuncSetAttribute(k_htranslate<KIND, KTV, false>,                                   \
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));           \
+            FMM_TRY(st, smem_allow(k_htranslate<KIND, KTV, false>,                                   \
+                                             (int)sm));           \
             k_htranslate<KIND, KTV, false><<<grid, kHTransThreads, sm, s>>>(tiles, ntiles, grouped, slots, tv, \
                                                                             pmax, rot, Z, in, out, prune, gs); \
         }                                                                                                      \
@@ -818,7 +818,7 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
 #define FMM_HF(IR, C, D, CHV)                                                                                 \
     do {                                                                                                      \
         size_t sm = sizeof(double) * HFormSmem<CHV, D>::doubles(pm);                                         \
-        FMM_TRY(st, cudaFuncSetAttribute(k_hform<IR, C, D, CHV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+        FMM_TRY(st, smem_allow(k_hform<IR, C, D, CHV>, \
                                          (int)sm));                                                           \
         k_hform<IR, C, D, CHV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);           \
         FMM_COUNT_LAUNCH();                                                                                   \
@@ -990,12 +990,12 @@ void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const doub
     int pm = max_p(lv);
     size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * kHEvalThreads);
     if (sm <= 226 * 1024) {
-        FMM_TRY(st, cudaFuncSetAttribute(k_heval<kHEvalThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        FMM_TRY(st, smem_allow(k_heval<kHEvalThreads>, (int)sm));
         k_heval<kHEvalThreads><<<nleaves, kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk,
                                                                   mpole, local, outs, outt, do_src, do_trg);
     } else {
         sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * 32);
-        FMM_TRY(st, cudaFuncSetAttribute(k_heval<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        FMM_TRY(st, smem_allow(k_heval<32>, (int)sm));
         k_heval<32><<<nleaves, 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
                                             outt, do_src, do_trg);
     }

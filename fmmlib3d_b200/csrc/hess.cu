@@ -383,7 +383,7 @@ void launch_eval_hess(const int *leaves, int nleaves, const TreeView &tv, const 
     const size_t arr = (size_t)(p + 3) * (p + 3) * sizeof(double2);
     const int per_phase = (int)std::min<size_t>(5, kHessSmemMax / arr);
     const size_t smem = per_phase * arr;
-    FMM_TRY(st, cudaFuncSetAttribute(k_eval_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMM_TRY(st, smem_allow(k_eval_hess, (int)smem));
     if (!st.ok()) return;
     k_eval_hess<<<nleaves, kEvalHThreads, smem, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, p, mpole, local, hs, ht,
                                                      do_src, do_trg, per_phase);
@@ -499,7 +499,7 @@ void launch_expeval_hess(bool loc, double rscale, const double *center, const do
     const size_t arr = (size_t)(nterms + 3) * (nterms + 3) * sizeof(double2);
     const int per_phase = (int)std::min<size_t>(nk, kHessSmemMax / arr);
     const size_t smem = per_phase * arr;
-    FMM_TRY(st, cudaFuncSetAttribute(k_expeval_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FMM_TRY(st, smem_allow(k_expeval_hess, (int)smem));
     if (!st.ok()) return;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

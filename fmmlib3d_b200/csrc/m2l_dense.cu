@@ -186,7 +186,7 @@ void launch_m2l_dense(const Tile *tiles, int ntiles, const int *grouped, const S
     dim3 g(ntiles, div_up((p + 1) * (p + 1), kTM));
     if (kt <= 16) {
         constexpr size_t sm = sizeof(double2) * 64 * (kTM + 16);
-        FMM_TRY(st, cudaFuncSetAttribute(k_m2l_dense<16, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        FMM_TRY(st, smem_allow(k_m2l_dense<16, 64>, (int)sm));
         k_m2l_dense<16, 64><<<g, kDenseThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, in, out, prune); FMM_COUNT_LAUNCH();
     } else {
         constexpr size_t sm = sizeof(double2) * 16 * (kTM + 64);

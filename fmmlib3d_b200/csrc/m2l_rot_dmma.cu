@@ -294,7 +294,7 @@ void launch_m2l_rot_dmma(const Tile *tiles, int ntiles, const int *grouped, cons
     const size_t sm = sizeof(double) * (32 * (size_t)rd_ld(p)) + sizeof(double2) * (p + 1) +
                       sizeof(double) * (2 * p + 3) +
                       sizeof(short) * (2 * rd_ntasks(p) + (p + 1) * (p + 1) + rd_nz(p));
-    FMM_TRY(st, cudaFuncSetAttribute(k_m2l_rot_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FMM_TRY(st, smem_allow(k_m2l_rot_dmma, (int)sm));
     if (!st.ok()) return;
     k_m2l_rot_dmma<<<ntiles, 32 * kRdWarps, sm, s>>>(tiles, grouped, slots, tv, p, rot, dc, lddc, in, out, prune);
     FMM_COUNT_LAUNCH();

@@ -327,7 +327,7 @@ static void launch_tc_t(const Tile *tiles, int ntiles, const int *grouped, const
                         Status &st)
 {
     const size_t sm = (size_t)S * 2 * (KC / 4) * (kTcLBO + NMAX * 16 + 16) + 128;
-    FMM_TRY(st, cudaFuncSetAttribute(k_m2l_tc<KC, S, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    FMM_TRY(st, smem_allow(k_m2l_tc<KC, S, NMAX>, (int)sm));
     dim3 g(ntiles, div_up((p + 1) * (p + 1), 64));
     k_m2l_tc<KC, S, NMAX><<<g, kTcThreads, sm, s>>>(tiles, grouped, slots, slot_toff, T, tv, p, mp, ldm, out, prune, nprod,
                                               group, err, g_tc_expire_waits); FMM_COUNT_LAUNCH();
@@ -477,7 +477,7 @@ extern "C" int fmm3d_tc_selftest(int N, int K, const float *A, const float *B, f
         ok(cudaMemcpy(dA, A, sizeof(float) * 128 * K, cudaMemcpyHostToDevice)) &&
         ok(cudaMemcpy(dB, B, sizeof(float) * N * K, cudaMemcpyHostToDevice)) && ok(cudaMemset(derr, 0, sizeof(int))) &&
         ok(cudaMemset(dD, 0, sizeof(float) * 128 * N)) &&
-        ok(cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) {
+        ok(smem_allow(k_tc_selftest, (int)sm))) {
         k_tc_selftest<<<1, kTcThreads, sm>>>(N, K, dA, dB, dD, nprod, derr);
         if (ok(cudaGetLastError()) && ok(cudaDeviceSynchronize()))
             if (ok(cudaMemcpy(D, dD, sizeof(float) * 128 * N, cudaMemcpyDeviceToHost)))

@@ -90,3 +90,40 @@ def test_precision_per_request():
         assert ier == 0 and np.array_equal(a.pot, pot) and np.array_equal(a.fld, fld), (r.tag, r.kernel, r.iprec)
     with pytest.raises(ValueError):
         F.set_precision_thread(2)
+
+
+def test_repeated_geometries_run_on_resident_plans():
+    """Laplace requests naming a repeated geometry run on a plan kept on the device: after the
+    first request of each geometry no tree is rebuilt (plan hits), every result carries the bits of
+    a plain call, and a plan budget smaller than two plans evicts the least recently used one and
+    still gives the same bits."""
+    from fmmlib3d_b200.serving import FMMServer, Request, run_stream
+    import fmmlib3d_b200 as F
+    rng = np.random.default_rng(9)
+    geoms = [(rng.random((20000, 3)), 1), (rng.normal(size=(8000, 3)) * 0.3, 0), (rng.random((3000, 3)), 2)]
+    reqs = []
+    for i in range(18):
+        g = i % 3
+        src, iprec = geoms[g]
+        q = rng.uniform(-1, 1, len(src)) + 1j * rng.uniform(-1, 1, len(src))
+        reqs.append(Request("laplace", src, q, iprec=iprec, tag=i, geometry=g))
+    want = []
+    for r in reqs:
+        ier, pot, fld, _, _ = F.lfmm3dparttarg(r.iprec, r.source, 1, r.charge, 0, None, None, 1, 1)
+        assert ier == 0
+        want.append((pot, fld))
+    for plan_bytes in (None, 1):
+        srv = FMMServer(slots=4, plan_bytes=plan_bytes)
+        try:
+            stats, res = run_stream(srv, reqs, float("inf"))
+            st = srv.stats()
+        finally:
+            srv.close()
+        assert stats["max_ier"] == 0
+        for r, a, (pot, fld) in zip(reqs, res, want):
+            assert a.tag == r.tag
+            assert np.array_equal(a.pot, pot) and np.array_equal(a.fld, fld)
+        if plan_bytes is None:
+            assert st["plans_built"] == 3 and st["plan_hits"] == 15 and st["plans_evicted"] == 0
+        else:
+            assert st["plans_evicted"] >= 1
