@@ -54,6 +54,7 @@ _lib.fmm3d_lfmm3dparttarg_batched_device.restype = _I
 _lib.fmm3d_lfmm3dparttarg_batched_device.argtypes = [_I, _I, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _P, _P, _I,
                                                      _P, _I, _P, _P]
 _lib.fmm3d_last_launches.restype = _I
+_lib.fmm3d_last_depth_capped.restype = _I
 _lib.lfmm3dparttarghess_.restype = None
 _lib.l3dtaevalhess_.restype = None
 _lib.l3dmpevalhess_.restype = None
@@ -649,6 +650,11 @@ def last_stats():
     if k > 9 + 128:  # Helmholtz: expansion order per level
         d["nterms_level"] = [int(v) for v in out[9 + 128:k]]
     return d
+
+
+def last_depth_capped():
+    """Boxes of level 21 in this thread's last tree that the reference (100 levels) would split further."""
+    return _lib.fmm3d_last_depth_capped()
 
 
 def last_error():

@@ -27,6 +27,7 @@ struct ThreadInfo {
     std::vector<long long> stats;
     std::string err;
     int launches = 0;
+    int depth_capped = 0;   // Tree::capped of this thread's last tree
 };
 extern thread_local ThreadInfo g_ti;
 

@@ -251,6 +251,7 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     alloc_fail_point(2);
     build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
+    g_ti.depth_capped = T.capped;
     tm.mark();
     // per-level orders and scales (src/hfmm3dpart.f:336-340, 398-405).  In
     // hfmm3dparttarg zk is not declared complex, so under its implicit real*8

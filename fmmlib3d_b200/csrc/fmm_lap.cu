@@ -640,7 +640,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     lap_init_constants(st);
     keep_pool_memory();
     const int p = l3dterms(eps);
-    if (p > 72) return 16;
+    if (p > 72) { g_ti.err = "expansion order " + std::to_string(p) + " above the supported 72"; return 16; }
     S.plan = get_plan(p, eps, s, st);
     if (!st.ok() || !S.plan) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     auto &plan = S.plan;
@@ -653,6 +653,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     if (so) build_forest(T, d_src, *so, d_trg, *to, nbox, s, st);
     else build_tree(T, d_src, ns, d_trg, nt, nbox, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 4; }
+    g_ti.depth_capped = T.capped;
     tm.mark();
     const int K = S.K;
     alloc_fail_point(3);
@@ -1701,5 +1702,7 @@ int fmm3d_last_stats(long long *out, int n)
 const char *fmm3d_last_error(void) { return g_ti.err.c_str(); }
 
 int fmm3d_last_launches(void) { return g_launch_count; }
+
+int fmm3d_last_depth_capped(void) { return g_ti.depth_capped; }
 
 }  // extern "C"

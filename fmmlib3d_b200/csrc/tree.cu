@@ -602,6 +602,15 @@ void build_forest(Tree &T, const double *d_src, const std::vector<int> &so, cons
     }
     T.nboxes = nboxes;
     T.nlev = (int)T.lev_start.size() - 1;
+    T.capped = 0;
+    if (opt_in.maxlevel > kMaxLevel && T.nlev == kMaxLevel && st.ok()) {
+        const int b0 = T.lev_start[kMaxLevel], nb = T.lev_count[kMaxLevel];
+        std::vector<int> hs(nb), ht(nb);
+        FMM_TRY(st, cudaMemcpyAsync(hs.data(), T.nsrc.p + b0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        FMM_TRY(st, cudaMemcpyAsync(ht.data(), T.ntrg.p + b0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        FMM_TRY(st, cudaStreamSynchronize(s));
+        for (int i = 0; i < nb && st.ok(); i++) T.capped += (hs[i] > nbox || ht[i] > nbox) ? 1 : 0;
+    }
     for (int d = 0; d < 3; d++) T.center0[d] = hgeom[d];
     T.size = hgeom[3];
 

@@ -15,6 +15,10 @@ struct Tree {
     DBuf<double> inst_geom;  // 4 per instance: center of the bounding cube, side
     int nboxes = 0, nlev = 0;
     int nleaves = 0;
+    // boxes of level kMaxLevel that the reference would split further (it refines to
+    // maxlevel 100; the keys here hold 21 levels): they stay leaves with more than nbox
+    // points, summed directly, so results keep their accuracy and only cost more
+    int capped = 0;
     double center0[3] = {0, 0, 0}, size = 0;
     std::vector<int> lev_start, lev_count;  // host copies, per level 0..nlev
 
@@ -44,7 +48,7 @@ struct Tree {
 // kMaxLevel here), and with ifempty = 1 its empty children are kept.  The
 // defaults are those d3tstrcr uses.
 struct TreeOptions {
-    int ifempty = 0, minlevel = 0, maxlevel = kMaxLevel;
+    int ifempty = 0, minlevel = 0, maxlevel = 100;   // 100: d3tstrcr's (src/d3tstrcr.f:181-182)
 };
 
 // Builds the tree for device arrays src (n x 3, AoS) and trg (m x 3).

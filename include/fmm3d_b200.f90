@@ -90,6 +90,35 @@ module fmm3d_b200
     end subroutine
 
     ! Arithmetic form of later calls: 0 FP64 (default), 1 mixed precision for iprec <= 1.
+    ! Hessians: the reference's one-point evaluators, and lfmm3dparttarg with Hessian outputs
+    ! (hess(6, n): dxx, dyy, dzz, dxy, dxz, dyz; no counterpart in the reference)
+    subroutine l3dtaevalhess(rscale, center, local, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier) &
+        bind(C, name="l3dtaevalhess_")
+      import :: c_int, c_double, c_double_complex
+      real(c_double) :: rscale, center(3), ztarg(3)
+      integer(c_int) :: nterms, iffld, ifhess, ier
+      complex(c_double_complex) :: local(0:nterms, -nterms:nterms), pot, fld(3), hess(6)
+    end subroutine
+
+    subroutine l3dmpevalhess(rscale, center, mpole, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier) &
+        bind(C, name="l3dmpevalhess_")
+      import :: c_int, c_double, c_double_complex
+      real(c_double) :: rscale, center(3), ztarg(3)
+      integer(c_int) :: nterms, iffld, ifhess, ier
+      complex(c_double_complex) :: mpole(0:nterms, -nterms:nterms), pot, fld(3), hess(6)
+    end subroutine
+
+    subroutine lfmm3dparttarghess(ier, iprec, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, &
+        ifpot, pot, iffld, fld, ifhess, hess, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg, &
+        ifhesstarg, hesstarg) bind(C, name="lfmm3dparttarghess_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld, ifhess, ntarget, ifpottarg, &
+          iffldtarg, ifhesstarg
+      real(c_double) :: source(3, *), dipvec(3, *), target(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), hess(6, *), pottarg(*), &
+          fldtarg(3, *), hesstarg(6, *)
+    end subroutine
+
     integer(c_int) function fmm3d_set_precision(mode) bind(C, name="fmm3d_set_precision")
       import :: c_int
       integer(c_int), value :: mode

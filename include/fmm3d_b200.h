@@ -383,6 +383,14 @@ const char *fmm3d_last_error(void);
 /* Number of CUDA kernels launched by the last call on this thread. */
 int fmm3d_last_launches(void);
 
+/* Depth cap: the reference refines its octree to 100 levels (src/d3tstrcr.f:181-182); the
+ * GPU tree's 64-bit keys hold 21.  Returns how many boxes of level 21 in this host thread's
+ * last tree still held more than nbox sources or targets, which the reference would split
+ * further (0 for any input whose points are not clustered below 2^-21 of the bounding cube).
+ * Such boxes stay leaves and their points are summed directly, so results keep the iprec
+ * accuracy and only the cost grows (quadratically in the box's point count). */
+int fmm3d_last_depth_capped(void);
+
 #ifdef __cplusplus
 }
 #endif

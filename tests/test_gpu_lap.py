@@ -426,3 +426,28 @@ def test_target_only_mode_prunes_list2(F):
     _, _, _, opt, oft = O.lfmm3dparttarg(1, src, q, None, None, trg, ifpot=0, iffld=0)
     assert rel(pt2, opt) < TOL_ORACLE and rel(ft2, oft) < TOL_ORACLE
     assert rel(pt2, pt) < TOL_ORACLE and rel(ft2, ft) < TOL_ORACLE
+
+
+def test_tree_depth_cap_keeps_accuracy(F):
+    """A cluster narrower than 2^-21 of the bounding cube: the reference refines it to 100 levels,
+    the GPU tree stops at 21 (64-bit keys) and keeps the over-full boxes as leaves, summed directly.
+    fmm3d_last_depth_capped reports them; the results stay within 2x the oracle's error (whose tree
+    goes deeper) and within the iprec bound.  A uniform input reports none."""
+    rng = np.random.default_rng(21)
+    far = rng.random((3000, 3))
+    cluster = np.array([0.3, 0.6, 0.45]) + 1e-9 * rng.random((600, 3))
+    src = np.concatenate([far, cluster])
+    n = len(src)
+    q = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+    ier, pot, fld, _, _ = F.lfmm3dparttarg(1, src, 1, q, 0, None, None, 1, 1)
+    assert ier == 0, F.last_error()
+    assert F.last_depth_capped() >= 1
+    oier, opot, ofld, _, _ = O.lfmm3dparttarg(1, src, q, None, None, None)
+    assert oier == 0
+    si = np.concatenate([rng.choice(3000, 100, replace=False), 3000 + rng.choice(600, 100, replace=False)])
+    dp, df = O.direct_at(src, src[si], si, q, None, None)
+    for a, o, d in ((pot[si], opot[si], dp), (fld[si], ofld[si], df)):
+        assert rel(a, d) <= 2 * rel(o, d) + 1e-14
+        assert rel(a, d) < EPS[1]
+    ier, _, _, _, _ = F.lfmm3dparttarg(1, far, 1, q[:3000], 0, None, None, 1, 1)
+    assert ier == 0 and F.last_depth_capped() == 0
