@@ -56,6 +56,14 @@ _lib.fmm3d_lfmm3dparttarg_batched_device.argtypes = [_I, _I, _P, _P, _I, _P, _I,
 _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_last_depth_capped.restype = _I
 _lib.lfmm3dparttarghess_.restype = None
+for _name in ("lfmm3dtriatarg_", "lfmm3dtriaself_", "lfmm3dtria_", "l3dtriadirect_"):
+    getattr(_lib, _name).restype = None
+_lib.fmm3d_lfmm3dtriatarg_device.restype = _I
+_lib.fmm3d_lfmm3dtriatarg_device.argtypes = [_I, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
+                                             _I, _P, _P]
+_lib.fmm3d_l3dtriadirect_device.restype = _I
+_lib.fmm3d_l3dtriadirect_device.argtypes = [_I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I,
+                                            _P, _P]
 _lib.l3dtaevalhess_.restype = None
 _lib.l3dmpevalhess_.restype = None
 _lib.fmm3d_lfmm3dparttarg_hess_device.restype = _I
@@ -253,6 +261,75 @@ def lfmm3dparttarg_hess_device(iprec, source, charge, dipstr, dipvec, pot, fld, 
         ptr(dipvec), int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), int(hess is not None),
         ptr(hess), m, ptr(target), int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg),
         int(hesstarg is not None), ptr(hesstarg), _P(stream))
+
+
+def _tri_args(triaflat, trianorm, source, charge, dipstr, target):
+    tri = np.ascontiguousarray(triaflat, dtype=np.float64).reshape(-1, 3, 3)
+    n = tri.shape[0]
+    nrm = np.ascontiguousarray(trianorm, dtype=np.float64).reshape(-1, 3) if trianorm is not None else None
+    if nrm is None:
+        e = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+        nrm = np.ascontiguousarray(e / np.linalg.norm(e, axis=1)[:, None])
+    src = _pts(source) if source is not None else np.ascontiguousarray(tri.mean(axis=1))
+    trg = _pts(target) if target is not None else np.zeros((0, 3))
+    return tri, n, nrm, src, trg, _cplx(charge, n), _cplx(dipstr, n)
+
+
+def lfmm3dtriatarg(iprec, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld,
+                   target=None, ifpottarg=0, iffldtarg=0):
+    """Laplace layer potentials of flat triangles (lfmm3dtriatarg, src/lfmm3dtria.f:121);
+    returns (ier, pot, fld, pottarg, fldtarg).  triaflat (N,3,3) vertices, trianorm (N,3) unit
+    normals (None: from the vertex order), source (N,3) centroids (None: computed)."""
+    tri, n, nrm, src, trg, q, ds = _tri_args(triaflat, trianorm, source, charge, dipstr, target)
+    m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = ctypes.c_int(0)
+    dv = np.zeros((max(n, 1), 3))
+    _lib.lfmm3dtriatarg_(ctypes.byref(ier), _iref(iprec), _iref(n), _ptr(tri), _ptr(nrm), _ptr(src), _iref(ifcharge),
+                         _ptr(q), _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld),
+                         _ptr(fld), _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg),
+                         _ptr(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dtriaself(iprec, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld):
+    """lfmm3dtriaself: (ier, pot, fld) at the centroids."""
+    ier, pot, fld, _, _ = lfmm3dtriatarg(iprec, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr,
+                                         ifpot, iffld)
+    return ier, pot, fld
+
+
+def l3dtriadirect(triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld,
+                  target=None, ifpottarg=0, iffldtarg=0):
+    """O(N^2) layer potentials by exact integrals (l3dtriadirect); returns (pot, fld, pottarg, fldtarg)."""
+    tri, n, nrm, src, trg, q, ds = _tri_args(triaflat, trianorm, source, charge, dipstr, target)
+    m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    dv = np.zeros((max(n, 1), 3))
+    _lib.l3dtriadirect_(_iref(n), _ptr(tri), _ptr(nrm), _ptr(src), _iref(ifcharge), _ptr(q), _iref(ifdipole),
+                        _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld), _iref(m),
+                        _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg), _ptr(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dtriatarg_device(iprec, triaflat, trianorm, source, charge, dipstr, pot, fld, target=None, pottarg=None,
+                          fldtarg=None, stream=0):
+    """lfmm3dtriatarg on device tensors: triaflat (N,9), trianorm / source / target (N,3) float64;
+    charge / dipstr (N,2); outputs pot (N,2), fld (N,6) or None.  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = source.shape[0]
+    m = 0 if target is None else target.shape[0]
+    return _lib.fmm3d_lfmm3dtriatarg_device(
+        iprec, n, ptr(triaflat), ptr(trianorm), ptr(source), int(charge is not None), ptr(charge),
+        int(dipstr is not None), ptr(dipstr), None, int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m,
+        ptr(target), int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
 
 
 def lfmm3dpartself(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld):

@@ -19,6 +19,7 @@
 #include "../../include/fmm3d_b200.h"
 #include "lap_kernels.cuh"
 #include "hess.cuh"
+#include "tri.cuh"
 #include "m2l_dense.cuh"
 #include "tree.cuh"
 #include "driver_common.cuh"
@@ -376,6 +377,19 @@ struct LapSetup {
     DBuf<double2> shess[6], thess[6];
     HessSoA hs, ht;
     double *hess_out = nullptr, *hesstarg_out = nullptr;
+    // triangle FMM (lfmm3dtriatarg), set before lap_setup: the sources are
+    // flat triangles, the tree's points their centroids; the far field runs
+    // on the triangles' quadrature nodes (Pq, box ranges tv_quad), the near
+    // field by exact integrals (ts).  Always FP64.
+    bool tri = false;
+    const double *tri_in = nullptr, *tri_norm = nullptr;
+    TriRule rule;
+    DBuf<double> tgeo, qx, qy, qz, qvx, qvy, qvz;
+    DBuf<double2> tq, tdq, qq, qdq;
+    DBuf<int> qsrc0, qnsrc;
+    TriSoA ts;
+    PointsSoA Pq;
+    TreeView tv_quad;
 };
 
 // Problem signature of the tuning cache: the form, the flags that select
@@ -383,11 +397,12 @@ struct LapSetup {
 static std::string lap_signature(const LapSetup &S)
 {
     const char *form = S.tcm2l ? "mixed-tc" : S.mixed ? "mixed-cuda" : S.dense ? "fp64-dense" : "fp64-rotation";
+    const char *kern = S.tri ? "laplace-triangles" : "laplace";
     char b[512];
     snprintf(b, sizeof b,
-             "laplace iprec=%d form=%s charge=%d dipole=%d out=%d%d%d%d inst=2^%d ns=2^%d nt=2^%d nlev=%d "
+             "%s iprec=%d form=%s charge=%d dipole=%d out=%d%d%d%d inst=2^%d ns=2^%d nt=2^%d nlev=%d "
              "nboxes=2^%d dev=%s",
-             S.iprec, form, S.ifcharge == 1, S.ifdipole == 1, S.ifpot == 1, S.iffld == 1,
+             kern, S.iprec, form, S.ifcharge == 1, S.ifdipole == 1, S.ifpot == 1, S.iffld == 1,
              S.do_trg && S.ifpottarg == 1, S.do_trg && S.iffldtarg == 1, log2_bucket(S.T.ninst),
              log2_bucket(S.ns), log2_bucket(S.do_trg ? S.nt : 0), S.T.nlev, log2_bucket(S.T.nboxes),
              device_tag().c_str());
@@ -636,6 +651,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     double eps;
     int nbox;
     if (ns < 1 || !lap_iprec(iprec, ns, nt, eps, nbox)) return 4;
+    if (S.tri) nbox = tri_nbox(iprec, ns, nt);
     if (nt < 0) nt = 0;
     lap_init_constants(st);
     keep_pool_memory();
@@ -695,7 +711,7 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.ot.pot = S.tpot.p; S.ot.fx = S.tfx.p; S.ot.fy = S.tfy.p; S.ot.fz = S.tfz.p;
 
     const int form = sw(kSwPrecision);
-    S.mixed = form == 1 && iprec <= 1 && plan->dense;
+    S.mixed = !S.tri && form == 1 && iprec <= 1 && plan->dense;
     S.dense = (plan->dense && sw(kSwM2LMode) != 1 && sw(kSwM2LMode) != 3) || S.mixed;
     S.tcm2l = S.mixed && sw(kSwTensorM2L) > 0;
     // launch shapes: the autotuner's cached setting for this problem, else automatic
@@ -711,6 +727,24 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     // mixed form: small list-3 / list-4 interactions join the near field (FP64 keeps the reference's lists)
     lap_widen_near(S, S.mixed ? (p + 2) * (p + 2) / 2 : 0, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    if (S.tri) {
+        // triangle data in tree order and the quadrature nodes (filled per call)
+        const size_t nn = (size_t)ns * S.rule.n;
+        bool okt = S.tgeo.alloc(30L * ns, s, st) && S.qx.alloc(nn, s, st) && S.qy.alloc(nn, s, st) &&
+                   S.qz.alloc(nn, s, st) && S.qsrc0.alloc(T.nboxes, s, st) && S.qnsrc.alloc(T.nboxes, s, st);
+        if (ifcharge == 1) okt = okt && S.tq.alloc(ns, s, st) && S.qq.alloc(nn, s, st);
+        if (ifdipole == 1)
+            okt = okt && S.tdq.alloc(ns, s, st) && S.qdq.alloc(nn, s, st) && S.qvx.alloc(nn, s, st) &&
+                  S.qvy.alloc(nn, s, st) && S.qvz.alloc(nn, s, st);
+        if (!okt) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+        S.ts.geo = S.tgeo.p; S.ts.q = S.tq.p; S.ts.dq = S.tdq.p;
+        S.Pq.x = S.qx.p; S.Pq.y = S.qy.p; S.Pq.z = S.qz.p; S.Pq.q = S.qq.p; S.Pq.dq = S.qdq.p;
+        S.Pq.vx = S.qvx.p; S.Pq.vy = S.qvy.p; S.Pq.vz = S.qvz.p;
+        launch_scale_ranges(T.nboxes, S.tv.src0, S.tv.nsrc, S.rule.n, S.qsrc0.p, S.qnsrc.p, s, st);
+        S.tv_quad = S.tv;
+        S.tv_quad.src0 = S.qsrc0.p;
+        S.tv_quad.nsrc = S.qnsrc.p;
+    }
     S.ldm = K + (K & 1);
     if (S.tcm2l && (!S.mp32.alloc((size_t)T.nboxes * S.ldm, s, st) || !S.tcerr.alloc(1, s, st))) {
         g_ti.err = cudaGetErrorString(st.err);
@@ -734,7 +768,10 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     const PointsSoA &P = S.P;
     const int prune = S.prune;
     wait_host_inputs(s, st);   // charges still in flight from the host
-    if (S.ifcharge == 1 || S.ifdipole == 1) {
+    if (S.tri) {
+        launch_tri_gather(ns, T.perm_src.p, S.tri_in, S.tri_norm, d_q, d_dq, S.ifcharge, S.ifdipole, S.rule, S.ts,
+                          S.Pq, s, st);
+    } else if (S.ifcharge == 1 || S.ifdipole == 1) {
         k_gather_q<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, d_q, d_dq, d_dv, S.ifcharge == 1,
                                                    S.ifdipole == 1, P); FMM_COUNT_LAUNCH();
     }
@@ -773,7 +810,10 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
         if (tm.on) cudaEventRecord(p2p0, s);
         // STEP 8: P2P over self and list 1 (adds to the outputs)
         const int ppt = S.do_trg ? S.ifpottarg : 0, pft = S.do_trg ? S.iffldtarg : 0;
-        if (S.mixed)
+        if (S.tri)
+            launch_p2p_tri(T.leaves.p, T.nleaves, tv, S.ts, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot,
+                           S.ifcharge, S.ifdipole, S.do_src, S.do_trg, S.iffld == 1, pft == 1, s, st);
+        else if (S.mixed)
             launch_p2p32(T.leaves.p, T.nleaves, S.tv_near, P, S.tx.p, S.ty.p, S.tz.p, S.os, S.ot, S.ifcharge,
                          S.ifdipole, S.ifpot, S.iffld, ppt, pft, S.knobs.p2p_ept, s, st);
         else
@@ -786,7 +826,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     };
     if (overlap) near_field();
     // STEP 1: P2M at every childless box
-    launch_p2m(T.leaves.p, T.nleaves, tv, P, S.ifcharge, S.ifdipole, p, S.mpole.p, f, st);
+    launch_p2m(T.leaves.p, T.nleaves, S.tri ? S.tv_quad : tv, S.tri ? S.Pq : P, S.ifcharge, S.ifdipole, p, S.mpole.p, f,
+               st);
     tm.mark_on(f);
     // STEP 3: M2M, levels nlev-1 .. 2
     for (auto &r : S.m2m_rng)
@@ -794,7 +835,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
                          plan->dc.p, plan->lddc, S.mpole.p, S.mpole.p, prune, S.trans_kt, f, st);
     tm.mark_on(f);
     // STEP 2: P2L from list 4 (every box; boxes with an empty list add nothing)
-    launch_p2l(T.grouped.p, T.nboxes, S.tv_far, P, S.ifcharge, S.ifdipole, p, S.local.p, f, st);
+    launch_p2l(T.grouped.p, T.nboxes, S.tri ? S.tv_quad : S.tv_far, S.tri ? S.Pq : P, S.ifcharge, S.ifdipole, p,
+               S.local.p, f, st);
     tm.mark_on(f);
     // STEP 4: M2L over list 2, all levels >= 2
     if (S.tcm2l) {
@@ -938,6 +980,115 @@ static int lap_fmm_device(int iprec, int ns, const double *d_src, int ifcharge, 
     tm.finish(g_ti.ms);
     if (g_ti.want_stats && st.ok()) lap_stats(S, s, st);
     return lap_finish(S, s, st);
+}
+
+// ---------------------------------------------------------------- triangles, one call
+// lfmm3dtriatarg (src/lfmm3dtria.f:121-546): the tree on the centroids and
+// targets with the triangle FMM's nbox, then the passes of
+// lfmm3dtriatargmain (:547-1160) in the FP64 form.
+static int tri_fmm_device(int iprec, int ns, const double *d_tri, const double *d_norm, const double *d_src,
+                          int ifcharge, const double *d_q, int ifdipole, const double *d_dq, int ifpot, double *d_pot,
+                          int iffld, double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
+                          int iffldtarg, double *d_fldtarg, cudaStream_t s)
+{
+    g_launch_count = 0;
+    Timer tm(s, g_ti.timing);
+    LapSetup S;
+    S.tri = true;
+    S.tri_in = d_tri;
+    S.tri_norm = d_norm;
+    S.rule = tri_rule(iprec);
+    int ier = lap_setup(S, iprec, ns, d_src, ifcharge, ifdipole, ifpot, iffld, nt, d_trg, ifpottarg, iffldtarg, s, tm);
+    if (ier) return ier;
+    g_last_signature = S.signature;
+    lap_effective_knobs(S, g_last_knobs);
+    Status st;
+    lap_passes(S, d_q, d_dq, nullptr, d_pot, d_fld, d_pottarg, d_fldtarg, s, tm, st);
+    tm.finish(g_ti.ms);
+    if (g_ti.want_stats && st.ok()) lap_stats(S, s, st);
+    return lap_finish(S, s, st);
+}
+
+// l3dtriadirect (src/lfmm3dtria.f:1385-1560): every triangle at every
+// centroid (its own by the in-plane values) and target.
+static int tri_direct_device(int ns, const double *d_tri, const double *d_src, int ifcharge, const double *d_q,
+                             int ifdipole, const double *d_dq, int ifpot, double *d_pot, int iffld, double *d_fld,
+                             int nt, const double *d_trg, int ifpottarg, double *d_pottarg, int iffldtarg,
+                             double *d_fldtarg, cudaStream_t s)
+{
+    g_launch_count = 0;
+    Status st;
+    if (ns < 0 || nt < 0) return 4;
+    DBuf<double> geo;
+    DBuf<double2> q, dq;
+    TriRule none;   // no quadrature nodes: the direct sum uses the exact integrals only
+    bool ok = geo.alloc(30L * std::max(ns, 1), s, st);
+    if (ifcharge == 1) ok = ok && q.alloc(std::max(ns, 1), s, st);
+    if (ifdipole == 1) ok = ok && dq.alloc(std::max(ns, 1), s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    TriSoA t;
+    t.geo = geo.p; t.q = q.p; t.dq = dq.p;
+    launch_tri_gather(ns, nullptr, d_tri, nullptr, d_q, d_dq, ifcharge, ifdipole, none, t, PointsSoA(), s, st);
+    auto run = [&](int npts, const double *pts, int centroids, int wp, double *op, int wf, double *of) {
+        if (!(wp == 1 || wf == 1) || npts <= 0) return;
+        launch_tri_direct(ns, t, ifcharge, ifdipole, npts, pts, centroids, wp == 1 ? op : nullptr,
+                          wf == 1 ? of : nullptr, s, st);
+    };
+    run(ns, d_src, 1, ifpot, d_pot, iffld, d_fld);
+    run(nt, d_trg, 0, ifpottarg, d_pottarg, iffldtarg, d_fldtarg);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+// Host arrays in and out for the triangle entry points (pageable or pinned):
+// device copies, the device call, copies back; a failed call leaves the
+// outputs untouched.
+template <class F>
+static int tri_host(int ns, const double *tri, const double *norm, const double *source, int ifcharge,
+                    const double *charge, int ifdipole, const double *dipstr, int ifpot, double *pot, int iffld,
+                    double *fld, int nt, const double *target, int ifpottarg, double *pottarg, int iffldtarg,
+                    double *fldtarg, F run)
+{
+    ns = std::max(ns, 0);
+    nt = std::max(nt, 0);
+    cudaStream_t s = thread_stream();
+    Status st;
+    DBuf<double> dtri, dnorm, dsrc, dq, ddq, dtrg, po, fo, pt, ft;
+    alloc_fail_point(1);
+    bool ok = dtri.alloc(9L * std::max(ns, 1), s, st) && dsrc.alloc(3L * std::max(ns, 1), s, st);
+    if (norm) ok = ok && dnorm.alloc(3L * std::max(ns, 1), s, st);
+    if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
+    if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st);
+    if (nt) ok = ok && dtrg.alloc(3L * nt, s, st);
+    if (ifpot == 1) ok = ok && po.alloc(2L * ns, s, st);
+    if (iffld == 1) ok = ok && fo.alloc(6L * ns, s, st);
+    if (nt && ifpottarg == 1) ok = ok && pt.alloc(2L * nt, s, st);
+    if (nt && iffldtarg == 1) ok = ok && ft.alloc(6L * nt, s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    auto h2d = [&](DBuf<double> &d, const double *h, size_t n) {
+        if (n) FMM_TRY(st, cudaMemcpyAsync(d.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    };
+    h2d(dtri, tri, 9L * ns);
+    h2d(dsrc, source, 3L * ns);
+    if (norm) h2d(dnorm, norm, 3L * ns);
+    if (ifcharge == 1) h2d(dq, charge, 2L * ns);
+    if (ifdipole == 1) h2d(ddq, dipstr, 2L * ns);
+    if (nt) h2d(dtrg, target, 3L * nt);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    int e = run(dtri.p, dnorm.p, dsrc.p, dq.p, ddq.p, po.p, fo.p, nt, dtrg.p, nt ? ifpottarg : 0, pt.p,
+                nt ? iffldtarg : 0, ft.p, s);
+    if (e) return e;
+    auto d2h = [&](double *h, DBuf<double> &d) {
+        if (d.n) FMM_TRY(st, cudaMemcpyAsync(h, d.p, sizeof(double) * d.n, cudaMemcpyDeviceToHost, s));
+    };
+    if (ifpot == 1) d2h(pot, po);
+    if (iffld == 1) d2h(fld, fo);
+    if (nt && ifpottarg == 1) d2h(pottarg, pt);
+    if (nt && iffldtarg == 1) d2h(fldtarg, ft);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    return 0;
 }
 
 // ---------------------------------------------------------------- plans: fixed geometry, new charges
@@ -1417,6 +1568,31 @@ int fmm3d_l3dmpevalhess_device(double rscale, const double *center, const double
     return 0;
 }
 
+int fmm3d_lfmm3dtriatarg_device(int iprec, int nsource, const double *d_triaflat, const double *d_trianorm,
+                                const double *d_source, int ifcharge, const double *d_charge, int ifdipole,
+                                const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot, int iffld,
+                                double *d_fld, int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
+                                int iffldtarg, double *d_fldtarg, void *stream)
+{
+    (void)d_dipvec;   // as in the reference, the dipoles are oriented by the triangles' normals
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return tri_fmm_device(iprec, nsource, d_triaflat, d_trianorm, d_source, ifcharge, d_charge, ifdipole, d_dipstr,
+                          ifpot, d_pot, iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
+}
+
+int fmm3d_l3dtriadirect_device(int nsource, const double *d_triaflat, const double *d_trianorm,
+                               const double *d_source, int ifcharge, const double *d_charge, int ifdipole,
+                               const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot, int iffld,
+                               double *d_fld, int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
+                               int iffldtarg, double *d_fldtarg, void *stream)
+{
+    (void)d_trianorm;
+    (void)d_dipvec;
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    return tri_direct_device(nsource, d_triaflat, d_source, ifcharge, d_charge, ifdipole, d_dipstr, ifpot, d_pot,
+                             iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
+}
+
 int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,
                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot,
                                double *d_pot, int iffld, double *d_fld, int ntarget, const double *d_target,
@@ -1494,6 +1670,60 @@ void lfmm3dparttarg_(int *ier, const int *iprec, const int *nsource, const doubl
                                   *ifpottarg, pt, *iffldtarg, ft, s);
         },
         true);
+}
+
+void lfmm3dtriatarg_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                     const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                     const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                     double *fld, const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
+                     const int *iffldtarg, double *fldtarg)
+{
+    (void)dipvec;
+    const int ip = *iprec, ns = *nsource, ifc = *ifcharge, ifd = *ifdipole, ifp = *ifpot, iff = *iffld;
+    *ier = tri_host(ns, triaflat, trianorm, source, ifc, charge, ifd, dipstr, ifp, pot, iff, fld, *ntarget, target,
+                    *ifpottarg, pottarg, *iffldtarg, fldtarg,
+                    [&](const double *t_, const double *n_, const double *s_, const double *q, const double *dq,
+                        double *po, double *fo, int nt, const double *tg, int ipt, double *pt, int ift, double *ft,
+                        cudaStream_t s) {
+                        return tri_fmm_device(ip, ns, t_, n_, s_, ifc, q, ifd, dq, ifp, po, iff, fo, nt, tg, ipt, pt,
+                                              ift, ft, s);
+                    });
+}
+
+void lfmm3dtriaself_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                     const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                     const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                     double *fld)
+{
+    int zero = 0;
+    lfmm3dtriatarg_(ier, iprec, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot,
+                    pot, iffld, fld, &zero, source, &zero, nullptr, &zero, nullptr);
+}
+
+void lfmm3dtria_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                 const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                 const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                 double *fld)
+{
+    lfmm3dtriaself_(ier, iprec, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot,
+                    pot, iffld, fld);
+}
+
+void l3dtriadirect_(const int *nsource, const double *triaflat, const double *trianorm, const double *source,
+                    const int *ifcharge, const double *charge, const int *ifdipole, const double *dipstr,
+                    const double *dipvec, const int *ifpot, double *pot, const int *iffld, double *fld,
+                    const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
+                    const int *iffldtarg, double *fldtarg)
+{
+    (void)trianorm;
+    (void)dipvec;
+    const int ns = *nsource, ifc = *ifcharge, ifd = *ifdipole, ifp = *ifpot, iff = *iffld;
+    tri_host(ns, triaflat, nullptr, source, ifc, charge, ifd, dipstr, ifp, pot, iff, fld, *ntarget, target, *ifpottarg,
+             pottarg, *iffldtarg, fldtarg,
+             [&](const double *t_, const double *, const double *s_, const double *q, const double *dq, double *po,
+                 double *fo, int nt, const double *tg, int ipt, double *pt, int ift, double *ft, cudaStream_t s) {
+                 return tri_direct_device(ns, t_, s_, ifc, q, ifd, dq, ifp, po, iff, fo, nt, tg, ipt, pt, ift, ft, s);
+             });
 }
 
 // Host arrays in and out, as lfmm3dparttarg_, plus the Hessians.  The

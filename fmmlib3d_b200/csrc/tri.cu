@@ -1,0 +1,358 @@
+// Laplace layer potentials on flat triangles: the kernels particular to the
+// triangle FMM (the far-field passes are the particle FMM's, run on the
+// triangles' quadrature nodes).
+//
+// Near field (direct3dtritarglaps2 / direct3dtritarglapd2 and the self terms
+// direct3dtrilaps2 / direct3dtrilapd2, src/triquadflatlib.f:147-818): for a
+// triangle with unit density, at x,
+//   S = int 1/|x-y| dS,   D = int n.(x-y)/|x-y|^3 dS   (n: vertex-order normal),
+// and their gradients, in closed form: with h = n.(x - v1) and per edge
+// a -> b (unit tangent t, outward in-plane normal m = t x n), s- = (a-x).t,
+// s+ = (b-x).t, p = (a-x).m, R- = |a-x|, R+ = |b-x|,
+//   f = log((R+ + s+)/(R- + s-)),
+//   beta = atan2(p s+, p^2 + h^2 + |h| R+) - atan2(p s-, p^2 + h^2 + |h| R-),
+//   S = sum p f - |h| sum beta,  grad S = -sum m f - sign(h) n sum beta,
+//   D = sign(h) sum beta,        grad D = -sum (u x w)(|u|+|w|)/(|u||w|(|u||w|+u.w)),
+// u = x - a, w = x - b.  At a triangle's own centroid h is taken as 0, as the
+// reference does (iquad = 0): the jumps of grad S . n and of D across the
+// triangle are split evenly (both vanish), grad D is continuous there.
+// Fields are -grad.
+#include "tri.cuh"
+
+#include <cmath>
+
+namespace fmm {
+
+constexpr int kTriGeo = 30;
+
+TriRule tri_rule(int iprec)
+{
+    // nqtri of lfmm3dtriatarg: 2 for iprec -2 / -1, 4 for 0, 6 for >= 1, else 1
+    int norder = (iprec == -2 || iprec == -1) ? 2 : iprec == 0 ? 4 : iprec >= 1 ? 6 : 1;
+    TriRule r;
+    if (norder <= 1) {
+        r.n = 1;
+        r.xi[0] = r.eta[0] = 1.0 / 3.0;
+        r.w[0] = 1.0;
+        return r;
+    }
+    const int k = norder / 2 + 1;   // exact to degree 2k - 2 = norder
+    std::vector<double> x, w;
+    gauss_legendre(k, x, w);
+    r.n = 0;
+    for (int i = 0; i < k; i++)
+        for (int j = 0; j < k; j++) {
+            const double u = 0.5 * (x[i] + 1), v = 0.5 * (x[j] + 1);
+            r.xi[r.n] = u;
+            r.eta[r.n] = (1 - u) * v;
+            r.w[r.n] = 2 * (0.5 * w[i]) * (0.5 * w[j]) * (1 - u);   // the reference triangle's area is 1/2
+            r.n++;
+        }
+    return r;
+}
+
+int tri_nbox(int iprec, int ns, int nt)
+{
+    switch (iprec) {
+    case -2: return 8 / 3;
+    case -1: return 15 / 3;
+    case 0: return 30 / 3;
+    case 1: return 60 / 3;
+    case 2: return 120 / 3;
+    case 3: return 240 / 3;
+    case 4: return 480 / 3;
+    case 5: return 700 / 3;
+    case 6: return ns + nt;
+    }
+    return -1;
+}
+
+__global__ void k_tri_gather(int n, const int *perm, const double *tri, const double *norm, const double *q,
+                             const double *dq, int ifcharge, int ifdipole, TriRule rule, TriSoA t, PointsSoA nodes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long j = perm ? perm[i] : i;
+    double v[9];
+    for (int c = 0; c < 9; c++) v[c] = tri[9 * j + c];
+    const double e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]}, e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+    double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]), area = 0.5 * len;
+    for (int c = 0; c < 3; c++) nr[c] /= len;
+    double *g = t.geo + (size_t)kTriGeo * i;
+    for (int c = 0; c < 9; c++) g[c] = v[c];
+    for (int c = 0; c < 3; c++) g[9 + c] = nr[c];
+    for (int k = 0; k < 3; k++) {
+        const int a = k, b = (k + 1) % 3;
+        double tv[3] = {v[3 * b] - v[3 * a], v[3 * b + 1] - v[3 * a + 1], v[3 * b + 2] - v[3 * a + 2]};
+        const double L = sqrt(tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2]);
+        for (int c = 0; c < 3; c++) tv[c] /= L;
+        g[12 + 3 * k] = tv[0]; g[13 + 3 * k] = tv[1]; g[14 + 3 * k] = tv[2];
+        g[21 + 3 * k] = tv[1] * nr[2] - tv[2] * nr[1];
+        g[22 + 3 * k] = tv[2] * nr[0] - tv[0] * nr[2];
+        g[23 + 3 * k] = tv[0] * nr[1] - tv[1] * nr[0];
+    }
+    double2 qi = cmk(0, 0), di = cmk(0, 0);
+    if (ifcharge) { qi = cmk(q[2 * j], q[2 * j + 1]); t.q[i] = qi; }
+    if (ifdipole) { di = cmk(dq[2 * j], dq[2 * j + 1]); t.dq[i] = di; }
+    for (int k = 0; k < rule.n; k++) {
+        const long o = (long)i * rule.n + k;
+        nodes.x[o] = v[0] + rule.xi[k] * e1[0] + rule.eta[k] * e2[0];
+        nodes.y[o] = v[1] + rule.xi[k] * e1[1] + rule.eta[k] * e2[1];
+        nodes.z[o] = v[2] + rule.xi[k] * e1[2] + rule.eta[k] * e2[2];
+        const double wa = rule.w[k] * area;
+        if (ifcharge) nodes.q[o] = cscal(wa, qi);
+        if (ifdipole) {
+            nodes.dq[o] = cscal(wa, di);
+            // the far field orients the dipoles by trianorm, as l3dformmptrid2_add does
+            nodes.vx[o] = norm[3 * j]; nodes.vy[o] = norm[3 * j + 1]; nodes.vz[o] = norm[3 * j + 2];
+        }
+    }
+}
+
+void launch_tri_gather(int n, const int *perm, const double *tri, const double *norm, const double *q,
+                       const double *dq, int ifcharge, int ifdipole, const TriRule &rule, TriSoA t, PointsSoA nodes,
+                       cudaStream_t s, Status &st)
+{
+    if (n <= 0 || !st.ok()) return;
+    k_tri_gather<<<(n + 127) / 128, 128, 0, s>>>(n, perm, tri, norm, q, dq, ifcharge == 1, ifdipole == 1, rule, t,
+                                                 nodes);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+__global__ void k_scale_ranges(int nb, const int *src0, const int *nsrc, int k, int *qs0, int *qns)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    qs0[b] = src0[b] * k;
+    qns[b] = nsrc[b] * k;
+}
+
+void launch_scale_ranges(int nboxes, const int *src0, const int *nsrc, int k, int *qsrc0, int *qnsrc, cudaStream_t s,
+                         Status &st)
+{
+    if (nboxes <= 0 || !st.ok()) return;
+    k_scale_ranges<<<(nboxes + 255) / 256, 256, 0, s>>>(nboxes, src0, nsrc, k, qsrc0, qnsrc);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// One triangle (geometry g, 30 doubles) at x: S, grad S (CHG), D, grad D (DIP).
+template <bool CHG, bool DIP>
+__device__ __forceinline__ void tri_pair(const double *g, double x0, double x1, double x2, bool self, bool fld,
+                                         double &S, double (&gS)[3], double &D, double (&gD)[3])
+{
+    double d[3][3], R[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        d[k][0] = g[3 * k] - x0;
+        d[k][1] = g[3 * k + 1] - x1;
+        d[k][2] = g[3 * k + 2] - x2;
+        R[k] = sqrt(d[k][0] * d[k][0] + d[k][1] * d[k][1] + d[k][2] * d[k][2]);
+    }
+    const double *n = g + 9;
+    const double h = self ? 0.0 : -(n[0] * d[0][0] + n[1] * d[0][1] + n[2] * d[0][2]);
+    const double ah = fabs(h), sg = h > 0 ? 1.0 : h < 0 ? -1.0 : 0.0;
+    double spf = 0, sb = 0, gm[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int a = i, b = (i + 1) % 3;
+        const double *t = g + 12 + 3 * i, *m = g + 21 + 3 * i;
+        const double sm = d[a][0] * t[0] + d[a][1] * t[1] + d[a][2] * t[2];
+        const double sp = d[b][0] * t[0] + d[b][1] * t[1] + d[b][2] * t[2];
+        const double pd = d[a][0] * m[0] + d[a][1] * m[1] + d[a][2] * m[2];
+        const double r0 = pd * pd + h * h;
+        sb += atan2(pd * sp, r0 + ah * R[b]) - atan2(pd * sm, r0 + ah * R[a]);
+        if (CHG) {
+            const double f = (sp + sm >= 0) ? log((R[b] + sp) / (R[a] + sm)) : log((R[a] - sm) / (R[b] - sp));
+            spf += pd * f;
+            if (fld) { gm[0] += m[0] * f; gm[1] += m[1] * f; gm[2] += m[2] * f; }
+        }
+        if (DIP && fld) {
+            const double co = (R[a] + R[b]) /
+                              (R[a] * R[b] * (R[a] * R[b] + d[a][0] * d[b][0] + d[a][1] * d[b][1] + d[a][2] * d[b][2]));
+            bs[0] += (d[a][1] * d[b][2] - d[a][2] * d[b][1]) * co;
+            bs[1] += (d[a][2] * d[b][0] - d[a][0] * d[b][2]) * co;
+            bs[2] += (d[a][0] * d[b][1] - d[a][1] * d[b][0]) * co;
+        }
+    }
+    if (CHG) {
+        S = spf - ah * sb;
+        gS[0] = -gm[0] - sg * n[0] * sb;
+        gS[1] = -gm[1] - sg * n[1] * sb;
+        gS[2] = -gm[2] - sg * n[2] * sb;
+    }
+    if (DIP) {
+        D = sg * sb;
+        gD[0] = -bs[0]; gD[1] = -bs[1]; gD[2] = -bs[2];
+    }
+}
+
+constexpr int kTriThreads = 128;
+
+// Adds triangle j's contribution (charge q, dipstr dq) at one point to pot / fld sums.
+template <bool CHG, bool DIP>
+__device__ __forceinline__ void tri_accum(const double *g, double2 q, double2 dq, double x0, double x1, double x2,
+                                          bool self, bool fld, double (&acc)[8])
+{
+    double S = 0, D = 0, gS[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
+    tri_pair<CHG, DIP>(g, x0, x1, x2, self, fld, S, gS, D, gD);
+    if (CHG) {
+        acc[0] = fma(q.x, S, acc[0]);
+        acc[1] = fma(q.y, S, acc[1]);
+        if (fld)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                acc[2 + 2 * c] = fma(-q.x, gS[c], acc[2 + 2 * c]);
+                acc[3 + 2 * c] = fma(-q.y, gS[c], acc[3 + 2 * c]);
+            }
+    }
+    if (DIP) {
+        acc[0] = fma(dq.x, D, acc[0]);
+        acc[1] = fma(dq.y, D, acc[1]);
+        if (fld)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                acc[2 + 2 * c] = fma(-dq.x, gD[c], acc[2 + 2 * c]);
+                acc[3 + 2 * c] = fma(-dq.y, gD[c], acc[3 + 2 * c]);
+            }
+    }
+}
+
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kTriThreads) k_p2p_tri(const int *leaves, TreeView tv, TriSoA t, const double *sx,
+                                                         const double *sy, const double *sz, const double *tx,
+                                                         const double *ty, const double *tz, OutSoA outs,
+                                                         OutSoA outt, int do_src, int do_trg, int want_fs,
+                                                         int want_ft)
+{
+    __shared__ double sg[kTriThreads * kTriGeo];
+    __shared__ double2 sq[kTriThreads], sd[kTriThreads];
+    const int b = leaves[blockIdx.x];
+    const int s0 = tv.src0[b], ns = do_src ? tv.nsrc[b] : 0;
+    const int t0 = tv.trg0[b], nt = do_trg ? tv.ntrg[b] : 0;
+    const int ne = ns + nt;
+    const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
+    for (int e0 = 0; e0 < ne; e0 += kTriThreads) {
+        const int e = e0 + threadIdx.x;
+        const bool act = e < ne, is_src = e < ns;
+        double x0 = 0, x1 = 0, x2 = 0;
+        int self = -1;
+        if (act) {
+            if (is_src) { const int i = s0 + e; x0 = sx[i]; x1 = sy[i]; x2 = sz[i]; self = i; }
+            else { const int i = t0 + e - ns; x0 = tx[i]; x1 = ty[i]; x2 = tz[i]; }
+        }
+        const bool fld = is_src ? want_fs != 0 : want_ft != 0;
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int j = 0; j < nl; j++) {
+            const int jb = j == 0 ? b : tv.l1_idx[l1a + j - 1];
+            const int js0 = tv.src0[jb], jn = tv.nsrc[jb];
+            for (int c0 = 0; c0 < jn; c0 += kTriThreads) {
+                const int cn = min(kTriThreads, jn - c0);
+                __syncthreads();
+                const double *gsrc = t.geo + (size_t)kTriGeo * (js0 + c0);
+                for (int k = threadIdx.x; k < cn * kTriGeo; k += kTriThreads) sg[k] = gsrc[k];
+                if (threadIdx.x < cn) {
+                    if (CHG) sq[threadIdx.x] = t.q[js0 + c0 + threadIdx.x];
+                    if (DIP) sd[threadIdx.x] = t.dq[js0 + c0 + threadIdx.x];
+                }
+                __syncthreads();
+                if (!act) continue;
+                const int selfk = self - (js0 + c0);
+                for (int k = 0; k < cn; k++)
+                    tri_accum<CHG, DIP>(sg + kTriGeo * k, CHG ? sq[k] : cmk(0, 0), DIP ? sd[k] : cmk(0, 0), x0, x1,
+                                        x2, k == selfk, fld, acc);
+            }
+        }
+        if (act) {
+            const OutSoA &o = is_src ? outs : outt;
+            const int i = is_src ? s0 + e : t0 + e - ns;
+            if (o.pot) o.pot[i] = cadd(o.pot[i], cmk(acc[0], acc[1]));
+            if (fld && o.fx) {
+                o.fx[i] = cadd(o.fx[i], cmk(acc[2], acc[3]));
+                o.fy[i] = cadd(o.fy[i], cmk(acc[4], acc[5]));
+                o.fz[i] = cadd(o.fz[i], cmk(acc[6], acc[7]));
+            }
+        }
+    }
+}
+
+void launch_p2p_tri(const int *leaves, int nleaves, const TreeView &tv, const TriSoA &t, const double *sx,
+                    const double *sy, const double *sz, const double *tx, const double *ty, const double *tz,
+                    OutSoA outs, OutSoA outt, int ifcharge, int ifdipole, int do_src, int do_trg, int want_fs,
+                    int want_ft, cudaStream_t s, Status &st)
+{
+    if (nleaves == 0 || !st.ok() || !(do_src || do_trg)) return;
+    const bool c = ifcharge == 1, d = ifdipole == 1;
+    if (c && d)
+        k_p2p_tri<true, true><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, outs, outt,
+                                                              do_src, do_trg, want_fs, want_ft);
+    else if (c)
+        k_p2p_tri<true, false><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, outs, outt,
+                                                               do_src, do_trg, want_fs, want_ft);
+    else if (d)
+        k_p2p_tri<false, true><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, outs, outt,
+                                                               do_src, do_trg, want_fs, want_ft);
+    else
+        return;
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// l3dtriadirect: one point per thread against every triangle, staged in chunks.
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kTriThreads) k_tri_direct(int ntri, TriSoA t, int npts, const double *pts,
+                                                            int centroids, int want_f, double *pot, double *fld)
+{
+    __shared__ double sg[kTriThreads * kTriGeo];
+    __shared__ double2 sq[kTriThreads], sd[kTriThreads];
+    const int i = blockIdx.x * kTriThreads + threadIdx.x;
+    const bool act = i < npts;
+    double x0 = 0, x1 = 0, x2 = 0;
+    int self = -1;
+    if (act) {
+        x0 = pts[3L * i]; x1 = pts[3L * i + 1]; x2 = pts[3L * i + 2];
+        if (centroids) self = i;
+    }
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c0 = 0; c0 < ntri; c0 += kTriThreads) {
+        const int cn = min(kTriThreads, ntri - c0);
+        __syncthreads();
+        const double *gsrc = t.geo + (size_t)kTriGeo * c0;
+        for (int k = threadIdx.x; k < cn * kTriGeo; k += kTriThreads) sg[k] = gsrc[k];
+        if (threadIdx.x < cn) {
+            if (CHG) sq[threadIdx.x] = t.q[c0 + threadIdx.x];
+            if (DIP) sd[threadIdx.x] = t.dq[c0 + threadIdx.x];
+        }
+        __syncthreads();
+        if (!act) continue;
+        for (int k = 0; k < cn; k++)
+            tri_accum<CHG, DIP>(sg + kTriGeo * k, CHG ? sq[k] : cmk(0, 0), DIP ? sd[k] : cmk(0, 0), x0, x1, x2,
+                                c0 + k == self, want_f != 0, acc);
+    }
+    if (!act) return;
+    if (pot) { pot[2L * i] = acc[0]; pot[2L * i + 1] = acc[1]; }
+    if (fld)
+        for (int c = 0; c < 6; c++) fld[6L * i + c] = acc[2 + c];
+}
+
+void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
+                       int centroids, double *pot, double *fld, cudaStream_t s, Status &st)
+{
+    if (npts <= 0 || !st.ok()) return;
+    const bool c = ifcharge == 1, d = ifdipole == 1;
+    const int grid = (npts + kTriThreads - 1) / kTriThreads;
+    if (!c && !d) {
+        if (pot) FMM_TRY(st, cudaMemsetAsync(pot, 0, sizeof(double) * 2 * npts, s));
+        if (fld) FMM_TRY(st, cudaMemsetAsync(fld, 0, sizeof(double) * 6 * npts, s));
+        return;
+    }
+    if (c && d) k_tri_direct<true, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
+    else if (c) k_tri_direct<true, false><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
+    else k_tri_direct<false, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+}  // namespace fmm

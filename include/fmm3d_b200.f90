@@ -90,6 +90,41 @@ module fmm3d_b200
     end subroutine
 
     ! Arithmetic form of later calls: 0 FP64 (default), 1 mixed precision for iprec <= 1.
+    ! Layer potentials of flat triangles (lfmm3dtriatarg, lfmm3dtriaself, lfmm3dtria, l3dtriadirect)
+    subroutine lfmm3dtriatarg(ier, iprec, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg) &
+        bind(C, name="lfmm3dtriatarg_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld, ntarget, ifpottarg, iffldtarg
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *), target(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), pottarg(*), fldtarg(3, *)
+    end subroutine
+
+    subroutine lfmm3dtriaself(ier, iprec, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld) bind(C, name="lfmm3dtriaself_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *)
+    end subroutine
+
+    subroutine lfmm3dtria(ier, iprec, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld) bind(C, name="lfmm3dtria_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *)
+    end subroutine
+
+    subroutine l3dtriadirect(nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, dipvec, &
+        ifpot, pot, iffld, fld, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg) &
+        bind(C, name="l3dtriadirect_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: nsource, ifcharge, ifdipole, ifpot, iffld, ntarget, ifpottarg, iffldtarg
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *), target(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), pottarg(*), fldtarg(3, *)
+    end subroutine
+
     ! Hessians: the reference's one-point evaluators, and lfmm3dparttarg with Hessian outputs
     ! (hess(6, n): dxx, dyy, dzz, dxy, dxz, dyz; no counterpart in the reference)
     subroutine l3dtaevalhess(rscale, center, local, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier) &

@@ -71,6 +71,43 @@ void h3dpartdirect_(const double *zk, const int *nsource, const double *source, 
                     const double *target, const int *ifpottarg, double *pottarg, const int *iffldtarg,
                     double *fldtarg);
 
+/* Replaces lfmm3dtriatarg (src/lfmm3dtria.f:121-546): Laplace layer
+ * potentials of flat triangles triaflat(3,3,nsource) (vertices), with
+ * piecewise-constant single-layer density charge and double-layer density
+ * dipstr, at the triangles' centroids source(3,nsource) and at targets.
+ * pot = sum int charge/|x-y| + dipstr n.(x-y)/|x-y|^3 dS_y, fld = -grad pot.
+ * As in the reference, the double layer is oriented by the triangle's
+ * vertex-order normal (v2-v1)x(v3-v1) in the near field and by trianorm in
+ * the far field (trianorm must equal that unit normal), and dipvec is not
+ * used.  nbox per iprec and the near field by exact integrals follow the
+ * reference; the far-field quadrature is a collapsed Gauss-Legendre rule of
+ * the reference's polynomial degree (the reference's triasymq tables are not
+ * used).  Always FP64.  ier as lfmm3dparttarg_. */
+void lfmm3dtriatarg_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                     const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                     const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                     double *fld, const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
+                     const int *iffldtarg, double *fldtarg);
+
+/* Replaces lfmm3dtriaself (src/lfmm3dtria.f:80-114) and lfmm3dtria (:39-73): no targets. */
+void lfmm3dtriaself_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                     const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                     const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                     double *fld);
+void lfmm3dtria_(int *ier, const int *iprec, const int *nsource, const double *triaflat, const double *trianorm,
+                 const double *source, const int *ifcharge, const double *charge, const int *ifdipole,
+                 const double *dipstr, const double *dipvec, const int *ifpot, double *pot, const int *iffld,
+                 double *fld);
+
+/* Replaces l3dtriadirect (src/lfmm3dtria.f:1385-1560): the O(N^2) sum of the
+ * exact triangle integrals (each centroid takes its own triangle's in-plane
+ * values). */
+void l3dtriadirect_(const int *nsource, const double *triaflat, const double *trianorm, const double *source,
+                    const int *ifcharge, const double *charge, const int *ifdipole, const double *dipstr,
+                    const double *dipvec, const int *ifpot, double *pot, const int *iffld, double *fld,
+                    const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
+                    const int *iffldtarg, double *fldtarg);
+
 /* Replaces l3dtaevalhess (src/laprouts3d.f:5297-5363; it calls
  * l3dtaevalhessdini + l3dtaevalhessd, :7613, :7384) and l3dmpevalhess
  * (:5229-5295; l3dmpevalhessdini + l3dmpevalhessd, :7129, :6945): potential,
@@ -104,6 +141,19 @@ void lfmm3dparttarghess_(int *ier, const int *iprec, const int *nsource, const d
                          double *hess, const int *ntarget, const double *target, const int *ifpottarg,
                          double *pottarg, const int *iffldtarg, double *fldtarg, const int *ifhesstarg,
                          double *hesstarg);
+
+/* lfmm3dtriatarg_ and l3dtriadirect_ on device-resident arrays (same
+ * layouts), enqueued on `stream`; the direct sum waits for its stream. */
+int fmm3d_lfmm3dtriatarg_device(int iprec, int nsource, const double *d_triaflat, const double *d_trianorm,
+                                const double *d_source, int ifcharge, const double *d_charge, int ifdipole,
+                                const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot, int iffld,
+                                double *d_fld, int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
+                                int iffldtarg, double *d_fldtarg, void *stream);
+int fmm3d_l3dtriadirect_device(int nsource, const double *d_triaflat, const double *d_trianorm,
+                               const double *d_source, int ifcharge, const double *d_charge, int ifdipole,
+                               const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot, int iffld,
+                               double *d_fld, int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
+                               int iffldtarg, double *d_fldtarg, void *stream);
 
 /* The same on device-resident arrays, enqueued on `stream`. */
 int fmm3d_lfmm3dparttarg_hess_device(int iprec, int nsource, const double *d_source, int ifcharge,

@@ -1079,6 +1079,93 @@ static void mpevalhess(double rscale, const double *center, const cplx *mp, int 
 static void direct_hess_one(int ns, const double *src, int ifcharge, const cplx *charge, int ifdipole,
                             const cplx *dipstr, const double *dipvec, const double *t, long skip, cplx h[6]);
 
+/* STEPS 3-5 of lfmm3dparttargmain (M2M, M2L over list 2, L2L), shared by the
+ * particle and the triangle FMM (src/lfmm3dtria.f:904 calls the same
+ * lfmm3d_list2).  tm[2..4] receive the pass start times. */
+static void far_passes(const otree *tp, int p, double eps, cplx *mpole, cplx *local, int ifprune, double *tm)
+{
+    const otree T = *tp;
+    const int K = (p + 1) * (p + 1);
+    (void)K;
+#define BX(b, f) T.box[20 * (size_t)(b) + (f)]
+#define LS(ty, b) T.lstart[ty][b]
+#define LE(ty, b) T.lstart[ty][(b) + 1]
+#define LI(ty, i) T.lidx[ty][i]
+    /* STEP 3: M2M, levels nlev-1..2 (src/lfmm3drouts.f:195-258) */
+    tm[2] = omp_get_wtime();
+    double *dc = make_dc(2 * p + 2);
+    int ldc = 2 * p + 2;
+    for (int lev = T.nlev - 1; lev >= 2; lev--) {
+        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
+#pragma omp parallel for schedule(dynamic)
+        for (int ib = b0; ib < b1; ib++) {
+            if (BX(ib, B_NSRC) == 0 || nkids(&T, ib) == 0) continue;
+            cplx *mo = mpole + (size_t)ib * K;
+            memset(mo, 0, sizeof(cplx) * K);
+            for (int k = 0; k < 8; k++) {
+                int jb = BX(ib, B_KID + k);
+                if (jb < 0) continue;
+                translate(0, T.center + 3 * (size_t)jb, T.center + 3 * (size_t)ib, mpole + (size_t)jb * K, p, p,
+                          mo, dc, ldc, NULL, NULL);
+            }
+        }
+    }
+    /* STEP 4: M2L over list 2, levels 2..nlev (src/lfmm3drouts.f:347-483),
+     * with precomputed rotations per offset (:297-337).                  */
+    tm[3] = omp_get_wtime();
+    int itable[343];
+    oracle_l3dterms_list2(eps, itable);
+    size_t rsz = (size_t)(p + 1) * (p + 1) * (2 * p + 1);
+    double *rotf = malloc(rsz * 343 * sizeof(double)), *rotb = malloc(rsz * 343 * sizeof(double));
+#pragma omp parallel for
+    for (int o = 0; o < 343; o++) {
+        int i = o / 49 - 3, j = (o / 7) % 7 - 3, k = o % 7 - 3;
+        if (i == 0 && j == 0 && k == 0) continue;
+        double rv[3] = {i, j, k}, d, th, ph;
+        cart2polarl(rv, &d, &th, &ph);
+        rot_init(rotf + rsz * o, p, th);
+        rot_init(rotb + rsz * o, p, -th);
+    }
+    for (int lev = 2; lev <= T.nlev; lev++) {
+        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
+#pragma omp parallel for schedule(dynamic)
+        for (int ib = b0; ib < b1; ib++) {
+            for (int li = LS(2, ib); li < LE(2, ib); li++) {
+                int jb = LI(2, li);
+                if (BX(jb, B_NSRC) == 0) continue;
+                if (BX(ib, B_NTRG) == 0 && ifprune) continue;
+                int ii = BX(jb, B_I) - BX(ib, B_I), jj = BX(jb, B_J) - BX(ib, B_J), kk = BX(jb, B_K) - BX(ib, B_K);
+                int nt = itable[((ii + 3) * 7 + (jj + 3)) * 7 + (kk + 3)];
+                if (nt > p) nt = p;
+                int o = ((-ii + 3) * 7 + (-jj + 3)) * 7 + (-kk + 3);
+                translate(1, T.center + 3 * (size_t)jb, T.center + 3 * (size_t)ib, mpole + (size_t)jb * K, p, nt,
+                          local + (size_t)ib * K, dc, ldc, rotf + rsz * o, rotb + rsz * o);
+            }
+        }
+    }
+    free(rotf); free(rotb);
+    /* STEP 5: L2L, levels 2..nlev-1 (src/lfmm3drouts.f:498-558) */
+    tm[4] = omp_get_wtime();
+    for (int lev = 2; lev <= T.nlev - 1; lev++) {
+        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
+#pragma omp parallel for schedule(dynamic)
+        for (int ib = b0; ib < b1; ib++) {
+            if (nkids(&T, ib) == 0) continue;
+            for (int k = 0; k < 8; k++) {
+                int jb = BX(ib, B_KID + k);
+                if (jb < 0) continue;
+                translate(2, T.center + 3 * (size_t)ib, T.center + 3 * (size_t)jb, local + (size_t)ib * K, p, p,
+                          local + (size_t)jb * K, dc, ldc, NULL, NULL);
+            }
+        }
+    }
+    free(dc);
+#undef BX
+#undef LS
+#undef LE
+#undef LI
+}
+
 /* lfmm3dparttarg with optional Hessian outputs (ifhess / ifhesstarg, 6 per
  * point).  Potentials and fields are computed exactly as without them; the
  * Hessians add, at each evaluation point, the list-3 multipoles
@@ -1151,76 +1238,7 @@ static void lfmm_core(int *ier, int iprec, int nsource, const double *source, in
                           T.center + 3 * (size_t)ib, p, local + (size_t)ib * K);
         }
     }
-    /* STEP 3: M2M, levels nlev-1..2 (src/lfmm3drouts.f:195-258) */
-    tm[2] = omp_get_wtime();
-    double *dc = make_dc(2 * p + 2);
-    int ldc = 2 * p + 2;
-    for (int lev = T.nlev - 1; lev >= 2; lev--) {
-        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
-#pragma omp parallel for schedule(dynamic)
-        for (int ib = b0; ib < b1; ib++) {
-            if (BX(ib, B_NSRC) == 0 || nkids(&T, ib) == 0) continue;
-            cplx *mo = mpole + (size_t)ib * K;
-            memset(mo, 0, sizeof(cplx) * K);
-            for (int k = 0; k < 8; k++) {
-                int jb = BX(ib, B_KID + k);
-                if (jb < 0) continue;
-                translate(0, T.center + 3 * (size_t)jb, T.center + 3 * (size_t)ib, mpole + (size_t)jb * K, p, p,
-                          mo, dc, ldc, NULL, NULL);
-            }
-        }
-    }
-    /* STEP 4: M2L over list 2, levels 2..nlev (src/lfmm3drouts.f:347-483),
-     * with precomputed rotations per offset (:297-337).                  */
-    tm[3] = omp_get_wtime();
-    int itable[343];
-    oracle_l3dterms_list2(eps, itable);
-    int ifprune = !(ifpot == 1 || iffld == 1 || ifhess == 1);
-    size_t rsz = (size_t)(p + 1) * (p + 1) * (2 * p + 1);
-    double *rotf = malloc(rsz * 343 * sizeof(double)), *rotb = malloc(rsz * 343 * sizeof(double));
-#pragma omp parallel for
-    for (int o = 0; o < 343; o++) {
-        int i = o / 49 - 3, j = (o / 7) % 7 - 3, k = o % 7 - 3;
-        if (i == 0 && j == 0 && k == 0) continue;
-        double rv[3] = {i, j, k}, d, th, ph;
-        cart2polarl(rv, &d, &th, &ph);
-        rot_init(rotf + rsz * o, p, th);
-        rot_init(rotb + rsz * o, p, -th);
-    }
-    for (int lev = 2; lev <= T.nlev; lev++) {
-        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
-#pragma omp parallel for schedule(dynamic)
-        for (int ib = b0; ib < b1; ib++) {
-            for (int li = LS(2, ib); li < LE(2, ib); li++) {
-                int jb = LI(2, li);
-                if (BX(jb, B_NSRC) == 0) continue;
-                if (BX(ib, B_NTRG) == 0 && ifprune) continue;
-                int ii = BX(jb, B_I) - BX(ib, B_I), jj = BX(jb, B_J) - BX(ib, B_J), kk = BX(jb, B_K) - BX(ib, B_K);
-                int nt = itable[((ii + 3) * 7 + (jj + 3)) * 7 + (kk + 3)];
-                if (nt > p) nt = p;
-                int o = ((-ii + 3) * 7 + (-jj + 3)) * 7 + (-kk + 3);
-                translate(1, T.center + 3 * (size_t)jb, T.center + 3 * (size_t)ib, mpole + (size_t)jb * K, p, nt,
-                          local + (size_t)ib * K, dc, ldc, rotf + rsz * o, rotb + rsz * o);
-            }
-        }
-    }
-    free(rotf); free(rotb);
-    /* STEP 5: L2L, levels 2..nlev-1 (src/lfmm3drouts.f:498-558) */
-    tm[4] = omp_get_wtime();
-    for (int lev = 2; lev <= T.nlev - 1; lev++) {
-        int b0 = T.laddr[2 * lev], b1 = b0 + T.laddr[2 * lev + 1];
-#pragma omp parallel for schedule(dynamic)
-        for (int ib = b0; ib < b1; ib++) {
-            if (nkids(&T, ib) == 0) continue;
-            for (int k = 0; k < 8; k++) {
-                int jb = BX(ib, B_KID + k);
-                if (jb < 0) continue;
-                translate(2, T.center + 3 * (size_t)ib, T.center + 3 * (size_t)jb, local + (size_t)ib * K, p, p,
-                          local + (size_t)jb * K, dc, ldc, NULL, NULL);
-            }
-        }
-    }
-    free(dc);
+    far_passes(&T, p, eps, mpole, local, !(ifpot == 1 || iffld == 1 || ifhess == 1), tm);
     /* STEP 6: M2P from list-3 boxes (src/lfmm3dpart.f:907-984) */
     tm[5] = omp_get_wtime();
 #pragma omp parallel
@@ -1370,3 +1388,6 @@ void oracle_lfmm3dparttarg_hess(int *ier, int iprec, int nsource, const double *
 
 /* Laplace Hessians (pair, local and multipole evaluators, FMM driver). */
 #include "lhess_oracle.c"
+
+/* Laplace layer potentials on flat triangles (lfmm3dtriatarg). */
+#include "ltri_oracle.c"

@@ -181,6 +181,64 @@ def lfmm3dparttarg_hess(iprec, source, charge=None, dipstr=None, dipvec=None, ta
     return ier.value, pot[:n], fld[:n], hs[:n], pt[:m], ft[:m], ht[:m]
 
 
+# ---------------------------------------------------------------- triangles
+
+def tri_near(tri, pts, self=False):
+    """Exact single / double layer integrals of one flat triangle (3,3) at pts:
+    (S, grad S, D, grad D); self: pts are the triangle's own centroid (in-plane values)."""
+    v = _f64(tri, (3, 3))
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    S, D = np.zeros(k), np.zeros(k)
+    gS, gD = np.zeros((k, 3)), np.zeros((k, 3))
+    lib().oracle_tri_near(_p(v), c_int(k), _p(pts), c_int(int(self)), _p(S), _p(gS), _p(D), _p(gD))
+    return S, gS, D, gD
+
+
+def tri_rule(norder):
+    xi, eta, w = np.zeros(64), np.zeros(64), np.zeros(64)
+    nq = c_int(0)
+    lib().oracle_tri_rule(c_int(norder), _p(xi), _p(eta), _p(w), ctypes.byref(nq))
+    return xi[:nq.value], eta[:nq.value], w[:nq.value]
+
+
+def tri_nbox(iprec, ns, nt=0):
+    lib().oracle_tri_nbox.restype = c_int
+    return lib().oracle_tri_nbox(c_int(iprec), c_int(ns), c_int(nt))
+
+
+def l3dtriadirect(triaflat, source, charge=None, dipstr=None, target=None, ifpot=1, iffld=1, ifpottarg=1,
+                  iffldtarg=1):
+    """O(N^2) layer potentials (l3dtriadirect): (pot, fld, pottarg, fldtarg)."""
+    tri = _f64(triaflat, (0, 3, 3)); n = tri.shape[0]
+    src = _f64(source, (0, 3))
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3)); m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128); fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128); ft = np.zeros((max(m, 1), 3), np.complex128)
+    lib().oracle_l3dtriadirect(c_int(n), _p(tri), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                               c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), c_int(ifpot), _p(pot),
+                               c_int(iffld), _p(fld), c_int(m), _p(trg if m else np.zeros((1, 3))),
+                               c_int(ifpottarg if m else 0), _p(pt), c_int(iffldtarg if m else 0), _p(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def lfmm3dtriatarg(iprec, triaflat, trianorm, source, charge=None, dipstr=None, target=None, ifpot=1, iffld=1,
+                   ifpottarg=1, iffldtarg=1):
+    """lfmm3dtriatarg: (ier, pot, fld, pottarg, fldtarg)."""
+    tri = _f64(triaflat, (0, 3, 3)); n = tri.shape[0]
+    nrm = _f64(trianorm, (0, 3))
+    src = _f64(source, (0, 3))
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3)); m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128); fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128); ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = c_int(0)
+    lib().oracle_lfmm3dtriatarg(ctypes.byref(ier), c_int(iprec), c_int(n), _p(tri), _p(nrm), _p(src),
+                                c_int(int(charge is not None)), _p(_c128(charge, n)), c_int(int(dipstr is not None)),
+                                _p(_c128(dipstr, n)), c_int(ifpot), _p(pot), c_int(iffld), _p(fld), c_int(m),
+                                _p(trg if m else np.zeros((1, 3))), c_int(ifpottarg if m else 0), _p(pt),
+                                c_int(iffldtarg if m else 0), _p(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
 class Tree:
     """The oracle's octree (d3tstrcr semantics) exported as numpy arrays."""
 
