@@ -59,6 +59,9 @@ cores with operands split into TF32 pairs, FP64 elsewhere; the headline) and
             in the mixed form; serving_repeated: the Laplace requests drawn from
             8 repeated source sets with fresh charges, served by resident plans
             (tree kept on the device, CUDA-graph replay).
+  laplace_triangles  lfmm3dtriaself on an icosphere of 327,680 flat
+            triangles (unit sphere), single and double layer, iprec 1, FP64;
+            errors against the exact direct sum at sampled centroids.
   helmholtz the Helmholtz workload measured in the same run (not the
             headline): hfmm3dpartself on N = 1,000,000 sources uniform on the
             unit sphere, zk = 8 pi, charges uniform in the unit disk, iprec = 2,
@@ -119,7 +122,9 @@ def parse_args(argv=None):
     ap.add_argument("--serve-rates", default="20,60,inf", help="Poisson arrival rates (requests/s)")
     ap.add_argument("--autotune", metavar="PATH", default=None,
                     help="tune the Laplace workloads' launch shapes into the JSON cache PATH and exit")
-    ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched"], default="all",
+    ap.add_argument("--tri-level", type=int, default=7,
+                    help="triangle workload: icosphere subdivision level (20 * 4^level triangles)")
+    ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched", "triangles"], default="all",
                     help="all: the Laplace headline line with the other workloads' objects (default); "
                          "laplace / helmholtz / batched: one workload only (profiling runs)")
     return ap.parse_args(argv)
@@ -208,6 +213,105 @@ def run_laplace_sphere(args, R, n=100_000):
             line.setdefault("parity", {})["laplace_sphere"] = rep
             out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
                                    "kind": "port", "sample": "the whole workload, one call (%.2f s)" % dt}
+
+        R.setdefault("cpu_jobs", []).append(cpu_job)
+    return out
+
+
+def run_triangles(args, R, k=7, iprec=1):
+    """lfmm3dtriaself on a triangulated unit sphere (icosphere of 20 * 4^k flat triangles), single and
+    double layer with densities in [-1, 1]^2, iprec 1, FP64: device time, errors against the exact
+    direct sum at sampled centroids, and the oracle (parity, CPU baseline) on the same inputs."""
+    from fmmlib3d_b200.meshes import icosphere, normals_centroids
+    torch, F = R["torch"], R["F"]
+    T = icosphere(k)
+    nrm, cen = normals_centroids(T)
+    n = len(T)
+    rng = np.random.default_rng(11)
+    q = np.stack([rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)], 1)
+    dq = np.stack([rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)], 1)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64).reshape(n, -1)).to(dev)
+    d_tri, d_nrm, d_cen, d_q, d_dq = d(T.reshape(n, 9)), d(nrm), d(cen), d(q), d(dq)
+    d_pot = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_fld = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step(pot=d_pot, fld=d_fld):
+        ier = F.lfmm3dtriatarg_device(iprec, d_tri, d_nrm, d_cen, d_q, d_dq, pot, fld, stream=stream)
+        if ier != 0:
+            raise RuntimeError("triangle FMM ier=%d: %s" % (ier, F.last_error()))
+
+    def timed(**kw):
+        for _ in range(args.warmup):
+            step(**kw)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(args.steps):
+            step(**kw)
+        ev[1].record()
+        torch.cuda.synchronize()
+        t = ev[0].elapsed_time(ev[1]) / args.steps
+        F.set_timing(True)
+        step(**kw)
+        torch.cuda.synchronize()
+        ps = F.last_timing()
+        F.set_timing(False)
+        return t, ps
+
+    ms, passes = timed()
+    # the mixed form: M2L on the tensor cores, the exact near field FP64
+    m_pot = torch.empty_like(d_pot)
+    m_fld = torch.empty_like(d_fld)
+    F.set_precision(1)
+    try:
+        ms_mixed, passes_mixed = timed(pot=m_pot, fld=m_fld)
+    finally:
+        F.set_precision(0)
+    m = min(args.err_samples, n)
+    si = np.sort(rng.choice(n, m, replace=False)).astype(np.int32)
+    it = torch.from_numpy(si).to(dev)
+    dp = torch.empty((m, 2), dtype=torch.float64, device=dev)
+    df = torch.empty((m, 6), dtype=torch.float64, device=dev)
+    ier = F.tri_direct_points_device(d_tri, d_q, d_dq, d_cen[it.long()].contiguous(), it, dp, df, stream=stream)
+    torch.cuda.synchronize()
+    if ier != 0:
+        raise RuntimeError("triangle direct ier=%d" % ier)
+    gp, gf = d_pot[it.long()], d_fld[it.long()]
+    out = {"workload": "laplace_lfmm3dtriaself_icosphere_%d_triangles_iprec%d" % (n, iprec), "n_triangles": n,
+           "iprec": iprec, "dtype": "f64", "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "pass_ms": {kk: round(v, 3) for kk, v in passes.items()},
+           "errors": {"pot": float("%.3e" % float(torch.linalg.norm(gp - dp) / torch.linalg.norm(dp))),
+                      "fld": float("%.3e" % float(torch.linalg.norm(gf - df) / torch.linalg.norm(df)))},
+           "note": "errors against the exact direct sum (l3dtriadirect) at %d sampled centroids" % m}
+    mp, mf = m_pot[it.long()], m_fld[it.long()]
+    out["mixed"] = {"value": n / (ms_mixed * 1e-3), "ms_per_step": ms_mixed,
+                    "pass_ms": {kk: round(v, 3) for kk, v in passes_mixed.items()},
+                    "errors": {"pot": float("%.3e" % float(torch.linalg.norm(mp - dp) / torch.linalg.norm(dp))),
+                               "fld": float("%.3e" % float(torch.linalg.norm(mf - df) / torch.linalg.norm(df)))},
+                    "form": "M2L on the tensor cores (split TF32); near field and other passes FP64"}
+    if R["rank"] == 0 and not args.no_cpu:
+        gv = {"pot": gp.cpu().numpy(), "fld": gf.cpu().numpy()}
+        mv = {"pot": mp.cpu().numpy(), "fld": mf.cpu().numpy()}
+        gd = {"pot": dp.cpu().numpy(), "fld": df.cpu().numpy()}
+
+        def cpu_job(line):
+            import oracle
+            c = lambda a: a[:, 0] + 1j * a[:, 1]
+            t0 = time.perf_counter()
+            oier, opot, ofld, _, _ = oracle.lfmm3dtriatarg(iprec, T, nrm, cen, c(q), c(dq))
+            dt = time.perf_counter() - t0
+            if oier != 0:
+                raise RuntimeError("oracle ier=%d" % oier)
+            tp, tf = oracle.tri_direct_at(T, cen[si], si, c(q), c(dq))
+            rep = parity_report({"pot": _as_pairs(opot[si], 2), "fld": _as_pairs(ofld[si], 6)},
+                                {"pot": _as_pairs(tp, 2), "fld": _as_pairs(tf, 6)}, {"fp64": gv, "mixed": mv}, gd)
+            rep.update(points="%d seeded centroids (own triangle in-plane)" % m,
+                       inputs="the triangle workload's own inputs", oracle_call_s=round(dt, 2))
+            line.setdefault("parity", {})["laplace_triangles"] = rep
+            out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
+                                   "kind": "port", "sample": "the whole workload, one call (%.1f s)" % dt}
 
         R.setdefault("cpu_jobs", []).append(cpu_job)
     return out
@@ -1040,6 +1144,18 @@ def main(argv=None):
             dt, line["parity"] = oracle_helm_parity(R.pop("helm_samples"))
         print(json.dumps(line), flush=True)
         return 0
+    if args.workload == "triangles":
+        import torch
+        import fmmlib3d_b200 as F
+        torch.cuda.set_device(dist_env()[2])
+        R = dict(torch=torch, F=F, rank=rank, ws=1, dist=None)
+        out = run_triangles(args, R, k=args.tri_level)
+        line = {"metric": "triangle FMM triangles/s (icosphere, iprec=1)", "value": out["value"], "unit": UNIT,
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "laplace_triangles": out}
+        for job in R.get("cpu_jobs", []):
+            job(line)
+        print(json.dumps(line), flush=True)
+        return 0
     if args.workload == "batched":
         import torch
         import fmmlib3d_b200 as F
@@ -1103,6 +1219,7 @@ def main(argv=None):
 
         cpu_jobs.append(cube_job)
     line["laplace_sphere"] = run_laplace_sphere(args, R)
+    line["laplace_triangles"] = run_triangles(args, R, k=args.tri_level)
     if args.n == 2_000_000 and args.iprec == 1:
         line["laplace_iprec2"] = run_iprec2(args, R)
     if args.batch_instances > 0:

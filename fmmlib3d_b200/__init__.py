@@ -61,6 +61,8 @@ for _name in ("lfmm3dtriatarg_", "lfmm3dtriaself_", "lfmm3dtria_", "l3dtriadirec
 _lib.fmm3d_lfmm3dtriatarg_device.restype = _I
 _lib.fmm3d_lfmm3dtriatarg_device.argtypes = [_I, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
                                              _I, _P, _P]
+_lib.fmm3d_l3dtriadirect_points_device.restype = _I
+_lib.fmm3d_l3dtriadirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _P]
 _lib.fmm3d_l3dtriadirect_device.restype = _I
 _lib.fmm3d_l3dtriadirect_device.argtypes = [_I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I,
                                             _P, _P]
@@ -330,6 +332,17 @@ def lfmm3dtriatarg_device(iprec, triaflat, trianorm, source, charge, dipstr, pot
         iprec, n, ptr(triaflat), ptr(trianorm), ptr(source), int(charge is not None), ptr(charge),
         int(dipstr is not None), ptr(dipstr), None, int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m,
         ptr(target), int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
+
+
+def tri_direct_points_device(triaflat, charge, dipstr, pts, self_idx, pot, fld, stream=0):
+    """Triangle direct sum at device points ``pts`` (M,3); ``self_idx`` int32 (M,) (the triangle whose
+    centroid the point is, or -1) or None; ``pot`` (M,2), ``fld`` (M,6) float64.  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = triaflat.shape[0]
+    return _lib.fmm3d_l3dtriadirect_points_device(n, ptr(triaflat), int(charge is not None), ptr(charge),
+                                                  int(dipstr is not None), ptr(dipstr), pts.shape[0], ptr(pts),
+                                                  ptr(self_idx), ptr(pot), ptr(fld), _P(stream))
 
 
 def lfmm3dpartself(iprec, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, iffld):

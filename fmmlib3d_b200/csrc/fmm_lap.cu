@@ -714,6 +714,9 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     S.mixed = !S.tri && form == 1 && iprec <= 1 && plan->dense;
     S.dense = (plan->dense && sw(kSwM2LMode) != 1 && sw(kSwM2LMode) != 3) || S.mixed;
     S.tcm2l = S.mixed && sw(kSwTensorM2L) > 0;
+    // triangles in the mixed form: the M2L runs on the tensor cores (split TF32), the exact
+    // near field and every other pass stay FP64
+    if (S.tri && form == 1 && iprec <= 1 && plan->dense && sw(kSwTensorM2L) > 0) S.dense = S.tcm2l = true;
     // launch shapes: the autotuner's cached setting for this problem, else automatic
     S.signature = lap_signature(S);
     TuneKnobs kn;
@@ -1031,7 +1034,7 @@ static int tri_direct_device(int ns, const double *d_tri, const double *d_src, i
     launch_tri_gather(ns, nullptr, d_tri, nullptr, d_q, d_dq, ifcharge, ifdipole, none, t, PointsSoA(), s, st);
     auto run = [&](int npts, const double *pts, int centroids, int wp, double *op, int wf, double *of) {
         if (!(wp == 1 || wf == 1) || npts <= 0) return;
-        launch_tri_direct(ns, t, ifcharge, ifdipole, npts, pts, centroids, wp == 1 ? op : nullptr,
+        launch_tri_direct(ns, t, ifcharge, ifdipole, npts, pts, centroids, nullptr, wp == 1 ? op : nullptr,
                           wf == 1 ? of : nullptr, s, st);
     };
     run(ns, d_src, 1, ifpot, d_pot, iffld, d_fld);
@@ -1591,6 +1594,30 @@ int fmm3d_l3dtriadirect_device(int nsource, const double *d_triaflat, const doub
     cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
     return tri_direct_device(nsource, d_triaflat, d_source, ifcharge, d_charge, ifdipole, d_dipstr, ifpot, d_pot,
                              iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg, iffldtarg, d_fldtarg, s);
+}
+
+int fmm3d_l3dtriadirect_points_device(int nsource, const double *d_triaflat, int ifcharge, const double *d_charge,
+                                      int ifdipole, const double *d_dipstr, int npts, const double *d_pts,
+                                      const int *d_self, double *d_pot, double *d_fld, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    g_launch_count = 0;
+    Status st;
+    DBuf<double> geo;
+    DBuf<double2> q, dq;
+    TriRule none;
+    bool ok = geo.alloc(30L * std::max(nsource, 1), s, st);
+    if (ifcharge == 1) ok = ok && q.alloc(std::max(nsource, 1), s, st);
+    if (ifdipole == 1) ok = ok && dq.alloc(std::max(nsource, 1), s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    TriSoA t;
+    t.geo = geo.p; t.q = q.p; t.dq = dq.p;
+    launch_tri_gather(nsource, nullptr, d_triaflat, nullptr, d_charge, d_dipstr, ifcharge, ifdipole, none, t,
+                      PointsSoA(), s, st);
+    launch_tri_direct(nsource, t, ifcharge, ifdipole, npts, d_pts, 0, d_self, d_pot, d_fld, s, st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
 }
 
 int fmm3d_l3dpartdirect_device(int nsource, const double *d_source, int ifcharge, const double *d_charge,

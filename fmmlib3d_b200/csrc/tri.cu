@@ -6,14 +6,12 @@
 // direct3dtrilaps2 / direct3dtrilapd2, src/triquadflatlib.f:147-818): for a
 // triangle with unit density, at x,
 //   S = int 1/|x-y| dS,   D = int n.(x-y)/|x-y|^3 dS   (n: vertex-order normal),
-// and their gradients, in closed form: with h = n.(x - v1) and per edge
-// a -> b (unit tangent t, outward in-plane normal m = t x n), s- = (a-x).t,
-// s+ = (b-x).t, p = (a-x).m, R- = |a-x|, R+ = |b-x|,
-//   f = log((R+ + s+)/(R- + s-)),
-//   beta = atan2(p s+, p^2 + h^2 + |h| R+) - atan2(p s-, p^2 + h^2 + |h| R-),
-//   S = sum p f - |h| sum beta,  grad S = -sum m f - sign(h) n sum beta,
-//   D = sign(h) sum beta,        grad D = -sum (u x w)(|u|+|w|)/(|u||w|(|u||w|+u.w)),
-// u = x - a, w = x - b.  At a triangle's own centroid h is taken as 0, as the
+// and their gradients, in closed form: with h = n.(x - v1), D the signed
+// solid angle the triangle subtends at x, and per edge a -> b (unit tangent
+// t, outward in-plane normal m = t x n), s- = (a-x).t, s+ = (b-x).t,
+// p = (a-x).m, R- = |a-x|, R+ = |b-x|, f = log((R+ + s+)/(R- + s-)):
+//   S = sum p f - h D,   grad S = -sum m f - n D,
+//   grad D = -sum (u x w)(|u|+|w|)/(|u||w|(|u||w|+u.w)),   u = x - a, w = x - b.  At a triangle's own centroid h is taken as 0, as the
 // reference does (iquad = 0): the jumps of grad S . n and of D across the
 // triangle are split evenly (both vanish), grad D is continuous there.
 // Fields are -grad.
@@ -139,6 +137,11 @@ void launch_scale_ranges(int nboxes, const int *src0, const int *nsrc, int k, in
 }
 
 // One triangle (geometry g, 30 doubles) at x: S, grad S (CHG), D, grad D (DIP).
+// The sum of the edge angles beta is the solid angle the triangle subtends,
+// taken in one atan2 (Van Oosterom and Strackee, IEEE Trans. Biomed. Eng. 30,
+// 1983): D = 2 atan2(-a.(b x c), |a||b||c| + (a.b)|c| + (a.c)|b| + (b.c)|a|)
+// with a, b, c = v1 - x, v2 - x, v3 - x; then S = sum p f - h D and
+// grad S = -sum m f - n D.
 template <bool CHG, bool DIP>
 __device__ __forceinline__ void tri_pair(const double *g, double x0, double x1, double x2, bool self, bool fld,
                                          double &S, double (&gS)[3], double &D, double (&gD)[3])
@@ -153,18 +156,26 @@ __device__ __forceinline__ void tri_pair(const double *g, double x0, double x1, 
     }
     const double *n = g + 9;
     const double h = self ? 0.0 : -(n[0] * d[0][0] + n[1] * d[0][1] + n[2] * d[0][2]);
-    const double ah = fabs(h), sg = h > 0 ? 1.0 : h < 0 ? -1.0 : 0.0;
-    double spf = 0, sb = 0, gm[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
+    double om = 0;
+    if (!self) {
+        const double bc0 = d[1][1] * d[2][2] - d[1][2] * d[2][1], bc1 = d[1][2] * d[2][0] - d[1][0] * d[2][2],
+                     bc2 = d[1][0] * d[2][1] - d[1][1] * d[2][0];
+        const double num = d[0][0] * bc0 + d[0][1] * bc1 + d[0][2] * bc2;
+        const double ab = d[0][0] * d[1][0] + d[0][1] * d[1][1] + d[0][2] * d[1][2];
+        const double ac = d[0][0] * d[2][0] + d[0][1] * d[2][1] + d[0][2] * d[2][2];
+        const double bcd = d[1][0] * d[2][0] + d[1][1] * d[2][1] + d[1][2] * d[2][2];
+        const double den = R[0] * R[1] * R[2] + ab * R[2] + ac * R[1] + bcd * R[0];
+        om = 2.0 * atan2(-num, den);
+    }
+    double spf = 0, gm[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const int a = i, b = (i + 1) % 3;
-        const double *t = g + 12 + 3 * i, *m = g + 21 + 3 * i;
-        const double sm = d[a][0] * t[0] + d[a][1] * t[1] + d[a][2] * t[2];
-        const double sp = d[b][0] * t[0] + d[b][1] * t[1] + d[b][2] * t[2];
-        const double pd = d[a][0] * m[0] + d[a][1] * m[1] + d[a][2] * m[2];
-        const double r0 = pd * pd + h * h;
-        sb += atan2(pd * sp, r0 + ah * R[b]) - atan2(pd * sm, r0 + ah * R[a]);
         if (CHG) {
+            const double *t = g + 12 + 3 * i, *m = g + 21 + 3 * i;
+            const double sm = d[a][0] * t[0] + d[a][1] * t[1] + d[a][2] * t[2];
+            const double sp = d[b][0] * t[0] + d[b][1] * t[1] + d[b][2] * t[2];
+            const double pd = d[a][0] * m[0] + d[a][1] * m[1] + d[a][2] * m[2];
             const double f = (sp + sm >= 0) ? log((R[b] + sp) / (R[a] + sm)) : log((R[a] - sm) / (R[b] - sp));
             spf += pd * f;
             if (fld) { gm[0] += m[0] * f; gm[1] += m[1] * f; gm[2] += m[2] * f; }
@@ -178,13 +189,13 @@ __device__ __forceinline__ void tri_pair(const double *g, double x0, double x1, 
         }
     }
     if (CHG) {
-        S = spf - ah * sb;
-        gS[0] = -gm[0] - sg * n[0] * sb;
-        gS[1] = -gm[1] - sg * n[1] * sb;
-        gS[2] = -gm[2] - sg * n[2] * sb;
+        S = spf - h * om;
+        gS[0] = -gm[0] - n[0] * om;
+        gS[1] = -gm[1] - n[1] * om;
+        gS[2] = -gm[2] - n[2] * om;
     }
     if (DIP) {
-        D = sg * sb;
+        D = om;
         gD[0] = -bs[0]; gD[1] = -bs[1]; gD[2] = -bs[2];
     }
 }
@@ -220,6 +231,12 @@ __device__ __forceinline__ void tri_accum(const double *g, double2 q, double2 dq
     }
 }
 
+// A leaf holds at most nbox (<= 233 below iprec 6) triangles, usually ~10-20:
+// one thread per evaluation point would leave most of a CTA idle.  So the
+// CTA's threads are split into G groups of np threads, np = min(points left,
+// 128): thread (group g, lane e) evaluates point e against every G-th staged
+// triangle from g on, and the groups' partial sums are added in shared memory
+// in group order (a fixed order for a given leaf).
 template <bool CHG, bool DIP>
 __global__ void __launch_bounds__(kTriThreads) k_p2p_tri(const int *leaves, TreeView tv, TriSoA t, const double *sx,
                                                          const double *sy, const double *sz, const double *tx,
@@ -229,14 +246,19 @@ __global__ void __launch_bounds__(kTriThreads) k_p2p_tri(const int *leaves, Tree
 {
     __shared__ double sg[kTriThreads * kTriGeo];
     __shared__ double2 sq[kTriThreads], sd[kTriThreads];
+    __shared__ double red[8][kTriThreads];
     const int b = leaves[blockIdx.x];
     const int s0 = tv.src0[b], ns = do_src ? tv.nsrc[b] : 0;
     const int t0 = tv.trg0[b], nt = do_trg ? tv.ntrg[b] : 0;
     const int ne = ns + nt;
     const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
     for (int e0 = 0; e0 < ne; e0 += kTriThreads) {
-        const int e = e0 + threadIdx.x;
-        const bool act = e < ne, is_src = e < ns;
+        const int np = min(kTriThreads, ne - e0);
+        const int G = kTriThreads / np;
+        const int lane = threadIdx.x % np, grp = threadIdx.x / np;
+        const int e = e0 + lane;
+        const bool act = grp < G;
+        const bool is_src = e < ns;
         double x0 = 0, x1 = 0, x2 = 0;
         int self = -1;
         if (act) {
@@ -260,19 +282,29 @@ __global__ void __launch_bounds__(kTriThreads) k_p2p_tri(const int *leaves, Tree
                 __syncthreads();
                 if (!act) continue;
                 const int selfk = self - (js0 + c0);
-                for (int k = 0; k < cn; k++)
+                for (int k = grp; k < cn; k += G)
                     tri_accum<CHG, DIP>(sg + kTriGeo * k, CHG ? sq[k] : cmk(0, 0), DIP ? sd[k] : cmk(0, 0), x0, x1,
                                         x2, k == selfk, fld, acc);
             }
         }
-        if (act) {
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 8; c++) red[c][threadIdx.x] = act ? acc[c] : 0.0;
+        __syncthreads();
+        if (threadIdx.x < np) {
+            double sum[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                sum[c] = red[c][threadIdx.x];
+                for (int g = 1; g < G; g++) sum[c] += red[c][threadIdx.x + g * np];
+            }
             const OutSoA &o = is_src ? outs : outt;
             const int i = is_src ? s0 + e : t0 + e - ns;
-            if (o.pot) o.pot[i] = cadd(o.pot[i], cmk(acc[0], acc[1]));
+            if (o.pot) o.pot[i] = cadd(o.pot[i], cmk(sum[0], sum[1]));
             if (fld && o.fx) {
-                o.fx[i] = cadd(o.fx[i], cmk(acc[2], acc[3]));
-                o.fy[i] = cadd(o.fy[i], cmk(acc[4], acc[5]));
-                o.fz[i] = cadd(o.fz[i], cmk(acc[6], acc[7]));
+                o.fx[i] = cadd(o.fx[i], cmk(sum[2], sum[3]));
+                o.fy[i] = cadd(o.fy[i], cmk(sum[4], sum[5]));
+                o.fz[i] = cadd(o.fz[i], cmk(sum[6], sum[7]));
             }
         }
     }
@@ -303,7 +335,8 @@ void launch_p2p_tri(const int *leaves, int nleaves, const TreeView &tv, const Tr
 // l3dtriadirect: one point per thread against every triangle, staged in chunks.
 template <bool CHG, bool DIP>
 __global__ void __launch_bounds__(kTriThreads) k_tri_direct(int ntri, TriSoA t, int npts, const double *pts,
-                                                            int centroids, int want_f, double *pot, double *fld)
+                                                            int centroids, const int *self_idx, int want_f,
+                                                            double *pot, double *fld)
 {
     __shared__ double sg[kTriThreads * kTriGeo];
     __shared__ double2 sq[kTriThreads], sd[kTriThreads];
@@ -313,7 +346,8 @@ __global__ void __launch_bounds__(kTriThreads) k_tri_direct(int ntri, TriSoA t, 
     int self = -1;
     if (act) {
         x0 = pts[3L * i]; x1 = pts[3L * i + 1]; x2 = pts[3L * i + 2];
-        if (centroids) self = i;
+        if (self_idx) self = self_idx[i];
+        else if (centroids) self = i;
     }
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int c0 = 0; c0 < ntri; c0 += kTriThreads) {
@@ -338,7 +372,7 @@ __global__ void __launch_bounds__(kTriThreads) k_tri_direct(int ntri, TriSoA t, 
 }
 
 void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
-                       int centroids, double *pot, double *fld, cudaStream_t s, Status &st)
+                       int centroids, const int *self_idx, double *pot, double *fld, cudaStream_t s, Status &st)
 {
     if (npts <= 0 || !st.ok()) return;
     const bool c = ifcharge == 1, d = ifdipole == 1;
@@ -348,9 +382,9 @@ void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, in
         if (fld) FMM_TRY(st, cudaMemsetAsync(fld, 0, sizeof(double) * 6 * npts, s));
         return;
     }
-    if (c && d) k_tri_direct<true, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
-    else if (c) k_tri_direct<true, false><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
-    else k_tri_direct<false, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, fld != nullptr, pot, fld);
+    if (c && d) k_tri_direct<true, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, fld != nullptr, pot, fld);
+    else if (c) k_tri_direct<true, false><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, fld != nullptr, pot, fld);
+    else k_tri_direct<false, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, fld != nullptr, pot, fld);
     FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }

@@ -57,9 +57,10 @@ void launch_p2p_tri(const int *leaves, int nleaves, const TreeView &tv, const Tr
                     int want_ft, cudaStream_t s, Status &st);
 
 // O(N^2) l3dtriadirect at npts points, triangles in the caller's order;
-// centroids = 1: point k is triangle k's centroid (its own triangle then
-// takes the in-plane values).  pot (2 doubles) / fld (6) per point written.
+// point k is the centroid of triangle self_idx[k] (-1: none) when self_idx is
+// given, else of triangle k when centroids = 1 (that triangle then takes the
+// in-plane values).  pot (2 doubles) / fld (6) per point written.
 void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
-                       int centroids, double *pot, double *fld, cudaStream_t s, Status &st);
+                       int centroids, const int *self_idx, double *pot, double *fld, cudaStream_t s, Status &st);
 
 }  // namespace fmm

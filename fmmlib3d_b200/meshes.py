@@ -1,4 +1,5 @@
-"""Triangulated surfaces for the triangle-FMM tests (numpy; no reference data)."""
+"""Triangulated surfaces (numpy) for the triangle FMM: icospheres and a two-body mesh, used by
+the tests and the bench as synthetic inputs."""
 import numpy as np
 
 
@@ -14,21 +15,18 @@ def icosphere(k, radius=1.0, center=(0.0, 0.0, 0.0), axes=(1.0, 1.0, 1.0)):
                   [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]])
     V /= np.linalg.norm(V, axis=1)[:, None]
     for _ in range(k):
-        cache = {}
-        verts = list(V)
-        faces = []
-
-        def mid(a, b):
-            key = (min(a, b), max(a, b))
-            if key not in cache:
-                m = (verts[a] + verts[b]) / 2
-                cache[key] = len(verts)
-                verts.append(m / np.linalg.norm(m))
-            return cache[key]
-        for a, b, c in F:
-            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
-            faces += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
-        V, F = np.array(verts), np.array(faces)
+        # one midpoint per edge: edges keyed by their sorted vertex pair
+        E = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+        key = np.sort(E, axis=1)
+        uniq, inv = np.unique(key[:, 0].astype(np.int64) * len(V) + key[:, 1], return_inverse=True)
+        a, b = uniq // len(V), uniq % len(V)
+        M = (V[a] + V[b]) / 2
+        M /= np.linalg.norm(M, axis=1)[:, None]
+        mid = len(V) + inv.reshape(3, -1)          # midpoints of edges (0,1), (1,2), (2,0) of every face
+        ab, bc, ca = mid[0], mid[1], mid[2]
+        F = np.concatenate([np.stack([F[:, 0], ab, ca], 1), np.stack([F[:, 1], bc, ab], 1),
+                            np.stack([F[:, 2], ca, bc], 1), np.stack([ab, bc, ca], 1)])
+        V = np.concatenate([V, M])
     T = V[F] * np.asarray(axes, float) * radius + np.asarray(center, float)
     # outward orientation
     n = np.cross(T[:, 1] - T[:, 0], T[:, 2] - T[:, 0])

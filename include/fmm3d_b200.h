@@ -155,6 +155,14 @@ int fmm3d_l3dtriadirect_device(int nsource, const double *d_triaflat, const doub
                                double *d_fld, int ntarget, const double *d_target, int ifpottarg, double *d_pottarg,
                                int iffldtarg, double *d_fldtarg, void *stream);
 
+/* The triangle direct sum at npts arbitrary device points pts(3,npts): point k
+ * is the centroid of triangle self[k] (0-based; -1 or self NULL: none), which
+ * then takes its own triangle's in-plane values.  pot(npts), fld(3,npts)
+ * complex*16 written.  The sampled form of l3dtriadirect. */
+int fmm3d_l3dtriadirect_points_device(int nsource, const double *d_triaflat, int ifcharge, const double *d_charge,
+                                      int ifdipole, const double *d_dipstr, int npts, const double *d_pts,
+                                      const int *d_self, double *d_pot, double *d_fld, void *stream);
+
 /* The same on device-resident arrays, enqueued on `stream`. */
 int fmm3d_lfmm3dparttarg_hess_device(int iprec, int nsource, const double *d_source, int ifcharge,
                                      const double *d_charge, int ifdipole, const double *d_dipstr,

@@ -27,7 +27,7 @@
  *   f    = log((R+ + s+)/(R- + s-)),
  *   beta = atan2(p s+, p^2 + h^2 + |h| R+) - atan2(p s-, p^2 + h^2 + |h| R-),
  *   S = sum p f - |h| sum beta,   grad S = -sum m f - sign(h) n sum beta,
- *   D = sign(h) sum beta (the signed solid angle),
+ *   D = sign(h) sum beta (the signed solid angle, taken in closed form below),
  *   grad D = - sum (u x w)(|u|+|w|) / (|u||w|(|u||w| + u.w)),  u = x-a, w = x-b.
  *
  * Far-field quadrature: the reference's symmetric rules (triasymq,
@@ -48,7 +48,10 @@ static void cross3(const double *a, const double *b, double *c)
 static double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 /* S, grad S, D, grad D of triangle v[9] (vertices v1, v2, v3) at x; self:
- * x is the triangle's own centroid (in-plane values). */
+ * x is the triangle's own centroid (in-plane values).  The sum of the edge
+ * angles beta (the solid angle) is taken in one atan2 by the formula of Van
+ * Oosterom and Strackee (1983); D = sign(h) sum beta is that signed solid
+ * angle, and S = sum p f - h D, grad S = -sum m f - n D. */
 static void tri_near(const double *v, const double *x, int self, double *S, double *gS, double *D, double *gD)
 {
     double e1[3], e2[3], n[3];
@@ -62,8 +65,16 @@ static void tri_near(const double *v, const double *x, int self, double *S, doub
         R[k] = sqrt(dot3(dv[k], dv[k]));
     }
     const double h = self ? 0.0 : -dot3(n, dv[0]);
-    const double ah = fabs(h), sg = h > 0 ? 1.0 : h < 0 ? -1.0 : 0.0;
-    double spf = 0, sb = 0, gm[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
+    double om = 0;
+    if (!self) {
+        double bc[3];
+        cross3(dv[1], dv[2], bc);
+        const double num = dot3(dv[0], bc);
+        const double den = R[0] * R[1] * R[2] + dot3(dv[0], dv[1]) * R[2] + dot3(dv[0], dv[2]) * R[1] +
+                           dot3(dv[1], dv[2]) * R[0];
+        om = 2.0 * atan2(-num, den);
+    }
+    double spf = 0, gm[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
     for (int i = 0; i < 3; i++) {
         const int a = i, b = (i + 1) % 3;
         double t[3], m[3];
@@ -72,11 +83,8 @@ static void tri_near(const double *v, const double *x, int self, double *S, doub
         for (int c = 0; c < 3; c++) t[c] /= L;
         cross3(t, n, m);
         const double sm = dot3(dv[a], t), sp = dot3(dv[b], t), pd = dot3(dv[a], m);
-        const double r0 = pd * pd + h * h;
         const double f = (sp + sm >= 0) ? log((R[b] + sp) / (R[a] + sm)) : log((R[a] - sm) / (R[b] - sp));
-        const double beta = atan2(pd * sp, r0 + ah * R[b]) - atan2(pd * sm, r0 + ah * R[a]);
         spf += pd * f;
-        sb += beta;
         for (int c = 0; c < 3; c++) gm[c] += m[c] * f;
         /* segment a -> b: (u x w)(|u|+|w|)/(|u||w|(|u||w|+u.w)), u = x-a = -dv[a], w = x-b = -dv[b] */
         double uw[3];
@@ -84,9 +92,9 @@ static void tri_near(const double *v, const double *x, int self, double *S, doub
         const double co = (R[a] + R[b]) / (R[a] * R[b] * (R[a] * R[b] + dot3(dv[a], dv[b])));
         for (int c = 0; c < 3; c++) bs[c] += uw[c] * co;
     }
-    *S = spf - ah * sb;
-    for (int c = 0; c < 3; c++) gS[c] = -gm[c] - sg * n[c] * sb;
-    *D = sg * sb;
+    *S = spf - h * om;
+    for (int c = 0; c < 3; c++) gS[c] = -gm[c] - n[c] * om;
+    *D = om;
     for (int c = 0; c < 3; c++) gD[c] = -bs[c];
 }
 
@@ -182,6 +190,19 @@ static void tri_point(int nj, const double *tri, int ifcharge, const cplx *q, in
             *pot += ds[j] * D;
             if (iffld) for (int c = 0; c < 3; c++) fld[c] -= ds[j] * gD[c];
         }
+    }
+}
+
+/* The direct sum at arbitrary points; point k is the centroid of triangle self[k] (or -1). */
+void oracle_tri_direct_points(int ns, const double *tri, int ifcharge, const cplx *charge, int ifdipole,
+                              const cplx *dipstr, int npts, const double *pts, const long *self, cplx *pot, cplx *fld)
+{
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long k = 0; k < npts; k++) {
+        cplx pv = 0, fv[3] = {0, 0, 0};
+        tri_point(ns, tri, ifcharge, charge, ifdipole, dipstr, pts + 3 * k, self ? self[k] : -1, 1, &pv, fv);
+        pot[k] = pv;
+        for (int c = 0; c < 3; c++) fld[3 * k + c] = fv[c];
     }
 }
 

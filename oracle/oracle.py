@@ -221,6 +221,18 @@ def l3dtriadirect(triaflat, source, charge=None, dipstr=None, target=None, ifpot
     return pot[:n], fld[:n], pt[:m], ft[:m]
 
 
+def tri_direct_at(triaflat, pts, self_idx=None, charge=None, dipstr=None):
+    """Triangle direct sum at pts; self_idx[k]: the triangle whose centroid point k is (or -1)."""
+    tri = _f64(triaflat, (0, 3, 3)); n = tri.shape[0]
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    sk = None if self_idx is None else np.ascontiguousarray(self_idx, np.int64)
+    pot = np.zeros(max(k, 1), np.complex128); fld = np.zeros((max(k, 1), 3), np.complex128)
+    lib().oracle_tri_direct_points(c_int(n), _p(tri), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                                   c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), c_int(k), _p(pts),
+                                   None if sk is None else _p(sk), _p(pot), _p(fld))
+    return pot[:k], fld[:k]
+
+
 def lfmm3dtriatarg(iprec, triaflat, trianorm, source, charge=None, dipstr=None, target=None, ifpot=1, iffld=1,
                    ifpottarg=1, iffldtarg=1):
     """lfmm3dtriatarg: (ier, pot, fld, pottarg, fldtarg)."""

@@ -18,7 +18,7 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 sys.path.insert(0, HERE)
 
 import oracle as O  # noqa: E402
-from meshes import icosphere, normals_centroids, two_spheres  # noqa: E402
+from fmmlib3d_b200.meshes import icosphere, normals_centroids, two_spheres  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 EPS = {-2: .5, -1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9}
@@ -113,3 +113,46 @@ def test_device_entry_point_matches_host_entry_point(F):
     c = lambda t, k: t.cpu().numpy().view(np.complex128).reshape(-1, k)
     for a, b, k in zip(out, (pot, fld, pt, ft), (1, 3, 1, 3)):
         assert np.array_equal(c(a, k).reshape(b.shape), b)
+
+
+def test_sampled_direct_sum_matches_oracle(F):
+    import torch
+    T = two_spheres(3, 4)
+    nrm, cen, q, ds, trg = _inputs(T, 9, 50)
+    n = len(T)
+    rng = np.random.default_rng(4)
+    si = np.sort(rng.choice(n, 300, replace=False)).astype(np.int32)
+    pts = np.concatenate([cen[si], trg])
+    self_idx = np.concatenate([si, -np.ones(len(trg), np.int32)]).astype(np.int32)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.float64).reshape(len(a), -1)).cuda()
+    pot = torch.zeros(len(pts), 2, dtype=torch.float64, device="cuda")
+    fld = torch.zeros(len(pts), 6, dtype=torch.float64, device="cuda")
+    ier = F.tri_direct_points_device(d(T.reshape(n, 9)), d(q), d(ds), d(pts), torch.from_numpy(self_idx).cuda(),
+                                     pot, fld)
+    assert ier == 0
+    op, of = O.tri_direct_at(T, pts, self_idx, q, ds)
+    c = lambda t, k: t.cpu().numpy().view(np.complex128).reshape(-1, k)
+    assert rel(c(pot, 1)[:, 0], op) < 1e-12 and rel(c(fld, 3), of) < 1e-12
+    # the full direct sum at the same centroids
+    g = F.l3dtriadirect(T, nrm, cen, 1, q, 1, ds, 1, 1)
+    assert rel(g[0][si], op[:300]) < 1e-12 and rel(g[1][si], of[:300]) < 1e-12
+
+
+@pytest.mark.parametrize("iprec", [0, 1])
+def test_mixed_form_within_twice_the_oracle_error(F, iprec):
+    """set_precision(1): the triangle FMM's M2L on the tensor cores (split TF32); the exact near
+    field stays FP64.  Errors against the direct sum within 2x the oracle's."""
+    T = two_spheres(4, 5)
+    nrm, cen, q, ds, trg = _inputs(T, 30 + iprec)
+    F.set_precision(1)
+    try:
+        ier, pot, fld, pt, ft = F.lfmm3dtriatarg(iprec, T, nrm, cen, 1, q, 1, ds, 1, 1, trg, 1, 1)
+        tuning, _ = F.last_tuning()
+    finally:
+        F.set_precision(0)
+    assert ier == 0, F.last_error()
+    assert tuning["form"] == "mixed-tc"
+    oier, opot, ofld, opt, oft = O.lfmm3dtriatarg(iprec, T, nrm, cen, q, ds, trg)
+    d = O.l3dtriadirect(T, cen, q, ds, trg)
+    for a, o, ref in ((pot, opot, d[0]), (fld, ofld, d[1]), (pt, opt, d[2]), (ft, oft, d[3])):
+        assert rel(a, ref) <= 2 * rel(o, ref)

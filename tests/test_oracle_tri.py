@@ -24,7 +24,8 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 sys.path.insert(0, HERE)
 
 import oracle as O  # noqa: E402
-from meshes import icosphere, normals_centroids, two_spheres  # noqa: E402
+sys.path.insert(0, os.path.join(HERE, "..", "fmmlib3d_b200"))
+from meshes import icosphere, normals_centroids, two_spheres  # noqa: E402  (numpy only; no library load)
 
 EPS = {-1: .5e-1, 0: .5e-2, 1: .5e-3, 2: .5e-6, 3: .5e-9}
 
