@@ -56,11 +56,17 @@ _lib.fmm3d_lfmm3dparttarg_batched_device.argtypes = [_I, _I, _P, _P, _I, _P, _I,
 _lib.fmm3d_last_launches.restype = _I
 _lib.fmm3d_last_depth_capped.restype = _I
 _lib.lfmm3dparttarghess_.restype = None
-for _name in ("lfmm3dtriatarg_", "lfmm3dtriaself_", "lfmm3dtria_", "l3dtriadirect_"):
+for _name in ("lfmm3dtriatarg_", "lfmm3dtriaself_", "lfmm3dtria_", "l3dtriadirect_", "hfmm3dtriatarg_",
+              "hfmm3dtriaself_", "hfmm3dtria_", "h3dtriadirect_"):
     getattr(_lib, _name).restype = None
 _lib.fmm3d_lfmm3dtriatarg_device.restype = _I
 _lib.fmm3d_lfmm3dtriatarg_device.argtypes = [_I, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I, _P,
                                              _I, _P, _P]
+_lib.fmm3d_hfmm3dtriatarg_device.restype = _I
+_lib.fmm3d_hfmm3dtriatarg_device.argtypes = [_I, _P, _I, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _I,
+                                             _P, _I, _P, _P]
+_lib.fmm3d_h3dtriadirect_points_device.restype = _I
+_lib.fmm3d_h3dtriadirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P]
 _lib.fmm3d_l3dtriadirect_points_device.restype = _I
 _lib.fmm3d_l3dtriadirect_points_device.argtypes = [_I, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _P]
 _lib.fmm3d_l3dtriadirect_device.restype = _I
@@ -295,6 +301,74 @@ def lfmm3dtriatarg(iprec, triaflat, trianorm, source, ifcharge, charge, ifdipole
                          _ptr(fld), _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg),
                          _ptr(ft))
     return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def hfmm3dtriatarg(iprec, zk, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld,
+                   target=None, ifpottarg=0, iffldtarg=0):
+    """Helmholtz layer potentials of flat triangles (hfmm3dtriatarg, src/hfmm3dtria.f:133);
+    returns (ier, pot, fld, pottarg, fldtarg); arguments as lfmm3dtriatarg plus zk."""
+    tri, n, nrm, src, trg, q, ds = _tri_args(triaflat, trianorm, source, charge, dipstr, target)
+    m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = ctypes.c_int(0)
+    dv = np.zeros((max(n, 1), 3))
+    z = np.array([complex(zk).real, complex(zk).imag])
+    _lib.hfmm3dtriatarg_(ctypes.byref(ier), _iref(iprec), _ptr(z), _iref(n), _ptr(tri), _ptr(nrm), _ptr(src),
+                         _iref(ifcharge), _ptr(q), _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot),
+                         _iref(iffld), _ptr(fld), _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt),
+                         _iref(iffldtarg), _ptr(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def hfmm3dtriaself(iprec, zk, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld):
+    ier, pot, fld, _, _ = hfmm3dtriatarg(iprec, zk, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr,
+                                         ifpot, iffld)
+    return ier, pot, fld
+
+
+def h3dtriadirect(nqtri, zk, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld,
+                  target=None, ifpottarg=0, iffldtarg=0):
+    """O(N^2) Helmholtz layer potentials (h3dtriadirect) with near-field quadrature degree nqtri."""
+    tri, n, nrm, src, trg, q, ds = _tri_args(triaflat, trianorm, source, charge, dipstr, target)
+    m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128)
+    fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128)
+    ft = np.zeros((max(m, 1), 3), np.complex128)
+    dv = np.zeros((max(n, 1), 3))
+    z = np.array([complex(zk).real, complex(zk).imag])
+    _lib.h3dtriadirect_(_iref(nqtri), _ptr(z), _iref(n), _ptr(tri), _ptr(nrm), _ptr(src), _iref(ifcharge), _ptr(q),
+                        _iref(ifdipole), _ptr(ds), _ptr(dv), _iref(ifpot), _ptr(pot), _iref(iffld), _ptr(fld),
+                        _iref(m), _ptr(trg if m else src), _iref(ifpottarg), _ptr(pt), _iref(iffldtarg), _ptr(ft))
+    return pot[:n], fld[:n], pt[:m], ft[:m]
+
+
+def htri_direct_points_device(nqtri, zk, triaflat, charge, dipstr, pts, self_idx, pot, fld, stream=0):
+    """Helmholtz triangle direct sum at device points; layouts as tri_direct_points_device."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    z = np.array([complex(zk).real, complex(zk).imag])
+    return _lib.fmm3d_h3dtriadirect_points_device(nqtri, _ptr(z), triaflat.shape[0], ptr(triaflat),
+                                                  int(charge is not None), ptr(charge), int(dipstr is not None),
+                                                  ptr(dipstr), pts.shape[0], ptr(pts), ptr(self_idx), 0, ptr(pot),
+                                                  ptr(fld), _P(stream))
+
+
+def hfmm3dtriatarg_device(iprec, zk, triaflat, trianorm, source, charge, dipstr, pot, fld, target=None, pottarg=None,
+                          fldtarg=None, stream=0):
+    """hfmm3dtriatarg on device tensors (layouts as lfmm3dtriatarg_device).  Returns ier."""
+    def ptr(t):
+        return None if t is None else _P(t.data_ptr())
+    n = source.shape[0]
+    m = 0 if target is None else target.shape[0]
+    z = np.array([complex(zk).real, complex(zk).imag])
+    return _lib.fmm3d_hfmm3dtriatarg_device(
+        iprec, _ptr(z), n, ptr(triaflat), ptr(trianorm), ptr(source), int(charge is not None), ptr(charge),
+        int(dipstr is not None), ptr(dipstr), None, int(pot is not None), ptr(pot), int(fld is not None), ptr(fld), m,
+        ptr(target), int(pottarg is not None), ptr(pottarg), int(fldtarg is not None), ptr(fldtarg), _P(stream))
 
 
 def lfmm3dtriaself(iprec, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, ifpot, iffld):

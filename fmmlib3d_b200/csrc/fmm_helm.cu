@@ -20,6 +20,7 @@
 #include "../../include/fmm3d_b200.h"
 #include "driver_common.cuh"
 #include "helm_kernels.cuh"
+#include "tri.cuh"
 
 namespace fmm {
 
@@ -233,16 +234,27 @@ __global__ void k_hm2l_count(int b0, int nb, TreeView tv, const HSlot *slots, in
     }
 }
 
+// Triangle mode (hfmm3dtriatarg, src/hfmm3dtria.f:133-1215): the sources
+// are flat triangles tri (3,3,n) with unit normals norm, d_src their
+// centroids; the far field runs on the far rule's nodes, the near field
+// integrates each triangle with the near rule (degrees norder / nqtri of
+// :730-751).
+struct HTriIn {
+    const double *tri = nullptr, *norm = nullptr;
+    TriRule far, near_;
+};
+
 static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, int ifcharge, const double *d_q,
                            int ifdipole, const double *d_dq, const double *d_dv, int ifpot, double *d_pot, int iffld,
                            double *d_fld, int nt, const double *d_trg, int ifpottarg, double *d_pottarg,
-                           int iffldtarg, double *d_fldtarg, cudaStream_t s)
+                           int iffldtarg, double *d_fldtarg, cudaStream_t s, const HTriIn *tri = nullptr)
 {
     Status st;
     g_launch_count = 0;
     double eps;
     int nbox;
     if (ns < 1 || !helm_iprec(iprec, ns, nt, eps, nbox)) return 4;
+    if (tri) nbox = tri_nbox(iprec, ns, nt);
     if (nt < 0) nt = 0;
     keep_pool_memory();
     Timer tm(s, g_ti.timing);
@@ -266,7 +278,8 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     int pmax = 1;
     for (int l = 0; l <= nlev; l++) {
         bsize[l] = T.size / pow(2.0, l);
-        double bs = std::abs(bsize[l] * zk.x);
+        // hfmm3dtriatarg declares zk complex*16: its rule sees |zk| (src/hfmm3dtria.f:248, 350-355)
+        double bs = tri ? std::abs(bsize[l] * zkc) : std::abs(bsize[l] * zk.x);
         lv.sc[l] = bs < 1 ? bs : 1.0;
         if (l >= 2) {
             int e;
@@ -313,6 +326,29 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     if (nt) { k_gather_pts<<<div_up(nt, 256), 256, 0, s>>>(nt, T.perm_trg.p, d_trg, tx.p, ty.p, tz.p); FMM_COUNT_LAUNCH(); }
     FMM_LAUNCH_CHECK(st);
     TreeView tv = make_treeview(T);
+    // triangles: tree-ordered geometry and densities, the far rule's nodes, box ranges in nodes
+    DBuf<double> tgeo, qx, qy, qz, qvx, qvy, qvz;
+    DBuf<double2> tq, tdq, qq, qdq;
+    DBuf<int> qsrc0, qnsrc;
+    TriSoA ts;
+    PointsSoA Pq;
+    TreeView tv_quad = tv;
+    if (tri) {
+        const size_t nn = (size_t)ns * tri->far.n;
+        bool okt = tgeo.alloc(30L * ns, s, st) && qx.alloc(nn, s, st) && qy.alloc(nn, s, st) && qz.alloc(nn, s, st) &&
+                   qsrc0.alloc(T.nboxes, s, st) && qnsrc.alloc(T.nboxes, s, st);
+        if (ifcharge == 1) okt = okt && tq.alloc(ns, s, st) && qq.alloc(nn, s, st);
+        if (ifdipole == 1)
+            okt = okt && tdq.alloc(ns, s, st) && qdq.alloc(nn, s, st) && qvx.alloc(nn, s, st) && qvy.alloc(nn, s, st) &&
+                  qvz.alloc(nn, s, st);
+        if (!okt) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+        ts.geo = tgeo.p; ts.q = tq.p; ts.dq = tdq.p;
+        Pq.x = qx.p; Pq.y = qy.p; Pq.z = qz.p; Pq.q = qq.p; Pq.dq = qdq.p; Pq.vx = qvx.p; Pq.vy = qvy.p; Pq.vz = qvz.p;
+        launch_tri_gather(ns, T.perm_src.p, tri->tri, tri->norm, d_q, d_dq, ifcharge, ifdipole, tri->far, ts, Pq, s, st);
+        launch_scale_ranges(T.nboxes, tv.src0, tv.nsrc, tri->far.n, qsrc0.p, qnsrc.p, s, st);
+        tv_quad.src0 = qsrc0.p;
+        tv_quad.nsrc = qnsrc.p;
+    }
     const int prune = !(ifpot == 1 || iffld == 1);
     OutSoA os, ot;
     os.pot = opot.p; os.fx = ofx.p; os.fy = ofy.p; os.fz = ofz.p;
@@ -456,7 +492,8 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
     tm.mark();
     if (far) {
         // STEP 1: P2M at leaves of level >= 2 (src/hfmm3dpart.f:696-760)
-        launch_hform(false, T.leaves.p, T.nleaves, tv, P, ifcharge, ifdipole, lv, NC, zk, mpole.p, s, st);
+        launch_hform(false, T.leaves.p, T.nleaves, tri ? tv_quad : tv, tri ? Pq : P, ifcharge, ifdipole, lv, NC, zk,
+                     mpole.p, s, st);
         tm.mark();
         // STEP 3: M2M, levels nlev-1 .. 2
         for (auto &r : m2m_rng)
@@ -464,7 +501,8 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
                               mpole.p, mpole.p, prune, kt, s, st);
         tm.mark();
         // STEP 2: P2L into boxes with a list 4 (src/hfmm3dpart.f:775-846)
-        launch_hform(true, T.grouped.p, T.nboxes, tv, P, ifcharge, ifdipole, lv, NC, zk, local.p, s, st);
+        launch_hform(true, T.grouped.p, T.nboxes, tri ? tv_quad : tv, tri ? Pq : P, ifcharge, ifdipole, lv, NC, zk,
+                     local.p, s, st);
         tm.mark();
         // STEP 4: M2L over list 2
         launch_htranslate(1, dtiles.p + m2l_a, m2l_n, T.grouped.p, dslots.p, tv, pmax, rp->rot.p, Z.p, mpole.p,
@@ -483,8 +521,12 @@ static int helm_fmm_device(int iprec, double2 zk, int ns, const double *d_src, i
         for (int i = 0; i < 6; i++) tm.mark();
     }
     // STEP 8: P2P over self and list 1
-    launch_hp2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, zk, os, ot, ifcharge, ifdipole, ifpot, iffld,
-                do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
+    if (tri)
+        launch_hp2p_tri(T.leaves.p, T.nleaves, tv, ts, sx.p, sy.p, sz.p, tx.p, ty.p, tz.p, zk, tri->near_, os, ot,
+                        ifcharge, ifdipole, do_src, do_trg, iffld == 1, do_trg && iffldtarg == 1, s, st);
+    else
+        launch_hp2p(T.leaves.p, T.nleaves, tv, P, tx.p, ty.p, tz.p, zk, os, ot, ifcharge, ifdipole, ifpot, iffld,
+                    do_trg ? ifpottarg : 0, do_trg ? iffldtarg : 0, s, st);
     tm.mark();
     if (do_src) {
         k_scatter_out<<<div_up(ns, 256), 256, 0, s>>>(ns, T.perm_src.p, os, ifpot == 1 ? d_pot : nullptr,
@@ -638,6 +680,122 @@ int fmm3d_h3ddirect_points_device(const double *zk, int nsource, const double *d
     FMM_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     return 0;
+}
+
+static HTriIn htri_in(int iprec, const double *tri, const double *norm)
+{
+    HTriIn t;
+    t.tri = tri;
+    t.norm = norm;
+    // norder / nqtri of hfmm3dtriatarg (src/hfmm3dtria.f:730-751)
+    const int norder = (iprec == -2 || iprec == -1) ? 2 : iprec >= 0 ? 4 : 1;
+    const int nqtri = (iprec == -2 || iprec == -1) ? 2 : iprec == 0 ? 4 : iprec >= 1 ? 6 : 1;
+    t.far = tri_rule_degree(norder);
+    t.near_ = tri_rule_degree(nqtri);
+    return t;
+}
+
+int fmm3d_hfmm3dtriatarg_device(int iprec, const double *zk, int nsource, const double *d_triaflat,
+                                const double *d_trianorm, const double *d_source, int ifcharge, const double *d_charge,
+                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot,
+                                int iffld, double *d_fld, int ntarget, const double *d_target, int ifpottarg,
+                                double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream)
+{
+    (void)d_dipvec;   // the dipoles are oriented by the triangles' normals, as in the reference
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    HTriIn t = htri_in(iprec, d_triaflat, d_trianorm);
+    return helm_fmm_device(iprec, make_double2(zk[0], zk[1]), nsource, d_source, ifcharge, d_charge, ifdipole,
+                           d_dipstr, d_trianorm, ifpot, d_pot, iffld, d_fld, ntarget, d_target, ifpottarg, d_pottarg,
+                           iffldtarg, d_fldtarg, s, &t);
+}
+
+int fmm3d_h3dtriadirect_points_device(int nqtri, const double *zk, int nsource, const double *d_triaflat,
+                                      int ifcharge, const double *d_charge, int ifdipole, const double *d_dipstr,
+                                      int npts, const double *d_pts, const int *d_self, int centroids, double *d_pot,
+                                      double *d_fld, void *stream)
+{
+    cudaStream_t s = stream ? (cudaStream_t)stream : thread_stream();
+    g_launch_count = 0;
+    Status st;
+    DBuf<double> geo;
+    DBuf<double2> q, dq;
+    TriRule none;
+    bool ok = geo.alloc(30L * std::max(nsource, 1), s, st);
+    if (ifcharge == 1) ok = ok && q.alloc(std::max(nsource, 1), s, st);
+    if (ifdipole == 1) ok = ok && dq.alloc(std::max(nsource, 1), s, st);
+    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
+    TriSoA t;
+    t.geo = geo.p; t.q = q.p; t.dq = dq.p;
+    launch_tri_gather(nsource, nullptr, d_triaflat, nullptr, d_charge, d_dipstr, ifcharge, ifdipole, none, t,
+                      PointsSoA(), s, st);
+    launch_htri_direct(nsource, t, ifcharge, ifdipole, npts, d_pts, centroids, d_self, make_double2(zk[0], zk[1]),
+                       tri_rule_degree(nqtri), d_pot, d_fld, s, st);
+    FMM_TRY(st, cudaStreamSynchronize(s));
+    if (!st.ok()) { g_ti.err = std::string(st.where ? st.where : "") + ": " + cudaGetErrorString(st.err); return 16; }
+    return 0;
+}
+
+void hfmm3dtriatarg_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                     const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                     const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                     const int *iffld, double *fld, const int *ntarget, const double *target, const int *ifpottarg,
+                     double *pottarg, const int *iffldtarg, double *fldtarg)
+{
+    (void)dipvec;
+    const int ip = *iprec, ns = *nsource, ifc = *ifcharge, ifd = *ifdipole, ifp = *ifpot, iff = *iffld;
+    const double2 k = make_double2(zk[0], zk[1]);
+    *ier = tri_host(ns, triaflat, trianorm, source, ifc, charge, ifd, dipstr, ifp, pot, iff, fld, *ntarget, target,
+                    *ifpottarg, pottarg, *iffldtarg, fldtarg,
+                    [&](const double *t_, const double *n_, const double *s_, const double *q, const double *dq,
+                        double *po, double *fo, int nt, const double *tg, int ipt, double *pt, int ift, double *ft,
+                        cudaStream_t s) {
+                        HTriIn t = htri_in(ip, t_, n_);
+                        return helm_fmm_device(ip, k, ns, s_, ifc, q, ifd, dq, n_, ifp, po, iff, fo, nt, tg, ipt, pt,
+                                               ift, ft, s, &t);
+                    });
+}
+
+void hfmm3dtriaself_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                     const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                     const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                     const int *iffld, double *fld)
+{
+    int zero = 0;
+    hfmm3dtriatarg_(ier, iprec, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, dipvec,
+                    ifpot, pot, iffld, fld, &zero, source, &zero, nullptr, &zero, nullptr);
+}
+
+void hfmm3dtria_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                 const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                 const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                 const int *iffld, double *fld)
+{
+    hfmm3dtriaself_(ier, iprec, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, dipvec,
+                    ifpot, pot, iffld, fld);
+}
+
+void h3dtriadirect_(const int *nqtri, const double *zk, const int *nsource, const double *triaflat,
+                    const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                    const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                    const int *iffld, double *fld, const int *ntarget, const double *target, const int *ifpottarg,
+                    double *pottarg, const int *iffldtarg, double *fldtarg)
+{
+    (void)trianorm;
+    (void)dipvec;
+    const int ns = *nsource, ifc = *ifcharge, ifd = *ifdipole, ifp = *ifpot, iff = *iffld, nq = *nqtri;
+    tri_host(ns, triaflat, nullptr, source, ifc, charge, ifd, dipstr, ifp, pot, iff, fld, *ntarget, target, *ifpottarg,
+             pottarg, *iffldtarg, fldtarg,
+             [&](const double *t_, const double *, const double *s_, const double *q, const double *dq, double *po,
+                 double *fo, int nt, const double *tg, int ipt, double *pt, int ift, double *ft, cudaStream_t s) {
+                 int e = 0;
+                 if (ifp == 1 || iff == 1)
+                     e = fmm3d_h3dtriadirect_points_device(nq, zk, ns, t_, ifc, q, ifd, dq, ns, s_, nullptr, 1,
+                                                           ifp == 1 ? po : nullptr, iff == 1 ? fo : nullptr, s);
+                 if (!e && nt && (ipt == 1 || ift == 1))
+                     e = fmm3d_h3dtriadirect_points_device(nq, zk, ns, t_, ifc, q, ifd, dq, nt, tg, nullptr, 0,
+                                                           ipt == 1 ? pt : nullptr, ift == 1 ? ft : nullptr, s);
+                 return e;
+             });
 }
 
 void hfmm3dparttarg_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *source,

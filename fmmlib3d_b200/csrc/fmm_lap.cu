@@ -1044,56 +1044,6 @@ static int tri_direct_device(int ns, const double *d_tri, const double *d_src, i
     return 0;
 }
 
-// Host arrays in and out for the triangle entry points (pageable or pinned):
-// device copies, the device call, copies back; a failed call leaves the
-// outputs untouched.
-template <class F>
-static int tri_host(int ns, const double *tri, const double *norm, const double *source, int ifcharge,
-                    const double *charge, int ifdipole, const double *dipstr, int ifpot, double *pot, int iffld,
-                    double *fld, int nt, const double *target, int ifpottarg, double *pottarg, int iffldtarg,
-                    double *fldtarg, F run)
-{
-    ns = std::max(ns, 0);
-    nt = std::max(nt, 0);
-    cudaStream_t s = thread_stream();
-    Status st;
-    DBuf<double> dtri, dnorm, dsrc, dq, ddq, dtrg, po, fo, pt, ft;
-    alloc_fail_point(1);
-    bool ok = dtri.alloc(9L * std::max(ns, 1), s, st) && dsrc.alloc(3L * std::max(ns, 1), s, st);
-    if (norm) ok = ok && dnorm.alloc(3L * std::max(ns, 1), s, st);
-    if (ifcharge == 1) ok = ok && dq.alloc(2L * ns, s, st);
-    if (ifdipole == 1) ok = ok && ddq.alloc(2L * ns, s, st);
-    if (nt) ok = ok && dtrg.alloc(3L * nt, s, st);
-    if (ifpot == 1) ok = ok && po.alloc(2L * ns, s, st);
-    if (iffld == 1) ok = ok && fo.alloc(6L * ns, s, st);
-    if (nt && ifpottarg == 1) ok = ok && pt.alloc(2L * nt, s, st);
-    if (nt && iffldtarg == 1) ok = ok && ft.alloc(6L * nt, s, st);
-    if (!ok) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    auto h2d = [&](DBuf<double> &d, const double *h, size_t n) {
-        if (n) FMM_TRY(st, cudaMemcpyAsync(d.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    };
-    h2d(dtri, tri, 9L * ns);
-    h2d(dsrc, source, 3L * ns);
-    if (norm) h2d(dnorm, norm, 3L * ns);
-    if (ifcharge == 1) h2d(dq, charge, 2L * ns);
-    if (ifdipole == 1) h2d(ddq, dipstr, 2L * ns);
-    if (nt) h2d(dtrg, target, 3L * nt);
-    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 8; }
-    int e = run(dtri.p, dnorm.p, dsrc.p, dq.p, ddq.p, po.p, fo.p, nt, dtrg.p, nt ? ifpottarg : 0, pt.p,
-                nt ? iffldtarg : 0, ft.p, s);
-    if (e) return e;
-    auto d2h = [&](double *h, DBuf<double> &d) {
-        if (d.n) FMM_TRY(st, cudaMemcpyAsync(h, d.p, sizeof(double) * d.n, cudaMemcpyDeviceToHost, s));
-    };
-    if (ifpot == 1) d2h(pot, po);
-    if (iffld == 1) d2h(fld, fo);
-    if (nt && ifpottarg == 1) d2h(pottarg, pt);
-    if (nt && iffldtarg == 1) d2h(fldtarg, ft);
-    FMM_TRY(st, cudaStreamSynchronize(s));
-    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
-    return 0;
-}
-
 // ---------------------------------------------------------------- plans: fixed geometry, new charges
 // A plan keeps one evaluation geometry on the device (tree, lists, sorted
 // coordinates, workspace) and runs the charge-dependent passes for any number

@@ -389,4 +389,321 @@ void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, in
     FMM_LAUNCH_CHECK(st);
 }
 
+// ================================================================ Helmholtz triangles
+// Near field of hfmm3dtriatarg (direct3dtritarghelms3, direct3dtrihelms2,
+// direct3dtritarghelmd3, direct3dtrihelmd2 with triquadhelm2 / triquadselfhelm
+// / triquadhelmd2 / triquadselfhelmd, src/triquadflatlib.f:819-2356): the
+// Laplace part of e^{ikr}/r integrated exactly (tri_pair), the difference by
+// the near rule on the triangle (series when |kr| < 0.01).  With z = ikr,
+// d = x - y, h = n.(x - v1), F = e^z (z-1) + 1:
+//   single layer: (e^z - 1)/r, gradient (d/r) F/r^2;
+//   double layer: h f2, gradient n f2 + h f2' d/r, f2 = -F/r^3,
+//   f2' = k^2 e^z/r^2 + 3F/r^4.
+// At the triangle's own centroid (h = 0): the single layer's gradient rule
+// takes (d/r)(F/r^2 - (ik)^2/2) and adds (ik)^2/2 int d/r = -(ik)^2/2 sum_e
+// m_e int_e r dl (closed form); the double layer's value and in-plane
+// gradient vanish, its normal gradient is int (f2 - k^2/(2r)) + (k^2/2) S.
+__device__ __forceinline__ double2 cexp2(double2 z)
+{
+    double sn, cs;
+    sincos(z.y, &sn, &cs);
+    const double e = exp(z.x);
+    return cmk(e * cs, e * sn);
+}
+
+template <bool CHG, bool DIP>
+__device__ __forceinline__ void htri_pair(const double *g, double x0, double x1, double x2, bool self, bool fld,
+                                          double2 ik, const TriRule &rule, double2 &S, double2 (&gS)[3], double2 &D,
+                                          double2 (&gD)[3])
+{
+    double Sl = 0, Dl = 0, gSl[3] = {0, 0, 0}, gDl[3] = {0, 0, 0};
+    tri_pair<true, DIP>(g, x0, x1, x2, self, true, Sl, gSl, Dl, gDl);   // S is needed by the double layer's self term
+    const double *n = g + 9;
+    const double e1[3] = {g[3] - g[0], g[4] - g[1], g[5] - g[2]}, e2[3] = {g[6] - g[0], g[7] - g[1], g[8] - g[2]};
+    const double c0 = e1[1] * e2[2] - e1[2] * e2[1], c1 = e1[2] * e2[0] - e1[0] * e2[2], c2 = e1[0] * e2[1] - e1[1] * e2[0];
+    const double area = 0.5 * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    const double h = self ? 0.0 : n[0] * (x0 - g[0]) + n[1] * (x1 - g[1]) + n[2] * (x2 - g[2]);
+    const double2 ik2 = cmul(ik, ik);
+    const double2 hik2 = cscal(0.5, ik2);
+    double2 sp = cmk(0, 0), dp = cmk(0, 0), dn = cmk(0, 0);
+    double2 sg[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, dg[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    for (int q = 0; q < rule.n; q++) {
+        const double d[3] = {x0 - (g[0] + rule.xi[q] * e1[0] + rule.eta[q] * e2[0]),
+                             x1 - (g[1] + rule.xi[q] * e1[1] + rule.eta[q] * e2[1]),
+                             x2 - (g[2] + rule.xi[q] * e1[2] + rule.eta[q] * e2[2])};
+        // a node on x itself (the one-node rule at a triangle's own centroid) adds the limit of the
+        // bounded difference kernel: its value ik, a zero gradient
+        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], rr = sqrt(r2), ir = rr > 0 ? 1.0 / rr : 0.0;
+        const double w = rule.w[q] * area;
+        const double2 z = cscal(rr, ik);
+        double2 gv, Fr2, f2, f2p, f2s;
+        if (z.x * z.x + z.y * z.y < 1e-4) {
+            const double2 ik3 = cmul(ik2, ik), ik4 = cmul(ik3, ik), ik5 = cmul(ik4, ik), ik6 = cmul(ik5, ik);
+            const double2 z2 = cmul(z, z), z3 = cmul(z2, z), z4 = cmul(z3, z);
+            double2 ser = cmk(1.0 + z.x / 2 + z2.x / 6 + z3.x / 24 + z4.x / 120, z.y / 2 + z2.y / 6 + z3.y / 24 + z4.y / 120);
+            gv = cmul(ik, ser);
+            Fr2 = cadd(cadd(hik2, cscal(rr / 3.0, ik3)), cadd(cscal(r2 / 8.0, ik4), cscal(r2 * rr / 30.0, ik5)));
+            f2s = cscal(-1.0, cadd(cadd(cscal(1.0 / 3.0, ik3), cscal(rr / 8.0, ik4)),
+                                   cadd(cscal(r2 / 30.0, ik5), cscal(r2 * rr / 144.0, ik6))));
+            f2 = csub(f2s, cscal(ir, hik2));
+            f2p = csub(csub(cscal(ir * ir, hik2), cscal(1.0 / 8.0, ik4)),
+                       cadd(cscal(2.0 * rr / 30.0, ik5), cscal(3.0 * r2 / 144.0, ik6)));
+        } else {
+            const double2 E = cexp2(z);
+            const double2 F = cadd(cmul(E, cmk(z.x - 1.0, z.y)), cmk(1.0, 0.0));
+            gv = cscal(ir, cmk(E.x - 1.0, E.y));
+            Fr2 = cscal(ir * ir, F);
+            f2 = cscal(-ir * ir * ir, F);
+            f2s = cadd(f2, cscal(ir, hik2));
+            f2p = cadd(cscal(-ir * ir, cmul(ik2, E)), cscal(3.0 * ir * ir * ir * ir, F));
+        }
+        if (CHG) {
+            sp = cadd(sp, cscal(w, gv));
+            if (fld) {
+                const double2 t = self ? csub(Fr2, hik2) : Fr2;
+#pragma unroll
+                for (int c = 0; c < 3; c++) sg[c] = cadd(sg[c], cscal(w * d[c] * ir, t));
+            }
+        }
+        if (DIP) {
+            if (self) {
+                if (fld) dn = cadd(dn, cscal(w, f2s));
+            } else {
+                dp = cadd(dp, cscal(w * h, f2));
+                if (fld)
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+                        dg[c] = cadd(dg[c], cadd(cscal(w * n[c], f2), cscal(w * h * d[c] * ir, f2p)));
+            }
+        }
+    }
+    if (CHG) {
+        S = cadd(cmk(Sl, 0), sp);
+#pragma unroll
+        for (int c = 0; c < 3; c++) gS[c] = cadd(cmk(gSl[c], 0), sg[c]);
+        if (self && fld) {
+            // (ik)^2/2 int d/r dS = -(ik)^2/2 sum_e m_e int_e r dl (the triangle's plane)
+            double dv[3][3], R[3], J[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                dv[k][0] = g[3 * k] - x0; dv[k][1] = g[3 * k + 1] - x1; dv[k][2] = g[3 * k + 2] - x2;
+                R[k] = sqrt(dv[k][0] * dv[k][0] + dv[k][1] * dv[k][1] + dv[k][2] * dv[k][2]);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int a = i, b = (i + 1) % 3;
+                const double *t = g + 12 + 3 * i, *m = g + 21 + 3 * i;
+                const double sm = dv[a][0] * t[0] + dv[a][1] * t[1] + dv[a][2] * t[2];
+                const double spp = dv[b][0] * t[0] + dv[b][1] * t[1] + dv[b][2] * t[2];
+                const double pd = dv[a][0] * m[0] + dv[a][1] * m[1] + dv[a][2] * m[2];
+                const double f = (spp + sm >= 0) ? log((R[b] + spp) / (R[a] + sm)) : log((R[a] - sm) / (R[b] - spp));
+                const double line = 0.5 * (spp * R[b] - sm * R[a] + pd * pd * f);
+                J[0] -= m[0] * line; J[1] -= m[1] * line; J[2] -= m[2] * line;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) gS[c] = cadd(gS[c], cscal(J[c], hik2));
+        }
+    }
+    if (DIP) {
+        if (self) {
+            D = cmk(0, 0);
+            const double2 nrm = csub(dn, cscal(Sl, hik2));
+#pragma unroll
+            for (int c = 0; c < 3; c++) gD[c] = cadd(cmk(gDl[c], 0), cscal(n[c], nrm));
+        } else {
+            D = cadd(cmk(Dl, 0), dp);
+#pragma unroll
+            for (int c = 0; c < 3; c++) gD[c] = cadd(cmk(gDl[c], 0), dg[c]);
+        }
+    }
+}
+
+template <bool CHG, bool DIP>
+__device__ __forceinline__ void htri_accum(const double *g, double2 q, double2 dq, double x0, double x1, double x2,
+                                           bool self, bool fld, double2 ik, const TriRule &rule, double2 (&acc)[4])
+{
+    double2 S = cmk(0, 0), D = cmk(0, 0), gS[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, gD[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    htri_pair<CHG, DIP>(g, x0, x1, x2, self, fld, ik, rule, S, gS, D, gD);
+    if (CHG) {
+        cfma(acc[0], q, S);
+        if (fld)
+#pragma unroll
+            for (int c = 0; c < 3; c++) cfma(acc[1 + c], cmk(-q.x, -q.y), gS[c]);
+    }
+    if (DIP) {
+        cfma(acc[0], dq, D);
+        if (fld)
+#pragma unroll
+            for (int c = 0; c < 3; c++) cfma(acc[1 + c], cmk(-dq.x, -dq.y), gD[c]);
+    }
+}
+
+// As k_p2p_tri, with complex sums.
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kTriThreads) k_hp2p_tri(const int *leaves, TreeView tv, TriSoA t, const double *sx,
+                                                          const double *sy, const double *sz, const double *tx,
+                                                          const double *ty, const double *tz, double2 zk, TriRule rule,
+                                                          OutSoA outs, OutSoA outt, int do_src, int do_trg,
+                                                          int want_fs, int want_ft)
+{
+    __shared__ double sg[kTriThreads * kTriGeo];
+    __shared__ double2 sq[kTriThreads], sd[kTriThreads];
+    __shared__ double2 red[4][kTriThreads];
+    const double2 ik = cmk(-zk.y, zk.x);
+    const int b = leaves[blockIdx.x];
+    const int s0 = tv.src0[b], ns = do_src ? tv.nsrc[b] : 0;
+    const int t0 = tv.trg0[b], nt = do_trg ? tv.ntrg[b] : 0;
+    const int ne = ns + nt;
+    const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
+    for (int e0 = 0; e0 < ne; e0 += kTriThreads) {
+        const int np = min(kTriThreads, ne - e0);
+        const int G = kTriThreads / np;
+        const int lane = threadIdx.x % np, grp = threadIdx.x / np;
+        const int e = e0 + lane;
+        const bool act = grp < G;
+        const bool is_src = e < ns;
+        double x0 = 0, x1 = 0, x2 = 0;
+        int self = -1;
+        if (act) {
+            if (is_src) { const int i = s0 + e; x0 = sx[i]; x1 = sy[i]; x2 = sz[i]; self = i; }
+            else { const int i = t0 + e - ns; x0 = tx[i]; x1 = ty[i]; x2 = tz[i]; }
+        }
+        const bool fld = is_src ? want_fs != 0 : want_ft != 0;
+        double2 acc[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+        for (int j = 0; j < nl; j++) {
+            const int jb = j == 0 ? b : tv.l1_idx[l1a + j - 1];
+            const int js0 = tv.src0[jb], jn = tv.nsrc[jb];
+            for (int c0 = 0; c0 < jn; c0 += kTriThreads) {
+                const int cn = min(kTriThreads, jn - c0);
+                __syncthreads();
+                const double *gsrc = t.geo + (size_t)kTriGeo * (js0 + c0);
+                for (int k = threadIdx.x; k < cn * kTriGeo; k += kTriThreads) sg[k] = gsrc[k];
+                if (threadIdx.x < cn) {
+                    if (CHG) sq[threadIdx.x] = t.q[js0 + c0 + threadIdx.x];
+                    if (DIP) sd[threadIdx.x] = t.dq[js0 + c0 + threadIdx.x];
+                }
+                __syncthreads();
+                if (!act) continue;
+                const int selfk = self - (js0 + c0);
+                for (int k = grp; k < cn; k += G)
+                    htri_accum<CHG, DIP>(sg + kTriGeo * k, CHG ? sq[k] : cmk(0, 0), DIP ? sd[k] : cmk(0, 0), x0, x1,
+                                         x2, k == selfk, fld, ik, rule, acc);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 4; c++) red[c][threadIdx.x] = act ? acc[c] : cmk(0, 0);
+        __syncthreads();
+        if (threadIdx.x < np) {
+            double2 sum[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                sum[c] = red[c][threadIdx.x];
+                for (int gi = 1; gi < G; gi++) sum[c] = cadd(sum[c], red[c][threadIdx.x + gi * np]);
+            }
+            const OutSoA &o = is_src ? outs : outt;
+            const int i = is_src ? s0 + e : t0 + e - ns;
+            if (o.pot) o.pot[i] = cadd(o.pot[i], sum[0]);
+            if (fld && o.fx) {
+                o.fx[i] = cadd(o.fx[i], sum[1]);
+                o.fy[i] = cadd(o.fy[i], sum[2]);
+                o.fz[i] = cadd(o.fz[i], sum[3]);
+            }
+        }
+    }
+}
+
+void launch_hp2p_tri(const int *leaves, int nleaves, const TreeView &tv, const TriSoA &t, const double *sx,
+                     const double *sy, const double *sz, const double *tx, const double *ty, const double *tz,
+                     double2 zk, const TriRule &rule, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
+                     int do_src, int do_trg, int want_fs, int want_ft, cudaStream_t s, Status &st)
+{
+    if (nleaves == 0 || !st.ok() || !(do_src || do_trg)) return;
+    const bool c = ifcharge == 1, d = ifdipole == 1;
+    if (c && d)
+        k_hp2p_tri<true, true><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, zk, rule, outs,
+                                                               outt, do_src, do_trg, want_fs, want_ft);
+    else if (c)
+        k_hp2p_tri<true, false><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, zk, rule, outs,
+                                                                outt, do_src, do_trg, want_fs, want_ft);
+    else if (d)
+        k_hp2p_tri<false, true><<<nleaves, kTriThreads, 0, s>>>(leaves, tv, t, sx, sy, sz, tx, ty, tz, zk, rule, outs,
+                                                                outt, do_src, do_trg, want_fs, want_ft);
+    else
+        return;
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+// h3dtriadirect at npts points (self_idx / centroids as in launch_tri_direct).
+template <bool CHG, bool DIP>
+__global__ void __launch_bounds__(kTriThreads) k_htri_direct(int ntri, TriSoA t, int npts, const double *pts,
+                                                             int centroids, const int *self_idx, double2 zk,
+                                                             TriRule rule, int want_f, double *pot, double *fld)
+{
+    __shared__ double sg[kTriThreads * kTriGeo];
+    __shared__ double2 sq[kTriThreads], sd[kTriThreads];
+    const double2 ik = cmk(-zk.y, zk.x);
+    const int i = blockIdx.x * kTriThreads + threadIdx.x;
+    const bool act = i < npts;
+    double x0 = 0, x1 = 0, x2 = 0;
+    int self = -1;
+    if (act) {
+        x0 = pts[3L * i]; x1 = pts[3L * i + 1]; x2 = pts[3L * i + 2];
+        if (self_idx) self = self_idx[i];
+        else if (centroids) self = i;
+    }
+    double2 acc[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    for (int c0 = 0; c0 < ntri; c0 += kTriThreads) {
+        const int cn = min(kTriThreads, ntri - c0);
+        __syncthreads();
+        const double *gsrc = t.geo + (size_t)kTriGeo * c0;
+        for (int k = threadIdx.x; k < cn * kTriGeo; k += kTriThreads) sg[k] = gsrc[k];
+        if (threadIdx.x < cn) {
+            if (CHG) sq[threadIdx.x] = t.q[c0 + threadIdx.x];
+            if (DIP) sd[threadIdx.x] = t.dq[c0 + threadIdx.x];
+        }
+        __syncthreads();
+        if (!act) continue;
+        for (int k = 0; k < cn; k++)
+            htri_accum<CHG, DIP>(sg + kTriGeo * k, CHG ? sq[k] : cmk(0, 0), DIP ? sd[k] : cmk(0, 0), x0, x1, x2,
+                                 c0 + k == self, want_f != 0, ik, rule, acc);
+    }
+    if (!act) return;
+    if (pot) { pot[2L * i] = acc[0].x; pot[2L * i + 1] = acc[0].y; }
+    if (fld)
+        for (int c = 0; c < 3; c++) { fld[6L * i + 2 * c] = acc[1 + c].x; fld[6L * i + 2 * c + 1] = acc[1 + c].y; }
+}
+
+void launch_htri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
+                        int centroids, const int *self_idx, double2 zk, const TriRule &rule, double *pot, double *fld,
+                        cudaStream_t s, Status &st)
+{
+    if (npts <= 0 || !st.ok()) return;
+    const bool c = ifcharge == 1, d = ifdipole == 1;
+    const int grid = (npts + kTriThreads - 1) / kTriThreads;
+    if (!c && !d) {
+        if (pot) FMM_TRY(st, cudaMemsetAsync(pot, 0, sizeof(double) * 2 * npts, s));
+        if (fld) FMM_TRY(st, cudaMemsetAsync(fld, 0, sizeof(double) * 6 * npts, s));
+        return;
+    }
+    if (c && d)
+        k_htri_direct<true, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, zk, rule,
+                                                               fld != nullptr, pot, fld);
+    else if (c)
+        k_htri_direct<true, false><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, zk, rule,
+                                                                fld != nullptr, pot, fld);
+    else
+        k_htri_direct<false, true><<<grid, kTriThreads, 0, s>>>(ntri, t, npts, pts, centroids, self_idx, zk, rule,
+                                                                fld != nullptr, pot, fld);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+}
+
+TriRule tri_rule_degree(int norder)
+{
+    // the rule of tri_rule for an iprec whose degree is norder
+    return tri_rule(norder <= 1 ? -3 : norder == 2 ? -1 : norder == 4 ? 0 : 1);
+}
+
 }  // namespace fmm

@@ -63,4 +63,17 @@ void launch_p2p_tri(const int *leaves, int nleaves, const TreeView &tv, const Tr
 void launch_tri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
                        int centroids, const int *self_idx, double *pot, double *fld, cudaStream_t s, Status &st);
 
+// The collapsed Gauss-Legendre rule of polynomial degree norder (1, 2, 4, 6).
+TriRule tri_rule_degree(int norder);
+
+// Helmholtz triangles (hfmm3dtriatarg): the near field with zk and the near
+// rule (degree nqtri), and the direct sum h3dtriadirect.
+void launch_hp2p_tri(const int *leaves, int nleaves, const TreeView &tv, const TriSoA &t, const double *sx,
+                     const double *sy, const double *sz, const double *tx, const double *ty, const double *tz,
+                     double2 zk, const TriRule &rule, OutSoA outs, OutSoA outt, int ifcharge, int ifdipole,
+                     int do_src, int do_trg, int want_fs, int want_ft, cudaStream_t s, Status &st);
+void launch_htri_direct(int ntri, const TriSoA &t, int ifcharge, int ifdipole, int npts, const double *pts,
+                        int centroids, const int *self_idx, double2 zk, const TriRule &rule, double *pot, double *fld,
+                        cudaStream_t s, Status &st);
+
 }  // namespace fmm

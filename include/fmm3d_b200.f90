@@ -125,6 +125,44 @@ module fmm3d_b200
       complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), pottarg(*), fldtarg(3, *)
     end subroutine
 
+    subroutine hfmm3dtriatarg(ier, iprec, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg) &
+        bind(C, name="hfmm3dtriatarg_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld, ntarget, ifpottarg, iffldtarg
+      complex(c_double_complex) :: zk
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *), target(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), pottarg(*), fldtarg(3, *)
+    end subroutine
+
+    subroutine hfmm3dtriaself(ier, iprec, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld) bind(C, name="hfmm3dtriaself_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld
+      complex(c_double_complex) :: zk
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *)
+    end subroutine
+
+    subroutine hfmm3dtria(ier, iprec, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, &
+        dipstr, dipvec, ifpot, pot, iffld, fld) bind(C, name="hfmm3dtria_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: ier, iprec, nsource, ifcharge, ifdipole, ifpot, iffld
+      complex(c_double_complex) :: zk
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *)
+    end subroutine
+
+    subroutine h3dtriadirect(nqtri, zk, nsource, triaflat, trianorm, source, ifcharge, charge, ifdipole, dipstr, &
+        dipvec, ifpot, pot, iffld, fld, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg) &
+        bind(C, name="h3dtriadirect_")
+      import :: c_int, c_double, c_double_complex
+      integer(c_int) :: nqtri, nsource, ifcharge, ifdipole, ifpot, iffld, ntarget, ifpottarg, iffldtarg
+      complex(c_double_complex) :: zk
+      real(c_double) :: triaflat(3, 3, *), trianorm(3, *), source(3, *), dipvec(3, *), target(3, *)
+      complex(c_double_complex) :: charge(*), dipstr(*), pot(*), fld(3, *), pottarg(*), fldtarg(3, *)
+    end subroutine
+
     ! Hessians: the reference's one-point evaluators, and lfmm3dparttarg with Hessian outputs
     ! (hess(6, n): dxx, dyy, dzz, dxy, dxz, dyz; no counterpart in the reference)
     subroutine l3dtaevalhess(rscale, center, local, nterms, ztarg, pot, iffld, fld, ifhess, hess, ier) &

@@ -108,6 +108,38 @@ void l3dtriadirect_(const int *nsource, const double *triaflat, const double *tr
                     const int *ntarget, const double *target, const int *ifpottarg, double *pottarg,
                     const int *iffldtarg, double *fldtarg);
 
+/* Replaces hfmm3dtriatarg (src/hfmm3dtria.f:133-560): Helmholtz layer
+ * potentials e^{ikr}/r of flat triangles, arguments as lfmm3dtriatarg_ with
+ * zk (complex*16) after iprec.  The near field integrates the Laplace part
+ * exactly and the difference e^{ikr}/r - 1/r (and its derivatives) with a
+ * quadrature rule of the reference's degree (nqtri), the far field runs on
+ * quadrature nodes of degree norder (src/hfmm3dtria.f:730-751); the rules
+ * are collapsed Gauss-Legendre rules, not the reference's triasymq tables.
+ * FP64.  The box scale uses |zk| here (zk is complex in this driver). */
+void hfmm3dtriatarg_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                     const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                     const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                     const int *iffld, double *fld, const int *ntarget, const double *target, const int *ifpottarg,
+                     double *pottarg, const int *iffldtarg, double *fldtarg);
+
+/* Replaces hfmm3dtriaself (src/hfmm3dtria.f:92-126) and hfmm3dtria (:51-85). */
+void hfmm3dtriaself_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                     const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                     const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                     const int *iffld, double *fld);
+void hfmm3dtria_(int *ier, const int *iprec, const double *zk, const int *nsource, const double *triaflat,
+                 const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                 const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                 const int *iffld, double *fld);
+
+/* Replaces h3dtriadirect (src/hfmm3dtria.f:1456): the O(N^2) sum with the
+ * near-field integrals of quadrature degree nqtri (1, 2, 4 or 6). */
+void h3dtriadirect_(const int *nqtri, const double *zk, const int *nsource, const double *triaflat,
+                    const double *trianorm, const double *source, const int *ifcharge, const double *charge,
+                    const int *ifdipole, const double *dipstr, const double *dipvec, const int *ifpot, double *pot,
+                    const int *iffld, double *fld, const int *ntarget, const double *target, const int *ifpottarg,
+                    double *pottarg, const int *iffldtarg, double *fldtarg);
+
 /* Replaces l3dtaevalhess (src/laprouts3d.f:5297-5363; it calls
  * l3dtaevalhessdini + l3dtaevalhessd, :7613, :7384) and l3dmpevalhess
  * (:5229-5295; l3dmpevalhessdini + l3dmpevalhessd, :7129, :6945): potential,
@@ -162,6 +194,20 @@ int fmm3d_l3dtriadirect_device(int nsource, const double *d_triaflat, const doub
 int fmm3d_l3dtriadirect_points_device(int nsource, const double *d_triaflat, int ifcharge, const double *d_charge,
                                       int ifdipole, const double *d_dipstr, int npts, const double *d_pts,
                                       const int *d_self, double *d_pot, double *d_fld, void *stream);
+
+/* hfmm3dtriatarg_ on device-resident arrays (zk: two host doubles), and the
+ * Helmholtz triangle direct sum at npts device points (point k is the
+ * centroid of triangle self[k] when self is given, of triangle k when
+ * centroids = 1; pot / fld written; synchronous). */
+int fmm3d_hfmm3dtriatarg_device(int iprec, const double *zk, int nsource, const double *d_triaflat,
+                                const double *d_trianorm, const double *d_source, int ifcharge, const double *d_charge,
+                                int ifdipole, const double *d_dipstr, const double *d_dipvec, int ifpot, double *d_pot,
+                                int iffld, double *d_fld, int ntarget, const double *d_target, int ifpottarg,
+                                double *d_pottarg, int iffldtarg, double *d_fldtarg, void *stream);
+int fmm3d_h3dtriadirect_points_device(int nqtri, const double *zk, int nsource, const double *d_triaflat,
+                                      int ifcharge, const double *d_charge, int ifdipole, const double *d_dipstr,
+                                      int npts, const double *d_pts, const int *d_self, int centroids, double *d_pot,
+                                      double *d_fld, void *stream);
 
 /* The same on device-resident arrays, enqueued on `stream`. */
 int fmm3d_lfmm3dparttarg_hess_device(int iprec, int nsource, const double *d_source, int ifcharge,

@@ -1383,11 +1383,14 @@ void oracle_lfmm3dparttarg_hess(int *ier, int iprec, int nsource, const double *
               hess, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg, ifhesstarg, hesstarg, NULL);
 }
 
+/* Laplace layer potentials on flat triangles (lfmm3dtriatarg). */
+#include "ltri_oracle.c"
+
 /* The Helmholtz restatement shares the tree, lists and rotations above. */
 #include "hfmm3d_oracle.c"
 
 /* Laplace Hessians (pair, local and multipole evaluators, FMM driver). */
 #include "lhess_oracle.c"
 
-/* Laplace layer potentials on flat triangles (lfmm3dtriatarg). */
-#include "ltri_oracle.c"
+/* Helmholtz layer potentials on flat triangles (hfmm3dtriatarg). */
+#include "htri_oracle.c"

@@ -1090,16 +1090,27 @@ void oracle_htranslate(int kind, double zkr, double zki, const double *c_from, c
  * (:545-1086) and hfmm3d_list2 (src/hfmm3drouts.f:153-564).  `tinfo`
  * (optional) receives the wall time of the tree and of steps 1..8;
  * `nterms_out` (optional, 200 ints) the expansion order of every level.   */
-void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsource, const double *source,
-                           int ifcharge, const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
-                           int ifpot, cplx *pot, int iffld, cplx *fld, int ntarget, const double *target,
-                           int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg, double *tinfo,
-                           int *nterms_out)
+/* Triangle mode of the Helmholtz FMM (hfmm3dtriatarg, src/hfmm3dtria.f:133-1215):
+ * the sources are flat triangles, the tree's points their centroids (source);
+ * the far field runs on the triangles' quadrature nodes (degree norder), the
+ * near field integrates over each triangle (htri_oracle.c, degree nqtri). */
+typedef struct {
+    const double *tri, *trinorm;
+    int norder, nqtri;
+} htri_args;
+static void htri_point(cplx zk, int nj, const double *tri, int ifcharge, const cplx *q, int ifdipole, const cplx *ds,
+                       const double *x, long self, int iffld, int nqtri, cplx *pot, cplx *fld);
+
+static void hfmm_core(int *ier, int iprec, double zkr, double zki, int nsource, const double *source,
+                      int ifcharge, const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
+                      int ifpot, cplx *pot, int iffld, cplx *fld, int ntarget, const double *target,
+                      int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg, double *tinfo,
+                      int *nterms_out, const htri_args *ta)
 {
     *ier = 0;
     cplx zk = zkr + I * zki;
     double eps = oracle_lap_eps(iprec);
-    int nbox = oracle_lap_nbox(iprec, nsource, ntarget);
+    int nbox = ta ? oracle_tri_nbox(iprec, nsource, ntarget) : oracle_lap_nbox(iprec, nsource, ntarget);
     if (nbox < 0 || nsource < 1) { *ier = 4; return; }
     double tt0 = omp_get_wtime();
     otree T;
@@ -1115,7 +1126,8 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
         scale[i] = 1.0;
         /* zk is implicitly real*8 in hfmm3dparttarg (src/hfmm3dpart.f:145, no
          * complex declaration), so this rule reads only Re(zk) (:337-341) */
-        double bs = fabs((T.size / pow(2.0, i)) * creal(zk));
+        /* hfmm3dtriatarg declares zk complex*16: there the rule sees |zk| (src/hfmm3dtria.f:248, 350-355) */
+        double bs = ta ? cabs((T.size / pow(2.0, i)) * zk) : fabs((T.size / pow(2.0, i)) * creal(zk));
         if (bs < 1) scale[i] = bs;
         bsize[i] = T.size / pow(2.0, i);
         int e;
@@ -1136,6 +1148,26 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
         if (ifdipole == 1) { dss[i] = dipstr[j]; memcpy(dvs + 3 * (size_t)i, dipvec + 3 * (size_t)j, 3 * sizeof(double)); }
     }
     for (int i = 0; i < ntarget; i++) memcpy(ts + 3 * (size_t)i, target + 3 * (size_t)T.iztarg[i], 3 * sizeof(double));
+    /* triangles: sorted vertices, and the far field's quadrature nodes in tree order */
+    double *trs = NULL, *qp = NULL, *qw = NULL, *qv = NULL;
+    cplx *qq = NULL, *qd = NULL;
+    int nq = 1;
+    if (ta) {
+        trs = malloc(sizeof(double) * 9 * (size_t)nsource);
+        for (int i = 0; i < nsource; i++) memcpy(trs + 9 * (size_t)i, ta->tri + 9 * (size_t)T.iz[i], 9 * sizeof(double));
+        double xi[64], eta[64], wr[64];
+        nq = tri_rule(ta->norder, xi, eta, wr);
+        size_t nn = (size_t)nsource * nq;
+        qp = malloc(sizeof(double) * 3 * nn); qw = malloc(sizeof(double) * nn); qv = malloc(sizeof(double) * 3 * nn);
+        qq = calloc(nn, sizeof(cplx)); qd = calloc(nn, sizeof(cplx));
+        tri_nodes(nsource, trs, ta->norder, qp, qw, &nq);
+        for (size_t i = 0; i < nn; i++) {
+            size_t t = i / nq;
+            if (ifcharge == 1) qq[i] = qs[t] * qw[i];
+            if (ifdipole == 1) qd[i] = dss[t] * qw[i];
+            memcpy(qv + 3 * i, ta->trinorm + 3 * (size_t)T.iz[t], 3 * sizeof(double));
+        }
+    }
     cplx *ps = calloc((size_t)nsource, sizeof(cplx)), *fs = calloc(3 * (size_t)nsource, sizeof(cplx));
     cplx *pt = calloc((size_t)(ntarget > 0 ? ntarget : 1), sizeof(cplx));
     cplx *ft = calloc(3 * (size_t)(ntarget > 0 ? ntarget : 1), sizeof(cplx));
@@ -1156,8 +1188,14 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
         int lev = BX(ib, B_LEV);
         if (lev < 2 || BX(ib, B_NSRC) == 0 || nkids(&T, ib) != 0) continue;
         int s0 = BX(ib, B_SRC0), n = BX(ib, B_NSRC);
-        oracle_hformmp(zkr, zki, scale[lev], n, ss + 3 * (size_t)s0, ifcharge, qs + s0, ifdipole, dss + s0,
-                       dvs + 3 * (size_t)s0, CEN(ib), nterms[lev], mpole + (size_t)ib * K);
+        if (ta) {
+            size_t q0 = (size_t)s0 * nq;
+            oracle_hformmp(zkr, zki, scale[lev], n * nq, qp + 3 * q0, ifcharge, qq + q0, ifdipole, qd + q0, qv + 3 * q0,
+                           CEN(ib), nterms[lev], mpole + (size_t)ib * K);
+        } else {
+            oracle_hformmp(zkr, zki, scale[lev], n, ss + 3 * (size_t)s0, ifcharge, qs + s0, ifdipole, dss + s0,
+                           dvs + 3 * (size_t)s0, CEN(ib), nterms[lev], mpole + (size_t)ib * K);
+        }
     }
     /* STEP 2: P2L of a leaf's sources into its list-3 boxes (src/hfmm3dpart.f:775-846),
      * gathered here per receiving box through the dual list 4.           */
@@ -1170,8 +1208,14 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
             int n = BX(jb, B_NSRC);
             if (n == 0) continue;
             int s0 = BX(jb, B_SRC0);
-            oracle_hformta(zkr, zki, scale[lev], n, ss + 3 * (size_t)s0, ifcharge, qs + s0, ifdipole, dss + s0,
-                           dvs + 3 * (size_t)s0, CEN(ib), nterms[lev], local + (size_t)ib * K);
+            if (ta) {
+                size_t q0 = (size_t)s0 * nq;
+                oracle_hformta(zkr, zki, scale[lev], n * nq, qp + 3 * q0, ifcharge, qq + q0, ifdipole, qd + q0,
+                               qv + 3 * q0, CEN(ib), nterms[lev], local + (size_t)ib * K);
+            } else {
+                oracle_hformta(zkr, zki, scale[lev], n, ss + 3 * (size_t)s0, ifcharge, qs + s0, ifdipole, dss + s0,
+                               dvs + 3 * (size_t)s0, CEN(ib), nterms[lev], local + (size_t)ib * K);
+            }
         }
     }
     /* STEP 3: M2M into parents of levels nlev-1..2 (src/hfmm3drouts.f:209-289) */
@@ -1295,15 +1339,23 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
             cplx pv, fv[3];
             if (ifpot == 1 || iffld == 1)
                 for (int i = s0; i < s0 + ns; i++) {
-                    hdirect_one(zk, jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
-                                dvs + 3 * (size_t)js0, ss + 3 * (size_t)i, jb == ib ? i - s0 : -1, iffld, &pv, fv);
+                    if (ta)
+                        htri_point(zk, jn, trs + 9 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                   ss + 3 * (size_t)i, jb == ib ? i - s0 : -1, iffld, ta->nqtri, &pv, fv);
+                    else
+                        hdirect_one(zk, jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                    dvs + 3 * (size_t)js0, ss + 3 * (size_t)i, jb == ib ? i - s0 : -1, iffld, &pv, fv);
                     if (ifpot == 1) ps[i] += pv;
                     if (iffld == 1) for (int d = 0; d < 3; d++) fs[3 * (size_t)i + d] += fv[d];
                 }
             if (ifpottarg == 1 || iffldtarg == 1)
                 for (int i = t0; i < t0 + ntg; i++) {
-                    hdirect_one(zk, jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
-                                dvs + 3 * (size_t)js0, ts + 3 * (size_t)i, -1, iffldtarg, &pv, fv);
+                    if (ta)
+                        htri_point(zk, jn, trs + 9 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                   ts + 3 * (size_t)i, -1, iffldtarg, ta->nqtri, &pv, fv);
+                    else
+                        hdirect_one(zk, jn, ss + 3 * (size_t)js0, ifcharge, qs + js0, ifdipole, dss + js0,
+                                    dvs + 3 * (size_t)js0, ts + 3 * (size_t)i, -1, iffldtarg, &pv, fv);
                     if (ifpottarg == 1) pt[i] += pv;
                     if (iffldtarg == 1) for (int d = 0; d < 3; d++) ft[3 * (size_t)i + d] += fv[d];
                 }
@@ -1331,5 +1383,16 @@ void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsou
     free(xq); free(wq);
     free(ss); free(ts); free(qs); free(dss); free(dvs); free(ps); free(fs); free(pt); free(ft);
     free(mpole); free(local);
+    free(trs); free(qp); free(qw); free(qv); free(qq); free(qd);
     tree_free(&T);
+}
+
+void oracle_hfmm3dparttarg(int *ier, int iprec, double zkr, double zki, int nsource, const double *source,
+                           int ifcharge, const cplx *charge, int ifdipole, const cplx *dipstr, const double *dipvec,
+                           int ifpot, cplx *pot, int iffld, cplx *fld, int ntarget, const double *target,
+                           int ifpottarg, cplx *pottarg, int iffldtarg, cplx *fldtarg, double *tinfo,
+                           int *nterms_out)
+{
+    hfmm_core(ier, iprec, zkr, zki, nsource, source, ifcharge, charge, ifdipole, dipstr, dipvec, ifpot, pot, iffld,
+              fld, ntarget, target, ifpottarg, pottarg, iffldtarg, fldtarg, tinfo, nterms_out, NULL);
 }

@@ -39,6 +39,8 @@
  * reference's degrees (nqtri = 2 for iprec -2 and -1, 4 for 0, 6 for
  * iprec >= 1, src/lfmm3dtria.f:679-701).                                    */
 
+void oracle_legewhts(int n, double *x, double *w);
+
 static void cross3(const double *a, const double *b, double *c)
 {
     c[0] = a[1] * b[2] - a[2] * b[1];

@@ -233,6 +233,56 @@ def tri_direct_at(triaflat, pts, self_idx=None, charge=None, dipstr=None):
     return pot[:k], fld[:k]
 
 
+def htri_near(zk, tri, pts, self=False, nqtri=6):
+    """Helmholtz single / double layer integrals of one flat triangle (3,3) at pts (the near-field
+    formulas of the triangle FMM): (S, grad S, D, grad D), complex."""
+    v = _f64(tri, (3, 3))
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    S, D = np.zeros(k, np.complex128), np.zeros(k, np.complex128)
+    gS, gD = np.zeros((k, 3), np.complex128), np.zeros((k, 3), np.complex128)
+    zk = complex(zk)
+    lib().oracle_htri_near(c_dbl(zk.real), c_dbl(zk.imag), _p(v), c_int(k), _p(pts), c_int(int(self)),
+                           c_int(nqtri), _p(S), _p(gS), _p(D), _p(gD))
+    return S, gS, D, gD
+
+
+def htri_nqtri(iprec):
+    lib().oracle_htri_nqtri.restype = c_int
+    return lib().oracle_htri_nqtri(c_int(iprec))
+
+
+def htri_direct_at(zk, triaflat, pts, self_idx=None, charge=None, dipstr=None, nqtri=6):
+    """Helmholtz triangle direct sum at pts (self_idx[k]: the triangle whose centroid point k is, or -1)."""
+    tri = _f64(triaflat, (0, 3, 3)); n = tri.shape[0]
+    pts = _f64(pts, (0, 3)); k = pts.shape[0]
+    sk = None if self_idx is None else np.ascontiguousarray(self_idx, np.int64)
+    pot = np.zeros(max(k, 1), np.complex128); fld = np.zeros((max(k, 1), 3), np.complex128)
+    zk = complex(zk)
+    lib().oracle_htri_direct_points(c_dbl(zk.real), c_dbl(zk.imag), c_int(n), _p(tri), c_int(int(charge is not None)),
+                                    _p(_c128(charge, n)), c_int(int(dipstr is not None)), _p(_c128(dipstr, n)),
+                                    c_int(k), _p(pts), None if sk is None else _p(sk), c_int(nqtri), _p(pot), _p(fld))
+    return pot[:k], fld[:k]
+
+
+def hfmm3dtriatarg(iprec, zk, triaflat, trianorm, source, charge=None, dipstr=None, target=None, ifpot=1, iffld=1,
+                   ifpottarg=1, iffldtarg=1):
+    """hfmm3dtriatarg: (ier, pot, fld, pottarg, fldtarg)."""
+    tri = _f64(triaflat, (0, 3, 3)); n = tri.shape[0]
+    nrm = _f64(trianorm, (0, 3))
+    src = _f64(source, (0, 3))
+    trg = _f64(target, (0, 3)) if target is not None else np.zeros((0, 3)); m = trg.shape[0]
+    pot = np.zeros(max(n, 1), np.complex128); fld = np.zeros((max(n, 1), 3), np.complex128)
+    pt = np.zeros(max(m, 1), np.complex128); ft = np.zeros((max(m, 1), 3), np.complex128)
+    ier = c_int(0)
+    zk = complex(zk)
+    lib().oracle_hfmm3dtriatarg(ctypes.byref(ier), c_int(iprec), c_dbl(zk.real), c_dbl(zk.imag), c_int(n), _p(tri),
+                                _p(nrm), _p(src), c_int(int(charge is not None)), _p(_c128(charge, n)),
+                                c_int(int(dipstr is not None)), _p(_c128(dipstr, n)), c_int(ifpot), _p(pot),
+                                c_int(iffld), _p(fld), c_int(m), _p(trg if m else np.zeros((1, 3))),
+                                c_int(ifpottarg if m else 0), _p(pt), c_int(iffldtarg if m else 0), _p(ft))
+    return ier.value, pot[:n], fld[:n], pt[:m], ft[:m]
+
+
 def lfmm3dtriatarg(iprec, triaflat, trianorm, source, charge=None, dipstr=None, target=None, ifpot=1, iffld=1,
                    ifpottarg=1, iffldtarg=1):
     """lfmm3dtriatarg: (ier, pot, fld, pottarg, fldtarg)."""
