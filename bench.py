@@ -77,6 +77,7 @@ JSON cache PATH and exits; every measured workload reports the knobs it ran with
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -124,6 +125,8 @@ def parse_args(argv=None):
                     help="tune the Laplace workloads' launch shapes into the JSON cache PATH and exit")
     ap.add_argument("--tri-level", type=int, default=7,
                     help="triangle workload: icosphere subdivision level (20 * 4^level triangles)")
+    ap.add_argument("--htri-level", type=int, default=6,
+                    help="Helmholtz triangle workload (zk = 4 pi): icosphere subdivision level (0: skip)")
     ap.add_argument("--workload", choices=["all", "laplace", "helmholtz", "batched", "triangles"], default="all",
                     help="all: the Laplace headline line with the other workloads' objects (default); "
                          "laplace / helmholtz / batched: one workload only (profiling runs)")
@@ -218,10 +221,12 @@ def run_laplace_sphere(args, R, n=100_000):
     return out
 
 
-def run_triangles(args, R, k=7, iprec=1):
+def run_triangles(args, R, k=7, iprec=1, zk=None):
     """lfmm3dtriaself on a triangulated unit sphere (icosphere of 20 * 4^k flat triangles), single and
     double layer with densities in [-1, 1]^2, iprec 1, FP64: device time, errors against the exact
-    direct sum at sampled centroids, and the oracle (parity, CPU baseline) on the same inputs."""
+    direct sum at sampled centroids, and the oracle (parity, CPU baseline) on the same inputs.
+    With zk: hfmm3dtriaself (Helmholtz, FP64 only), errors against the direct sum of the same
+    near-field rule (h3dtriadirect)."""
     from fmmlib3d_b200.meshes import icosphere, normals_centroids
     torch, F = R["torch"], R["F"]
     T = icosphere(k)
@@ -238,7 +243,10 @@ def run_triangles(args, R, k=7, iprec=1):
     stream = torch.cuda.current_stream().cuda_stream
 
     def step(pot=d_pot, fld=d_fld):
-        ier = F.lfmm3dtriatarg_device(iprec, d_tri, d_nrm, d_cen, d_q, d_dq, pot, fld, stream=stream)
+        if zk is None:
+            ier = F.lfmm3dtriatarg_device(iprec, d_tri, d_nrm, d_cen, d_q, d_dq, pot, fld, stream=stream)
+        else:
+            ier = F.hfmm3dtriatarg_device(iprec, zk, d_tri, d_nrm, d_cen, d_q, d_dq, pot, fld, stream=stream)
         if ier != 0:
             raise RuntimeError("triangle FMM ier=%d: %s" % (ier, F.last_error()))
 
@@ -261,55 +269,77 @@ def run_triangles(args, R, k=7, iprec=1):
         return t, ps
 
     ms, passes = timed()
-    # the mixed form: M2L on the tensor cores, the exact near field FP64
-    m_pot = torch.empty_like(d_pot)
-    m_fld = torch.empty_like(d_fld)
-    F.set_precision(1)
-    try:
-        ms_mixed, passes_mixed = timed(pot=m_pot, fld=m_fld)
-    finally:
-        F.set_precision(0)
+    m_pot = m_fld = None
+    if zk is None:
+        # the mixed form: M2L on the tensor cores, the exact near field FP64
+        m_pot = torch.empty_like(d_pot)
+        m_fld = torch.empty_like(d_fld)
+        F.set_precision(1)
+        try:
+            ms_mixed, passes_mixed = timed(pot=m_pot, fld=m_fld)
+        finally:
+            F.set_precision(0)
     m = min(args.err_samples, n)
     si = np.sort(rng.choice(n, m, replace=False)).astype(np.int32)
     it = torch.from_numpy(si).to(dev)
     dp = torch.empty((m, 2), dtype=torch.float64, device=dev)
     df = torch.empty((m, 6), dtype=torch.float64, device=dev)
-    ier = F.tri_direct_points_device(d_tri, d_q, d_dq, d_cen[it.long()].contiguous(), it, dp, df, stream=stream)
+    # the near-field rule degree of hfmm3dtriatarg (src/hfmm3dtria.f:730-751)
+    nqtri = 2 if iprec in (-2, -1) else 4 if iprec == 0 else 6 if iprec >= 1 else 1
+    if zk is None:
+        ier = F.tri_direct_points_device(d_tri, d_q, d_dq, d_cen[it.long()].contiguous(), it, dp, df, stream=stream)
+    else:
+        ier = F.htri_direct_points_device(nqtri, zk, d_tri, d_q, d_dq, d_cen[it.long()].contiguous(), it, dp, df,
+                                          stream=stream)
     torch.cuda.synchronize()
     if ier != 0:
         raise RuntimeError("triangle direct ier=%d" % ier)
     gp, gf = d_pot[it.long()], d_fld[it.long()]
-    out = {"workload": "laplace_lfmm3dtriaself_icosphere_%d_triangles_iprec%d" % (n, iprec), "n_triangles": n,
+    kind = "laplace_lfmm3dtriaself" if zk is None else "helmholtz_hfmm3dtriaself_zk%g" % zk.real
+    out = {"workload": "%s_icosphere_%d_triangles_iprec%d" % (kind, n, iprec), "n_triangles": n,
            "iprec": iprec, "dtype": "f64", "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
            "pass_ms": {kk: round(v, 3) for kk, v in passes.items()},
            "errors": {"pot": float("%.3e" % float(torch.linalg.norm(gp - dp) / torch.linalg.norm(dp))),
                       "fld": float("%.3e" % float(torch.linalg.norm(gf - df) / torch.linalg.norm(df)))},
-           "note": "errors against the exact direct sum (l3dtriadirect) at %d sampled centroids" % m}
-    mp, mf = m_pot[it.long()], m_fld[it.long()]
-    out["mixed"] = {"value": n / (ms_mixed * 1e-3), "ms_per_step": ms_mixed,
-                    "pass_ms": {kk: round(v, 3) for kk, v in passes_mixed.items()},
-                    "errors": {"pot": float("%.3e" % float(torch.linalg.norm(mp - dp) / torch.linalg.norm(dp))),
-                               "fld": float("%.3e" % float(torch.linalg.norm(mf - df) / torch.linalg.norm(df)))},
-                    "form": "M2L on the tensor cores (split TF32); near field and other passes FP64"}
+           "note": "errors against the direct sum (%s) at %d sampled centroids"
+                   % ("l3dtriadirect" if zk is None else "h3dtriadirect, nqtri %d" % nqtri, m)}
+    if zk is not None:
+        out["zk"] = [zk.real, zk.imag]
+    forms = {"fp64": None}
+    if m_pot is not None:
+        mp, mf = m_pot[it.long()], m_fld[it.long()]
+        out["mixed"] = {"value": n / (ms_mixed * 1e-3), "ms_per_step": ms_mixed,
+                        "pass_ms": {kk: round(v, 3) for kk, v in passes_mixed.items()},
+                        "errors": {"pot": float("%.3e" % float(torch.linalg.norm(mp - dp) / torch.linalg.norm(dp))),
+                                   "fld": float("%.3e" % float(torch.linalg.norm(mf - df) / torch.linalg.norm(df)))},
+                        "form": "M2L on the tensor cores (split TF32); near field and other passes FP64"}
     if R["rank"] == 0 and not args.no_cpu:
-        gv = {"pot": gp.cpu().numpy(), "fld": gf.cpu().numpy()}
-        mv = {"pot": mp.cpu().numpy(), "fld": mf.cpu().numpy()}
+        forms["fp64"] = {"pot": gp.cpu().numpy(), "fld": gf.cpu().numpy()}
+        if m_pot is not None:
+            forms["mixed"] = {"pot": mp.cpu().numpy(), "fld": mf.cpu().numpy()}
         gd = {"pot": dp.cpu().numpy(), "fld": df.cpu().numpy()}
+        key = "laplace_triangles" if zk is None else "helmholtz_triangles"
 
         def cpu_job(line):
             import oracle
             c = lambda a: a[:, 0] + 1j * a[:, 1]
             t0 = time.perf_counter()
-            oier, opot, ofld, _, _ = oracle.lfmm3dtriatarg(iprec, T, nrm, cen, c(q), c(dq))
+            if zk is None:
+                oier, opot, ofld, _, _ = oracle.lfmm3dtriatarg(iprec, T, nrm, cen, c(q), c(dq))
+            else:
+                oier, opot, ofld, _, _ = oracle.hfmm3dtriatarg(iprec, zk, T, nrm, cen, c(q), c(dq))
             dt = time.perf_counter() - t0
             if oier != 0:
                 raise RuntimeError("oracle ier=%d" % oier)
-            tp, tf = oracle.tri_direct_at(T, cen[si], si, c(q), c(dq))
+            if zk is None:
+                tp, tf = oracle.tri_direct_at(T, cen[si], si, c(q), c(dq))
+            else:
+                tp, tf = oracle.htri_direct_at(zk, T, cen[si], si, c(q), c(dq), nqtri=nqtri)
             rep = parity_report({"pot": _as_pairs(opot[si], 2), "fld": _as_pairs(ofld[si], 6)},
-                                {"pot": _as_pairs(tp, 2), "fld": _as_pairs(tf, 6)}, {"fp64": gv, "mixed": mv}, gd)
+                                {"pot": _as_pairs(tp, 2), "fld": _as_pairs(tf, 6)}, forms, gd)
             rep.update(points="%d seeded centroids (own triangle in-plane)" % m,
                        inputs="the triangle workload's own inputs", oracle_call_s=round(dt, 2))
-            line.setdefault("parity", {})["laplace_triangles"] = rep
+            line.setdefault("parity", {})[key] = rep
             out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", "1")),
                                    "kind": "port", "sample": "the whole workload, one call (%.1f s)" % dt}
 
@@ -1152,6 +1182,8 @@ def main(argv=None):
         out = run_triangles(args, R, k=args.tri_level)
         line = {"metric": "triangle FMM triangles/s (icosphere, iprec=1)", "value": out["value"], "unit": UNIT,
                 "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "laplace_triangles": out}
+        if args.htri_level > 0:
+            line["helmholtz_triangles"] = run_triangles(args, R, k=args.htri_level, zk=complex(4 * math.pi))
         for job in R.get("cpu_jobs", []):
             job(line)
         print(json.dumps(line), flush=True)
@@ -1220,6 +1252,8 @@ def main(argv=None):
         cpu_jobs.append(cube_job)
     line["laplace_sphere"] = run_laplace_sphere(args, R)
     line["laplace_triangles"] = run_triangles(args, R, k=args.tri_level)
+    if args.htri_level > 0:
+        line["helmholtz_triangles"] = run_triangles(args, R, k=args.htri_level, zk=complex(4 * math.pi))
     if args.n == 2_000_000 and args.iprec == 1:
         line["laplace_iprec2"] = run_iprec2(args, R)
     if args.batch_instances > 0:
