@@ -855,7 +855,7 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
 // (broadcast), each thread keeps its point's radial functions in a shared
 // column, and walks the orders m (outer) and degrees n (inner) with the
 // Legendre column recurrence in registers.
-constexpr int kHEvalThreads = 128;
+constexpr int kHEvalThreads = 128, kHM2PThreads = 64;
 
 // T threads per CTA: 128, or 32 at orders whose radial columns of 128 points
 // would not fit in shared memory beside the coefficients.
@@ -864,11 +864,13 @@ __global__ void __launch_bounds__(T) k_heval(const int *leaves, TreeView tv, con
                                                         const double *sy, const double *sz, const double *tx,
                                                         const double *ty, const double *tz, HLevels lv, int NC,
                                                         double2 zk, const double2 *mpole, const double2 *local,
-                                                        OutSoA outs, OutSoA outt, int do_src, int do_trg)
+                                                        OutSoA outs, OutSoA outt, int do_src, int do_trg,
+                                                        int with_l3)
 {
     extern __shared__ double2 hsm[];
     const int b = leaves[blockIdx.x];
     const int blev = tv.level[b];
+    if (!with_l3 && blev < 2) return;
     const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
     if (ne == 0) return;
     const int pm = max_p(lv);
@@ -876,7 +878,9 @@ __global__ void __launch_bounds__(T) k_heval(const int *leaves, TreeView tv, con
     double2 *E = hsm;
     double2 *Fs = hsm + KM;  // radial functions, [n][thread]
     const int t = threadIdx.x;
-    const int l3a = tv.l3_start[b], nl3 = tv.l3_start[b + 1] - l3a;
+    const int l3a = tv.l3_start[b], nl3 = with_l3 ? tv.l3_start[b + 1] - l3a : 0;
+    // CTA (leaf, y) serves the leaf's point chunks y, y + gridDim.y, ... of T points
+    for (int c0 = blockIdx.y * T; c0 < ne; c0 += gridDim.y * T)
     for (int xi = -1; xi < nl3; xi++) {
         int eb;
         const bool isloc = xi < 0;
@@ -895,7 +899,7 @@ __global__ void __launch_bounds__(T) k_heval(const int *leaves, TreeView tv, con
         for (int i = t; i < K; i += T) E[i] = ex[i];
         __syncthreads();
         const double *c = tv.center + 3L * eb;
-        for (int c0 = 0; c0 < ne; c0 += T) {
+        {
             const int e = c0 + t;
             if (e >= ne) continue;
             const bool is_src = e < ns;
@@ -980,6 +984,184 @@ __global__ void __launch_bounds__(T) k_heval(const int *leaves, TreeView tv, con
     }
 }
 
+// M2P of the list-3 boxes (h3dmpeval_trunc0, src/helmrouts3d.f:2405) apart from the
+// local expansions.  List 3 is very uneven on adaptive trees (on a sphere surface
+// most leaves have none and a few have over a hundred), so the work is cut into
+// items of one leaf, one chunk of T of its points and one group of at most
+// kHM2PGroup of its list-3 boxes, one CTA each.  An item writes its points' sums
+// over its group to its own slot of a scratch array; k_hm2p_add then adds the
+// groups' sums to the outputs in group order, so results do not depend on the
+// schedule.  The scaled Hankel functions f_n = h_n(z) scale^n of h3dall (the
+// upward recurrence f_{n+1} = (2n+1) scale/z f_n - scale^2 f_{n-1} of hank_dev,
+// from f_0 = e^{iz}/(iz) and f_1) are regenerated along each order's run of
+// degrees from the pair (f_{m-1}, f_m) that the previous order's run passed, so
+// every value is the one hank_dev stores and shared memory holds only the staged
+// multipole.
+constexpr int kHM2PGroup = 16;
+
+__global__ void k_hm2p_count(const int *leaves, int nleaves, TreeView tv, int do_src, int do_trg, int *cnt)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nleaves) return;
+    const int b = leaves[l];
+    const int ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
+    const int nl3 = tv.l3_start[b + 1] - tv.l3_start[b];
+    cnt[l] = (ne > 0 && nl3 > 0) ? ((ne + kHM2PThreads - 1) / kHM2PThreads) * ((nl3 + kHM2PGroup - 1) / kHM2PGroup)
+                                 : 0;
+}
+
+// The leaf of work item `item`: the last l with off[l] <= item (leaves without items
+// share their offset with the next leaf).
+__device__ __forceinline__ int hm2p_leaf(const int *off, int nleaves, int item)
+{
+    int lo = 0, hi = nleaves - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) k_hm2p(const int *leaves, int nleaves, const int *off, TreeView tv,
+                                             const double *sx, const double *sy, const double *sz, const double *tx,
+                                             const double *ty, const double *tz, HLevels lv, int NC, double2 zk,
+                                             const double2 *mpole, int do_src, int do_trg, double *part)
+{
+    extern __shared__ double2 hsm[];
+    const int item = blockIdx.x;
+    const int l = hm2p_leaf(off, nleaves, item), b = leaves[l];
+    const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
+    const int l3a = tv.l3_start[b], nl3 = tv.l3_start[b + 1] - l3a;
+    const int ngr = (nl3 + kHM2PGroup - 1) / kHM2PGroup;
+    const int local = item - off[l], ck = local / ngr, grp = local - ck * ngr;
+    const int c0 = ck * T, x1 = min(nl3, (grp + 1) * kHM2PGroup);
+    double2 *E = hsm;
+    const int t = threadIdx.x;
+    // this item's sums at its point: pot, then -fld (x, y, z)
+    double2 spot = cmk(0, 0), sfx = cmk(0, 0), sfy = cmk(0, 0), sfz = cmk(0, 0);
+    for (int xi = grp * kHM2PGroup; xi < x1; xi++) {
+        const int eb = tv.l3_idx[l3a + xi];
+        if (tv.nsrc[eb] == 0) continue;
+        const int lev = tv.level[eb], p = lv.p[lev];
+        const double sc = lv.sc[lev];
+        const int K = (p + 1) * (p + 1);
+        const double2 *ex = mpole + (size_t)eb * NC;
+        __syncthreads();
+        for (int i = t; i < K; i += T) E[i] = ex[i];
+        __syncthreads();
+        const double *c = tv.center + 3L * eb;
+        {
+            const int e = c0 + t;
+            if (e >= ne) continue;
+            const bool is_src = e < ns;
+            const int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
+            double px = is_src ? sx[i] : tx[i], py = is_src ? sy[i] : ty[i], pz = is_src ? sz[i] : tz[i];
+            const PtGeo g = pt_geo(px - c[0], py - c[1], pz - c[2]);
+            const double2 z = cscal(g.r, zk);
+            if (cabsd(z) < 1.0e-15) continue;
+            const double r = g.r, ct = g.ct, st = g.st, u = -st;
+            const double isc = 1.0 / sc, ir = 1.0 / r;
+            const double2 zi = cdiv(cmk(1, 0), z), e1 = cmk(g.cp, g.sp);
+            // f_0, f_1 as hank_dev (h3d01, src/helmrouts3d.f:666-704)
+            const double2 h0 = cdiv(cexpi(z), cmk(-z.y, z.x));
+            const double2 f1 = cscal(sc, cmul(h0, cmk(zi.x, zi.y - 1.0)));
+            const double s2 = sc * sc;
+            const double2 zs = cscal(sc, zi);
+            double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
+            double2 em = cmk(1, 0);
+            double ymm = 1.0;
+            double2 sa = cmk(0, 0), sb = h0;   // f_{m-1}, f_m at the start of order m
+            for (int m = 0; m <= p; m++) {
+                if (m == 1) ymm = -sqrt(0.5);
+                else if (m > 1) ymm *= u * __ldg(&g_hc[m]);
+                if (m > 0) em = cmul(em, e1);
+                LegCol L;
+                L.x = ct;
+                L.m = m;
+                L.w = m == 0 ? 1.0 : u * u;
+                L.y1 = ymm;
+                L.d1 = m == 0 ? 0.0 : ymm * (-m) * ct;
+                L.y2 = 0;
+                L.d2 = 0;
+                double2 fa = sa, fb = sb;      // f_{n-1}, f_n
+                for (int n = m; n <= p; n++) {
+                    if (n > m) L.step(n);
+                    const double sn = __ldg(&g_hs[n]);
+                    const double y = L.y1 * sn, dd = L.d1 * sn;
+                    const double2 fn = fb;
+                    double2 fd = n == 0 ? cscal(-isc, f1) : csub(cscal(sc, fa), cmul(cscal(n + 1.0, zi), fn));
+                    const double2 fu = cscal(ir, fn);
+                    fd = cmul(fd, zk);
+                    if (m == 0) {
+                        const double2 a = E[eidx(n, 0)];
+                        cfma(pot, fn, cscal(y, a));
+                        cfma(ur, fd, cscal(y, a));
+                        cfma(ut, fu, cscal(-dd * st, a));
+                    } else {
+                        const double2 z2 = cmul(E[eidx(n, m)], em), z3 = cmul(E[eidx(n, -m)], cconj(em));
+                        const double2 zs2 = cadd(z2, z3), zd = csub(z2, z3);
+                        cfma(pot, fn, cscal(y * st, zs2));
+                        cfma(ur, fd, cscal(y * st, zs2));
+                        cfma(ut, fu, cscal(-dd, zs2));
+                        cfma(up, fu, cscal(y * m, cmk(-zd.y, zd.x)));  // i m (z2 - z3)
+                    }
+                    if (n < p) {
+                        const double2 fc = n == 0 ? f1 : csub(cmul(cscal(2 * n + 1.0, zs), fb), cscal(s2, fa));
+                        fa = fb;
+                        fb = fc;
+                        if (n == m) { sa = fa; sb = fb; }   // (f_m, f_{m+1}) start order m + 1
+                    }
+                }
+            }
+            const double cp = g.cp, sp = g.sp;
+            spot = cadd(spot, pot);
+            sfx = csub(sfx, cadd(cadd(cscal(st * cp, ur), cscal(ct * cp, ut)), cscal(-sp, up)));
+            sfy = csub(sfy, cadd(cadd(cscal(st * sp, ur), cscal(ct * sp, ut)), cscal(cp, up)));
+            sfz = csub(sfz, csub(cscal(ct, ur), cscal(st, ut)));
+        }
+    }
+    double *o = part + (size_t)item * 8 * T + t;
+    o[0] = spot.x; o[T] = spot.y; o[2 * T] = sfx.x; o[3 * T] = sfx.y;
+    o[4 * T] = sfy.x; o[5 * T] = sfy.y; o[6 * T] = sfz.x; o[7 * T] = sfz.y;
+}
+
+// Adds the list-3 groups' sums of a leaf to its outputs, group by group.
+template <int T>
+__global__ void k_hm2p_add(const int *leaves, const int *off, TreeView tv, OutSoA outs, OutSoA outt, int do_src,
+                           int do_trg, const double *part)
+{
+    const int l = blockIdx.x, b = leaves[l];
+    const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
+    const int nl3 = tv.l3_start[b + 1] - tv.l3_start[b];
+    if (ne == 0 || nl3 == 0) return;
+    const int ngr = (nl3 + kHM2PGroup - 1) / kHM2PGroup, nch = (ne + T - 1) / T;
+    for (int ck = blockIdx.y; ck < nch; ck += gridDim.y) {
+        const int e = ck * T + threadIdx.x;
+        if (e >= ne) continue;
+        const bool is_src = e < ns;
+        const int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
+        double2 *po = is_src ? outs.pot : outt.pot;
+        double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy, *oz = is_src ? outs.fz : outt.fz;
+        double2 vp = po ? po[i] : cmk(0, 0), vx = ox ? ox[i] : cmk(0, 0), vy = ox ? oy[i] : cmk(0, 0),
+                vz = ox ? oz[i] : cmk(0, 0);
+        for (int g = 0; g < ngr; g++) {
+            const double *q = part + (size_t)(off[l] + ck * ngr + g) * 8 * T + threadIdx.x;
+            vp = cadd(vp, cmk(q[0], q[T]));
+            vx = cadd(vx, cmk(q[2 * T], q[3 * T]));
+            vy = cadd(vy, cmk(q[4 * T], q[5 * T]));
+            vz = cadd(vz, cmk(q[6 * T], q[7 * T]));
+        }
+        if (po) po[i] = vp;
+        if (ox) {
+            ox[i] = vx;
+            oy[i] = vy;
+            oz[i] = vz;
+        }
+    }
+}
+
 void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const double *sx, const double *sy,
                   const double *sz, const double *tx, const double *ty, const double *tz, HLevels lv, int NC,
                   double2 zk, const double2 *mpole, const double2 *local, OutSoA outs, OutSoA outt, int do_src,
@@ -988,17 +1170,39 @@ void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const doub
     if (nleaves == 0 || !st.ok() || (!do_src && !do_trg)) return;
     htab_init(s, st);
     int pm = max_p(lv);
+    // L2P (the leaves' own local expansions) first, then M2P of list 3
     size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * kHEvalThreads);
     if (sm <= 226 * 1024) {
         FMM_TRY(st, smem_allow(k_heval<kHEvalThreads>, (int)sm));
-        k_heval<kHEvalThreads><<<nleaves, kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk,
-                                                                  mpole, local, outs, outt, do_src, do_trg);
+        k_heval<kHEvalThreads><<<dim3(nleaves, 2), kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv,
+                                                                           NC, zk, mpole, local, outs, outt, do_src,
+                                                                           do_trg, 0);
     } else {
         sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * 32);
         FMM_TRY(st, smem_allow(k_heval<32>, (int)sm));
-        k_heval<32><<<nleaves, 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local, outs,
-                                            outt, do_src, do_trg);
+        k_heval<32><<<dim3(nleaves, 8), 32, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, mpole, local,
+                                                     outs, outt, do_src, do_trg, 0);
     }
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    // M2P work items: (leaf, chunk of points, group of list-3 boxes)
+    DBuf<int> cnt, off;
+    if (!cnt.alloc(nleaves, s, st) || !off.alloc(nleaves, s, st)) return;
+    k_hm2p_count<<<div_up(nleaves, 256), 256, 0, s>>>(leaves, nleaves, tv, do_src, do_trg, cnt.p);
+    FMM_COUNT_LAUNCH();
+    FMM_LAUNCH_CHECK(st);
+    int nitems = 0;
+    scan_exclusive_int(cnt.p, off.p, nleaves, s, st, &nitems);
+    if (!st.ok() || nitems == 0) return;
+    DBuf<double> part;
+    if (!part.alloc((size_t)nitems * 8 * kHM2PThreads, s, st)) return;
+    sm = sizeof(double2) * (size_t)(pm + 1) * (pm + 1);
+    FMM_TRY(st, smem_allow(k_hm2p<kHM2PThreads>, (int)sm));
+    k_hm2p<kHM2PThreads><<<nitems, kHM2PThreads, sm, s>>>(leaves, nleaves, off.p, tv, sx, sy, sz, tx, ty, tz, lv, NC,
+                                                          zk, mpole, do_src, do_trg, part.p);
+    FMM_COUNT_LAUNCH();
+    k_hm2p_add<kHM2PThreads><<<dim3(nleaves, 4), kHM2PThreads, 0, s>>>(leaves, off.p, tv, outs, outt, do_src, do_trg,
+                                                                       part.p);
     FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }
