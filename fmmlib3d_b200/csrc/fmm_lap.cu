@@ -346,6 +346,7 @@ static int device_sms()
 // tiles.  A single call builds it and runs the passes once; a plan
 // (fmm3d_lfmm3d_plan_*) keeps it and runs the passes for new charges.
 struct LapSetup {
+    EvalItems ev;   // work items of the evaluation pass
     int iprec = 0, p = 0, K = 0, ns = 0, nt = 0, ldm = 0;
     int ifcharge = 0, ifdipole = 0, ifpot = 0, iffld = 0, ifpottarg = 0, iffldtarg = 0;
     int do_src = 0, do_trg = 0, prune = 0;
@@ -730,6 +731,8 @@ static int lap_setup(LapSetup &S, int iprec, int ns, const double *d_src, int if
     // mixed form: small list-3 / list-4 interactions join the near field (FP64 keeps the reference's lists)
     lap_widen_near(S, S.mixed ? (p + 2) * (p + 2) / 2 : 0, s, st);
     if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
+    eval_items_prepare(T.leaves.p, T.nleaves, S.tv_far, S.do_src, S.do_trg, S.ev, s, st);
+    if (!st.ok()) { g_ti.err = cudaGetErrorString(st.err); return 16; }
     if (S.tri) {
         // triangle data in tree order and the quadrature nodes (filled per call)
         const size_t nn = (size_t)ns * S.rule.n;
@@ -875,8 +878,8 @@ static void lap_passes(LapSetup &S, const double *d_q, const double *d_dq, const
     }
     tm.mark();
     // STEPS 6, 7: M2P from list 3 and L2P (add the far field to the outputs)
-    launch_eval(T.leaves.p, T.nleaves, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
-                S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
+    launch_eval(T.leaves.p, T.nleaves, S.ev, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p,
+                S.mpole.p, S.local.p, S.os, S.ot, S.do_src, S.do_trg, s, st);
     launch_eval_hess(T.leaves.p, T.nleaves, S.tv_far, S.sx.p, S.sy.p, S.sz.p, S.tx.p, S.ty.p, S.tz.p, p, S.mpole.p,
                      S.local.p, S.hs, S.ht, hsrc, htrg, s, st);
     tm.mark();

@@ -64,8 +64,19 @@ void launch_p2m(const int *boxes, int nboxes, const TreeView &tv, const PointsSo
 void launch_p2l(const int *boxes, int nboxes, const TreeView &tv, const PointsSoA &src, int ifcharge,
                 int ifdipole, int p, double2 *local, cudaStream_t s, Status &st);
 
-void launch_eval(const int *leaves, int nleaves, const TreeView &tv, const double *sx, const double *sy,
-                 const double *sz, const double *tx, const double *ty, const double *tz, int p,
+// Work items of the evaluation pass (L2P + M2P): item offsets per leaf, scratch
+// offsets of the leaves with more than one group of source expansions, and the
+// scratch.  Built with the tree (host-synchronising); the launch then only
+// enqueues kernels (graph-capturable).
+struct EvalItems {
+    DBuf<int> off, soff;
+    DBuf<double> part;
+    int nitems = 0, nscratch = 0;
+};
+int eval_items_prepare(const int *leaves, int nleaves, const TreeView &tv, int do_src, int do_trg, EvalItems &E,
+                       cudaStream_t s, Status &st);
+void launch_eval(const int *leaves, int nleaves, const EvalItems &E, const TreeView &tv, const double *sx,
+                 const double *sy, const double *sz, const double *tx, const double *ty, const double *tz, int p,
                  const double2 *mpole, const double2 *local, OutSoA outs, OutSoA outt, int do_src, int do_trg,
                  cudaStream_t s, Status &st);
 
