@@ -1267,7 +1267,8 @@ __global__ void __launch_bounds__(kHP2PThreads) k_hp2p(const int *leaves, TreeVi
     const int ne = ns + nt;
     const int l1a = tv.l1_start[b], nl = 1 + tv.l1_start[b + 1] - l1a;
     const double2 k2 = cmul(zk, zk);
-    for (int e0 = 0; e0 < ne; e0 += kHP2PThreads) {
+    // CTA (leaf, y) serves the leaf's point chunks y, y + gridDim.y, ...
+    for (int e0 = blockIdx.y * kHP2PThreads; e0 < ne; e0 += gridDim.y * kHP2PThreads) {
         const int e = e0 + threadIdx.x;
         const bool act = e < ne;
         const bool is_src = e < ns;
@@ -1326,9 +1327,9 @@ void launch_hp2p(const int *leaves, int nleaves, const TreeView &tv, const Point
     int do_src = (ifpot == 1 || iffld == 1), do_trg = (ifpottarg == 1 || iffldtarg == 1);
     bool c = ifcharge == 1, d = ifdipole == 1;
     if (!c && !d) return;
-    if (c && d) k_hp2p<true, true><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
-    else if (c) k_hp2p<true, false><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
-    else k_hp2p<false, true><<<nleaves, kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    if (c && d) k_hp2p<true, true><<<dim3(nleaves, 4), kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    else if (c) k_hp2p<true, false><<<dim3(nleaves, 4), kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
+    else k_hp2p<false, true><<<dim3(nleaves, 4), kHP2PThreads, 0, s>>>(leaves, tv, src, tx, ty, tz, zk, outs, outt, do_src, do_trg);
     FMM_COUNT_LAUNCH();
     FMM_LAUNCH_CHECK(st);
 }

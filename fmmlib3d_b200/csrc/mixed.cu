@@ -329,19 +329,24 @@ __global__ void __launch_bounds__(kP2P32Threads, 16) k_p2p32(const int *leaves, 
     const int ne = (do_src ? tv.nsrc[b] : 0) + (do_trg ? tv.ntrg[b] : 0);
     // passes of 32, 64 or 128 evaluation points (one, two or four per lane, at most
     // max_ept); every point's sums run over the same sources in the same order
-    for (int e0 = 0; e0 < ne;) {
+    // CTA (leaf, y) runs the leaf's passes y, y + gridDim.y, ... of the same sequence
+    for (int e0 = 0, pass = 0; e0 < ne; pass++) {
         const int left = ne - e0;
+        const bool mine = pass % gridDim.y == blockIdx.y;
         if (left <= 32 || max_ept == 1) {
-            p2p32_pass<CHG, DIP, 1>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
+            if (mine)
+                p2p32_pass<CHG, DIP, 1>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                        want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 32;
         } else if (left <= 64 || max_ept == 2) {
-            p2p32_pass<CHG, DIP, 2>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
+            if (mine)
+                p2p32_pass<CHG, DIP, 2>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                        want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 64;
         } else {
-            p2p32_pass<CHG, DIP, 4>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
-                                    want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
+            if (mine)
+                p2p32_pass<CHG, DIP, 4>(e0, b, tv, src, tx, ty, tz, outs, outt, do_src, do_trg, want_fs, want_ft,
+                                        want_ps, want_pt, wA, wB, wC, wD, wE, whi, wlo);
             e0 += 128;
         }
     }
@@ -356,15 +361,15 @@ void launch_p2p32(const int *leaves, int nleaves, const TreeView &tv, const Poin
     bool c = ifcharge == 1, d = ifdipole == 1;
     if (max_ept != 1 && max_ept != 2) max_ept = 4;
     if (c && d) {
-        k_p2p32<true, true><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
+        k_p2p32<true, true><<<dim3(nleaves, 3), kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                              do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
                                                              ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     } else if (c) {
-        k_p2p32<true, false><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
+        k_p2p32<true, false><<<dim3(nleaves, 3), kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                               do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
                                                               ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     } else if (d) {
-        k_p2p32<false, true><<<nleaves, kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
+        k_p2p32<false, true><<<dim3(nleaves, 3), kP2P32Threads, 0, s>>>(leaves, tv, src, tx, ty, tz, outs, outt, do_src,
                                                               do_trg, iffld == 1, iffldtarg == 1, ifpot == 1,
                                                               ifpottarg == 1, max_ept); FMM_COUNT_LAUNCH();
     }
