@@ -1162,6 +1162,184 @@ __global__ void k_hm2p_add(const int *leaves, const int *off, TreeView tv, OutSo
     }
 }
 
+// L2P of the leaves' local expansions (h3dtaeval_trunc0, src/helmrouts3d.f:2732)
+// with half a warp per point.  A warp takes its points in batches of
+// kHL2PBatch: first each of 16 lanes builds one point's scaled Bessel column
+// (Miller's downward recurrence, so stored) in shared memory, then each half-warp
+// evaluates one point at a time, its 16 lanes sharing the orders m (lane l
+// takes m = l and 31 - l, mod 32, so the triangle of degrees splits evenly),
+// and the lanes' sums are added by shuffles.  The coefficients are staged
+// diagonal-major, entry (s = n - m, m) holding E(n, m) and E(n, -m), so lanes at
+// the same step read consecutive entries.  Shared memory per point is one
+// radial column instead of one per thread, which doubles the CTAs per SM.
+constexpr int kHL2PWarps = 4, kHL2PBatch = 16;
+
+static size_t hl2p_smem(int pm)
+{
+    return (size_t)(pm + 1) * (pm + 2) * sizeof(double2) +
+           (size_t)kHL2PWarps * kHL2PBatch * ((pm + 2) * sizeof(double2) + sizeof(int));
+}
+
+__global__ void __launch_bounds__(32 * kHL2PWarps) k_hl2p(const int *leaves, TreeView tv, const double *sx,
+                                                        const double *sy, const double *sz, const double *tx,
+                                                        const double *ty, const double *tz, HLevels lv, int NC,
+                                                        double2 zk, const double2 *local, OutSoA outs, OutSoA outt,
+                                                        int do_src, int do_trg, int pm)
+{
+    extern __shared__ double2 hsm[];
+    const int b = leaves[blockIdx.x];
+    const int lev = tv.level[b];
+    if (lev < 2) return;
+    const int ns = do_src ? tv.nsrc[b] : 0, nt = do_trg ? tv.ntrg[b] : 0, ne = ns + nt;
+    if (ne == 0) return;
+    const int p = lv.p[lev], P1 = p + 1, P2 = pm + 2;
+    const double sc = lv.sc[lev], isc = 1.0 / sc;
+    const int ntri = (p + 1) * (p + 2) / 2;
+    double2 *Ep = hsm;                                          // [ntri][2]
+    double2 *Fall = hsm + (size_t)(pm + 1) * (pm + 2);          // [warps][batch][pm + 2]
+    int *okall = (int *)(Fall + (size_t)kHL2PWarps * kHL2PBatch * P2);
+    // diagonal index d(s, m) = base(s) + m, base(s) = s (p + 1) - s (s - 1) / 2
+    const double2 *ex = local + (size_t)b * NC;
+    for (int d = threadIdx.x; d < ntri; d += blockDim.x) {
+        int sd = 0;
+        while (sd + 1 <= p && (sd + 1) * P1 - (sd + 1) * sd / 2 <= d) sd++;
+        const int m = d - (sd * P1 - sd * (sd - 1) / 2), n = m + sd;
+        Ep[2 * d] = ex[eidx(n, m)];
+        Ep[2 * d + 1] = ex[eidx(n, -m)];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+    double2 *F = Fall + (size_t)warp * kHL2PBatch * P2;
+    int *okp = okall + warp * kHL2PBatch;
+    const double *c = tv.center + 3L * b;
+    auto point = [&](int e, double &px, double &py, double &pz) {
+        const bool is_src = e < ns;
+        const int i = is_src ? tv.src0[b] + e : tv.trg0[b] + e - ns;
+        px = is_src ? sx[i] : tx[i];
+        py = is_src ? sy[i] : ty[i];
+        pz = is_src ? sz[i] : tz[i];
+        return i;
+    };
+    for (int base = warp * kHL2PBatch; base < ne; base += kHL2PWarps * kHL2PBatch) {
+        if (lane < kHL2PBatch) {
+            const int e = base + lane;
+            int ok = 0;
+            if (e < ne) {
+                double px, py, pz;
+                point(e, px, py, pz);
+                const PtGeo g = pt_geo(px - c[0], py - c[1], pz - c[2]);
+                ok = bess_dev(p > 1 ? p : 1, cscal(g.r, zk), sc, F + lane * P2, nullptr, 1) == 0;
+            }
+            okp[lane] = ok;
+        }
+        __syncwarp();
+        for (int it = 0; it < kHL2PBatch / 2; it++) {
+            const int pt = 2 * it + half, e = base + pt;
+            const bool act = e < ne && okp[pt];
+            double2 pot = cmk(0, 0), ur = cmk(0, 0), ut = cmk(0, 0), up = cmk(0, 0);
+            PtGeo g = {1.0, 1.0, 0.0, 1.0, 0.0};
+            int oi = 0;
+            if (act) {
+                double px, py, pz;
+                oi = point(e, px, py, pz);
+                g = pt_geo(px - c[0], py - c[1], pz - c[2]);
+                const double ct = g.ct, st = g.st, u = -st;
+                const double2 e1 = cmk(g.cp, g.sp);
+                const double2 *f = F + pt * P2;
+                for (int mb = 0; mb <= p; mb += 32) {
+#pragma unroll 1
+                    for (int which = 0; which < 2; which++) {
+                        const int m = mb + (which == 0 ? hl : 31 - hl);
+                        if (m > p) continue;
+                        double ymm = 1.0;
+                        if (m >= 1) {
+                            ymm = -sqrt(0.5);
+                            for (int k = 2; k <= m; k++) ymm *= u * __ldg(&g_hc[k]);
+                        }
+                        double2 em = cmk(1, 0), bp = e1;   // e^{i m phi} by binary powers
+                        for (int t = m; t; t >>= 1) {
+                            if (t & 1) em = cmul(em, bp);
+                            bp = cmul(bp, bp);
+                        }
+                        LegCol L;
+                        L.x = ct;
+                        L.m = m;
+                        L.w = m == 0 ? 1.0 : u * u;
+                        L.y1 = ymm;
+                        L.d1 = m == 0 ? 0.0 : ymm * (-m) * ct;
+                        L.y2 = 0;
+                        L.d2 = 0;
+                        int d = m;
+                        for (int n = m; n <= p; n++) {
+                            if (n > m) {
+                                L.step(n);
+                                d += P1 - (n - m - 1);
+                            }
+                            const double sn = __ldg(&g_hs[n]);
+                            const double y = L.y1 * sn, dd = L.d1 * sn;
+                            const double2 fn = f[n];
+                            double2 fd, fu;
+                            if (n == 0) {
+                                fd = cscal(-sc, f[1]);
+                                fu = cmk(0, 0);
+                            } else {
+                                // j_n' = [n j_{n-1} - (n+1) j_{n+1}] / (2n+1) in the scaled functions
+                                const double2 fm = f[n - 1], fp = f[n + 1];
+                                const double d1 = __ldg(&g_hq[n]), d2 = 1.0 - d1;
+                                fd = csub(cscal(d1 * isc, fm), cscal(d2 * sc, fp));
+                                fu = cscal(__ldg(&g_hr[n]), cmul(zk, cadd(cscal(sc, fp), cscal(isc, fm))));
+                            }
+                            fd = cmul(fd, zk);
+                            if (m == 0) {
+                                const double2 a = Ep[2 * d];
+                                cfma(pot, fn, cscal(y, a));
+                                cfma(ur, fd, cscal(y, a));
+                                cfma(ut, fu, cscal(-dd * st, a));
+                            } else {
+                                const double2 z2 = cmul(Ep[2 * d], em), z3 = cmul(Ep[2 * d + 1], cconj(em));
+                                const double2 zs = cadd(z2, z3), zd = csub(z2, z3);
+                                cfma(pot, fn, cscal(y * st, zs));
+                                cfma(ur, fd, cscal(y * st, zs));
+                                cfma(ut, fu, cscal(-dd, zs));
+                                cfma(up, fu, cscal(y * m, cmk(-zd.y, zd.x)));  // i m (z2 - z3)
+                            }
+                        }
+                    }
+                }
+            }
+            // the half-warp's sums (offsets below 16 stay within the half)
+#pragma unroll
+            for (int o = 8; o >= 1; o >>= 1) {
+                pot.x += __shfl_xor_sync(0xffffffffu, pot.x, o);
+                pot.y += __shfl_xor_sync(0xffffffffu, pot.y, o);
+                ur.x += __shfl_xor_sync(0xffffffffu, ur.x, o);
+                ur.y += __shfl_xor_sync(0xffffffffu, ur.y, o);
+                ut.x += __shfl_xor_sync(0xffffffffu, ut.x, o);
+                ut.y += __shfl_xor_sync(0xffffffffu, ut.y, o);
+                up.x += __shfl_xor_sync(0xffffffffu, up.x, o);
+                up.y += __shfl_xor_sync(0xffffffffu, up.y, o);
+            }
+            if (act && hl == 0) {
+                const double ct = g.ct, st = g.st, cp = g.cp, sp = g.sp;
+                const double2 fx = cadd(cadd(cscal(st * cp, ur), cscal(ct * cp, ut)), cscal(-sp, up));
+                const double2 fy = cadd(cadd(cscal(st * sp, ur), cscal(ct * sp, ut)), cscal(cp, up));
+                const double2 fz = csub(cscal(ct, ur), cscal(st, ut));
+                const bool is_src = e < ns;
+                double2 *po = is_src ? outs.pot : outt.pot;
+                double2 *ox = is_src ? outs.fx : outt.fx, *oy = is_src ? outs.fy : outt.fy,
+                        *oz = is_src ? outs.fz : outt.fz;
+                if (po) po[oi] = cadd(po[oi], pot);
+                if (ox) {
+                    ox[oi] = csub(ox[oi], fx);
+                    oy[oi] = csub(oy[oi], fy);
+                    oz[oi] = csub(oz[oi], fz);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const double *sx, const double *sy,
                   const double *sz, const double *tx, const double *ty, const double *tz, HLevels lv, int NC,
                   double2 zk, const double2 *mpole, const double2 *local, OutSoA outs, OutSoA outt, int do_src,
@@ -1172,7 +1350,12 @@ void launch_heval(const int *leaves, int nleaves, const TreeView &tv, const doub
     int pm = max_p(lv);
     // L2P (the leaves' own local expansions) first, then M2P of list 3
     size_t sm = sizeof(double2) * ((size_t)(pm + 1) * (pm + 1) + (size_t)(pm + 2) * kHEvalThreads);
-    if (sm <= 226 * 1024) {
+    if (hl2p_smem(pm) <= 100 * 1024) {
+        const size_t sl = hl2p_smem(pm);
+        FMM_TRY(st, smem_allow(k_hl2p, (int)sl));
+        k_hl2p<<<nleaves, 32 * kHL2PWarps, sl, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv, NC, zk, local, outs, outt,
+                                                    do_src, do_trg, pm);
+    } else if (sm <= 226 * 1024) {
         FMM_TRY(st, smem_allow(k_heval<kHEvalThreads>, (int)sm));
         k_heval<kHEvalThreads><<<dim3(nleaves, 2), kHEvalThreads, sm, s>>>(leaves, tv, sx, sy, sz, tx, ty, tz, lv,
                                                                            NC, zk, mpole, local, outs, outt, do_src,
