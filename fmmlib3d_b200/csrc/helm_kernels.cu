@@ -1480,11 +1480,15 @@ __global__ void __launch_bounds__(kHP2PThreads) k_hp2p(const int *leaves, TreeVi
                 __syncthreads();
                 if (!act) continue;
                 const int selfk = self - (js0 + c0);
+                // the self pair adds exact zeros (no strength, unit offset) instead of a branch,
+                // so consecutive pairs interleave
+#pragma unroll 2
                 for (int k = 0; k < cn; k++) {
-                    if (k == selfk) continue;
-                    hpair<CHG, DIP>(ex - sx[k], ey - sy[k], ez - sz[k], zk, k2, CHG ? sq[k] : cmk(0, 0),
-                                    DIP ? sd[k] : cmk(0, 0), DIP ? svx[k] : 0.0, DIP ? svy[k] : 0.0,
-                                    DIP ? svz[k] : 0.0, pot, fx, fy, fz);
+                    const bool me = k == selfk;
+                    hpair<CHG, DIP>(me ? 1.0 : ex - sx[k], me ? 0.0 : ey - sy[k], me ? 0.0 : ez - sz[k], zk, k2,
+                                    CHG && !me ? sq[k] : cmk(0, 0), DIP && !me ? sd[k] : cmk(0, 0),
+                                    DIP && !me ? svx[k] : 0.0, DIP && !me ? svy[k] : 0.0, DIP && !me ? svz[k] : 0.0,
+                                    pot, fx, fy, fz);
                 }
             }
         }
