@@ -631,20 +631,22 @@ __device__ __forceinline__ PtGeo pt_geo(double dx, double dy, double dz)
 // (h3dformmp_add_trunc / h3dformta_add_trunc, src/helmrouts3d.f:2972, 3299;
 // dipoles h3dformmp_dp_add_trunc :3580, h3dformta_dp_add_trunc :3978).
 constexpr int kHFormThreads = 256, kHFormPer = 4;
+// Source set-up in batches of kHFormSetA x kHFormSetCH (32) sources, tables per kHFormSetCH.
+constexpr int kHFormSetCH = 8, kHFormSetA = 4;
 
-template <int CH, bool DIP>
+template <int CH, bool DIP, int AX = 1>
 struct HFormSmem {
     // sizes in doubles for expansion order p
     static __host__ __device__ size_t doubles(int p)
     {
         size_t W = p + 2, T = (size_t)(p + 1) * (p + 2) / 2;
-        size_t d = CH * (2 * W + 2 * (p + 1) + (p + 1) + T + 16);  // f, e^{-im phi}, diagonal, Y, scalars
-        if (DIP) d += CH * (T + 4 * (p + 1));                        // D, fd, fu
+        size_t d = AX * CH * (2 * W + 2 * (p + 1) + (p + 1) + 16) + CH * T;  // f, e^{-im phi}, diagonal, scalars; Y
+        if (DIP) d += CH * T + AX * CH * 4 * (p + 1);                         // D; fd, fu
         return d;
     }
 };
 
-template <bool IRREG, bool CHG, bool DIP, int CH>
+template <bool IRREG, bool CHG, bool DIP, int CH, int AX = 1>
 __global__ void __launch_bounds__(kHFormThreads) k_hform(const int *boxes, TreeView tv, PointsSoA src, HLevels lv,
                                                         int NC, double2 zk, double2 *exps)
 {
@@ -657,14 +659,16 @@ __global__ void __launch_bounds__(kHFormThreads) k_hform(const int *boxes, TreeV
     const int p = lv.p[lev];
     const double sc = lv.sc[lev];
     const int W = p + 2, P1 = p + 1, TS = (p + 1) * (p + 2) / 2, K = (p + 1) * (p + 1);
-    double2 *F = (double2 *)hsd;            // [CH][W]
-    double2 *Em = F + CH * W;               // [CH][P1]   e^{-i m phi}
-    double *Dg = (double *)(Em + CH * P1);  // [CH][P1]   diagonal Y_m^m (2s form)
-    double *Y = Dg + CH * P1;               // [CH][TS]
-    double *Sc = Y + CH * TS;               // [CH][16]   per-source scalars
-    double *D = Sc + CH * 16;               // [CH][TS]   (dipoles)
-    double2 *Fd = (double2 *)(D + (DIP ? CH * TS : 0));  // [CH][P1]
-    double2 *Fu = Fd + (DIP ? CH * P1 : 0);              // [CH][P1]
+    // per-source arrays for AX CH sources (set up together in phase A), the
+    // Legendre tables for CH (phases B and C run on AX sub-chunks in turn)
+    double2 *F = (double2 *)hsd;                 // [AX CH][W]
+    double2 *Em = F + AX * CH * W;               // [AX CH][P1]   e^{-i m phi}
+    double *Dg = (double *)(Em + AX * CH * P1);  // [AX CH][P1]   diagonal Y_m^m (2s form)
+    double *Y = Dg + AX * CH * P1;               // [CH][TS]
+    double *Sc = Y + CH * TS;                    // [AX CH][16]   per-source scalars
+    double *D = Sc + AX * CH * 16;               // [CH][TS]      (dipoles)
+    double2 *Fd = (double2 *)(D + (DIP ? CH * TS : 0));  // [AX CH][P1]
+    double2 *Fu = Fd + (DIP ? AX * CH * P1 : 0);         // [AX CH][P1]
     const int e0 = blockIdx.y * kHFormThreads * kHFormPer;  // this CTA's coefficient range
     if (e0 >= K) return;
     double2 acc[kHFormPer];
@@ -683,11 +687,11 @@ __global__ void __launch_bounds__(kHFormThreads) k_hform(const int *boxes, TreeV
     for (int si = 0; si < nsb; si++) {
         const int sb = IRREG ? tv.l4_idx[tv.l4_start[b] + si] : b;
         const int s0 = tv.src0[sb], ns = tv.nsrc[sb];
-        for (int c0 = 0; c0 < ns; c0 += CH) {
-            const int nb = min(CH, ns - c0);
+        for (int c0 = 0; c0 < ns; c0 += AX * CH) {
+            const int nba = min(AX * CH, ns - c0);
             __syncthreads();
             // phase A: per source, radial functions, phases, diagonal, scalars
-            if (threadIdx.x < nb) {
+            if (threadIdx.x < nba) {
                 const int j = threadIdx.x, i = s0 + c0 + j;
                 const PtGeo g = pt_geo(src.x[i] - c[0], src.y[i] - c[1], src.z[i] - c[2]);
                 double2 *f = F + j * W;
@@ -739,51 +743,59 @@ __global__ void __launch_bounds__(kHFormThreads) k_hform(const int *boxes, TreeV
                 }
             }
             __syncthreads();
-            // phase B: Legendre columns, one (source, m) task per thread
-            for (int task = threadIdx.x; task < nb * P1; task += kHFormThreads) {
-                const int j = task / P1, m = task % P1;
-                const double x = Sc[j * 16], u = -Sc[j * 16 + 1];
-                LegCol L;
-                L.x = x; L.m = m; L.w = m == 0 ? 1.0 : u * u;
-                L.y1 = Dg[j * P1 + m];
-                L.d1 = m == 0 ? 0.0 : L.y1 * (-m) * x;
-                L.y2 = 0; L.d2 = 0;
-                for (int n = m; n <= p; n++) {
-                    if (n > m) L.step(n);
-                    const double sn = __ldg(&g_hs[n]);
-                    Y[j * TS + tidx(n, m)] = L.y1 * sn;
-                    if (DIP) D[j * TS + tidx(n, m)] = L.d1 * sn;
-                }
-            }
-            __syncthreads();
-            // phase C: accumulate into this thread's coefficients
-#pragma unroll
-            for (int q = 0; q < kHFormPer; q++) {
-                const int n = en[q];
-                if (n < 0) continue;
-                const int m = em_[q], am = m < 0 ? -m : m, ti = tidx(n, am);
-                for (int j = 0; j < nb; j++) {
-                    const double *S = Sc + j * 16;
-                    const double st = S[1];
-                    double2 E = Em[j * P1 + am];
-                    if (m < 0) E = cconj(E);
-                    const double ys = Y[j * TS + ti];
-                    if (CHG) {
-                        const double yr = am == 0 ? ys : ys * st;
-                        cfma(acc[q], cmul(cmk(S[2], S[3]), cscal(yr, F[j * W + n])), E);
+            for (int sub = 0; sub < AX; sub++) {
+                const int jb = sub * CH, nb = min(CH, nba - jb);
+                if (nb <= 0) break;
+                if (sub > 0) __syncthreads();   // the previous sub-chunk's tables are read
+                const double2 *Fs = F + jb * W, *Ems = Em + jb * P1;
+                const double *Dgs = Dg + jb * P1, *Scs = Sc + jb * 16;
+                const double2 *Fds = Fd + (DIP ? jb * P1 : 0), *Fus = Fu + (DIP ? jb * P1 : 0);
+                // phase B: Legendre columns, one (source, m) task per thread
+                for (int task = threadIdx.x; task < nb * P1; task += kHFormThreads) {
+                    const int j = task / P1, m = task % P1;
+                    const double x = Scs[j * 16], u = -Scs[j * 16 + 1];
+                    LegCol L;
+                    L.x = x; L.m = m; L.w = m == 0 ? 1.0 : u * u;
+                    L.y1 = Dgs[j * P1 + m];
+                    L.d1 = m == 0 ? 0.0 : L.y1 * (-m) * x;
+                    L.y2 = 0; L.d2 = 0;
+                    for (int n = m; n <= p; n++) {
+                        if (n > m) L.step(n);
+                        const double sn = __ldg(&g_hs[n]);
+                        Y[j * TS + tidx(n, m)] = L.y1 * sn;
+                        if (DIP) D[j * TS + tidx(n, m)] = L.d1 * sn;
                     }
-                    if (DIP) {
-                        const double dd = D[j * TS + ti];
-                        const double2 fd = Fd[j * P1 + n], fu = Fu[j * P1 + n];
-                        double2 A, B = cmk(0, 0);
-                        if (am == 0) A = csub(cscal(ys * S[6], fd), cscal(dd * st * S[7], fu));
-                        else {
-                            A = csub(cscal(ys * st * S[6], fd), cscal(dd * S[7], fu));
-                            B = cscal((m > 0 ? am : -am) * ys * S[8], fu);
+                }
+                __syncthreads();
+                // phase C: accumulate into this thread's coefficients
+    #pragma unroll
+                for (int q = 0; q < kHFormPer; q++) {
+                    const int n = en[q];
+                    if (n < 0) continue;
+                    const int m = em_[q], am = m < 0 ? -m : m, ti = tidx(n, am);
+                    for (int j = 0; j < nb; j++) {
+                        const double *S = Scs + j * 16;
+                        const double st = S[1];
+                        double2 E = Ems[j * P1 + am];
+                        if (m < 0) E = cconj(E);
+                        const double ys = Y[j * TS + ti];
+                        if (CHG) {
+                            const double yr = am == 0 ? ys : ys * st;
+                            cfma(acc[q], cmul(cmk(S[2], S[3]), cscal(yr, Fs[j * W + n])), E);
                         }
-                        // ds E (A - i sgn(m) B)
-                        const double2 AB = cmk(A.x + B.y, A.y - B.x);
-                        cfma(acc[q], cmul(cmk(S[4], S[5]), AB), E);
+                        if (DIP) {
+                            const double dd = D[j * TS + ti];
+                            const double2 fd = Fds[j * P1 + n], fu = Fus[j * P1 + n];
+                            double2 A, B = cmk(0, 0);
+                            if (am == 0) A = csub(cscal(ys * S[6], fd), cscal(dd * st * S[7], fu));
+                            else {
+                                A = csub(cscal(ys * st * S[6], fd), cscal(dd * S[7], fu));
+                                B = cscal((m > 0 ? am : -am) * ys * S[8], fu);
+                            }
+                            // ds E (A - i sgn(m) B)
+                            const double2 AB = cmk(A.x + B.y, A.y - B.x);
+                            cfma(acc[q], cmul(cmk(S[4], S[5]), AB), E);
+                        }
                     }
                 }
             }
@@ -815,20 +827,25 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
     htab_init(s, st);
     const int pm = max_p(lv);
     const dim3 grid(nboxes, div_up((pm + 1) * (pm + 1), kHFormThreads * kHFormPer));
-#define FMM_HF(IR, C, D, CHV)                                                                                 \
+#define FMM_HF2(IR, C, D, CHV, AXV)                                                                           \
     do {                                                                                                      \
-        size_t sm = sizeof(double) * HFormSmem<CHV, D>::doubles(pm);                                         \
-        FMM_TRY(st, smem_allow(k_hform<IR, C, D, CHV>, \
-                                         (int)sm));                                                           \
-        k_hform<IR, C, D, CHV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);           \
+        size_t sm = sizeof(double) * HFormSmem<CHV, D, AXV>::doubles(pm);                                    \
+        FMM_TRY(st, smem_allow(k_hform<IR, C, D, CHV, AXV>, (int)sm));                                       \
+        k_hform<IR, C, D, CHV, AXV><<<grid, kHFormThreads, sm, s>>>(boxes, tv, src, lv, NC, zk, exps);      \
         FMM_COUNT_LAUNCH();                                                                                   \
     } while (0)
+#define FMM_HF(IR, C, D, CHV) FMM_HF2(IR, C, D, CHV, 1)
     // chunks of 8 or 16 sources; 4, 2 or 1 at orders whose staging would not
     // fit (above ~54, ~80, ~110).  The chunk size does not change the order of
     // any sum.
+    // The sources' set-up (phase A) runs one thread per source, so it takes 32 sources
+    // at a time where that fits two CTAs per SM (the tables stay per 8 sources; phases
+    // B and C walk the four sub-chunks in order, so no sum changes order).
 #define FMM_HF_FIT(IR, C, D, CHV)                                                                             \
     do {                                                                                                      \
-        if (sizeof(double) * HFormSmem<CHV, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, CHV);           \
+        if (sizeof(double) * HFormSmem<kHFormSetCH, D, kHFormSetA>::doubles(pm) <= 110 * 1024)               \
+            FMM_HF2(IR, C, D, kHFormSetCH, kHFormSetA);                                                       \
+        else if (sizeof(double) * HFormSmem<CHV, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, CHV);      \
         else if (sizeof(double) * HFormSmem<4, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, 4);          \
         else if (sizeof(double) * HFormSmem<2, D>::doubles(pm) <= 226 * 1024) FMM_HF(IR, C, D, 2);          \
         else FMM_HF(IR, C, D, 1);                                                                             \
@@ -844,6 +861,7 @@ void launch_hform(bool irreg, const int *boxes, int nboxes, const TreeView &tv, 
     }
 #undef FMM_HF_FIT
 #undef FMM_HF
+#undef FMM_HF2
     FMM_LAUNCH_CHECK(st);
 }
 
