@@ -178,7 +178,7 @@ __global__ void k_radix_scatter(const uint64_t *kin, const int *vin, uint64_t *k
             vout[pos] = v;
         }
         __syncthreads();
-        // advance digit bases by this round's totals
+        // advance digit bases by this digit pass's totals
         for (int dd = threadIdx.x; dd < kRadix; dd += kSortThreads) {
             int t = 0;
             for (int ww = 0; ww < kSortThreads / 32; ww++) t += wcnt[ww][dd];
